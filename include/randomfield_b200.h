@@ -1,0 +1,135 @@
+/*
+ * randomfield_b200.h -- C-ABI of the B200-native spectral-sum random-field
+ * generator (the randomFieldND Shinozuka / isotropic path of
+ * cottereau/randomField).
+ *
+ * Plain C types only: pointers, sizes, doubles.  Layouts are Fortran
+ * column-major, as the reference's callers hold them:
+ *   xPoints   nDim x n   (the coordinates of one point are contiguous)
+ *   randField n x Nmc    (one realization is contiguous)
+ * The caller allocates everything; the library never frees caller memory.
+ * Every entry point returns RF_OK (0) or a negative RF_E* code and never
+ * aborts or exits; rf_last_error() gives a one-line reason (thread-local).
+ */
+#ifndef RANDOMFIELD_B200_H
+#define RANDOMFIELD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RF_ABI_VERSION 1
+
+/* Methods, correlation models and marginals: constants_RF.f90:12-21. */
+#define RF_ISOTROPIC 1
+#define RF_SHINOZUKA 2
+#define RF_CM_GAUSSIAN 1
+#define RF_CM_COS 2
+#define RF_FOM_GAUSSIAN 1
+#define RF_FOM_LOGNORMAL 2
+
+/* Precision forms of the contraction. */
+#define RF_PREC_BF16 0      /* BF16 trig tiles, hi/lo BF16 amplitude side, tcgen05 (default) */
+#define RF_PREC_FP16 1      /* FP16 trig tiles and scaled FP16 amplitude side, tcgen05     */
+#define RF_PREC_FP32 2      /* plain FP32 operands on the FFMA pipes                       */
+#define RF_PREC_BF16_FAST 3 /* BF16 trig tiles, single BF16 amplitude side, tcgen05        */
+
+/* Status codes.  The reference stops or calls MPI_ABORT instead. */
+#define RF_OK 0
+#define RF_EINVAL_NMC -1        /* Nmc < 1                     (type_inputRF.f90:1159-1206) */
+#define RF_EINVAL_NDIM -2       /* nDim outside 1..3, or < 2 for isotropic                   */
+#define RF_EINVAL_CORRL -3      /* corrL(i) <= 0               (type_inputRF.f90:1159-1206) */
+#define RF_EINVAL_LOGNORMAL -4  /* lognormal with fieldAvg <= 0 (randomFieldND.f90:162-166) */
+#define RF_EINVAL_METHOD -5     /* method not 1 or 2                                        */
+#define RF_EINVAL_CORRMOD -6    /* corrMod not 1 or 2; cm_COS with 6 or fewer wavevectors    */
+#define RF_EINVAL_MARGINAL -7   /* margiFirst not 1 or 2                                    */
+#define RF_EINVAL_RANGE -8      /* zero extent along an axis (kDelta would be infinite)      */
+#define RF_EINVAL_ARG -9        /* null pointer, n < 1, bad option value                     */
+#define RF_ENOTSUP -10          /* valid request outside what this build implements          */
+#define RF_ECUDA -20            /* CUDA runtime error                                       */
+#define RF_ENOMEM -21           /* device or pinned allocation failed                       */
+#define RF_ETIMEDOUT -22        /* a bounded device wait expired; the kernel returned        */
+#define RF_ENOMEM_ADMISSION -23 /* request larger than the context's HBM budget              */
+#define RF_ENODEV -25           /* no CUDA device                                           */
+
+/*
+ * Options.  Zero-initialise (or call rf_options_init) and set what differs;
+ * a NULL options pointer means all defaults.
+ */
+typedef struct rf_options {
+  int32_t size;          /* sizeof(rf_options); set by rf_options_init                 */
+  int32_t precision;     /* RF_PREC_*                                                   */
+  int64_t seed_start;    /* the reference's seedStart (>= 0); rnglib generator 1 seeded */
+                         /* with (72 + 18 s, 72 + 18 s + 37), after math_RF.f90:561     */
+  int32_t k_nstep[3];    /* Shinozuka: wavenumbers per axis; 0 = reference rule         */
+                         /* kNStep = 1 + ceil(kMax / (2 pi / (1.1 xRange))) (spectra_RF.f90:87-92) */
+  int32_t iso_n_radial;  /* isotropic: radial points; 0 = 1 + 5 ceil(kMax/kDelta) (:75-80) */
+  int32_t iso_n_dir;     /* isotropic: directions per radius; 0 = 32                    */
+  int32_t literal;       /* 1: reproduce the reference's deterministic defects B1/B2    */
+  int32_t normalize;     /* 1: empirical per-realization normalisation (randomFieldND.f90:820-926) */
+  double x_range[3];     /* physical extent per axis; 0 = extent of xPoints             */
+  int32_t device;        /* CUDA device ordinal                                         */
+  int32_t reserved[7];
+} rf_options;
+
+/* Fills defaults: BF16 form, seed_start 0, reference rules, device 0. */
+void rf_options_init(rf_options* opt);
+
+/*
+ * The drop-in for createStandardGaussianFieldUnstruct(xPoints, corrMod,
+ * margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, randField)
+ * (README.md:58-92; in code create_RF_Unstruct_Init, randomFieldND.f90:27-38,
+ * reached through interface createRandomField, calls_RF.f90:20-22, with
+ * gen_Std_Gauss_* :44-132/:184-337/:368-514 and multiVariateTransformation
+ * :139-178).  Host buffers; synchronous; the result is FP64 as in the
+ * reference.  corrL has nDim entries.
+ */
+int rf_create_standard_gaussian_field_unstruct(
+    const double* xPoints, int nDim, int64_t n, int corrMod, int margiFirst,
+    const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method,
+    double* randField, const rf_options* opt);
+
+/*
+ * Device-resident form of the same call for callers that keep data on the
+ * GPU: d_xPoints and d_randField are device pointers; the work is queued on
+ * `stream` (a cudaStream_t, 0 = legacy default) and the call returns once it
+ * is queued.  The context owns device tables and scratch; one context per
+ * host thread (calls on one context are serialised by its stream).
+ */
+typedef struct rf_context rf_context;
+int rf_context_create(int device, rf_context** out);
+int rf_context_destroy(rf_context* ctx);
+int rf_generate_device(rf_context* ctx, const double* d_xPoints, int nDim, int64_t n,
+                       int corrMod, int margiFirst, const double* corrL,
+                       double fieldAvg, double fieldVar, int Nmc, int method,
+                       double* d_randField, const rf_options* opt, void* stream);
+/* Waits for the context's queued work; reports a device-side timeout. */
+int rf_context_synchronize(rf_context* ctx);
+
+/* Phase timers.  With timing enabled the context records CUDA events on the
+ * launching stream around each phase of a generation; rf_context_last_times
+ * waits for the last one and returns the device milliseconds of the table
+ * build, the contraction (with its fused epilogue) and the optional
+ * normalisation pass, and how many kernels the call launched. */
+int rf_context_set_timing(rf_context* ctx, int enable);
+int rf_context_last_times(rf_context* ctx, double* tables_ms, double* contract_ms, double* post_ms,
+                          int32_t* kernel_launches);
+
+/* Problem geometry exactly as the generator will use it (host only, no GPU):
+ * K wavevectors, kNStep, kDelta, ampMult (randomFieldND.f90:260-266). */
+int rf_query_geometry(const double* xPoints, int nDim, int64_t n, int corrMod,
+                      const double* corrL, int method, const rf_options* opt,
+                      int64_t* K, int32_t* kNStep, double* kDelta, double* ampMult);
+
+/* One-line reason for the last error on this thread ("" when none). */
+const char* rf_last_error(void);
+/* RF_ABI_VERSION of the loaded library. */
+int rf_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RANDOMFIELD_B200_H */

@@ -1,0 +1,230 @@
+"""ctypes front end of the FP64 CPU oracle (oracle/rf_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
+as the checker, and by the CPU baseline leg of ``bench.py``.  The product in
+``randomfield_b200/`` never imports it.
+
+Parity status: unpinned against reference output (the Fortran reference ships
+no golden vectors and cannot be compiled here); see rf_oracle.h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librfo.so")
+
+ISOTROPIC, SHINOZUKA = 1, 2
+CM_GAUSSIAN, CM_COS = 1, 2
+FOM_GAUSSIAN, FOM_LOGNORMAL = 1, 2
+
+
+class Request(C.Structure):
+    _fields_ = [
+        ("nDim", C.c_int32),
+        ("n", C.c_int64),
+        ("xPoints", C.POINTER(C.c_double)),
+        ("corrMod", C.c_int32),
+        ("margiFirst", C.c_int32),
+        ("corrL", C.c_double * 3),
+        ("fieldAvg", C.c_double),
+        ("fieldVar", C.c_double),
+        ("Nmc", C.c_int32),
+        ("method", C.c_int32),
+        ("seedStart", C.c_int64),
+        ("kNStep", C.c_int32 * 3),
+        ("isoNRadial", C.c_int32),
+        ("isoNDir", C.c_int32),
+        ("literal", C.c_int32),
+        ("normalize", C.c_int32),
+        ("xRange", C.c_double * 3),
+    ]
+
+
+class Geometry(C.Structure):
+    _fields_ = [
+        ("nDim", C.c_int32),
+        ("K", C.c_int64),
+        ("kNStep", C.c_int32 * 3),
+        ("kDelta", C.c_double * 3),
+        ("kMax", C.c_double),
+        ("ampMult", C.c_double),
+        ("xRangeNorm", C.c_double * 3),
+        ("xSlab", C.c_int64),
+    ]
+
+
+class RNG(C.Structure):
+    _fields_ = [(nm, C.c_int32 * 32) for nm in ("ig1", "ig2", "lg1", "lg2", "cg1", "cg2", "anti")] + [
+        ("g", C.c_int32),
+        ("initialized", C.c_int32),
+    ]
+
+
+_lib = None
+
+
+def build() -> None:
+    """Compile librfo.so with the committed Makefile (gcc, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(
+            os.path.join(HERE, "rf_oracle.c")
+        ):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        d = C.c_double
+        L.rfo_multmod.argtypes = [C.c_int32] * 3
+        L.rfo_multmod.restype = C.c_int32
+        L.rfo_rng_seed.argtypes = [P(RNG), C.c_int64]
+        L.rfo_rng_initialize.argtypes = [P(RNG)]
+        L.rfo_rng_set_initial_seed.argtypes = [P(RNG), C.c_int32, C.c_int32]
+        L.rfo_rng_init_generator.argtypes = [P(RNG), C.c_int32]
+        L.rfo_rng_advance_state.argtypes = [P(RNG), C.c_int32]
+        L.rfo_rng_cgn_set.argtypes = [P(RNG), C.c_int32]
+        L.rfo_rng_i4_uni.argtypes = [P(RNG)]
+        L.rfo_rng_i4_uni.restype = C.c_int32
+        L.rfo_rng_r8_uni_01.argtypes = [P(RNG)]
+        L.rfo_rng_r8_uni_01.restype = d
+        L.rfo_geometry_of.argtypes = [P(Request), P(Geometry)]
+        L.rfo_kpoints.argtypes = [P(Request), P(d), P(d), P(d)]
+        L.rfo_phase_matrix.argtypes = [P(Request), P(d), P(d)]
+        L.rfo_generate.argtypes = [P(Request), P(C.c_int64), C.c_int64, P(d), C.c_int32]
+        L.rfo_generate_recast.argtypes = [P(Request), P(C.c_int64), C.c_int64, P(d), C.c_int32]
+        L.rfo_marginal.argtypes = [C.c_int32, d, d, P(d), C.c_int64]
+        L.rfo_normalize.argtypes = [P(d), C.c_int64, C.c_int32]
+        L.rfo_set_grid.argtypes = [C.c_int32, P(d), P(d), P(C.c_int32), P(d)]
+        L.rfo_unity_partition.argtypes = [C.c_int32, P(C.c_int32), P(C.c_int32), C.c_uint32, P(d)]
+        L.rfo_overlap_npoints.argtypes = [d, d, d]
+        L.rfo_overlap_npoints.restype = C.c_int32
+        L.rfo_baseline_shinozuka.argtypes = [P(Request), C.c_int64, C.c_int64, C.c_int32, C.c_int32, P(d), C.c_int32]
+        L.rfo_baseline_shinozuka.restype = d
+        _lib = L
+    return _lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class OracleRequest:
+    """One generation request; field names follow the reference's RF type."""
+
+    def __init__(self, xPoints, corrMod=CM_GAUSSIAN, margiFirst=FOM_GAUSSIAN, corrL=(1.0, 1.0, 1.0),
+                 fieldAvg=0.0, fieldVar=1.0, Nmc=1, method=SHINOZUKA, seedStart=0, kNStep=(0, 0, 0),
+                 isoNRadial=0, isoNDir=0, literal=False, normalize=False, xRange=(0.0, 0.0, 0.0)):
+        x = np.ascontiguousarray(np.asarray(xPoints, dtype=np.float64))
+        if x.ndim == 1:
+            x = x.reshape(-1, 1)
+        # xPoints is nDim x n in Fortran order == n x nDim in C order
+        self.x = x
+        self.nDim = x.shape[1]
+        self.n = x.shape[0]
+        r = Request()
+        r.nDim = self.nDim
+        r.n = self.n
+        r.xPoints = _dptr(self.x)
+        r.corrMod = corrMod
+        r.margiFirst = margiFirst
+        for i in range(3):
+            r.corrL[i] = float(corrL[i]) if i < len(corrL) else 1.0
+            r.kNStep[i] = int(kNStep[i]) if i < len(kNStep) else 0
+            r.xRange[i] = float(xRange[i]) if i < len(xRange) else 0.0
+        r.fieldAvg = fieldAvg
+        r.fieldVar = fieldVar
+        r.Nmc = Nmc
+        r.method = method
+        r.seedStart = seedStart
+        r.isoNRadial = isoNRadial
+        r.isoNDir = isoNDir
+        r.literal = int(bool(literal))
+        r.normalize = int(bool(normalize))
+        self.req = r
+
+    def geometry(self) -> Geometry:
+        g = Geometry()
+        rc = lib().rfo_geometry_of(C.byref(self.req), C.byref(g))
+        if rc:
+            raise ValueError(f"oracle rejected the request (rc={rc})")
+        return g
+
+    def kpoints(self):
+        g = self.geometry()
+        kp = np.zeros((g.K, self.nDim))
+        amp = np.zeros(g.K)
+        S = np.zeros(g.K)
+        rc = lib().rfo_kpoints(C.byref(self.req), _dptr(kp), _dptr(amp), _dptr(S))
+        if rc:
+            raise ValueError(rc)
+        return kp, amp, S
+
+    def phase_matrix(self):
+        g = self.geometry()
+        Bc = np.zeros((self.req.Nmc, g.K))
+        Bs = np.zeros((self.req.Nmc, g.K))
+        rc = lib().rfo_phase_matrix(C.byref(self.req), _dptr(Bc), _dptr(Bs))
+        if rc:
+            raise ValueError(rc)
+        return Bc, Bs  # [r, k]
+
+    def generate(self, rows=None, nthreads=0, recast=False):
+        """Field (nrows x Nmc, column-major in memory: returned as [r, i])."""
+        nrows = self.n if rows is None else len(rows)
+        out = np.zeros((self.req.Nmc, nrows))
+        rp = None
+        if rows is not None:
+            rows = np.ascontiguousarray(np.asarray(rows, dtype=np.int64))
+            rp = rows.ctypes.data_as(C.POINTER(C.c_int64))
+        fn = lib().rfo_generate_recast if recast else lib().rfo_generate
+        rc = fn(C.byref(self.req), rp, nrows, _dptr(out), nthreads)
+        if rc:
+            raise ValueError(f"oracle rejected the request (rc={rc})")
+        return out
+
+    def baseline(self, row0, nrows, r0, nr, nthreads=0):
+        out = np.zeros((nr, nrows))
+        t = lib().rfo_baseline_shinozuka(C.byref(self.req), row0, nrows, r0, nr, _dptr(out), nthreads)
+        if t < 0:
+            raise ValueError("baseline rejected the request")
+        return out, t
+
+
+def rng(seedStart=None) -> RNG:
+    r = RNG()
+    if seedStart is None:
+        lib().rfo_rng_initialize(C.byref(r))
+    else:
+        if lib().rfo_rng_seed(C.byref(r), seedStart):
+            raise ValueError(seedStart)
+    return r
+
+
+def grid(xMin, xStep, xNStep):
+    """setGrid (axis 1 fastest): returns n x nDim."""
+    nd = len(xNStep)
+    n = int(np.prod(xNStep))
+    out = np.zeros((n, nd))
+    a = np.asarray(xMin, dtype=np.float64)
+    b = np.asarray(xStep, dtype=np.float64)
+    c = np.asarray(xNStep, dtype=np.int32)
+    lib().rfo_set_grid(nd, _dptr(a), _dptr(b), c.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(out))
+    return out
+
+
+def unity_partition(xNStep, overlapNPoints, faceMask=0xFFFFFFFF):
+    nd = len(xNStep)
+    a = np.asarray(xNStep, dtype=np.int32)
+    b = np.asarray(overlapNPoints, dtype=np.int32)
+    out = np.zeros(int(np.prod(xNStep)))
+    lib().rfo_unity_partition(nd, a.ctypes.data_as(C.POINTER(C.c_int32)), b.ctypes.data_as(C.POINTER(C.c_int32)),
+                              faceMask, _dptr(out))
+    return out

@@ -1,0 +1,256 @@
+"""B200-native spectral-sum random-field generator (randomFieldND path of
+cottereau/randomField) behind a C-ABI.
+
+The Python layer is a thin ctypes mirror of the reference interface
+``createStandardGaussianFieldUnstruct(xPoints, corrMod, margiFirst, corrL,
+fieldAvg, fieldVar, Nmc, method, randField)`` (README.md:58-92): the same
+argument names, meanings and layouts (xPoints nDim x n, randField n x Nmc,
+Fortran column-major), strings or integer ids for corrMod/margiFirst, and
+the reference's error rules raised as :class:`RandomFieldError` instead of
+``stop``/``MPI_ABORT``.  All computation happens in librf_b200.so on the GPU;
+there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = [
+    "RandomFieldError", "Options", "Context", "lib", "create_standard_gaussian_field_unstruct",
+    "query_geometry", "ISOTROPIC", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
+    "PREC_BF16", "PREC_FP16", "PREC_FP32", "PREC_BF16_FAST", "LIB_PATH", "STATUS",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librf_b200.so")
+
+# constants_RF.f90:12-21
+ISOTROPIC, SHINOZUKA = 1, 2
+CM_GAUSSIAN, CM_COS = 1, 2
+FOM_GAUSSIAN, FOM_LOGNORMAL = 1, 2
+PREC_BF16, PREC_FP16, PREC_FP32, PREC_BF16_FAST = 0, 1, 2, 3
+
+STATUS = {
+    0: "RF_OK", -1: "RF_EINVAL_NMC", -2: "RF_EINVAL_NDIM", -3: "RF_EINVAL_CORRL", -4: "RF_EINVAL_LOGNORMAL",
+    -5: "RF_EINVAL_METHOD", -6: "RF_EINVAL_CORRMOD", -7: "RF_EINVAL_MARGINAL", -8: "RF_EINVAL_RANGE",
+    -9: "RF_EINVAL_ARG", -10: "RF_ENOTSUP", -20: "RF_ECUDA", -21: "RF_ENOMEM", -22: "RF_ETIMEDOUT",
+    -23: "RF_ENOMEM_ADMISSION", -25: "RF_ENODEV",
+}
+
+_CORRMOD = {"gaussian": CM_GAUSSIAN, "cos": CM_COS, "cm_gaussian": CM_GAUSSIAN, "cm_cos": CM_COS}
+_MARGI = {"gaussian": FOM_GAUSSIAN, "lognormal": FOM_LOGNORMAL}
+_PREC = {"bf16": PREC_BF16, "fp16": PREC_FP16, "fp32": PREC_FP32, "bf16_fast": PREC_BF16_FAST}
+
+# Every symbol include/randomfield_b200.h declares.
+EXPORTS = [
+    "rf_options_init", "rf_create_standard_gaussian_field_unstruct", "rf_context_create", "rf_context_destroy",
+    "rf_generate_device", "rf_context_synchronize", "rf_query_geometry", "rf_last_error", "rf_abi_version",
+    "rf_context_set_timing", "rf_context_last_times",
+]
+
+
+class RandomFieldError(RuntimeError):
+    """A non-zero status of the C-ABI (the reference would stop or abort)."""
+
+    def __init__(self, code: int, message: str):
+        self.code = code
+        self.status = STATUS.get(code, str(code))
+        super().__init__(f"{self.status} ({code}): {message}")
+
+
+class Options(C.Structure):
+    """rf_options (include/randomfield_b200.h)."""
+
+    _fields_ = [
+        ("size", C.c_int32),
+        ("precision", C.c_int32),
+        ("seed_start", C.c_int64),
+        ("k_nstep", C.c_int32 * 3),
+        ("iso_n_radial", C.c_int32),
+        ("iso_n_dir", C.c_int32),
+        ("literal", C.c_int32),
+        ("normalize", C.c_int32),
+        ("x_range", C.c_double * 3),
+        ("device", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+    @classmethod
+    def make(cls, precision="bf16", seed_start=0, k_nstep=(0, 0, 0), iso_n_radial=0, iso_n_dir=0,
+             literal=False, normalize=False, x_range=(0.0, 0.0, 0.0), device=0) -> "Options":
+        o = cls()
+        lib().rf_options_init(C.byref(o))
+        o.precision = _PREC[precision] if isinstance(precision, str) else int(precision)
+        o.seed_start = int(seed_start)
+        for i in range(3):
+            o.k_nstep[i] = int(k_nstep[i]) if i < len(k_nstep) else 0
+            o.x_range[i] = float(x_range[i]) if i < len(x_range) else 0.0
+        o.iso_n_radial = int(iso_n_radial)
+        o.iso_n_dir = int(iso_n_dir)
+        o.literal = int(bool(literal))
+        o.normalize = int(bool(normalize))
+        o.device = int(device)
+        return o
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded librf_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RandomFieldError(-25, f"{LIB_PATH} is missing: run `python -m randomfield_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        P, d, i32, i64 = C.POINTER, C.c_double, C.c_int, C.c_int64
+        L.rf_options_init.argtypes = [P(Options)]
+        L.rf_options_init.restype = None
+        L.rf_last_error.restype = C.c_char_p
+        L.rf_abi_version.restype = C.c_int
+        L.rf_create_standard_gaussian_field_unstruct.argtypes = [
+            P(d), i32, i64, i32, i32, P(d), d, d, i32, i32, P(d), P(Options)]
+        L.rf_context_create.argtypes = [i32, P(C.c_void_p)]
+        L.rf_context_destroy.argtypes = [C.c_void_p]
+        L.rf_context_synchronize.argtypes = [C.c_void_p]
+        L.rf_context_set_timing.argtypes = [C.c_void_p, i32]
+        L.rf_context_last_times.argtypes = [C.c_void_p, P(d), P(d), P(d), P(C.c_int32)]
+        L.rf_generate_device.argtypes = [C.c_void_p, C.c_void_p, i32, i64, i32, i32, P(d), d, d, i32, i32,
+                                         C.c_void_p, P(Options), C.c_void_p]
+        L.rf_query_geometry.argtypes = [P(d), i32, i64, i32, P(d), i32, P(Options), P(i64), P(C.c_int32), P(d),
+                                        P(d)]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise RandomFieldError(rc, lib().rf_last_error().decode())
+
+
+def _id(v, table, what):
+    if isinstance(v, str):
+        key = v.strip().lower()
+        if key not in table:
+            raise RandomFieldError(-9, f"unknown {what} '{v}'")
+        return table[key]
+    return int(v)
+
+
+def _points(xPoints) -> np.ndarray:
+    """xPoints as nDim x n (reference layout) -> Fortran-ordered float64."""
+    x = np.asarray(xPoints, dtype=np.float64)
+    if x.ndim == 1:
+        x = x.reshape(1, -1)
+    return np.asfortranarray(x)
+
+
+def _opts(opts) -> Options:
+    if opts is None:
+        return Options.make()
+    if isinstance(opts, Options):
+        return opts
+    return Options.make(**opts)
+
+
+def create_standard_gaussian_field_unstruct(xPoints, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method,
+                                            randField=None, options=None, **kw):
+    """Generate Nmc realizations at the points; returns randField (n x Nmc).
+
+    Mirrors createStandardGaussianFieldUnstruct (README.md:58-92).  ``xPoints``
+    is nDim x n; ``randField``, if given, must be a Fortran-ordered float64
+    n x Nmc array and is filled in place.  Extra keywords build an
+    :class:`Options` (precision, seed_start, k_nstep, iso_n_radial, iso_n_dir,
+    literal, normalize, x_range, device).
+    """
+    x = _points(xPoints)
+    nDim, n = x.shape
+    cm = _id(corrMod, _CORRMOD, "corrMod")
+    mf = _id(margiFirst, _MARGI, "margiFirst")
+    cl = np.ascontiguousarray(np.asarray(corrL, dtype=np.float64).reshape(-1))
+    if cl.size < nDim:
+        raise RandomFieldError(-9, f"corrL needs {nDim} entries")
+    if randField is None:
+        randField = np.empty((n, int(Nmc)), dtype=np.float64, order="F")
+    elif (randField.dtype != np.float64 or not randField.flags.f_contiguous
+          or randField.shape != (n, int(Nmc))):
+        raise RandomFieldError(-9, "randField must be a Fortran-ordered float64 n x Nmc array")
+    o = _opts(options if options is not None else (kw or None))
+    P = C.POINTER(C.c_double)
+    _check(lib().rf_create_standard_gaussian_field_unstruct(
+        x.ctypes.data_as(P), nDim, n, cm, mf, cl.ctypes.data_as(P), float(fieldAvg), float(fieldVar), int(Nmc),
+        int(method), randField.ctypes.data_as(P), C.byref(o)))
+    return randField
+
+
+def query_geometry(xPoints, corrMod, corrL, method, options=None, **kw):
+    """(K, kNStep[3], kDelta[3], ampMult) exactly as the generator uses them."""
+    x = _points(xPoints)
+    nDim, n = x.shape
+    cl = np.ascontiguousarray(np.asarray(corrL, dtype=np.float64).reshape(-1))
+    o = _opts(options if options is not None else (kw or None))
+    K = C.c_int64()
+    kn = (C.c_int32 * 3)()
+    kd = (C.c_double * 3)()
+    am = C.c_double()
+    P = C.POINTER(C.c_double)
+    _check(lib().rf_query_geometry(x.ctypes.data_as(P), nDim, n, _id(corrMod, _CORRMOD, "corrMod"),
+                                   cl.ctypes.data_as(P), int(method), C.byref(o), C.byref(K), kn, kd,
+                                   C.byref(am)))
+    return K.value, list(kn), list(kd), am.value
+
+
+class Context:
+    """rf_context: device-resident generation on a CUDA stream.
+
+    ``generate(d_x, d_out, ...)`` takes device pointers (ints) or objects with
+    ``data_ptr()`` (torch tensors): d_x holds nDim x n float64 (point-major),
+    d_out n x Nmc float64 column-major.
+    """
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().rf_context_create(int(device), C.byref(h)))
+        self._h = h
+        self.device = int(device)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            lib().rf_context_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _ptr(t) -> int:
+        return int(t.data_ptr()) if hasattr(t, "data_ptr") else int(t)
+
+    def generate(self, d_x, nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, d_out,
+                 options=None, stream=0, **kw) -> None:
+        cl = np.ascontiguousarray(np.asarray(corrL, dtype=np.float64).reshape(-1))
+        o = _opts(options if options is not None else (kw or None))
+        s = stream if isinstance(stream, int) else int(getattr(stream, "cuda_stream", 0))
+        _check(lib().rf_generate_device(self._h, C.c_void_p(self._ptr(d_x)), int(nDim), int(n),
+                                        _id(corrMod, _CORRMOD, "corrMod"), _id(margiFirst, _MARGI, "margiFirst"),
+                                        cl.ctypes.data_as(C.POINTER(C.c_double)), float(fieldAvg), float(fieldVar),
+                                        int(Nmc), int(method), C.c_void_p(self._ptr(d_out)), C.byref(o),
+                                        C.c_void_p(s)))
+
+    def synchronize(self) -> None:
+        _check(lib().rf_context_synchronize(self._h))
+
+    def set_timing(self, enable: bool = True) -> None:
+        _check(lib().rf_context_set_timing(self._h, int(bool(enable))))
+
+    def last_times(self):
+        """(tables_ms, contract_ms, post_ms, kernel_launches) of the last call."""
+        a, b, p = C.c_double(), C.c_double(), C.c_double()
+        n = C.c_int32()
+        _check(lib().rf_context_last_times(self._h, C.byref(a), C.byref(b), C.byref(p), C.byref(n)))
+        return a.value, b.value, p.value, n.value

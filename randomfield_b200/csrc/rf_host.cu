@@ -1,0 +1,636 @@
+// rf_host.cu -- the C-ABI (include/randomfield_b200.h): validation with the
+// reference's rules, problem geometry, device contexts, transfers and
+// dispatch to the kernels.  No CPU fallback: without a usable CUDA device
+// every generating entry point fails with RF_ENODEV / RF_ECUDA.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/randomfield_b200.h"
+#include "rf_device.cuh"
+#include "rf_launch.h"
+#include "rf_plan.h"
+
+using namespace rfb;
+
+// ------------------------------------------------------------------ errors
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  if (e == cudaErrorMemoryAllocation) return fail(RF_ENOMEM, "%s: %s", where, cudaGetErrorString(e));
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+    return fail(RF_ENODEV, "%s: %s", where, cudaGetErrorString(e));
+  return fail(RF_ECUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+#define RF_CUDA(call, where)                   \
+  do {                                         \
+    cudaError_t e_ = (call);                   \
+    if (e_ != cudaSuccess) return cuda_fail(e_, where); \
+  } while (0)
+
+// rnglib jump table: a^(2^j) mod m (rnglib.f90:548-659 multipliers).
+const JumpTable& jump_table() {
+  static JumpTable jt = [] {
+    JumpTable t;
+    int64_t b1 = kA1, b2 = kA2;
+    for (int j = 0; j < 64; ++j) {
+      t.p1[j] = b1;
+      t.p2[j] = b2;
+      b1 = (int64_t)(((unsigned __int128)b1 * (unsigned __int128)b1) % (unsigned __int128)kM1);
+      b2 = (int64_t)(((unsigned __int128)b2 * (unsigned __int128)b2) % (unsigned __int128)kM2);
+    }
+    return t;
+  }();
+  return jt;
+}
+
+// spectra_RF.f90:15-44 (cm_GAUSSIAN values, also used for cm_COS whose
+// reference kMax is left at init_RF's -1).
+double kmax_nd(int nDim) { return nDim == 1 ? 6.457 : (nDim == 2 ? 7.035 : 7.355); }
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+struct Request {
+  int nDim;
+  int64_t n;
+  int corrMod, margiFirst, Nmc, method;
+  double corrL[3];
+  double fieldAvg, fieldVar;
+  rf_options opt;
+};
+
+// type_inputRF.f90:1159-1206, randomFieldND.f90:162-166, constants_RF.f90:12-21
+int validate(const Request& r) {
+  if (r.n < 1) return fail(RF_EINVAL_ARG, "n must be >= 1 (got %lld)", (long long)r.n);
+  if (r.nDim < 1 || r.nDim > 3) return fail(RF_EINVAL_NDIM, "nDim must be 1, 2 or 3 (got %d)", r.nDim);
+  if (r.Nmc < 1) return fail(RF_EINVAL_NMC, "Nmc must be >= 1 (got %d)", r.Nmc);
+  for (int d = 0; d < r.nDim; ++d)
+    if (!(r.corrL[d] > 0.0)) return fail(RF_EINVAL_CORRL, "corrL(%d) must be > 0", d + 1);
+  if (r.method != RF_ISOTROPIC && r.method != RF_SHINOZUKA)
+    return fail(RF_EINVAL_METHOD, "method must be 1 (isotropic) or 2 (Shinozuka), got %d", r.method);
+  if (r.method == RF_ISOTROPIC && r.nDim < 2)
+    return fail(RF_EINVAL_NDIM, "the isotropic method needs nDim 2 or 3");
+  if (r.corrMod != RF_CM_GAUSSIAN && r.corrMod != RF_CM_COS)
+    return fail(RF_EINVAL_CORRMOD, "corrMod must be 1 (gaussian) or 2 (cos), got %d", r.corrMod);
+  if (r.margiFirst != RF_FOM_GAUSSIAN && r.margiFirst != RF_FOM_LOGNORMAL)
+    return fail(RF_EINVAL_MARGINAL, "margiFirst must be 1 (gaussian) or 2 (lognormal), got %d", r.margiFirst);
+  if (r.margiFirst == RF_FOM_LOGNORMAL && r.fieldAvg <= 0.0)
+    return fail(RF_EINVAL_LOGNORMAL, "when using lognormal fieldAvg should be a positive number");
+  const rf_options& o = r.opt;
+  if (o.precision < RF_PREC_BF16 || o.precision > RF_PREC_BF16_FAST)
+    return fail(RF_EINVAL_ARG, "unknown precision form %d", o.precision);
+  if (o.literal && r.method != RF_SHINOZUKA)
+    return fail(RF_EINVAL_ARG, "literal mode exists for the Shinozuka method only");
+  for (int d = 0; d < 3; ++d)
+    if (o.k_nstep[d] < 0 || o.k_nstep[d] == 1) return fail(RF_EINVAL_ARG, "k_nstep must be 0 or >= 2");
+  if (o.iso_n_radial < 0 || o.iso_n_radial == 1 || o.iso_n_dir < 0)
+    return fail(RF_EINVAL_ARG, "iso_n_radial must be 0 or >= 2, iso_n_dir >= 0");
+  return RF_OK;
+}
+
+// Geometry of spectra_RF.f90:50-133 (Shinozuka grid, isotropic radial rule),
+// ampMult of randomFieldND.f90:260-266.  ext[d] is the physical extent.
+int geometry(const Request& r, const double* ext, Plan& P) {
+  const rf_options& o = r.opt;
+  memset(&P, 0, sizeof(P));
+  P.nDim = r.nDim;
+  P.n = r.n;
+  P.Nmc = r.Nmc;
+  P.method = r.method;
+  P.corrMod = r.corrMod;
+  P.margiFirst = r.margiFirst;
+  P.literal = o.literal ? 1 : 0;
+  P.normalize = o.normalize ? 1 : 0;
+  P.prec = o.precision;
+  for (int d = 0; d < 3; ++d) P.corrL[d] = d < r.nDim ? r.corrL[d] : 1.0;
+  P.fieldAvg = r.fieldAvg;
+  P.fieldVar = r.fieldVar;
+  P.kMax = kmax_nd(r.nDim);
+  double xr[3] = {0, 0, 0};
+  for (int d = 0; d < r.nDim; ++d) {
+    const double e = o.x_range[d] > 0.0 ? o.x_range[d] : ext[d];
+    if (!(e > 0.0) || !std::isfinite(e))
+      return fail(RF_EINVAL_RANGE, "zero extent along axis %d: kDelta = 2 pi/(1.1 xRange) is infinite", d + 1);
+    xr[d] = e / r.corrL[d];  // randomFieldND.f90:72
+  }
+  if (r.method == RF_SHINOZUKA) {
+    int64_t kn = 1;
+    double prod = 1.0;
+    for (int d = 0; d < r.nDim; ++d) {
+      const double kd = 2.0 * kRefPi / (1.1 * xr[d]);
+      const int ns = o.k_nstep[d] > 0 ? o.k_nstep[d] : 1 + (int)(1.0 * std::ceil(P.kMax / kd));
+      if (ns < 2) return fail(RF_EINVAL_RANGE, "fewer than 2 wavenumbers along axis %d", d + 1);
+      P.kNStep[d] = ns;
+      P.kDelta[d] = P.kMax / (double)(ns - 1);
+      kn *= ns;
+      prod *= P.kDelta[d];
+    }
+    P.K = kn * ((int64_t)1 << (r.nDim - 1));
+    P.ampMult = 2.0 * std::sqrt(prod / std::pow(2.0 * kRefPi, (double)r.nDim));
+  } else {
+    double r2 = 0.0;
+    for (int d = 0; d < r.nDim; ++d) r2 += xr[d] * xr[d];
+    const double kd = 2.0 * kRefPi / (1.1 * std::sqrt(r2));
+    const int nr = o.iso_n_radial > 0 ? o.iso_n_radial : 1 + (int)(5.0 * std::ceil(P.kMax / kd));
+    const int nd = o.iso_n_dir > 0 ? o.iso_n_dir : 32;
+    P.kNStep[0] = nr;
+    P.kNStep[1] = nd;
+    P.kDelta[0] = P.kMax / (double)(nr - 1);
+    P.K = (int64_t)nr * nd;
+    P.ampMult = 1.0;
+  }
+  if (r.corrMod == RF_CM_COS && P.K <= 6)
+    return fail(RF_EINVAL_CORRMOD, "the cos correlation model needs more than 6 wavevectors");
+  return RF_OK;
+}
+
+// Seed words after math_RF.f90:561: seed = 72 + 18*seedStart + 37*(i-1).
+int seeds(int64_t seedStart, Plan& P) {
+  if (seedStart < 0) {
+    // stochastic seed from the clock, as calculate_random_seed does
+    const auto t = std::chrono::steady_clock::now().time_since_epoch().count();
+    seedStart = (int64_t)((uint64_t)t % 100000000ull);
+  }
+  const int64_t ig1 = 72 + 18 * seedStart, ig2 = ig1 + 37;
+  if (ig2 >= kM2) return fail(RF_EINVAL_ARG, "seed_start too large for rnglib seeds");
+  P.ig1 = (int32_t)ig1;
+  P.ig2 = (int32_t)ig2;
+  return RF_OK;
+}
+
+// Kernel layout of the plan.
+int layout(Plan& P) {
+  const bool tc = P.prec != PREC_FP32;
+  P.gen = GEN_TABLE;
+  if (P.method == RF_SHINOZUKA && P.nDim == 3 && !P.literal && P.kNStep[0] <= kMaxGridN &&
+      P.kNStep[1] <= kMaxGridN && P.kNStep[2] <= kMaxGridN)
+    P.gen = GEN_GRID3;
+  if (P.gen == GEN_GRID3) {
+    P.lPad = (int32_t)round_up(P.kNStep[2], 8);  // 8-aligned TMEM stores per half
+    P.chunkK = 2 * P.lPad;
+    P.nChunks = (int64_t)P.kNStep[0] * P.kNStep[1] * 2;
+  } else {
+    P.lPad = 0;
+    P.chunkK = kTableChunk;
+    P.nChunks = (P.K + kTableChunk - 1) / kTableChunk;
+  }
+  if (tc) {
+    P.nmcPad = (int32_t)round_up(P.Nmc, 16);
+    if (P.nmcPad > kMaxNmcPad) return fail(RF_ENOTSUP, "Nmc > %d per launch", kMaxNmcPad);
+    P.bRows = P.prec == PREC_BF16 ? 2 * P.nmcPad : P.nmcPad;
+    P.stageBytes = (int64_t)2 * P.chunkK * P.bRows * 2;
+  } else {
+    int rpt = 1;
+    while (rpt < 8 && 8 * rpt < P.Nmc) rpt *= 2;
+    P.nmcPad = (int32_t)round_up(P.Nmc, 8 * rpt);
+    P.bRows = P.nmcPad;
+    P.stageBytes = (int64_t)2 * P.chunkK * P.nmcPad * 4;
+  }
+  // FP16 operand side: scale B by 2^s so that the largest |B| sits near 2^15.
+  P.bScaleLog2 = 0;
+  if (P.prec == PREC_FP16) {
+    double bound = 1.0;  // Shinozuka: sqrt(S) <= 1
+    if (P.method == RF_ISOTROPIC) {
+      bound = 0.0;
+      const int D = P.nDim;
+      for (int j = 0; j < P.kNStep[0]; ++j) {
+        const double rr = j * P.kDelta[0];
+        const double S = P.corrMod == RF_CM_GAUSSIAN ? std::exp(-(rr * rr) / (4.0 * kRefPi)) : (j == 5 ? 1.0 : 0.0);
+        const double shell = D == 3 ? 4.0 * kRefPi * rr * rr : 2.0 * kRefPi * rr;
+        const double A = std::sqrt(2.0 * shell * S * P.kDelta[0] / (std::pow(2.0 * kRefPi, D) * P.kNStep[1]));
+        bound = std::max(bound, A * std::sqrt(3.0));
+      }
+      if (bound <= 0.0) bound = 1.0;
+    }
+    P.bScaleLog2 = (int32_t)std::floor(std::log2(32768.0 / bound));
+  }
+  P.outScale = P.ampMult * std::ldexp(1.0, -P.bScaleLog2);
+  // multiVariateTransformation (randomFieldND.f90:139-178)
+  if (P.margiFirst == RF_FOM_GAUSSIAN) {
+    P.margSd = std::sqrt(P.fieldVar);
+    P.margAvg = P.fieldAvg;
+    P.lognormal = 0;
+  } else {
+    const double nv = std::log(1 + P.fieldVar / (P.fieldAvg * P.fieldAvg));
+    P.margSd = std::sqrt(nv);
+    P.margAvg = std::log(P.fieldAvg) - nv / 2;
+    P.lognormal = 1;
+  }
+  P.applyMarginal = P.normalize ? 0 : 1;
+  return RF_OK;
+}
+
+// ----------------------------------------------------------------- extent
+__global__ void rf_extent_kernel(const double* __restrict__ x, int64_t n, int nDim, double* __restrict__ part) {
+  __shared__ double smin[3][256], smax[3][256];
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    for (int d = 0; d < nDim; ++d) {
+      const double v = x[i * nDim + d];
+      lo[d] = fmin(lo[d], v);
+      hi[d] = fmax(hi[d], v);
+    }
+  for (int d = 0; d < 3; ++d) {
+    smin[d][threadIdx.x] = lo[d];
+    smax[d][threadIdx.x] = hi[d];
+  }
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+      for (int d = 0; d < 3; ++d) {
+        smin[d][threadIdx.x] = fmin(smin[d][threadIdx.x], smin[d][threadIdx.x + s]);
+        smax[d][threadIdx.x] = fmax(smax[d][threadIdx.x], smax[d][threadIdx.x + s]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int d = 0; d < 3; ++d) {
+      part[blockIdx.x * 6 + d] = smin[d][0];
+      part[blockIdx.x * 6 + 3 + d] = smax[d][0];
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- context
+struct rf_context {
+  int device = 0;
+  int numSMs = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  void* dB = nullptr;
+  size_t capB = 0;
+  double* dKtab = nullptr;
+  size_t capK = 0;
+  double* dWork = nullptr;  // extent partials and moments
+  size_t capWork = 0;
+  double* hWork = nullptr;  // pinned mirror of dWork
+  uint32_t* dErr = nullptr;
+  double* dX = nullptr;     // flat API staging of the points
+  size_t capX = 0;
+  double* dOut = nullptr;   // flat API result buffer
+  size_t capOut = 0;
+  bool timing = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool evValid = false;
+  int32_t launches = 0;     // kernels launched by the last generation
+};
+
+namespace {
+
+template <typename T>
+int ensure(T*& p, size_t& cap, size_t bytes, const char* what) {
+  if (bytes <= cap && p) return RF_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(RF_ENOMEM, "cannot allocate %zu bytes of device memory for %s", bytes, what);
+  }
+  p = reinterpret_cast<T*>(q);
+  cap = bytes;
+  return RF_OK;
+}
+
+constexpr int kExtentBlocks = 128;
+
+int context_init(rf_context* c, int device) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(RF_ENODEV, "no CUDA device available");
+  }
+  if (device < 0 || device >= count) return fail(RF_ENODEV, "device %d does not exist (%d present)", device, count);
+  c->device = device;
+  RF_CUDA(cudaSetDevice(device), "cudaSetDevice");
+  cudaDeviceProp prop;
+  RF_CUDA(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+  if (prop.major != 10) return fail(RF_ENODEV, "device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
+  c->numSMs = prop.multiProcessorCount;
+  RF_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  RF_CUDA(cudaMalloc(&c->dErr, sizeof(uint32_t)), "cudaMalloc(err)");
+  RF_CUDA(cudaMemset(c->dErr, 0, sizeof(uint32_t)), "cudaMemset(err)");
+  const size_t work = sizeof(double) * std::max<size_t>(6 * kExtentBlocks, 2 * 65536);
+  if (int rc = ensure(c->dWork, c->capWork, work, "work")) return rc;
+  RF_CUDA(cudaMallocHost(&c->hWork, work), "cudaMallocHost(work)");
+  return RF_OK;
+}
+
+void context_free(rf_context* c) {
+  if (c->device >= 0) cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->dB);
+  cudaFree(c->dKtab);
+  cudaFree(c->dWork);
+  cudaFree(c->dErr);
+  cudaFree(c->dX);
+  cudaFree(c->dOut);
+  if (c->hWork) cudaFreeHost(c->hWork);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+// Extent of the device-resident points per axis (needed for xRange).
+int device_extent(rf_context* c, const double* dX, int nDim, int64_t n, cudaStream_t st, double* ext) {
+  rf_extent_kernel<<<kExtentBlocks, 256, 0, st>>>(dX, n, nDim, c->dWork);
+  RF_CUDA(cudaGetLastError(), "extent kernel");
+  ++c->launches;
+  RF_CUDA(cudaMemcpyAsync(c->hWork, c->dWork, sizeof(double) * 6 * kExtentBlocks, cudaMemcpyDeviceToHost, st),
+          "extent copy");
+  RF_CUDA(cudaStreamSynchronize(st), "extent sync");
+  for (int d = 0; d < nDim; ++d) {
+    double lo = INFINITY, hi = -INFINITY;
+    for (int b = 0; b < kExtentBlocks; ++b) {
+      lo = std::min(lo, c->hWork[b * 6 + d]);
+      hi = std::max(hi, c->hWork[b * 6 + 3 + d]);
+    }
+    ext[d] = hi - lo;
+  }
+  return RF_OK;
+}
+
+int build_plan(const Request& rq, const double* ext, Plan& P) {
+  if (int rc = geometry(rq, ext, P)) return rc;
+  if (int rc = seeds(rq.opt.seed_start, P)) return rc;
+  return layout(P);
+}
+
+// Tables + contraction (+ normalisation) for a plan whose points sit in dX.
+int run_plan(rf_context* c, const Plan& P, const double* dX, double* dOut, cudaStream_t st) {
+  const size_t bBytes = (size_t)P.nChunks * P.stageBytes;
+  if (int rc = ensure(c->dB, c->capB, bBytes, "contraction operand")) return rc;
+  double* ktab = nullptr;
+  if (P.gen == GEN_TABLE) {
+    if (int rc = ensure(c->dKtab, c->capK, (size_t)P.nChunks * 3 * kTableChunk * sizeof(double), "wavevector table"))
+      return rc;
+    ktab = c->dKtab;
+  }
+  if (P.prec != PREC_FP32 && tc_smem_bytes(P, nullptr) == 0)
+    return fail(RF_ENOTSUP, "stage too large for shared memory (Nmc or wavenumbers per axis too large)");
+  int64_t xSlab = P.n, nSlab = 1;
+  if (P.literal) {
+    // randomFieldND.f90:237-239
+    xSlab = (int64_t)((double)P.nDim * 1e8 / (double)P.K);
+    if (xSlab > P.n) xSlab = P.n;
+    if (xSlab < 1) xSlab = 1;
+    nSlab = (P.n + xSlab - 1) / xSlab;
+  }
+  if (c->timing) {
+    for (auto& e : c->ev)
+      if (!e) RF_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+    RF_CUDA(cudaEventRecord(c->ev[0], st), "cudaEventRecord");
+  }
+  for (int64_t m = 0; m < nSlab; ++m) {
+    const int64_t row0 = m * xSlab;
+    const int64_t rows = std::min(xSlab, P.n - row0);
+    RF_CUDA(launch_tables(P, jump_table(), c->dB, ktab, P.literal ? m : -1, nSlab, st), "table kernel");
+    if (c->timing && m == 0) RF_CUDA(cudaEventRecord(c->ev[1], st), "cudaEventRecord");
+    if (P.prec == PREC_FP32) {
+      RF_CUDA(launch_fp32(P, dX, c->dB, ktab, dOut, row0, rows, st), "FP32 contraction kernel");
+    } else {
+      RF_CUDA(launch_tc(P, dX, c->dB, ktab, dOut, row0, rows, c->dErr, c->numSMs, st), "tcgen05 contraction kernel");
+    }
+    c->launches += 2;
+  }
+  if (c->timing) RF_CUDA(cudaEventRecord(c->ev[2], st), "cudaEventRecord");
+  if (P.normalize) {
+    if ((size_t)2 * P.Nmc * sizeof(double) > c->capWork)
+      if (int rc = ensure(c->dWork, c->capWork, (size_t)2 * P.Nmc * sizeof(double), "moments")) return rc;
+    RF_CUDA(launch_normalize_and_map(P, dOut, P.literal ? 1 : P.Nmc, c->dWork, st), "normalisation kernels");
+    c->launches += 3;
+  }
+  if (c->timing) {
+    RF_CUDA(cudaEventRecord(c->ev[3], st), "cudaEventRecord");
+    c->evValid = true;
+  }
+  return RF_OK;
+}
+
+int check_device_error(rf_context* c) {
+  uint32_t err = 0;
+  RF_CUDA(cudaMemcpy(&err, c->dErr, sizeof(err), cudaMemcpyDeviceToHost), "error word");
+  if (err) {
+    cudaMemset(c->dErr, 0, sizeof(uint32_t));
+    return fail(RF_ETIMEDOUT, "a bounded device wait expired (error word 0x%x); results are invalid", err);
+  }
+  return RF_OK;
+}
+
+std::mutex g_default_mu;
+rf_context* g_default[64] = {nullptr};
+
+int default_context(int device, rf_context** out) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  if (device < 0 || device >= 64) return fail(RF_ENODEV, "bad device ordinal %d", device);
+  if (!g_default[device]) {
+    rf_context* c = new rf_context();
+    if (int rc = context_init(c, device)) {
+      context_free(c);
+      delete c;
+      return rc;
+    }
+    g_default[device] = c;
+  }
+  *out = g_default[device];
+  return RF_OK;
+}
+
+Request make_request(int nDim, int64_t n, int corrMod, int margiFirst, const double* corrL, double fieldAvg,
+                     double fieldVar, int Nmc, int method, const rf_options* opt) {
+  Request r;
+  r.nDim = nDim;
+  r.n = n;
+  r.corrMod = corrMod;
+  r.margiFirst = margiFirst;
+  r.Nmc = Nmc;
+  r.method = method;
+  for (int d = 0; d < 3; ++d) r.corrL[d] = (corrL && d < nDim && d >= 0) ? corrL[d] : 1.0;
+  r.fieldAvg = fieldAvg;
+  r.fieldVar = fieldVar;
+  rf_options_init(&r.opt);
+  if (opt) {
+    const size_t sz = (opt->size > 0 && (size_t)opt->size < sizeof(rf_options)) ? (size_t)opt->size : sizeof(rf_options);
+    memcpy(&r.opt, opt, sz);
+    r.opt.size = sizeof(rf_options);
+  }
+  return r;
+}
+
+}  // namespace
+
+// ================================================================== C-ABI
+extern "C" {
+
+void rf_options_init(rf_options* opt) {
+  if (!opt) return;
+  memset(opt, 0, sizeof(*opt));
+  opt->size = sizeof(rf_options);
+  opt->precision = RF_PREC_BF16;
+}
+
+const char* rf_last_error(void) { return g_err.c_str(); }
+
+int rf_abi_version(void) { return RF_ABI_VERSION; }
+
+int rf_query_geometry(const double* xPoints, int nDim, int64_t n, int corrMod, const double* corrL, int method,
+                      const rf_options* opt, int64_t* K, int32_t* kNStep, double* kDelta, double* ampMult) {
+  g_err.clear();
+  if (!xPoints || !corrL) return fail(RF_EINVAL_ARG, "null pointer argument");
+  Request rq = make_request(nDim, n, corrMod, RF_FOM_GAUSSIAN, corrL, 0.0, 1.0, 1, method, opt);
+  if (int rc = validate(rq)) return rc;
+  double ext[3] = {0, 0, 0};
+  for (int d = 0; d < nDim; ++d) {
+    double lo = xPoints[d], hi = xPoints[d];
+    for (int64_t i = 1; i < n; ++i) {
+      lo = std::min(lo, xPoints[i * nDim + d]);
+      hi = std::max(hi, xPoints[i * nDim + d]);
+    }
+    ext[d] = hi - lo;
+  }
+  Plan P;
+  if (int rc = geometry(rq, ext, P)) return rc;
+  if (K) *K = P.K;
+  for (int d = 0; d < 3; ++d) {
+    if (kNStep) kNStep[d] = P.kNStep[d];
+    if (kDelta) kDelta[d] = P.kDelta[d];
+  }
+  if (ampMult) *ampMult = P.ampMult;
+  return RF_OK;
+}
+
+int rf_context_create(int device, rf_context** out) {
+  g_err.clear();
+  if (!out) return fail(RF_EINVAL_ARG, "null output pointer");
+  *out = nullptr;
+  rf_context* c = new rf_context();
+  if (int rc = context_init(c, device)) {
+    context_free(c);
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return RF_OK;
+}
+
+int rf_context_destroy(rf_context* ctx) {
+  if (!ctx) return RF_OK;
+  context_free(ctx);
+  delete ctx;
+  return RF_OK;
+}
+
+int rf_context_synchronize(rf_context* ctx) {
+  g_err.clear();
+  if (!ctx) return fail(RF_EINVAL_ARG, "null context");
+  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  RF_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  return check_device_error(ctx);
+}
+
+int rf_context_set_timing(rf_context* ctx, int enable) {
+  g_err.clear();
+  if (!ctx) return fail(RF_EINVAL_ARG, "null context");
+  ctx->timing = enable != 0;
+  ctx->evValid = false;
+  return RF_OK;
+}
+
+int rf_context_last_times(rf_context* ctx, double* tables_ms, double* contract_ms, double* post_ms,
+                          int32_t* kernel_launches) {
+  g_err.clear();
+  if (!ctx) return fail(RF_EINVAL_ARG, "null context");
+  if (kernel_launches) *kernel_launches = ctx->launches;
+  if (!ctx->evValid) return fail(RF_EINVAL_ARG, "no timed generation on this context (enable timing first)");
+  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  RF_CUDA(cudaEventSynchronize(ctx->ev[3]), "cudaEventSynchronize");
+  float a = 0, b = 0, p = 0;
+  RF_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]), "cudaEventElapsedTime");
+  RF_CUDA(cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]), "cudaEventElapsedTime");
+  RF_CUDA(cudaEventElapsedTime(&p, ctx->ev[2], ctx->ev[3]), "cudaEventElapsedTime");
+  if (tables_ms) *tables_ms = a;
+  if (contract_ms) *contract_ms = b;
+  if (post_ms) *post_ms = p;
+  return RF_OK;
+}
+
+int rf_generate_device(rf_context* ctx, const double* d_xPoints, int nDim, int64_t n, int corrMod, int margiFirst,
+                       const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method,
+                       double* d_randField, const rf_options* opt, void* stream) {
+  g_err.clear();
+  if (!ctx || !d_xPoints || !corrL || !d_randField) return fail(RF_EINVAL_ARG, "null pointer argument");
+  Request rq = make_request(nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
+  if (int rc = validate(rq)) return rc;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
+  ctx->launches = 0;
+  ctx->evValid = false;
+  double ext[3] = {0, 0, 0};
+  bool need = false;
+  for (int d = 0; d < nDim; ++d) need = need || !(rq.opt.x_range[d] > 0.0);
+  if (need)
+    if (int rc = device_extent(ctx, d_xPoints, nDim, n, st, ext)) return rc;
+  Plan P;
+  if (int rc = build_plan(rq, ext, P)) return rc;
+  return run_plan(ctx, P, d_xPoints, d_randField, st);
+}
+
+int rf_create_standard_gaussian_field_unstruct(const double* xPoints, int nDim, int64_t n, int corrMod,
+                                               int margiFirst, const double* corrL, double fieldAvg,
+                                               double fieldVar, int Nmc, int method, double* randField,
+                                               const rf_options* opt) {
+  g_err.clear();
+  if (!xPoints || !corrL || !randField) return fail(RF_EINVAL_ARG, "null pointer argument");
+  Request rq = make_request(nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
+  if (int rc = validate(rq)) return rc;
+  rf_context* c = nullptr;
+  if (int rc = default_context(rq.opt.device, &c)) return rc;
+  std::lock_guard<std::mutex> lk(c->mu);
+  RF_CUDA(cudaSetDevice(c->device), "cudaSetDevice");
+  c->launches = 0;
+  c->evValid = false;
+  const size_t xBytes = sizeof(double) * (size_t)nDim * (size_t)n;
+  const size_t oBytes = sizeof(double) * (size_t)n * (size_t)Nmc;
+  if (int rc = ensure(c->dX, c->capX, xBytes, "points")) return rc;
+  if (int rc = ensure(c->dOut, c->capOut, oBytes, "field")) return rc;
+  cudaStream_t st = c->stream;
+  RF_CUDA(cudaMemcpyAsync(c->dX, xPoints, xBytes, cudaMemcpyHostToDevice, st), "copy of xPoints");
+  double ext[3] = {0, 0, 0};
+  bool need = false;
+  for (int d = 0; d < nDim; ++d) need = need || !(rq.opt.x_range[d] > 0.0);
+  if (need)
+    if (int rc = device_extent(c, c->dX, nDim, n, st, ext)) return rc;
+  Plan P;
+  if (int rc = build_plan(rq, ext, P)) return rc;
+  if (int rc = run_plan(c, P, c->dX, c->dOut, st)) return rc;
+  RF_CUDA(cudaMemcpyAsync(randField, c->dOut, oBytes, cudaMemcpyDeviceToHost, st), "copy of randField");
+  RF_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  return check_device_error(c);
+}
+
+}  // extern "C"

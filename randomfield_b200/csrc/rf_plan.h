@@ -1,0 +1,60 @@
+// rf_plan.h -- host/device description of one generation request as the
+// kernels consume it.  Plain C++ (no CUDA types) so the host code and every
+// .cu file share it.
+#pragma once
+#include <stdint.h>
+
+namespace rfb {
+
+// constants_RF.f90:5 -- the reference's PI, used wherever PI enters a formula
+// (kDelta, S(k), ampMult, phase = 2*PI*U).  Range reduction of a phase uses the
+// true 2*pi instead, because cos is periodic in the true 2*pi.
+constexpr double kRefPi = 3.1415926535898;
+
+// rnglib.f90:548-659 moduli and multipliers of the combined MLCG.
+constexpr int64_t kM1 = 2147483563, kM2 = 2147483399;
+constexpr int64_t kA1 = 40014, kA2 = 40692;
+constexpr double kR8Scale = 4.656613057E-10;  // rnglib.f90:1517
+
+enum Generator : int32_t {
+  GEN_TABLE = 0,  // explicit wavevector table, one FP64 phase + SFU sincos per (point, k)
+  GEN_GRID3 = 1,  // 3-D tensor-grid wavevectors: per-axis tables and angle addition
+};
+
+enum Precision : int32_t { PREC_BF16 = 0, PREC_FP16 = 1, PREC_FP32 = 2, PREC_BF16_FAST = 3 };
+
+constexpr int kTileM = 128;        // points per tile (MMA M)
+constexpr int kStageCols = 64;     // TMEM columns per A stage (k-values per stage, max)
+constexpr int kTableChunk = 32;    // k-values per stage for GEN_TABLE
+constexpr int kMaxGridN = 32;      // GEN_GRID3: max wavenumbers per axis
+constexpr int kMaxNmcPad = 256;    // realizations per launch (MMA N <= 256)
+
+struct Plan {
+  // request
+  int32_t nDim, Nmc, method, corrMod, margiFirst, literal, normalize, prec;
+  int64_t n;
+  double corrL[3];
+  double fieldAvg, fieldVar;
+  // geometry (spectra_RF.f90 / randomFieldND.f90)
+  int64_t K;                  // wavevectors in the reference's count
+  int32_t kNStep[3];          // Shinozuka per axis; isotropic [0]=n_r, [1]=n_dir
+  double kDelta[3];           // Shinozuka per axis; isotropic [0]=dr
+  double kMax, ampMult;
+  int32_t ig1, ig2;           // rnglib generator-1 seed words
+  // kernel layout
+  int32_t gen;                // Generator
+  int32_t nmcPad;             // realizations padded (16 for tcgen05, 8 for FP32)
+  int32_t bRows;              // rows of B per stage (nmcPad, or 2*nmcPad with hi/lo)
+  int32_t chunkK;             // k-values per stage
+  int32_t lPad;               // GEN_GRID3: inner (axis 3) length padded to a multiple of 8
+  int64_t nChunks;            // stages per tile
+  int64_t stageBytes;         // bytes of one B stage
+  int32_t bScaleLog2;         // FP16: B stored times 2^bScaleLog2
+  double outScale;            // epilogue factor: ampMult * 2^-bScaleLog2
+  // marginal map (randomFieldND.f90:139-178), applied in the epilogue
+  int32_t applyMarginal;      // 0 when a normalisation pass follows
+  int32_t lognormal;
+  double margSd, margAvg;
+};
+
+}  // namespace rfb

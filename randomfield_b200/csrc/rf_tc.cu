@@ -1,0 +1,349 @@
+// rf_tc.cu -- the spectral-sum contraction on tcgen05 tensor cores.
+//
+// Replaces the hot loop of gen_Std_Gauss_Shinozuka (randomFieldND.f90:276-330:
+// DGEMM k.x + phi, cos, DGEMM with sqrt(S)) and of the isotropic generator
+// (:456-490) by one persistent kernel per launch:
+//
+//   D (128 points x Nmc, FP32 in TMEM) += A (128 x 16, trig tile in TMEM)
+//                                         x B (16 x Nmc, amplitude/phase in SMEM)
+//
+// Warp roles (320 threads, one CTA per SM):
+//   warps 0-7  generators: build the trig tile of a stage straight into TMEM
+//              (tcgen05.st), lane = point, two warpgroups split the columns;
+//              after the last stage of a tile they run the fused epilogue
+//              (tcgen05.ld, ampMult, marginal map, FP64 stores);
+//   warp 8     MMA issuer (one thread): tcgen05.mma kind::f16, A from TMEM,
+//              B by descriptor from SMEM; tcgen05.commit frees stages;
+//   warp 9     producer (one thread): 1-D bulk copies (TMA) of B stages from
+//              HBM/L2 into SMEM; no multicast.
+// Every wait is bounded (globaltimer); on expiry the kernel raises an error
+// word, drains its own async work, frees TMEM and returns.
+#include "rf_device.cuh"
+#include "rf_gen.cuh"
+#include "rf_launch.h"
+
+namespace rfb {
+
+namespace {
+
+constexpr int kGenWarps = 8;
+constexpr int kMmaWarp = 8;
+constexpr int kProdWarp = 9;
+constexpr int kThreads = 320;
+constexpr int kMaxStages = 4;
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kDCol = 0;      // accumulator columns [0, nmcPad)
+constexpr uint32_t kACol = 256;    // A stages: [256 + s*64, +64)
+constexpr int kKtabStageBytes = 3 * kTableChunk * 8;
+
+struct Bars {
+  uint64_t full_b[kMaxStages];
+  uint64_t full_a[kMaxStages];
+  uint64_t empty[kMaxStages];
+  uint64_t acc_full;
+  uint64_t acc_empty;
+  uint64_t done;
+  uint64_t e12_ready;
+  uint32_t tmem_base;
+  int abort_flag;
+};
+constexpr int kHeaderBytes = 256;
+static_assert(sizeof(Bars) <= kHeaderBytes, "header");
+
+struct TcArgs {
+  Plan P;
+  const double* x;
+  const unsigned char* B;
+  const double* ktab;
+  double* out;
+  uint32_t* err;
+  int64_t row0, rows;
+  int stages;
+};
+
+__device__ __forceinline__ void raise_abort(Bars* bars, uint32_t* err) {
+  *reinterpret_cast<volatile int*>(&bars->abort_flag) = 1;
+  atomicOr(err, kErrTimeout);
+}
+
+// Epilogue value: ampMult (and FP16 unscale), then multiVariateTransformation
+// (randomFieldND.f90:171-176) unless a normalisation pass follows.
+__device__ __forceinline__ double finish_value(const Plan& P, float acc) {
+  double v = (double)acc * P.outScale;
+  if (P.applyMarginal) {
+    v = v * P.margSd + P.margAvg;
+    if (P.lognormal) v = exp(v);
+  }
+  return v;
+}
+
+template <int GEN, int PREC>
+__global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constant__ TcArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const Plan& P = a.P;
+  Bars* bars = reinterpret_cast<Bars*>(smem);
+  unsigned char* sB = smem + kHeaderBytes;
+  double* sK = reinterpret_cast<double*>(sB + (size_t)a.stages * P.stageBytes);
+  float2* e12 = reinterpret_cast<float2*>(sK + (GEN == GEN_TABLE ? a.stages * 3 * kTableChunk : 0));
+  volatile int* abort_flag = &bars->abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = a.stages;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&bars->full_b[s], 1);
+      mbar_init(&bars->full_a[s], kGenWarps);
+      mbar_init(&bars->empty[s], 1);
+    }
+    mbar_init(&bars->acc_full, 1);
+    mbar_init(&bars->acc_empty, kGenWarps);
+    mbar_init(&bars->done, 1);
+    mbar_init(&bars->e12_ready, kGenWarps);
+    bars->abort_flag = 0;
+    mbar_fence_init();
+  }
+  if (warp == kMmaWarp) {
+    tmem_alloc(&bars->tmem_base, kTmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = bars->tmem_base;
+
+  const int64_t numTiles = (a.rows + kTileM - 1) / kTileM;
+  const int64_t nChunks = P.nChunks;
+  const int chunkCols = P.chunkK;  // one TMEM column per k-value
+
+  if (warp == kProdWarp) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      uint32_t s = 0, ph = 0;
+      int64_t issued = 0;
+      const uint32_t bytes = (uint32_t)P.stageBytes + (GEN == GEN_TABLE ? kKtabStageBytes : 0);
+      for (int64_t tile = blockIdx.x; tile < numTiles && !*abort_flag; tile += gridDim.x) {
+        for (int64_t ch = 0; ch < nChunks; ++ch) {
+          if (!mbar_wait(&bars->empty[s], ph ^ 1, abort_flag)) {
+            raise_abort(bars, a.err);
+            break;
+          }
+          mbar_arrive_expect_tx(&bars->full_b[s], bytes);
+          bulk_g2s(sB + (size_t)s * P.stageBytes, a.B + ch * P.stageBytes, (uint32_t)P.stageBytes,
+                   &bars->full_b[s]);
+          if (GEN == GEN_TABLE)
+            bulk_g2s(sK + s * 3 * kTableChunk, a.ktab + ch * 3 * kTableChunk, kKtabStageBytes, &bars->full_b[s]);
+          ++issued;
+          if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+        }
+        if (*abort_flag) break;
+      }
+      if (*abort_flag) {
+        // Drain: wait (bounded, ignoring the abort flag) for the copies still
+        // in flight so that no bulk copy lands after the CTA exits.
+        volatile int never = 0;
+        for (int i = 0; i < S && issued > 0; ++i, --issued) {
+          if (s == 0) { s = S; ph ^= 1; }
+          --s;
+          mbar_wait(&bars->full_b[s], ph, &never);
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == kMmaWarp) {
+    // ---------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = make_idesc(PREC == PREC_FP16 ? 0u : 1u, 128u, (uint32_t)P.nmcPad);
+      const uint32_t lbo = (uint32_t)P.bRows * 16u, sbo = 128u;
+      const uint32_t loOff = (uint32_t)(P.nmcPad / 8) * 128u;
+      uint32_t s = 0, ph = 0, accPh = 0;
+      bool ok = true;
+      for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
+        if (!mbar_wait(&bars->acc_empty, accPh ^ 1, abort_flag)) { ok = false; break; }
+        tc_fence_after();
+        for (int64_t ch = 0; ch < nChunks; ++ch) {
+          if (!mbar_wait(&bars->full_b[s], ph, abort_flag) || !mbar_wait(&bars->full_a[s], ph, abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t bBase = smem_u32(sB + (size_t)s * P.stageBytes);
+          const uint32_t aBase = tbase + kACol + s * kStageCols;
+          for (int j = 0; j < chunkCols / 8; ++j) {
+            const uint64_t bd = make_sdesc(bBase + 2u * j * lbo, lbo, sbo);
+            mma_ts(tbase + kDCol, aBase + 8u * j, bd, idesc, (ch | j) != 0 ? 1u : 0u);
+            if (PREC == PREC_BF16) {
+              const uint64_t bl = make_sdesc(bBase + 2u * j * lbo + loOff, lbo, sbo);
+              mma_ts(tbase + kDCol, aBase + 8u * j, bl, idesc, 1u);
+            }
+          }
+          mma_commit(&bars->empty[s]);
+          if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+        }
+        if (!ok) break;
+        mma_commit(&bars->acc_full);
+        accPh ^= 1;
+      }
+      if (!ok) raise_abort(bars, a.err);
+      // Drain every MMA this thread issued before TMEM is released.
+      mma_commit(&bars->done);
+      volatile int never = 0;
+      mbar_wait(&bars->done, 0, &never);
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------- generators + epilogue
+    const int q = warp & 3, h = warp >> 2;
+    const int row = q * 32 + lane;
+    const uint32_t laneOff = (uint32_t)(q * 32) << 16;
+    uint32_t s = 0, ph = 0, accPh = 0, e12Ph = 0;
+    bool ok = true;
+    for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
+      const int64_t p = a.row0 + tile * kTileM + row;
+      const bool valid = (p < a.row0 + a.rows);
+      double x[3] = {0.0, 0.0, 0.0};
+      if (valid)
+        for (int d = 0; d < P.nDim; ++d) x[d] = a.x[p * P.nDim + d] / P.corrL[d];
+
+      Grid3Thread g3;
+      if (GEN == GEN_GRID3) {
+        grid3_thread_setup(g3, P, h, x);
+        // Axis 1 (half 0) and axis 2 (half 1) phasors of this point into the
+        // shared table; every generator thread reads both after the barrier.
+        if (h == 0) {
+          for (int i = 0; i < P.kNStep[0]; ++i) e12[i * kTileM + row] = axis_phasor(P.kDelta[0], i, x[0]);
+        } else {
+          for (int i = 0; i < P.kNStep[1]; ++i)
+            e12[(P.kNStep[0] + i) * kTileM + row] = axis_phasor(P.kDelta[1], i, x[1]);
+        }
+        // Bounded (mbarrier) rendezvous of the 8 generator warps: a plain
+        // named barrier could not give up if another warp had aborted.
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bars->e12_ready);
+        const bool w = mbar_wait(&bars->e12_ready, e12Ph, abort_flag);
+        e12Ph ^= 1;
+        if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
+      }
+
+      for (int64_t ch = 0; ch < nChunks; ++ch) {
+        bool w = mbar_wait(&bars->empty[s], ph ^ 1, abort_flag);
+        if (GEN == GEN_TABLE) w = w && mbar_wait(&bars->full_b[s], ph, abort_flag);
+        if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
+        uint32_t words[32];
+        const uint32_t aAddr = tbase + laneOff + kACol + s * kStageCols;
+        auto emit = [&](int idx, float c, float sn) {
+          words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
+        };
+        if (GEN == GEN_GRID3) {
+          const int LH = P.lPad / 2;
+          const float2 Pq = grid3_outer(P, e12, row, ch);
+          grid3_pairs(g3, Pq, LH, emit);
+          const uint32_t col = aAddr + (uint32_t)(h * P.lPad);
+          // lPad is a multiple of 8: every store covers 8 columns at an
+          // 8-aligned column offset.
+#pragma unroll
+          for (int pc = 0; pc < 4; ++pc)
+            if (pc * 8 < P.lPad) tmem_st8(col + pc * 8, &words[pc * 8]);
+        } else {
+          table_pairs(sK + s * 3 * kTableChunk, h, x, emit);
+          const uint32_t col = aAddr + (uint32_t)(h * (kTableChunk / 2));
+          tmem_st8(col, &words[0]);
+          tmem_st8(col + 8, &words[8]);
+        }
+        tmem_st_wait();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bars->full_a[s]);
+        if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+      }
+      if (!ok) break;
+
+      // ---------------------------------------------------------- epilogue
+      {
+        const bool w = mbar_wait(&bars->acc_full, accPh, abort_flag);
+        if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
+      }
+      tc_fence_after();
+      const int half = P.nmcPad / 2;
+      for (int cb = h * half; cb < (h + 1) * half; cb += 8) {
+        uint32_t v[8];
+        tmem_ld8(tbase + laneOff + kDCol + cb, v);
+        tmem_ld_wait();
+        if (valid) {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int r = cb + j;
+            if (r < P.Nmc) a.out[(int64_t)r * P.n + p] = finish_value(P, __uint_as_float(v[j]));
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bars->acc_empty);
+      accPh ^= 1;
+    }
+    if (!ok) raise_abort(bars, a.err);
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == kMmaWarp) tmem_dealloc(tbase, kTmemCols);
+}
+
+template <int GEN, int PREC>
+cudaError_t launch_one(const TcArgs& args, size_t smem, int grid, cudaStream_t st) {
+  auto fn = rf_tc_kernel<GEN, PREC>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fn<<<grid, kThreads, smem, st>>>(args);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t tc_smem_bytes(const Plan& P, int* stages) {
+  const size_t e12 = (P.gen == GEN_GRID3) ? (size_t)(P.kNStep[0] + P.kNStep[1]) * kTileM * sizeof(float2) : 0;
+  const size_t perStage = (size_t)P.stageBytes + (P.gen == GEN_TABLE ? kKtabStageBytes : 0);
+  const size_t limit = 227 * 1024;
+  // The kernel allocates all 512 TMEM columns, so two CTAs must never share
+  // an SM: asking for more than half of the SM's shared memory guarantees it.
+  const size_t floor = 120 * 1024;
+  for (int s = kMaxStages; s >= 2; --s) {
+    const size_t total = kHeaderBytes + s * perStage + e12;
+    if (total <= limit) {
+      if (stages) *stages = s;
+      return total < floor ? floor : total;
+    }
+  }
+  return 0;
+}
+
+cudaError_t launch_tc(const Plan& P, const double* dX, const void* dB, const double* dKtab, double* dOut,
+                      int64_t row0, int64_t rows, uint32_t* dErr, int numSMs, cudaStream_t st) {
+  TcArgs args;
+  args.P = P;
+  args.x = dX;
+  args.B = reinterpret_cast<const unsigned char*>(dB);
+  args.ktab = dKtab;
+  args.out = dOut;
+  args.err = dErr;
+  args.row0 = row0;
+  args.rows = rows;
+  int stages = 0;
+  const size_t smem = tc_smem_bytes(P, &stages);
+  if (smem == 0) return cudaErrorInvalidValue;
+  args.stages = stages;
+  const int64_t tiles = (rows + kTileM - 1) / kTileM;
+  const int grid = (int)(tiles < numSMs ? tiles : numSMs);
+  if (P.gen == GEN_GRID3) {
+    if (P.prec == PREC_FP16) return launch_one<GEN_GRID3, PREC_FP16>(args, smem, grid, st);
+    if (P.prec == PREC_BF16_FAST) return launch_one<GEN_GRID3, PREC_BF16_FAST>(args, smem, grid, st);
+    return launch_one<GEN_GRID3, PREC_BF16>(args, smem, grid, st);
+  }
+  if (P.prec == PREC_FP16) return launch_one<GEN_TABLE, PREC_FP16>(args, smem, grid, st);
+  if (P.prec == PREC_BF16_FAST) return launch_one<GEN_TABLE, PREC_BF16_FAST>(args, smem, grid, st);
+  return launch_one<GEN_TABLE, PREC_BF16>(args, smem, grid, st);
+}
+
+}  // namespace rfb
