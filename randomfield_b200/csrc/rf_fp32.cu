@@ -74,6 +74,7 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
     for (int j = 0; j < 4; ++j) acc64[i][j] = 0.0;
 
   const int kel = 2 * P.chunkK;
+  Grid3Outer outer;
   for (int64_t ch = 0; ch < P.nChunks; ++ch) {
     __syncthreads();  // previous stage fully consumed (and e12 written)
     // B stage: rows kel, columns [rBase, rBase + NB)
@@ -89,7 +90,8 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
     // trig tile: element 2c = cos, 2c+1 = sin of stage column c
     if (GEN == GEN_GRID3) {
       const int LH = P.lPad / 2;
-      const float2 Pq = grid3_outer(P, e12, row, ch);
+      const float2 Pq = grid3_outer(P, e12, row, outer);
+      outer.next(P.kNStep[0], P.kNStep[1]);
       const int col0 = h * P.lPad;
       grid3_pairs(g3, Pq, LH, [&](int idx, float c, float sn) {
         As[(2 * (col0 + idx)) * kTileM + row] = c;

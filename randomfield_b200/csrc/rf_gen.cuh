@@ -66,17 +66,27 @@ __device__ __forceinline__ void grid3_thread_setup(Grid3Thread& g, const Plan& P
   }
 }
 
-// Outer phasor P = E1(i1) * E2(i2)^{s2} of stage g from the shared table
+// Outer index (i1, i2, s2) of stage g = i1 + n1*(i2 + n2*s2), advanced by
+// one stage at a time without integer division.
+struct Grid3Outer {
+  int i1 = 0, i2 = 0, s2 = 0;
+  __device__ __forceinline__ void next(int n1, int n2) {
+    if (++i1 == n1) {
+      i1 = 0;
+      if (++i2 == n2) {
+        i2 = 0;
+        ++s2;
+      }
+    }
+  }
+};
+
+// Outer phasor P = E1(i1) * E2(i2)^{s2} from the shared table
 // e12[(i)*128 + row] (i < n1: axis 1; n1 <= i < n1+n2: axis 2).
-__device__ __forceinline__ float2 grid3_outer(const Plan& P, const float2* e12, int row, int64_t stage) {
-  const int n1 = P.kNStep[0], n2 = P.kNStep[1];
-  const int i1 = (int)(stage % n1);
-  const int64_t t = stage / n1;
-  const int i2 = (int)(t % n2);
-  const int s2 = (int)(t / n2);
-  const float2 e1 = e12[i1 * kTileM + row];
-  float2 e2 = e12[(n1 + i2) * kTileM + row];
-  if (s2) e2.y = -e2.y;
+__device__ __forceinline__ float2 grid3_outer(const Plan& P, const float2* e12, int row, const Grid3Outer& o) {
+  const float2 e1 = e12[o.i1 * kTileM + row];
+  float2 e2 = e12[(P.kNStep[0] + o.i2) * kTileM + row];
+  if (o.s2) e2.y = -e2.y;
   return make_float2(e1.x * e2.x - e1.y * e2.y, e1.x * e2.y + e1.y * e2.x);
 }
 

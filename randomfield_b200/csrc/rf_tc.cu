@@ -225,6 +225,7 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
         if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
       }
 
+      Grid3Outer outer;
       for (int64_t ch = 0; ch < nChunks; ++ch) {
         bool w = mbar_wait(&bars->empty[s], ph ^ 1, abort_flag);
         if (GEN == GEN_TABLE) w = w && mbar_wait(&bars->full_b[s], ph, abort_flag);
@@ -236,7 +237,8 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
         };
         if (GEN == GEN_GRID3) {
           const int LH = P.lPad / 2;
-          const float2 Pq = grid3_outer(P, e12, row, ch);
+          const float2 Pq = grid3_outer(P, e12, row, outer);
+          outer.next(P.kNStep[0], P.kNStep[1]);
           grid3_pairs(g3, Pq, LH, emit);
           const uint32_t col = aAddr + (uint32_t)(h * P.lPad);
           // lPad is a multiple of 8: every store covers 8 columns at an

@@ -48,12 +48,17 @@ def oracle(x, rows=None, **kw):
 
 
 def check(prec, got, ref):
+    """FP32: max-abs bound.  Tensor-core forms: the relative-L2 bound over the
+    whole compared field, and per realization 1.25x the bound (a realization
+    of a sum with few wavevectors, e.g. K = 40 in 1-D, carries few rounding
+    errors and its relative error fluctuates more)."""
     if prec == "fp32":
         mx, _ = errors(got, ref)
         assert mx <= FP32_MAXABS * ref.std(), (mx, ref.std())
     else:
+        assert errors(got, ref)[1] <= REL_L2[prec]
         for r, (mx, rl2) in enumerate(per_realization_errors(got, ref)):
-            assert rl2 <= REL_L2[prec], (r, rl2, mx)
+            assert rl2 <= 1.25 * REL_L2[prec], (r, rl2, mx)
 
 
 # ------------------------------------------------------------------ configs
