@@ -51,9 +51,23 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// Non-blocking probe of the phase of the given parity.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
 // Bounded wait for the phase of the given parity.  Returns false once the
-// wall-clock limit passes, or at once when *abort is already set.
+// wall-clock limit passes, or at once when *abort is already set.  A cheap
+// non-blocking probe first: most waits on the hot path find the phase done.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  if (mbar_test_wait(bar, parity)) return true;
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   while (true) {
@@ -61,6 +75,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
     if (*abort) return false;
     if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
   }
+}
+
+// Warp-wide bounded wait: lane 0 alone polls the barrier (256 threads
+// spinning on one mbarrier word would contend its shared-memory bank and slow
+// every barrier operation of the CTA), then the result is broadcast and the
+// warp reconverges.  Call from all 32 lanes.
+// With lanes_acquire set, every lane then probes the (completed) phase once
+// itself, which gives each lane acquire ordering on data the barrier guards
+// (bulk-copied shared memory).
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                               bool lanes_acquire = false) {
+  bool ok = true;
+  if ((threadIdx.x & 31) == 0) ok = mbar_wait(bar, parity, abort);
+  ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+  if (ok && lanes_acquire) ok = mbar_test_wait(bar, parity);
+  return __all_sync(0xffffffffu, ok);
 }
 
 // ------------------------------------------------------------ bulk copy (TMA)

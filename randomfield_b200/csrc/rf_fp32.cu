@@ -54,8 +54,11 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
   const bool valid = p < a.row0 + a.rows;
 
   double x[3] = {0.0, 0.0, 0.0};
-  if (valid)
-    for (int d = 0; d < P.nDim; ++d) x[d] = a.x[p * P.nDim + d] / P.corrL[d];
+  if (valid) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (d < P.nDim) x[d] = a.x[p * P.nDim + d] / P.corrL[d];
+  }
 
   Grid3Thread g3;
   if (GEN == GEN_GRID3) {
@@ -135,11 +138,11 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
 #pragma unroll
   for (int i = 0; i < RPT; ++i) {
     const int r = rBase + rg * RPT + i;
-    if (r >= P.Nmc) continue;
+    if (r >= P.nmcBlk) continue;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int64_t pp = a.row0 + tile * kTileM + 4 * pg + j;
-      if (pp < a.row0 + a.rows) a.out[(int64_t)r * P.n + pp] = finish_value(P, acc64[i][j]);
+      if (pp < a.row0 + a.rows) a.out[(int64_t)(P.rOff + r) * P.n + pp] = finish_value(P, acc64[i][j]);
     }
   }
 }

@@ -194,15 +194,22 @@ int layout(Plan& P) {
     P.chunkK = kTableChunk;
     P.nChunks = (P.K + kTableChunk - 1) / kTableChunk;
   }
+  if (P.nmcBlk <= 0) {
+    // the first realization block: one MMA holds at most 256 accumulator
+    // columns and the hi/lo form uses two per realization
+    const int32_t blk = P.prec == PREC_FP32 ? P.Nmc : (P.prec == PREC_BF16 ? kMaxNmcPad / 2 : kMaxNmcPad);
+    P.nmcBlk = std::min(P.Nmc, blk);
+  }
   if (tc) {
-    P.nmcPad = (int32_t)round_up(P.Nmc, 16);
-    if (P.nmcPad > kMaxNmcPad) return fail(RF_ENOTSUP, "Nmc > %d per launch", kMaxNmcPad);
+    P.nmcPad = (int32_t)round_up(P.nmcBlk, 16);
     P.bRows = P.prec == PREC_BF16 ? 2 * P.nmcPad : P.nmcPad;
+    // one MMA covers all bRows (N <= 256); the accumulator uses bRows columns
+    if (P.bRows > kMaxNmcPad) return fail(RF_ENOTSUP, "realization block too large for one MMA");
     P.stageBytes = (int64_t)2 * P.chunkK * P.bRows * 2;
   } else {
     int rpt = 1;
-    while (rpt < 8 && 8 * rpt < P.Nmc) rpt *= 2;
-    P.nmcPad = (int32_t)round_up(P.Nmc, 8 * rpt);
+    while (rpt < 8 && 8 * rpt < P.nmcBlk) rpt *= 2;
+    P.nmcPad = (int32_t)round_up(P.nmcBlk, 8 * rpt);
     P.bRows = P.nmcPad;
     P.stageBytes = (int64_t)2 * P.chunkK * P.nmcPad * 4;
   }
@@ -380,8 +387,46 @@ int build_plan(const Request& rq, const double* ext, Plan& P) {
   return layout(P);
 }
 
-// Tables + contraction (+ normalisation) for a plan whose points sit in dX.
-int run_plan(rf_context* c, const Plan& P, const double* dX, double* dOut, cudaStream_t st) {
+// Realizations per launch: one MMA holds at most 256 accumulator columns,
+// and the hi/lo form uses two per realization.
+int32_t realization_block(const Plan& P) {
+  if (P.prec == PREC_FP32) return P.Nmc;
+  return P.prec == PREC_BF16 ? kMaxNmcPad / 2 : kMaxNmcPad;
+}
+
+int run_block(rf_context* c, const Plan& P, const double* dX, double* dOut, cudaStream_t st);
+
+// Tables + contraction (+ normalisation) for a plan whose points sit in dX,
+// one launch pair per realization block.
+int run_plan(rf_context* c, const Plan& P0, const double* dX, double* dOut, cudaStream_t st) {
+  const int32_t blk = realization_block(P0);
+  if (c->timing) {
+    for (auto& e : c->ev)
+      if (!e) RF_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+    RF_CUDA(cudaEventRecord(c->ev[0], st), "cudaEventRecord");
+  }
+  for (int32_t r0 = 0; r0 < P0.Nmc; r0 += blk) {
+    Plan P = P0;
+    P.rOff = r0;
+    P.nmcBlk = std::min(blk, P0.Nmc - r0);
+    if (int rc = layout(P)) return rc;
+    if (int rc = run_block(c, P, dX, dOut, st)) return rc;
+  }
+  if (c->timing) RF_CUDA(cudaEventRecord(c->ev[2], st), "cudaEventRecord");
+  if (P0.normalize) {
+    if ((size_t)2 * P0.Nmc * sizeof(double) > c->capWork)
+      if (int rc = ensure(c->dWork, c->capWork, (size_t)2 * P0.Nmc * sizeof(double), "moments")) return rc;
+    RF_CUDA(launch_normalize_and_map(P0, dOut, P0.literal ? 1 : P0.Nmc, c->dWork, st), "normalisation kernels");
+    c->launches += 3;
+  }
+  if (c->timing) {
+    RF_CUDA(cudaEventRecord(c->ev[3], st), "cudaEventRecord");
+    c->evValid = true;
+  }
+  return RF_OK;
+}
+
+int run_block(rf_context* c, const Plan& P, const double* dX, double* dOut, cudaStream_t st) {
   const size_t bBytes = (size_t)P.nChunks * P.stageBytes;
   if (int rc = ensure(c->dB, c->capB, bBytes, "contraction operand")) return rc;
   double* ktab = nullptr;
@@ -400,33 +445,17 @@ int run_plan(rf_context* c, const Plan& P, const double* dX, double* dOut, cudaS
     if (xSlab < 1) xSlab = 1;
     nSlab = (P.n + xSlab - 1) / xSlab;
   }
-  if (c->timing) {
-    for (auto& e : c->ev)
-      if (!e) RF_CUDA(cudaEventCreate(&e), "cudaEventCreate");
-    RF_CUDA(cudaEventRecord(c->ev[0], st), "cudaEventRecord");
-  }
   for (int64_t m = 0; m < nSlab; ++m) {
     const int64_t row0 = m * xSlab;
     const int64_t rows = std::min(xSlab, P.n - row0);
     RF_CUDA(launch_tables(P, jump_table(), c->dB, ktab, P.literal ? m : -1, nSlab, st), "table kernel");
-    if (c->timing && m == 0) RF_CUDA(cudaEventRecord(c->ev[1], st), "cudaEventRecord");
+    if (c->timing && m == 0 && P.rOff == 0) RF_CUDA(cudaEventRecord(c->ev[1], st), "cudaEventRecord");
     if (P.prec == PREC_FP32) {
       RF_CUDA(launch_fp32(P, dX, c->dB, ktab, dOut, row0, rows, st), "FP32 contraction kernel");
     } else {
       RF_CUDA(launch_tc(P, dX, c->dB, ktab, dOut, row0, rows, c->dErr, c->numSMs, st), "tcgen05 contraction kernel");
     }
     c->launches += 2;
-  }
-  if (c->timing) RF_CUDA(cudaEventRecord(c->ev[2], st), "cudaEventRecord");
-  if (P.normalize) {
-    if ((size_t)2 * P.Nmc * sizeof(double) > c->capWork)
-      if (int rc = ensure(c->dWork, c->capWork, (size_t)2 * P.Nmc * sizeof(double), "moments")) return rc;
-    RF_CUDA(launch_normalize_and_map(P, dOut, P.literal ? 1 : P.Nmc, c->dWork, st), "normalisation kernels");
-    c->launches += 3;
-  }
-  if (c->timing) {
-    RF_CUDA(cudaEventRecord(c->ev[3], st), "cudaEventRecord");
-    c->evValid = true;
   }
   return RF_OK;
 }

@@ -41,9 +41,11 @@ struct Plan {
   double kDelta[3];           // Shinozuka per axis; isotropic [0]=dr
   double kMax, ampMult;
   int32_t ig1, ig2;           // rnglib generator-1 seed words
+  // realization block of this launch: columns [rOff, rOff + nmcBlk) of Nmc
+  int32_t rOff, nmcBlk;
   // kernel layout
   int32_t gen;                // Generator
-  int32_t nmcPad;             // realizations padded (16 for tcgen05, 8 for FP32)
+  int32_t nmcPad;             // nmcBlk padded (16 for tcgen05, 8 * 2^j for FP32)
   int32_t bRows;              // rows of B per stage (nmcPad, or 2*nmcPad with hi/lo)
   int32_t chunkK;             // k-values per stage
   int32_t lPad;               // GEN_GRID3: inner (axis 3) length padded to a multiple of 8

@@ -127,22 +127,23 @@ __global__ void rf_tables_kernel(const Plan P, const JumpTable jt, void* __restr
   }
 
   double bc = 0.0, bs = 0.0;
-  if (v.ref >= 0 && r < P.Nmc) {
+  if (v.ref >= 0 && r < P.nmcBlk) {
+    const int64_t rg = (int64_t)P.rOff + r;  // realization index in the request
     double phi, gam = 1.0, amp = v.amp;
     const int64_t s1 = P.ig1, s2 = P.ig2;
     if (P.method == 2) {
-      phi = 2.0 * kRefPi * r8_uni_at(jt, s1, s2, (uint64_t)((int64_t)r * P.K + v.ref + 1));
+      phi = 2.0 * kRefPi * r8_uni_at(jt, s1, s2, (uint64_t)(rg * P.K + v.ref + 1));
       if (P.literal && literalSlab >= 0) {
         // B1: slab m of realization n uses S^(1/2^t), t = (n-1)*nSlab + m
         // (randomFieldND.f90:312 inside the loops :276 and :284).
         const double S = (P.corrMod == 1) ? gauss_spectrum(v.k, P.nDim) : ((v.ref == 5) ? 1.0 : 0.0);
-        int64_t t = (int64_t)r * nSlab + literalSlab + 1;
+        int64_t t = rg * nSlab + literalSlab + 1;
         if (t > 200) t = 200;  // the iterate is exactly 1.0 (or 0.0) long before
         amp = S;
         for (int64_t i = 0; i < t; ++i) amp = sqrt(amp);
       }
     } else {
-      const int64_t base = (P.nDim == 3 ? 2 : 1) * P.K + (int64_t)r * 2 * P.K;
+      const int64_t base = (P.nDim == 3 ? 2 : 1) * P.K + rg * 2 * P.K;
       const double ug = r8_uni_at(jt, s1, s2, (uint64_t)(base + v.ref + 1));
       const double up = r8_uni_at(jt, s1, s2, (uint64_t)(base + P.K + v.ref + 1));
       gam = (double)sqrtf(12.0f) * (ug - 0.5);  // randomFieldND.f90:468 (single-precision sqrt(12.0))

@@ -32,7 +32,7 @@ constexpr int kProdWarp = 9;
 constexpr int kThreads = 320;
 constexpr int kMaxStages = 4;
 constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kDCol = 0;      // accumulator columns [0, nmcPad)
+constexpr uint32_t kDCol = 0;      // accumulator columns [0, bRows)
 constexpr uint32_t kACol = 256;    // A stages: [256 + s*64, +64)
 constexpr int kKtabStageBytes = 3 * kTableChunk * 8;
 
@@ -153,9 +153,17 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------- MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = make_idesc(PREC == PREC_FP16 ? 0u : 1u, 128u, (uint32_t)P.nmcPad);
+      // The hi/lo amplitude rows sit one above the other in each B stage, so
+      // one MMA with N = bRows computes both products into 2*nmcPad
+      // accumulator columns; the epilogue adds the halves.  Descriptors are
+      // advanced by plain adds of the start address field (it cannot
+      // overflow: shared memory is below 256 KB).
+      const uint32_t idesc = make_idesc(PREC == PREC_FP16 ? 0u : 1u, 128u, (uint32_t)P.bRows);
       const uint32_t lbo = (uint32_t)P.bRows * 16u, sbo = 128u;
-      const uint32_t loOff = (uint32_t)(P.nmcPad / 8) * 128u;
+      const uint64_t desc0 = make_sdesc(smem_u32(sB), lbo, sbo);
+      const uint64_t sStep = (uint64_t)(P.stageBytes >> 4);
+      const uint64_t jStep = (uint64_t)((2u * lbo) >> 4);
+      const int steps = chunkCols / 8;
       uint32_t s = 0, ph = 0, accPh = 0;
       bool ok = true;
       for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
@@ -167,15 +175,11 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
             break;
           }
           tc_fence_after();
-          const uint32_t bBase = smem_u32(sB + (size_t)s * P.stageBytes);
           const uint32_t aBase = tbase + kACol + s * kStageCols;
-          for (int j = 0; j < chunkCols / 8; ++j) {
-            const uint64_t bd = make_sdesc(bBase + 2u * j * lbo, lbo, sbo);
-            mma_ts(tbase + kDCol, aBase + 8u * j, bd, idesc, (ch | j) != 0 ? 1u : 0u);
-            if (PREC == PREC_BF16) {
-              const uint64_t bl = make_sdesc(bBase + 2u * j * lbo + loOff, lbo, sbo);
-              mma_ts(tbase + kDCol, aBase + 8u * j, bl, idesc, 1u);
-            }
+          const uint64_t d0 = desc0 + sStep * s;
+#pragma unroll
+          for (int j = 0; j < kStageCols / 8; ++j) {
+            if (j < steps) mma_ts(tbase + kDCol, aBase + 8u * j, d0 + jStep * j, idesc, (ch | j) != 0 ? 1u : 0u);
           }
           mma_commit(&bars->empty[s]);
           if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
@@ -202,8 +206,11 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
       const int64_t p = a.row0 + tile * kTileM + row;
       const bool valid = (p < a.row0 + a.rows);
       double x[3] = {0.0, 0.0, 0.0};
-      if (valid)
-        for (int d = 0; d < P.nDim; ++d) x[d] = a.x[p * P.nDim + d] / P.corrL[d];
+      if (valid) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          if (d < P.nDim) x[d] = a.x[p * P.nDim + d] / P.corrL[d];
+      }
 
       Grid3Thread g3;
       if (GEN == GEN_GRID3) {
@@ -220,16 +227,17 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
         // named barrier could not give up if another warp had aborted.
         __syncwarp();
         if (lane == 0) mbar_arrive(&bars->e12_ready);
-        const bool w = mbar_wait(&bars->e12_ready, e12Ph, abort_flag);
+        const bool w = mbar_wait_warp(&bars->e12_ready, e12Ph, abort_flag);
         e12Ph ^= 1;
-        if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
+        if (!w) { ok = false; break; }
       }
 
       Grid3Outer outer;
       for (int64_t ch = 0; ch < nChunks; ++ch) {
-        bool w = mbar_wait(&bars->empty[s], ph ^ 1, abort_flag);
-        if (GEN == GEN_TABLE) w = w && mbar_wait(&bars->full_b[s], ph, abort_flag);
-        if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
+        bool w = mbar_wait_warp(&bars->empty[s], ph ^ 1, abort_flag);
+        if (GEN == GEN_TABLE) w = w && mbar_wait_warp(&bars->full_b[s], ph, abort_flag, true);
+        if (!w) { ok = false; break; }
+        tc_fence_after();
         uint32_t words[32];
         const uint32_t aAddr = tbase + laneOff + kACol + s * kStageCols;
         auto emit = [&](int idx, float c, float sn) {
@@ -261,21 +269,21 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
       if (!ok) break;
 
       // ---------------------------------------------------------- epilogue
-      {
-        const bool w = mbar_wait(&bars->acc_full, accPh, abort_flag);
-        if (!__all_sync(0xffffffffu, w)) { ok = false; break; }
-      }
+      if (!mbar_wait_warp(&bars->acc_full, accPh, abort_flag)) { ok = false; break; }
       tc_fence_after();
       const int half = P.nmcPad / 2;
       for (int cb = h * half; cb < (h + 1) * half; cb += 8) {
-        uint32_t v[8];
+        uint32_t v[8], lo[8];
         tmem_ld8(tbase + laneOff + kDCol + cb, v);
+        if (PREC == PREC_BF16) tmem_ld8(tbase + laneOff + kDCol + P.nmcPad + cb, lo);
         tmem_ld_wait();
         if (valid) {
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             const int r = cb + j;
-            if (r < P.Nmc) a.out[(int64_t)r * P.n + p] = finish_value(P, __uint_as_float(v[j]));
+            float acc = __uint_as_float(v[j]);
+            if (PREC == PREC_BF16) acc += __uint_as_float(lo[j]);
+            if (r < P.nmcBlk) a.out[(int64_t)(P.rOff + r) * P.n + p] = finish_value(P, acc);
           }
         }
       }
