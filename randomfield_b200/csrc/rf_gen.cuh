@@ -15,17 +15,17 @@
 
 namespace rfb {
 
-// Kernel order of GEN_GRID3: stage g holds outer index (i1, i2, s2) with
-// g = i1 + n1*(i2 + n2*s2); inside a stage, column c in [0, 2*lPad):
-// half h = c / lPad, cc = c % lPad, i3 = h*(lPad/2) + cc/2, s3 = cc & 1.
-// Returns the reference index k = q*n1*n2*n3 + i1 + n1*(i2 + n2*i3) with the
-// quadrant q = 2*s2 + s3 of set_kSign (spectra_RF.f90:267-286), or -1 for a
-// padding column (i3 >= n3).
-__host__ __device__ inline int64_t grid3_ref_index(const int32_t* kn, int32_t lPad, int64_t stage, int32_t c,
+// Kernel order of GEN_GRID3: a stage holds gps consecutive outer groups
+// (i1, i2, s2), group g = i1 + n1*(i2 + n2*s2); inside a group, column
+// c in [0, 2*lPad): half h = c / lPad, cc = c % lPad, i3 = h*(lPad/2) + cc/2,
+// s3 = cc & 1.  Returns the reference index k = q*n1*n2*n3 +
+// i1 + n1*(i2 + n2*i3) with the quadrant q = 2*s2 + s3 of set_kSign
+// (spectra_RF.f90:267-286), or -1 for a padding column (i3 >= n3).
+__host__ __device__ inline int64_t grid3_ref_index(const int32_t* kn, int32_t lPad, int64_t group, int32_t c,
                                                    int32_t* i_out, int32_t* s_out) {
   const int64_t n1 = kn[0], n2 = kn[1], n3 = kn[2];
-  const int32_t i1 = (int32_t)(stage % n1);
-  const int64_t t = stage / n1;
+  const int32_t i1 = (int32_t)(group % n1);
+  const int64_t t = group / n1;
   const int32_t i2 = (int32_t)(t % n2);
   const int32_t s2 = (int32_t)(t / n2);
   const int32_t h = c / lPad, cc = c % lPad;
@@ -47,27 +47,31 @@ __device__ __forceinline__ float2 axis_phasor(double kDelta, int32_t i, double x
   return make_float2(c, s);
 }
 
-// Per-thread GEN_GRID3 state: this thread's half of the axis-3 phasors.
+// Per-thread GEN_GRID3 state: this thread's half of the axis-3 phasors as
+// pairs of entries, c2[u] = (cos_2u, cos_2u+1), d2[u] = (sin_2u, sin_2u+1),
+// the layout the packed FP32x2 arithmetic of grid3_pairs consumes.
 struct Grid3Thread {
-  float2 e3[kMaxGridN / 2];
+  float2 c2[kMaxGridN / 4];
+  float2 d2[kMaxGridN / 4];
 };
 
-// Fill e3 for i3 = h*LH + t, t < LH.
+// Fill the entries i3 = h*LH + t, t < LH (LH = lPad/2, a multiple of 4).
 __device__ __forceinline__ void grid3_thread_setup(Grid3Thread& g, const Plan& P, int h, const double* x) {
   const int LH = P.lPad / 2;
 #pragma unroll
-  for (int t = 0; t < kMaxGridN / 2; ++t) {
-    if (t < LH) {
-      const int i3 = h * LH + t;
-      g.e3[t] = axis_phasor(P.kDelta[2], i3, x[2]);
-    } else {
-      g.e3[t] = make_float2(0.f, 0.f);
+  for (int u = 0; u < kMaxGridN / 4; ++u) {
+    float2 e0 = make_float2(0.f, 0.f), e1 = make_float2(0.f, 0.f);
+    if (2 * u < LH) {
+      e0 = axis_phasor(P.kDelta[2], h * LH + 2 * u, x[2]);
+      e1 = axis_phasor(P.kDelta[2], h * LH + 2 * u + 1, x[2]);
     }
+    g.c2[u] = make_float2(e0.x, e1.x);
+    g.d2[u] = make_float2(e0.y, e1.y);
   }
 }
 
-// Outer index (i1, i2, s2) of stage g = i1 + n1*(i2 + n2*s2), advanced by
-// one stage at a time without integer division.
+// Outer index (i1, i2, s2) of group g = i1 + n1*(i2 + n2*s2), advanced by
+// one group at a time without integer division.
 struct Grid3Outer {
   int i1 = 0, i2 = 0, s2 = 0;
   __device__ __forceinline__ void next(int n1, int n2) {
@@ -91,17 +95,28 @@ __device__ __forceinline__ float2 grid3_outer(const Plan& P, const float2* e12, 
 }
 
 // The 2*LH (cos, sin) pairs of one half-stage: for t < LH, pair 2t is
-// P*E3(t) (s3 = +) and pair 2t+1 is P*conj(E3(t)) (s3 = -).
+// P*E3(t) (s3 = +) and pair 2t+1 is P*conj(E3(t)) (s3 = -).  With P = a+ib
+// and E3 = c+id, both signs share a*c and b*c:
+//   P E3 = (ac - bd) + i(bc + ad),  P conj(E3) = (ac + bd) + i(bc - ad);
+// two E3 entries go through one packed FP32x2 instruction (sm_100), so four
+// pairs cost two multiplies and four fused multiply-adds.
 template <typename Emit>
 __device__ __forceinline__ void grid3_pairs(const Grid3Thread& g, float2 Pq, int LH, Emit&& emit) {
-  const float a = Pq.x, b = Pq.y;
+  const float2 a2 = make_float2(Pq.x, Pq.x), b2 = make_float2(Pq.y, Pq.y);
+  const float2 na2 = make_float2(-Pq.x, -Pq.x), nb2 = make_float2(-Pq.y, -Pq.y);
 #pragma unroll
-  for (int t = 0; t < kMaxGridN / 2; ++t) {
-    if (t < LH) {
-      const float c = g.e3[t].x, d = g.e3[t].y;
-      const float bd = b * d, ad = a * d;
-      emit(2 * t, fmaf(a, c, -bd), fmaf(b, c, ad));
-      emit(2 * t + 1, fmaf(a, c, bd), fmaf(b, c, -ad));
+  for (int u = 0; u < kMaxGridN / 4; ++u) {
+    if (2 * u < LH) {
+      const float2 ac = __fmul2_rn(a2, g.c2[u]);
+      const float2 bc = __fmul2_rn(b2, g.c2[u]);
+      const float2 rp = __ffma2_rn(nb2, g.d2[u], ac);
+      const float2 rm = __ffma2_rn(b2, g.d2[u], ac);
+      const float2 ip = __ffma2_rn(a2, g.d2[u], bc);
+      const float2 im = __ffma2_rn(na2, g.d2[u], bc);
+      emit(4 * u + 0, rp.x, ip.x);
+      emit(4 * u + 1, rm.x, im.x);
+      emit(4 * u + 2, rp.y, ip.y);
+      emit(4 * u + 3, rm.y, im.y);
     }
   }
 }

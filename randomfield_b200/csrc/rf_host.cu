@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -187,10 +188,17 @@ int layout(Plan& P) {
     P.gen = GEN_GRID3;
   if (P.gen == GEN_GRID3) {
     P.lPad = (int32_t)round_up(P.kNStep[2], 8);  // 8-aligned TMEM stores per half
-    P.chunkK = 2 * P.lPad;
-    P.nChunks = (int64_t)P.kNStep[0] * P.kNStep[1] * 2;
+    // Two outer groups per stage on the tensor-core path (up to 128 TMEM
+    // columns): more MMAs per barrier wait of the issuing thread.  The number
+    // of groups, n1*n2*2, is always even.
+    P.gps = (tc && 4 * P.lPad <= kMaxStageCols) ? 2 : 1;
+    P.teams = 1;  // a second generator team measured slower (it competes with the MMA issuer)
+    P.chunkK = 2 * P.lPad * P.gps;
+    P.nChunks = (int64_t)P.kNStep[0] * P.kNStep[1] * 2 / P.gps;
   } else {
     P.lPad = 0;
+    P.gps = 1;
+    P.teams = 1;
     P.chunkK = kTableChunk;
     P.nChunks = (P.K + kTableChunk - 1) / kTableChunk;
   }

@@ -24,7 +24,8 @@ enum Generator : int32_t {
 enum Precision : int32_t { PREC_BF16 = 0, PREC_FP16 = 1, PREC_FP32 = 2, PREC_BF16_FAST = 3 };
 
 constexpr int kTileM = 128;        // points per tile (MMA M)
-constexpr int kStageCols = 64;     // TMEM columns per A stage (k-values per stage, max)
+constexpr int kStageCols = 64;     // max k-values (TMEM columns) per GEN_GRID3 group or FP32 stage
+constexpr int kMaxStageCols = 128; // max k-values per tcgen05 stage (two groups)
 constexpr int kTableChunk = 32;    // k-values per stage for GEN_TABLE
 constexpr int kMaxGridN = 32;      // GEN_GRID3: max wavenumbers per axis
 constexpr int kMaxNmcPad = 256;    // realizations per launch (MMA N <= 256)
@@ -49,6 +50,8 @@ struct Plan {
   int32_t bRows;              // rows of B per stage (nmcPad, or 2*nmcPad with hi/lo)
   int32_t chunkK;             // k-values per stage
   int32_t lPad;               // GEN_GRID3: inner (axis 3) length padded to a multiple of 8
+  int32_t gps;                // GEN_GRID3: outer groups (i1, i2, s2) per stage
+  int32_t teams;              // tcgen05 path: generator teams of 8 warps (1 or 2)
   int64_t nChunks;            // stages per tile
   int64_t stageBytes;         // bytes of one B stage
   int32_t bScaleLog2;         // FP16: B stored times 2^bScaleLog2

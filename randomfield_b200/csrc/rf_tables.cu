@@ -44,7 +44,8 @@ __device__ KVal kvalue(const Plan& P, const JumpTable& jt, int64_t kk) {
   const int32_t c = (int32_t)(kk % P.chunkK);
   if (P.gen == GEN_GRID3) {
     int32_t idx[3], sg[3];
-    v.ref = grid3_ref_index(P.kNStep, P.lPad, stage, c, idx, sg);
+    const int32_t gw = 2 * P.lPad;  // columns per group
+    v.ref = grid3_ref_index(P.kNStep, P.lPad, stage * P.gps + c / gw, c % gw, idx, sg);
     if (v.ref < 0) return v;
     for (int d = 0; d < 3; ++d) {
       const double base = 0.0 + P.kDelta[d] * (double)idx[d];

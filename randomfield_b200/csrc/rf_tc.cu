@@ -7,15 +7,23 @@
 //   D (128 points x Nmc, FP32 in TMEM) += A (128 x 16, trig tile in TMEM)
 //                                         x B (16 x Nmc, amplitude/phase in SMEM)
 //
-// Warp roles (320 threads, one CTA per SM):
-//   warps 0-7  generators: build the trig tile of a stage straight into TMEM
-//              (tcgen05.st), lane = point, two warpgroups split the columns;
-//              after the last stage of a tile they run the fused epilogue
-//              (tcgen05.ld, ampMult, marginal map, FP64 stores);
-//   warp 8     MMA issuer (one thread): tcgen05.mma kind::f16, A from TMEM,
-//              B by descriptor from SMEM; tcgen05.commit frees stages;
-//   warp 9     producer (one thread): 1-D bulk copies (TMA) of B stages from
-//              HBM/L2 into SMEM; no multicast.
+// Warp roles (one CTA per SM), with T generator teams of 8 warps:
+//   warps 0..8T-1  generators: team t builds the trig tiles of stages
+//                  g = t (mod T) straight into TMEM (tcgen05.st), lane =
+//                  point, two warps per lane quarter split the columns.  Team
+//                  0 runs the fused epilogue after the last stage of a tile
+//                  (tcgen05.ld, ampMult, marginal map, FP64 stores);
+//   warp 8T        MMA issuer (one thread): tcgen05.mma kind::f16, A from
+//                  TMEM, B by descriptor from SMEM; tcgen05.commit frees
+//                  stages;
+//   warp 8T+1      producer (one thread): 1-D bulk copies (TMA) of B stages
+//                  from HBM/L2 into SMEM; no multicast.
+// The issuing thread can run only about one MMA ahead of the tensor core, so
+// anything it waits for between MMAs idles the tensor pipe: it waits on one
+// barrier per stage (the bulk copy completes on the same barrier the
+// generators arrive on), probes the next stage's barrier while the last MMA
+// of the current stage runs, and a stage holds up to 16 MMAs.
+// TMEM: accumulator columns [0, bRows), then A stages of chunkK columns.
 // Every wait is bounded (globaltimer); on expiry the kernel raises an error
 // word, drains its own async work, frees TMEM and returns.
 #include "rf_device.cuh"
@@ -26,28 +34,24 @@ namespace rfb {
 
 namespace {
 
-constexpr int kGenWarps = 8;
-constexpr int kMmaWarp = 8;
-constexpr int kProdWarp = 9;
-constexpr int kThreads = 320;
-constexpr int kMaxStages = 4;
+constexpr int kTeamWarps = 8;
+constexpr int kMaxStages = 8;
 constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kDCol = 0;      // accumulator columns [0, bRows)
-constexpr uint32_t kACol = 256;    // A stages: [256 + s*64, +64)
 constexpr int kKtabStageBytes = 3 * kTableChunk * 8;
 
 struct Bars {
-  uint64_t full_b[kMaxStages];
-  uint64_t full_a[kMaxStages];
+  uint64_t full[kMaxStages];   // generators (8 warps) + producer (bytes)
+  uint64_t kfull[kMaxStages];  // GEN_TABLE wavevector chunk (bytes)
   uint64_t empty[kMaxStages];
   uint64_t acc_full;
   uint64_t acc_empty;
   uint64_t done;
+  uint64_t e12_free;
   uint64_t e12_ready;
   uint32_t tmem_base;
   int abort_flag;
 };
-constexpr int kHeaderBytes = 256;
+constexpr int kHeaderBytes = 512;
 static_assert(sizeof(Bars) <= kHeaderBytes, "header");
 
 struct TcArgs {
@@ -77,8 +81,12 @@ __device__ __forceinline__ double finish_value(const Plan& P, float acc) {
   return v;
 }
 
-template <int GEN, int PREC>
-__global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constant__ TcArgs a) {
+template <int GEN, int PREC, int TEAMS>
+__global__ void __launch_bounds__((TEAMS * kTeamWarps + 2) * 32, 1)
+    rf_tc_kernel(const __grid_constant__ TcArgs a) {
+  constexpr int kGenWarps = TEAMS * kTeamWarps;
+  constexpr int kMmaWarp = kGenWarps;
+  constexpr int kProdWarp = kGenWarps + 1;
   extern __shared__ __align__(1024) unsigned char smem[];
   const Plan& P = a.P;
   Bars* bars = reinterpret_cast<Bars*>(smem);
@@ -89,17 +97,20 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = a.stages;
+  const uint32_t aCol0 = (uint32_t)P.bRows;     // first A column (accumulator below)
+  const uint32_t aStride = (uint32_t)P.chunkK;  // TMEM columns per A stage
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
-      mbar_init(&bars->full_b[s], 1);
-      mbar_init(&bars->full_a[s], kGenWarps);
+      mbar_init(&bars->full[s], kTeamWarps + 1);
+      mbar_init(&bars->kfull[s], 1);
       mbar_init(&bars->empty[s], 1);
     }
     mbar_init(&bars->acc_full, 1);
-    mbar_init(&bars->acc_empty, kGenWarps);
+    mbar_init(&bars->acc_empty, kTeamWarps);
     mbar_init(&bars->done, 1);
-    mbar_init(&bars->e12_ready, kGenWarps);
+    mbar_init(&bars->e12_free, kGenWarps);
+    mbar_init(&bars->e12_ready, kTeamWarps);
     bars->abort_flag = 0;
     mbar_fence_init();
   }
@@ -114,25 +125,24 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
 
   const int64_t numTiles = (a.rows + kTileM - 1) / kTileM;
   const int64_t nChunks = P.nChunks;
-  const int chunkCols = P.chunkK;  // one TMEM column per k-value
 
   if (warp == kProdWarp) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
       uint32_t s = 0, ph = 0;
       int64_t issued = 0;
-      const uint32_t bytes = (uint32_t)P.stageBytes + (GEN == GEN_TABLE ? kKtabStageBytes : 0);
       for (int64_t tile = blockIdx.x; tile < numTiles && !*abort_flag; tile += gridDim.x) {
         for (int64_t ch = 0; ch < nChunks; ++ch) {
           if (!mbar_wait(&bars->empty[s], ph ^ 1, abort_flag)) {
             raise_abort(bars, a.err);
             break;
           }
-          mbar_arrive_expect_tx(&bars->full_b[s], bytes);
-          bulk_g2s(sB + (size_t)s * P.stageBytes, a.B + ch * P.stageBytes, (uint32_t)P.stageBytes,
-                   &bars->full_b[s]);
-          if (GEN == GEN_TABLE)
-            bulk_g2s(sK + s * 3 * kTableChunk, a.ktab + ch * 3 * kTableChunk, kKtabStageBytes, &bars->full_b[s]);
+          mbar_arrive_expect_tx(&bars->full[s], (uint32_t)P.stageBytes);
+          bulk_g2s(sB + (size_t)s * P.stageBytes, a.B + ch * P.stageBytes, (uint32_t)P.stageBytes, &bars->full[s]);
+          if (GEN == GEN_TABLE) {
+            mbar_arrive_expect_tx(&bars->kfull[s], (uint32_t)kKtabStageBytes);
+            bulk_g2s(sK + s * 3 * kTableChunk, a.ktab + ch * 3 * kTableChunk, kKtabStageBytes, &bars->kfull[s]);
+          }
           ++issued;
           if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
         }
@@ -140,12 +150,20 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
       }
       if (*abort_flag) {
         // Drain: wait (bounded, ignoring the abort flag) for the copies still
-        // in flight so that no bulk copy lands after the CTA exits.
+        // in flight so that no bulk copy lands after the CTA exits.  A stage's
+        // copies are done once its kfull phase (table) has completed, and its
+        // B bytes once the full phase could complete: wait on both with the
+        // phase of the last use of each slot.
         volatile int never = 0;
         for (int i = 0; i < S && issued > 0; ++i, --issued) {
           if (s == 0) { s = S; ph ^= 1; }
           --s;
-          mbar_wait(&bars->full_b[s], ph, &never);
+          if (GEN == GEN_TABLE) mbar_wait(&bars->kfull[s], ph, &never);
+        }
+        // the B copies complete_tx on full[s]; the generators' arrivals may
+        // never come, so wait for the transfer by time instead
+        const uint64_t t0 = globaltimer_ns();
+        while (globaltimer_ns() - t0 < 1000000ull) {
         }
       }
     }
@@ -163,26 +181,31 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
       const uint64_t desc0 = make_sdesc(smem_u32(sB), lbo, sbo);
       const uint64_t sStep = (uint64_t)(P.stageBytes >> 4);
       const uint64_t jStep = (uint64_t)((2u * lbo) >> 4);
-      const int steps = chunkCols / 8;
+      const int steps = P.chunkK / 8;
       uint32_t s = 0, ph = 0, accPh = 0;
-      bool ok = true;
+      bool ok = true, ready = false;  // ready: full[s] of the next stage already observed
       for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
         if (!mbar_wait(&bars->acc_empty, accPh ^ 1, abort_flag)) { ok = false; break; }
         tc_fence_after();
         for (int64_t ch = 0; ch < nChunks; ++ch) {
-          if (!mbar_wait(&bars->full_b[s], ph, abort_flag) || !mbar_wait(&bars->full_a[s], ph, abort_flag)) {
-            ok = false;
-            break;
-          }
+          if (!ready && !mbar_wait(&bars->full[s], ph, abort_flag)) { ok = false; break; }
           tc_fence_after();
-          const uint32_t aBase = tbase + kACol + s * kStageCols;
+          const uint32_t aBase = tbase + aCol0 + s * aStride;
           const uint64_t d0 = desc0 + sStep * s;
+          const uint32_t sn = (s + 1 == (uint32_t)S) ? 0u : s + 1;
+          const uint32_t phn = (s + 1 == (uint32_t)S) ? ph ^ 1 : ph;
+          const bool more = (ch + 1 < nChunks) || (tile + gridDim.x < numTiles);
 #pragma unroll
-          for (int j = 0; j < kStageCols / 8; ++j) {
-            if (j < steps) mma_ts(tbase + kDCol, aBase + 8u * j, d0 + jStep * j, idesc, (ch | j) != 0 ? 1u : 0u);
+          for (int j = 0; j < kMaxStageCols / 8; ++j) {
+            if (j < steps) {
+              // probe the next stage while this stage's last MMA is queued
+              if (j == steps - 1) ready = more && mbar_test_wait(&bars->full[sn], phn);
+              mma_ts(tbase, aBase + 8u * j, d0 + jStep * j, idesc, (ch | j) != 0 ? 1u : 0u);
+            }
           }
           mma_commit(&bars->empty[s]);
-          if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+          s = sn;
+          ph = phn;
         }
         if (!ok) break;
         mma_commit(&bars->acc_full);
@@ -197,10 +220,12 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
     __syncwarp();
   } else {
     // ------------------------------------------------- generators + epilogue
-    const int q = warp & 3, h = warp >> 2;
+    const int team = warp / kTeamWarps, wi = warp % kTeamWarps;
+    const int q = wi & 3, h = wi >> 2;
     const int row = q * 32 + lane;
     const uint32_t laneOff = (uint32_t)(q * 32) << 16;
-    uint32_t s = 0, ph = 0, accPh = 0, e12Ph = 0;
+    uint32_t s = 0, ph = 0, accPh = 0, ePh = 0;
+    int64_t g = 0;  // stage counter of this CTA; team t takes g = t (mod TEAMS)
     bool ok = true;
     for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
       const int64_t p = a.row0 + tile * kTileM + row;
@@ -215,47 +240,65 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
       Grid3Thread g3;
       if (GEN == GEN_GRID3) {
         grid3_thread_setup(g3, P, h, x);
-        // Axis 1 (half 0) and axis 2 (half 1) phasors of this point into the
-        // shared table; every generator thread reads both after the barrier.
-        if (h == 0) {
-          for (int i = 0; i < P.kNStep[0]; ++i) e12[i * kTileM + row] = axis_phasor(P.kDelta[0], i, x[0]);
-        } else {
-          for (int i = 0; i < P.kNStep[1]; ++i)
-            e12[(P.kNStep[0] + i) * kTileM + row] = axis_phasor(P.kDelta[1], i, x[1]);
-        }
-        // Bounded (mbarrier) rendezvous of the 8 generator warps: a plain
-        // named barrier could not give up if another warp had aborted.
+        // The shared axis-1/axis-2 phasor table is rewritten per tile: every
+        // generator warp first declares it is done with the previous tile's
+        // table, team 0 writes (half 0: axis 1, half 1: axis 2), then all
+        // read.  Bounded mbarrier rendezvous, not named barriers, so that an
+        // aborting warp cannot leave the others blocked.
         __syncwarp();
-        if (lane == 0) mbar_arrive(&bars->e12_ready);
-        const bool w = mbar_wait_warp(&bars->e12_ready, e12Ph, abort_flag);
-        e12Ph ^= 1;
-        if (!w) { ok = false; break; }
+        if (lane == 0) mbar_arrive(&bars->e12_free);
+        if (team == 0) {
+          if (!mbar_wait_warp(&bars->e12_free, ePh, abort_flag)) { ok = false; break; }
+          if (h == 0) {
+            for (int i = 0; i < P.kNStep[0]; ++i) e12[i * kTileM + row] = axis_phasor(P.kDelta[0], i, x[0]);
+          } else {
+            for (int i = 0; i < P.kNStep[1]; ++i)
+              e12[(P.kNStep[0] + i) * kTileM + row] = axis_phasor(P.kDelta[1], i, x[1]);
+          }
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&bars->e12_ready);
+        }
+        if (!mbar_wait_warp(&bars->e12_ready, ePh, abort_flag)) { ok = false; break; }
+        ePh ^= 1;
       }
 
       Grid3Outer outer;
-      for (int64_t ch = 0; ch < nChunks; ++ch) {
-        bool w = mbar_wait_warp(&bars->empty[s], ph ^ 1, abort_flag);
-        if (GEN == GEN_TABLE) w = w && mbar_wait_warp(&bars->full_b[s], ph, abort_flag, true);
+      for (int64_t ch = 0; ch < nChunks; ++ch, ++g) {
+        const uint32_t sc = s, phc = ph;
+        if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+        if ((int)(g % TEAMS) != team) {
+          if (GEN == GEN_GRID3)
+            for (int u = 0; u < P.gps; ++u) outer.next(P.kNStep[0], P.kNStep[1]);
+          continue;
+        }
+        bool w = mbar_wait_warp(&bars->empty[sc], phc ^ 1, abort_flag);
+        if (GEN == GEN_TABLE) w = w && mbar_wait_warp(&bars->kfull[sc], phc, abort_flag, true);
         if (!w) { ok = false; break; }
         tc_fence_after();
-        uint32_t words[32];
-        const uint32_t aAddr = tbase + laneOff + kACol + s * kStageCols;
-        auto emit = [&](int idx, float c, float sn) {
-          words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
-        };
+        const uint32_t aAddr = tbase + laneOff + aCol0 + sc * aStride;
         if (GEN == GEN_GRID3) {
           const int LH = P.lPad / 2;
-          const float2 Pq = grid3_outer(P, e12, row, outer);
-          outer.next(P.kNStep[0], P.kNStep[1]);
-          grid3_pairs(g3, Pq, LH, emit);
-          const uint32_t col = aAddr + (uint32_t)(h * P.lPad);
-          // lPad is a multiple of 8: every store covers 8 columns at an
-          // 8-aligned column offset.
+          for (int u = 0; u < P.gps; ++u) {
+            uint32_t words[kMaxGridN];
+            auto emit = [&](int idx, float c, float sn) {
+              words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
+            };
+            const float2 Pq = grid3_outer(P, e12, row, outer);
+            outer.next(P.kNStep[0], P.kNStep[1]);
+            grid3_pairs(g3, Pq, LH, emit);
+            // lPad is a multiple of 8: every store covers 8 columns at an
+            // 8-aligned column offset.
+            const uint32_t col = aAddr + (uint32_t)(u * 2 * P.lPad + h * P.lPad);
 #pragma unroll
-          for (int pc = 0; pc < 4; ++pc)
-            if (pc * 8 < P.lPad) tmem_st8(col + pc * 8, &words[pc * 8]);
+            for (int pc = 0; pc < kMaxGridN / 8; ++pc)
+              if (pc * 8 < P.lPad) tmem_st8(col + pc * 8, &words[pc * 8]);
+          }
         } else {
-          table_pairs(sK + s * 3 * kTableChunk, h, x, emit);
+          uint32_t words[kTableChunk / 2];
+          auto emit = [&](int idx, float c, float sn) {
+            words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
+          };
+          table_pairs(sK + sc * 3 * kTableChunk, h, x, emit);
           const uint32_t col = aAddr + (uint32_t)(h * (kTableChunk / 2));
           tmem_st8(col, &words[0]);
           tmem_st8(col + 8, &words[8]);
@@ -263,10 +306,10 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
         tmem_st_wait();
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&bars->full_a[s]);
-        if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+        if (lane == 0) mbar_arrive(&bars->full[sc]);
       }
       if (!ok) break;
+      if (team != 0) continue;
 
       // ---------------------------------------------------------- epilogue
       if (!mbar_wait_warp(&bars->acc_full, accPh, abort_flag)) { ok = false; break; }
@@ -274,8 +317,8 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
       const int half = P.nmcPad / 2;
       for (int cb = h * half; cb < (h + 1) * half; cb += 8) {
         uint32_t v[8], lo[8];
-        tmem_ld8(tbase + laneOff + kDCol + cb, v);
-        if (PREC == PREC_BF16) tmem_ld8(tbase + laneOff + kDCol + P.nmcPad + cb, lo);
+        tmem_ld8(tbase + laneOff + cb, v);
+        if (PREC == PREC_BF16) tmem_ld8(tbase + laneOff + P.nmcPad + cb, lo);
         tmem_ld_wait();
         if (valid) {
 #pragma unroll
@@ -301,13 +344,19 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
   if (warp == kMmaWarp) tmem_dealloc(tbase, kTmemCols);
 }
 
-template <int GEN, int PREC>
+template <int GEN, int PREC, int TEAMS>
 cudaError_t launch_one(const TcArgs& args, size_t smem, int grid, cudaStream_t st) {
-  auto fn = rf_tc_kernel<GEN, PREC>;
+  auto fn = rf_tc_kernel<GEN, PREC, TEAMS>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  fn<<<grid, kThreads, smem, st>>>(args);
+  fn<<<grid, (TEAMS * kTeamWarps + 2) * 32, smem, st>>>(args);
   return cudaGetLastError();
+}
+
+template <int GEN, int PREC>
+cudaError_t launch_teams(const TcArgs& args, int teams, size_t smem, int grid, cudaStream_t st) {
+  if (teams == 2) return launch_one<GEN, PREC, 2>(args, smem, grid, st);
+  return launch_one<GEN, PREC, 1>(args, smem, grid, st);
 }
 
 }  // namespace
@@ -316,10 +365,13 @@ size_t tc_smem_bytes(const Plan& P, int* stages) {
   const size_t e12 = (P.gen == GEN_GRID3) ? (size_t)(P.kNStep[0] + P.kNStep[1]) * kTileM * sizeof(float2) : 0;
   const size_t perStage = (size_t)P.stageBytes + (P.gen == GEN_TABLE ? kKtabStageBytes : 0);
   const size_t limit = 227 * 1024;
+  // A stages live in TMEM after the bRows accumulator columns
+  int maxS = (int)((kTmemCols - (uint32_t)P.bRows) / (uint32_t)P.chunkK);
+  if (maxS > kMaxStages) maxS = kMaxStages;
   // The kernel allocates all 512 TMEM columns, so two CTAs must never share
   // an SM: asking for more than half of the SM's shared memory guarantees it.
   const size_t floor = 120 * 1024;
-  for (int s = kMaxStages; s >= 2; --s) {
+  for (int s = maxS; s >= 2; --s) {
     const size_t total = kHeaderBytes + s * perStage + e12;
     if (total <= limit) {
       if (stages) *stages = s;
@@ -346,14 +398,15 @@ cudaError_t launch_tc(const Plan& P, const double* dX, const void* dB, const dou
   args.stages = stages;
   const int64_t tiles = (rows + kTileM - 1) / kTileM;
   const int grid = (int)(tiles < numSMs ? tiles : numSMs);
+  const int teams = P.teams == 2 ? 2 : 1;
   if (P.gen == GEN_GRID3) {
-    if (P.prec == PREC_FP16) return launch_one<GEN_GRID3, PREC_FP16>(args, smem, grid, st);
-    if (P.prec == PREC_BF16_FAST) return launch_one<GEN_GRID3, PREC_BF16_FAST>(args, smem, grid, st);
-    return launch_one<GEN_GRID3, PREC_BF16>(args, smem, grid, st);
+    if (P.prec == PREC_FP16) return launch_teams<GEN_GRID3, PREC_FP16>(args, teams, smem, grid, st);
+    if (P.prec == PREC_BF16_FAST) return launch_teams<GEN_GRID3, PREC_BF16_FAST>(args, teams, smem, grid, st);
+    return launch_teams<GEN_GRID3, PREC_BF16>(args, teams, smem, grid, st);
   }
-  if (P.prec == PREC_FP16) return launch_one<GEN_TABLE, PREC_FP16>(args, smem, grid, st);
-  if (P.prec == PREC_BF16_FAST) return launch_one<GEN_TABLE, PREC_BF16_FAST>(args, smem, grid, st);
-  return launch_one<GEN_TABLE, PREC_BF16>(args, smem, grid, st);
+  if (P.prec == PREC_FP16) return launch_teams<GEN_TABLE, PREC_FP16>(args, teams, smem, grid, st);
+  if (P.prec == PREC_BF16_FAST) return launch_teams<GEN_TABLE, PREC_BF16_FAST>(args, teams, smem, grid, st);
+  return launch_teams<GEN_TABLE, PREC_BF16>(args, teams, smem, grid, st);
 }
 
 }  // namespace rfb
