@@ -53,6 +53,7 @@ extern "C" {
 #define RF_ENOMEM -21           /* device or pinned allocation failed                       */
 #define RF_ETIMEDOUT -22        /* a bounded device wait expired; the kernel returned        */
 #define RF_ENOMEM_ADMISSION -23 /* request larger than the context's HBM budget              */
+#define RF_ESCRATCH -24         /* request larger than rf_generate_device_noalloc's scratch */
 #define RF_ENODEV -25           /* no CUDA device                                           */
 
 /*
@@ -106,6 +107,27 @@ int rf_generate_device(rf_context* ctx, const double* d_xPoints, int nDim, int64
                        int corrMod, int margiFirst, const double* corrL,
                        double fieldAvg, double fieldVar, int Nmc, int method,
                        double* d_randField, const rf_options* opt, void* stream);
+/*
+ * Allocation-free variant of rf_generate_device.  No counterpart in the
+ * reference (which allocates its work arrays itself); it exists for callers
+ * that must not allocate device memory while generating: applications whose
+ * allocator (a caching pool, an OpenACC or CUDA Fortran runtime) owns and has
+ * reserved nearly all device memory, or latency-critical loops that cannot
+ * afford cudaMalloc's implicit synchronisation.  The caller passes device
+ * buffers for the points and the field; all other working memory is one
+ * fixed 32 MiB device array per GPU, placed by the CUDA runtime on every
+ * device where the library is loaded and held until the process exits.
+ * Requests whose tables do not fit it fail with RF_ESCRATCH.  The first call
+ * on a device resolves the array's address (cudaGetSymbolAddress) and should
+ * come before any stream capture on that device.  All calls share the array:
+ * calls whose work overlaps on the GPU race, so serialise them.  Runs on
+ * opt->device on `stream` (0 = legacy default) and returns when the field is
+ * complete; allocates nothing (no cudaMalloc, cudaFree or context).
+ */
+int rf_generate_device_noalloc(const double* d_xPoints, int nDim, int64_t n, int corrMod, int margiFirst,
+                               const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method,
+                               double* d_randField, const rf_options* opt, void* stream);
+
 /* Waits for the context's queued work; reports a device-side timeout. */
 int rf_context_synchronize(rf_context* ctx);
 

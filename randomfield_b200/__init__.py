@@ -19,7 +19,7 @@ import numpy as np
 
 __all__ = [
     "RandomFieldError", "Options", "Context", "lib", "create_standard_gaussian_field_unstruct",
-    "query_geometry", "ISOTROPIC", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
+    "query_geometry", "generate_device_noalloc", "ISOTROPIC", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
     "PREC_BF16", "PREC_FP16", "PREC_FP32", "PREC_BF16_FAST", "LIB_PATH", "STATUS",
 ]
 
@@ -36,7 +36,7 @@ STATUS = {
     0: "RF_OK", -1: "RF_EINVAL_NMC", -2: "RF_EINVAL_NDIM", -3: "RF_EINVAL_CORRL", -4: "RF_EINVAL_LOGNORMAL",
     -5: "RF_EINVAL_METHOD", -6: "RF_EINVAL_CORRMOD", -7: "RF_EINVAL_MARGINAL", -8: "RF_EINVAL_RANGE",
     -9: "RF_EINVAL_ARG", -10: "RF_ENOTSUP", -20: "RF_ECUDA", -21: "RF_ENOMEM", -22: "RF_ETIMEDOUT",
-    -23: "RF_ENOMEM_ADMISSION", -25: "RF_ENODEV",
+    -23: "RF_ENOMEM_ADMISSION", -24: "RF_ESCRATCH", -25: "RF_ENODEV",
 }
 
 _CORRMOD = {"gaussian": CM_GAUSSIAN, "cos": CM_COS, "cm_gaussian": CM_GAUSSIAN, "cm_cos": CM_COS}
@@ -47,7 +47,7 @@ _PREC = {"bf16": PREC_BF16, "fp16": PREC_FP16, "fp32": PREC_FP32, "bf16_fast": P
 EXPORTS = [
     "rf_options_init", "rf_create_standard_gaussian_field_unstruct", "rf_context_create", "rf_context_destroy",
     "rf_generate_device", "rf_context_synchronize", "rf_query_geometry", "rf_last_error", "rf_abi_version",
-    "rf_context_set_timing", "rf_context_last_times",
+    "rf_context_set_timing", "rf_context_last_times", "rf_generate_device_noalloc",
 ]
 
 
@@ -119,6 +119,8 @@ def lib() -> C.CDLL:
         L.rf_context_last_times.argtypes = [C.c_void_p, P(d), P(d), P(d), P(C.c_int32)]
         L.rf_generate_device.argtypes = [C.c_void_p, C.c_void_p, i32, i64, i32, i32, P(d), d, d, i32, i32,
                                          C.c_void_p, P(Options), C.c_void_p]
+        L.rf_generate_device_noalloc.argtypes = [C.c_void_p, i32, i64, i32, i32, P(d), d, d, i32, i32, C.c_void_p,
+                                                 P(Options), C.c_void_p]
         L.rf_query_geometry.argtypes = [P(d), i32, i64, i32, P(d), i32, P(Options), P(i64), P(C.c_int32), P(d),
                                         P(d)]
         _lib = L
@@ -200,6 +202,21 @@ def query_geometry(xPoints, corrMod, corrL, method, options=None, **kw):
                                    cl.ctypes.data_as(P), int(method), C.byref(o), C.byref(K), kn, kd,
                                    C.byref(am)))
     return K.value, list(kn), list(kd), am.value
+
+
+def generate_device_noalloc(d_x, nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, d_out,
+                            options=None, stream=0, **kw) -> None:
+    """rf_generate_device_noalloc: device buffers in, field out, no device
+    allocation by the library (a fixed 32 MiB scratch array per GPU instead);
+    for callers whose allocator owns device memory.  Returns when done."""
+    cl = np.ascontiguousarray(np.asarray(corrL, dtype=np.float64).reshape(-1))
+    o = _opts(options if options is not None else (kw or None))
+    s = stream if isinstance(stream, int) else int(getattr(stream, "cuda_stream", 0))
+    ptr = Context._ptr
+    _check(lib().rf_generate_device_noalloc(C.c_void_p(ptr(d_x)), int(nDim), int(n), _id(corrMod, _CORRMOD, "corrMod"),
+                                            _id(margiFirst, _MARGI, "margiFirst"),
+                                            cl.ctypes.data_as(C.POINTER(C.c_double)), float(fieldAvg), float(fieldVar),
+                                            int(Nmc), int(method), C.c_void_p(ptr(d_out)), C.byref(o), C.c_void_p(s)))
 
 
 class Context:

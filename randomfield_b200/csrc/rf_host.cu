@@ -520,6 +520,43 @@ Request make_request(int nDim, int64_t n, int corrMod, int margiFirst, const dou
 
 }  // namespace
 
+// ------------------------------------------------- planning for other units
+// Thin wrappers over the validation and planning above for entry points
+// implemented in other translation units (rf_noalloc.cu).
+namespace rfb {
+
+int host_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+
+void host_clear_error() { g_err.clear(); }
+
+const JumpTable& host_jump_table() { return jump_table(); }
+
+int host_validate(int nDim, int64_t n, int corrMod, int margiFirst, const double* corrL, double fieldAvg,
+                  double fieldVar, int Nmc, int method, const rf_options* opt, bool* needExtent) {
+  Request rq = make_request(nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
+  if (int rc = validate(rq)) return rc;
+  bool need = false;
+  for (int d = 0; d < nDim; ++d) need = need || !(rq.opt.x_range[d] > 0.0);
+  if (needExtent) *needExtent = need;
+  return RF_OK;
+}
+
+int host_build_plan(int nDim, int64_t n, int corrMod, int margiFirst, const double* corrL, double fieldAvg,
+                    double fieldVar, int Nmc, int method, const rf_options* opt, const double* ext, Plan* P) {
+  Request rq = make_request(nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
+  return build_plan(rq, ext, *P);
+}
+
+int host_block_layout(Plan* P, int32_t rOff, int32_t nmcBlk) {
+  P->rOff = rOff;
+  P->nmcBlk = nmcBlk;
+  return layout(*P);
+}
+
+int32_t host_realization_block(const Plan& P) { return realization_block(P); }
+
+}  // namespace rfb
+
 // ================================================================== C-ABI
 extern "C" {
 
