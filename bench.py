@@ -25,7 +25,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
@@ -37,15 +36,20 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 GRID_N, SPACING, NMC, KN = 128, 0.05, 64, 24
+GRID = (GRID_N, GRID_N, GRID_N)
 CORRL = (2.0, 1.0, 0.5)
 WORKLOAD = "shinozuka-3d-grid128^3-h0.05-corrL(2,1,0.5)-Nmc64-K24^3x4"
 FLUSH_BYTES = 256 << 20
 
 
 def grid_points():
-    ax = np.arange(GRID_N, dtype=np.float64) * SPACING
-    z, y, x = np.meshgrid(ax, ax, ax, indexing="ij")  # axis 1 fastest (setGrid)
+    ax = [np.arange(g, dtype=np.float64) * SPACING for g in GRID]
+    z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")  # axis 1 fastest (setGrid)
     return np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)  # n x 3 == Fortran 3 x n
+
+
+def extent():
+    return tuple((g - 1) * SPACING for g in GRID)
 
 
 def peaks():
@@ -116,8 +120,7 @@ def cpu_rate(x, rows, nr, nthreads=0):
     """Reference CPU algorithm on `rows` points x `nr` realizations, full K."""
     from oracle import oracle as O
 
-    rq = O.OracleRequest(x, Nmc=NMC, kNStep=(KN, KN, KN), corrL=CORRL,
-                         xRange=tuple((GRID_N - 1) * SPACING for _ in range(3)))
+    rq = O.OracleRequest(x, Nmc=NMC, kNStep=(KN, KN, KN), corrL=CORRL, xRange=extent())
     row0 = (x.shape[0] // 2) - rows // 2
     _, t = rq.baseline(row0, rows, 0, nr, nthreads=nthreads)
     return rows * nr / t, t
@@ -161,6 +164,33 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def end_to_end(args, rf, torch, dist, xh, n, opts, world, local):
+    """The flat C-ABI call with pinned host buffers: H2D of the points and
+    D2H of the whole FP64 field inside the timed region."""
+    values = n * NMC
+    xpin = torch.from_numpy(np.ascontiguousarray(xh)).pin_memory()
+    opin = torch.empty((NMC, n), dtype=torch.float64).pin_memory()
+    xa = xpin.numpy().T  # 3 x n view, Fortran order
+    oa = opin.numpy().T  # n x Nmc view, Fortran order
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(2):
+        rf.create_standard_gaussian_field_unstruct(xa, 1, 1, CORRL, 0.0, 1.0, NMC, 2, randField=oa, **opts)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        rf.create_standard_gaussian_field_unstruct(xa, 1, 1, CORRL, 0.0, 1.0, NMC, 2, randField=oa, **opts)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * values * e2e_steps / e2e_s, "unit": "field values/s",
+           "h2d_bytes_per_step": int(xh.nbytes), "d2h_bytes_per_step": int(n * NMC * 8),
+           "api": "rf_create_standard_gaussian_field_unstruct (host buffers, pinned)"}
+    return e2e
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -170,7 +200,13 @@ def main():
     ap.add_argument("--precision", default="bf16", choices=["bf16", "fp16", "bf16_fast", "fp32"])
     ap.add_argument("--no-forms", action="store_true", help="skip the other precision forms")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
+    ap.add_argument("--grid", default="128,128,128",
+                    help="grid points per axis; a smaller grid (e.g. 32,32,18 = one wave of 144 tiles) "
+                         "keeps profiler captures short; the headline workload is 128,128,128")
     args = ap.parse_args()
+    global GRID
+    GRID = tuple(int(v) for v in args.grid.split(","))
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -192,9 +228,7 @@ def main():
 
     xh = grid_points()
     n = xh.shape[0]
-    ext = (GRID_N - 1) * SPACING
-    opts = dict(precision=args.precision, k_nstep=(KN, KN, KN), seed_start=rank, x_range=(ext, ext, ext),
-                device=local)
+    opts = dict(precision=args.precision, k_nstep=(KN, KN, KN), seed_start=rank, x_range=extent(), device=local)
     ctx = rf.Context(local)
     ctx.set_timing(True)
     stream = torch.cuda.Stream(device=local)
@@ -250,7 +284,7 @@ def main():
     acc = None
     if rank == 0:
         rows = np.random.RandomState(7).choice(n, 48, replace=False)
-        rq = O.OracleRequest(xh, Nmc=NMC, kNStep=(KN, KN, KN), corrL=CORRL, seedStart=rank, xRange=(ext, ext, ext))
+        rq = O.OracleRequest(xh, Nmc=NMC, kNStep=(KN, KN, KN), corrL=CORRL, seedStart=rank, xRange=extent())
         ref = rq.generate(rows=rows)
         got = dout.cpu().numpy()[:, rows]
         d = got - ref
@@ -274,27 +308,11 @@ def main():
             forms["bf16_over_fp32_plain"] = value / forms["fp32"]["value"]
 
     # end to end through the flat C-ABI with pinned host buffers
-    xpin = torch.from_numpy(np.ascontiguousarray(xh)).pin_memory()
-    opin = torch.empty((NMC, n), dtype=torch.float64).pin_memory()
-    xa = xpin.numpy().T  # 3 x n view, Fortran order
-    oa = opin.numpy().T  # n x Nmc view, Fortran order
-    e2e_steps = max(3, args.steps // 2)
-    for _ in range(2):
-        rf.create_standard_gaussian_field_unstruct(xa, 1, 1, CORRL, 0.0, 1.0, NMC, 2, randField=oa, **opts)
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        rf.create_standard_gaussian_field_unstruct(xa, 1, 1, CORRL, 0.0, 1.0, NMC, 2, randField=oa, **opts)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": world * values * e2e_steps / e2e_s, "unit": "field values/s",
-           "h2d_bytes_per_step": int(xh.nbytes), "d2h_bytes_per_step": int(n * NMC * 8),
-           "api": "rf_create_standard_gaussian_field_unstruct (host buffers, pinned)"}
+    e2e = None
+    if not args.no_e2e:
+        e2e = end_to_end(args, rf, torch, dist, xh, n, opts, world, local)
 
+    pk, src = peaks()
     pk, src = peaks()
     K = 4 * KN ** 3
     flops = 2.0 * n * (2 * K) * NMC  # algorithmic: the hi/lo split's second MMA is not credited
@@ -302,7 +320,7 @@ def main():
     peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
+    if os.path.exists(tp) and GRID == (128, 128, 128):
         with open(tp) as f:
             traffic = json.load(f).get(args.precision)
     roof = {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s", "frac": tflops / peak,
@@ -327,7 +345,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"bf16": "bf16", "fp16": "f16", "bf16_fast": "bf16", "fp32": "f32"}[args.precision],
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_points": n, "Nmc": NMC, "K": K, "precision": args.precision,
+            "config": {"workload": WORKLOAD if GRID == (128, 128, 128) else f"{WORKLOAD} on a {GRID} grid", "n_points": n, "Nmc": NMC, "K": K, "precision": args.precision,
                        "l2": "flushed between timed steps (256 MiB write); output 1 GiB per step",
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": launches,
