@@ -35,7 +35,7 @@ __device__ __forceinline__ double finish_value(const Plan& P, double acc) {
   return v;
 }
 
-template <int GEN, int RPT>
+template <int GEN, int RPT, int LPAD>
 __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant__ Fp32Args a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Plan& P = a.P;
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
 
   Grid3Thread g3;
   if (GEN == GEN_GRID3) {
-    grid3_thread_setup(g3, P, h, x);
+    grid3_thread_setup<LPAD>(g3, P, h, x);
     if (h == 0) {
       for (int i = 0; i < P.kNStep[0]; ++i) e12[i * kTileM + row] = axis_phasor(P.kDelta[0], i, x[0]);
     } else {
@@ -92,11 +92,10 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
     }
     // trig tile: element 2c = cos, 2c+1 = sin of stage column c
     if (GEN == GEN_GRID3) {
-      const int LH = P.lPad / 2;
       const float2 Pq = grid3_outer(P, e12, row, outer);
       outer.next(P.kNStep[0], P.kNStep[1]);
-      const int col0 = h * P.lPad;
-      grid3_pairs(g3, Pq, LH, [&](int idx, float c, float sn) {
+      const int col0 = h * LPAD;
+      grid3_pairs<LPAD>(g3, Pq, [&](int idx, float c, float sn) {
         As[(2 * (col0 + idx)) * kTileM + row] = c;
         As[(2 * (col0 + idx) + 1) * kTileM + row] = sn;
       });
@@ -147,22 +146,24 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
   }
 }
 
-template <int GEN, int RPT>
+template <int GEN, int RPT, int LPAD>
 cudaError_t launch_one(const Fp32Args& args, size_t smem, dim3 grid, cudaStream_t st) {
-  auto fn = rf_fp32_kernel<GEN, RPT>;
+  auto fn = rf_fp32_kernel<GEN, RPT, LPAD>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   fn<<<grid, kThreads, smem, st>>>(args);
   return cudaGetLastError();
 }
 
-template <int GEN>
-cudaError_t launch_gen(const Fp32Args& args, int rpt, size_t smem, dim3 grid, cudaStream_t st) {
-  switch (rpt) {
-    case 1: return launch_one<GEN, 1>(args, smem, grid, st);
-    case 2: return launch_one<GEN, 2>(args, smem, grid, st);
-    case 4: return launch_one<GEN, 4>(args, smem, grid, st);
-    default: return launch_one<GEN, 8>(args, smem, grid, st);
+template <int RPT>
+cudaError_t launch_rpt(const Plan& P, const Fp32Args& args, size_t smem, dim3 grid, cudaStream_t st) {
+  if (P.gen != GEN_GRID3) return launch_one<GEN_TABLE, RPT, 0>(args, smem, grid, st);
+  switch (P.lPad) {
+    case 8: return launch_one<GEN_GRID3, RPT, 8>(args, smem, grid, st);
+    case 16: return launch_one<GEN_GRID3, RPT, 16>(args, smem, grid, st);
+    case 24: return launch_one<GEN_GRID3, RPT, 24>(args, smem, grid, st);
+    case 32: return launch_one<GEN_GRID3, RPT, 32>(args, smem, grid, st);
+    default: return cudaErrorInvalidValue;
   }
 }
 
@@ -198,8 +199,12 @@ cudaError_t launch_fp32(const Plan& P, const double* dX, const void* dB, const d
   const size_t smem = fp32_smem_bytes(P);
   const int64_t tiles = (rows + kTileM - 1) / kTileM;
   dim3 grid((unsigned)tiles, (unsigned)((P.nmcPad + args.nb - 1) / args.nb));
-  if (P.gen == GEN_GRID3) return launch_gen<GEN_GRID3>(args, rpt, smem, grid, st);
-  return launch_gen<GEN_TABLE>(args, rpt, smem, grid, st);
+  switch (rpt) {
+    case 1: return launch_rpt<1>(P, args, smem, grid, st);
+    case 2: return launch_rpt<2>(P, args, smem, grid, st);
+    case 4: return launch_rpt<4>(P, args, smem, grid, st);
+    default: return launch_rpt<8>(P, args, smem, grid, st);
+  }
 }
 
 }  // namespace rfb

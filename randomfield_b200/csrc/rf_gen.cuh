@@ -55,16 +55,17 @@ struct Grid3Thread {
   float2 d2[kMaxGridN / 4];
 };
 
-// Fill the entries i3 = h*LH + t, t < LH (LH = lPad/2, a multiple of 4).
+// Fill the entries i3 = h*LH + t, t < LH (LH = LPAD/2, a multiple of 4).
+// LPAD is a compile-time constant so that every loop over the stage is
+// straight-line code: guarded unrolled loops cost the warp a branch
+// resolution per iteration.
+template <int LPAD>
 __device__ __forceinline__ void grid3_thread_setup(Grid3Thread& g, const Plan& P, int h, const double* x) {
-  const int LH = P.lPad / 2;
+  constexpr int LH = LPAD / 2;
 #pragma unroll
-  for (int u = 0; u < kMaxGridN / 4; ++u) {
-    float2 e0 = make_float2(0.f, 0.f), e1 = make_float2(0.f, 0.f);
-    if (2 * u < LH) {
-      e0 = axis_phasor(P.kDelta[2], h * LH + 2 * u, x[2]);
-      e1 = axis_phasor(P.kDelta[2], h * LH + 2 * u + 1, x[2]);
-    }
+  for (int u = 0; u < LH / 2; ++u) {
+    const float2 e0 = axis_phasor(P.kDelta[2], h * LH + 2 * u, x[2]);
+    const float2 e1 = axis_phasor(P.kDelta[2], h * LH + 2 * u + 1, x[2]);
     g.c2[u] = make_float2(e0.x, e1.x);
     g.d2[u] = make_float2(e0.y, e1.y);
   }
@@ -100,24 +101,23 @@ __device__ __forceinline__ float2 grid3_outer(const Plan& P, const float2* e12, 
 //   P E3 = (ac - bd) + i(bc + ad),  P conj(E3) = (ac + bd) + i(bc - ad);
 // two E3 entries go through one packed FP32x2 instruction (sm_100), so four
 // pairs cost two multiplies and four fused multiply-adds.
-template <typename Emit>
-__device__ __forceinline__ void grid3_pairs(const Grid3Thread& g, float2 Pq, int LH, Emit&& emit) {
+template <int LPAD, typename Emit>
+__device__ __forceinline__ void grid3_pairs(const Grid3Thread& g, float2 Pq, Emit&& emit) {
+  constexpr int LH = LPAD / 2;
   const float2 a2 = make_float2(Pq.x, Pq.x), b2 = make_float2(Pq.y, Pq.y);
   const float2 na2 = make_float2(-Pq.x, -Pq.x), nb2 = make_float2(-Pq.y, -Pq.y);
 #pragma unroll
-  for (int u = 0; u < kMaxGridN / 4; ++u) {
-    if (2 * u < LH) {
-      const float2 ac = __fmul2_rn(a2, g.c2[u]);
-      const float2 bc = __fmul2_rn(b2, g.c2[u]);
-      const float2 rp = __ffma2_rn(nb2, g.d2[u], ac);
-      const float2 rm = __ffma2_rn(b2, g.d2[u], ac);
-      const float2 ip = __ffma2_rn(a2, g.d2[u], bc);
-      const float2 im = __ffma2_rn(na2, g.d2[u], bc);
-      emit(4 * u + 0, rp.x, ip.x);
-      emit(4 * u + 1, rm.x, im.x);
-      emit(4 * u + 2, rp.y, ip.y);
-      emit(4 * u + 3, rm.y, im.y);
-    }
+  for (int u = 0; u < LH / 2; ++u) {
+    const float2 ac = __fmul2_rn(a2, g.c2[u]);
+    const float2 bc = __fmul2_rn(b2, g.c2[u]);
+    const float2 rp = __ffma2_rn(nb2, g.d2[u], ac);
+    const float2 rm = __ffma2_rn(b2, g.d2[u], ac);
+    const float2 ip = __ffma2_rn(a2, g.d2[u], bc);
+    const float2 im = __ffma2_rn(na2, g.d2[u], bc);
+    emit(4 * u + 0, rp.x, ip.x);
+    emit(4 * u + 1, rm.x, im.x);
+    emit(4 * u + 2, rp.y, ip.y);
+    emit(4 * u + 3, rm.y, im.y);
   }
 }
 

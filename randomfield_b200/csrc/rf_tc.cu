@@ -7,22 +7,24 @@
 //   D (128 points x Nmc, FP32 in TMEM) += A (128 x 16, trig tile in TMEM)
 //                                         x B (16 x Nmc, amplitude/phase in SMEM)
 //
-// Warp roles (one CTA per SM), with T generator teams of 8 warps:
-//   warps 0..8T-1  generators: team t builds the trig tiles of stages
-//                  g = t (mod T) straight into TMEM (tcgen05.st), lane =
-//                  point, two warps per lane quarter split the columns.  Team
-//                  0 runs the fused epilogue after the last stage of a tile
-//                  (tcgen05.ld, ampMult, marginal map, FP64 stores);
-//   warp 8T        MMA issuer (one thread): tcgen05.mma kind::f16, A from
-//                  TMEM, B by descriptor from SMEM; tcgen05.commit frees
-//                  stages;
-//   warp 8T+1      producer (one thread): 1-D bulk copies (TMA) of B stages
-//                  from HBM/L2 into SMEM; no multicast.
+// Warp roles (320 threads, one CTA per SM):
+//   warps 0-7   generators: build the trig tile of each stage straight into
+//               TMEM (tcgen05.st), lane = point, two warps per lane quarter
+//               split the columns; after the last stage of a tile they run
+//               the fused epilogue (tcgen05.ld, ampMult, marginal map, FP64
+//               stores);
+//   warp 8      MMA issuer (one thread): tcgen05.mma kind::f16, A from TMEM,
+//               B by descriptor from SMEM; tcgen05.commit frees stages;
+//   warp 9      producer (one thread): 1-D bulk copies (TMA) of B stages from
+//               HBM/L2 into SMEM; no multicast.
 // The issuing thread can run only about one MMA ahead of the tensor core, so
-// anything it waits for between MMAs idles the tensor pipe: it waits on one
+// anything it does between MMAs idles the tensor pipe: it waits on one
 // barrier per stage (the bulk copy completes on the same barrier the
 // generators arrive on), probes the next stage's barrier while the last MMA
-// of the current stage runs, and a stage holds up to 16 MMAs.
+// of the current stage runs, and issues the MMAs of a stage as straight-line
+// code (the kernel is specialised on the padded axis-3 length LPAD, which
+// fixes the MMAs per stage; a runtime-guarded unrolled loop cost a branch
+// resolution per MMA and halved the tensor throughput).
 // TMEM: accumulator columns [0, bRows), then A stages of chunkK columns.
 // Every wait is bounded (globaltimer); on expiry the kernel raises an error
 // word, drains its own async work, frees TMEM and returns.
@@ -34,7 +36,11 @@ namespace rfb {
 
 namespace {
 
-constexpr int kTeamWarps = 8;
+constexpr int kTeamWarps = 8;  // generator warps
+constexpr int kGenWarps = kTeamWarps;
+constexpr int kMmaWarp = kGenWarps;
+constexpr int kProdWarp = kGenWarps + 1;
+constexpr int kThreads = (kProdWarp + 1) * 32;
 constexpr int kMaxStages = 8;
 constexpr uint32_t kTmemCols = 512;
 constexpr int kKtabStageBytes = 3 * kTableChunk * 8;
@@ -81,12 +87,11 @@ __device__ __forceinline__ double finish_value(const Plan& P, float acc) {
   return v;
 }
 
-template <int GEN, int PREC, int TEAMS>
-__global__ void __launch_bounds__((TEAMS * kTeamWarps + 2) * 32, 1)
-    rf_tc_kernel(const __grid_constant__ TcArgs a) {
-  constexpr int kGenWarps = TEAMS * kTeamWarps;
-  constexpr int kMmaWarp = kGenWarps;
-  constexpr int kProdWarp = kGenWarps + 1;
+// LPAD: GEN_GRID3 axis-3 length padded to 8/16/24/32 (0 for GEN_TABLE).
+template <int GEN, int PREC, int LPAD>
+__global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constant__ TcArgs a) {
+  // MMAs (K = 16) per stage: two groups of 2*LPAD columns, or one table chunk
+  constexpr int STEPS = (GEN == GEN_GRID3) ? LPAD / 2 : kTableChunk / 8;
   extern __shared__ __align__(1024) unsigned char smem[];
   const Plan& P = a.P;
   Bars* bars = reinterpret_cast<Bars*>(smem);
@@ -181,7 +186,6 @@ __global__ void __launch_bounds__((TEAMS * kTeamWarps + 2) * 32, 1)
       const uint64_t desc0 = make_sdesc(smem_u32(sB), lbo, sbo);
       const uint64_t sStep = (uint64_t)(P.stageBytes >> 4);
       const uint64_t jStep = (uint64_t)((2u * lbo) >> 4);
-      const int steps = P.chunkK / 8;
       uint32_t s = 0, ph = 0, accPh = 0;
       bool ok = true, ready = false;  // ready: full[s] of the next stage already observed
       for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
@@ -195,14 +199,12 @@ __global__ void __launch_bounds__((TEAMS * kTeamWarps + 2) * 32, 1)
           const uint32_t sn = (s + 1 == (uint32_t)S) ? 0u : s + 1;
           const uint32_t phn = (s + 1 == (uint32_t)S) ? ph ^ 1 : ph;
           const bool more = (ch + 1 < nChunks) || (tile + gridDim.x < numTiles);
+          mma_ts(tbase, aBase, d0, idesc, ch != 0 ? 1u : 0u);  // the tile's first MMA overwrites D
 #pragma unroll
-          for (int j = 0; j < kMaxStageCols / 8; ++j) {
-            if (j < steps) {
-              // probe the next stage while this stage's last MMA is queued
-              if (j == steps - 1) ready = more && mbar_test_wait(&bars->full[sn], phn);
-              mma_ts(tbase, aBase + 8u * j, d0 + jStep * j, idesc, (ch | j) != 0 ? 1u : 0u);
-            }
-          }
+          for (int j = 1; j < STEPS - 1; ++j) mma_ts(tbase, aBase + 8u * j, d0 + jStep * j, idesc, 1u);
+          // probe the next stage while this stage's last MMA is queued
+          ready = more && mbar_test_wait(&bars->full[sn], phn);
+          mma_ts(tbase, aBase + 8u * (STEPS - 1), d0 + jStep * (STEPS - 1), idesc, 1u);
           mma_commit(&bars->empty[s]);
           s = sn;
           ph = phn;
@@ -220,12 +222,10 @@ __global__ void __launch_bounds__((TEAMS * kTeamWarps + 2) * 32, 1)
     __syncwarp();
   } else {
     // ------------------------------------------------- generators + epilogue
-    const int team = warp / kTeamWarps, wi = warp % kTeamWarps;
-    const int q = wi & 3, h = wi >> 2;
+    const int q = warp & 3, h = warp >> 2;
     const int row = q * 32 + lane;
     const uint32_t laneOff = (uint32_t)(q * 32) << 16;
     uint32_t s = 0, ph = 0, accPh = 0, ePh = 0;
-    int64_t g = 0;  // stage counter of this CTA; team t takes g = t (mod TEAMS)
     bool ok = true;
     for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
       const int64_t p = a.row0 + tile * kTileM + row;
@@ -239,59 +239,50 @@ __global__ void __launch_bounds__((TEAMS * kTeamWarps + 2) * 32, 1)
 
       Grid3Thread g3;
       if (GEN == GEN_GRID3) {
-        grid3_thread_setup(g3, P, h, x);
+        grid3_thread_setup<LPAD>(g3, P, h, x);
         // The shared axis-1/axis-2 phasor table is rewritten per tile: every
         // generator warp first declares it is done with the previous tile's
-        // table, team 0 writes (half 0: axis 1, half 1: axis 2), then all
-        // read.  Bounded mbarrier rendezvous, not named barriers, so that an
-        // aborting warp cannot leave the others blocked.
+        // table, then writes its part (half 0: axis 1, half 1: axis 2), then
+        // all read.  Bounded mbarrier rendezvous, not named barriers, so that
+        // an aborting warp cannot leave the others blocked.
         __syncwarp();
         if (lane == 0) mbar_arrive(&bars->e12_free);
-        if (team == 0) {
-          if (!mbar_wait_warp(&bars->e12_free, ePh, abort_flag)) { ok = false; break; }
-          if (h == 0) {
-            for (int i = 0; i < P.kNStep[0]; ++i) e12[i * kTileM + row] = axis_phasor(P.kDelta[0], i, x[0]);
-          } else {
-            for (int i = 0; i < P.kNStep[1]; ++i)
-              e12[(P.kNStep[0] + i) * kTileM + row] = axis_phasor(P.kDelta[1], i, x[1]);
-          }
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&bars->e12_ready);
+        if (!mbar_wait_warp(&bars->e12_free, ePh, abort_flag)) { ok = false; break; }
+        if (h == 0) {
+          for (int i = 0; i < P.kNStep[0]; ++i) e12[i * kTileM + row] = axis_phasor(P.kDelta[0], i, x[0]);
+        } else {
+          for (int i = 0; i < P.kNStep[1]; ++i) e12[(P.kNStep[0] + i) * kTileM + row] = axis_phasor(P.kDelta[1], i, x[1]);
         }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bars->e12_ready);
         if (!mbar_wait_warp(&bars->e12_ready, ePh, abort_flag)) { ok = false; break; }
         ePh ^= 1;
       }
 
       Grid3Outer outer;
-      for (int64_t ch = 0; ch < nChunks; ++ch, ++g) {
+      for (int64_t ch = 0; ch < nChunks; ++ch) {
         const uint32_t sc = s, phc = ph;
         if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
-        if ((int)(g % TEAMS) != team) {
-          if (GEN == GEN_GRID3)
-            for (int u = 0; u < P.gps; ++u) outer.next(P.kNStep[0], P.kNStep[1]);
-          continue;
-        }
         bool w = mbar_wait_warp(&bars->empty[sc], phc ^ 1, abort_flag);
         if (GEN == GEN_TABLE) w = w && mbar_wait_warp(&bars->kfull[sc], phc, abort_flag, true);
         if (!w) { ok = false; break; }
         tc_fence_after();
         const uint32_t aAddr = tbase + laneOff + aCol0 + sc * aStride;
         if (GEN == GEN_GRID3) {
-          const int LH = P.lPad / 2;
-          for (int u = 0; u < P.gps; ++u) {
-            uint32_t words[kMaxGridN];
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {  // two groups per stage
+            uint32_t words[LPAD > 0 ? LPAD : 1];
             auto emit = [&](int idx, float c, float sn) {
               words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
             };
             const float2 Pq = grid3_outer(P, e12, row, outer);
             outer.next(P.kNStep[0], P.kNStep[1]);
-            grid3_pairs(g3, Pq, LH, emit);
-            // lPad is a multiple of 8: every store covers 8 columns at an
+            grid3_pairs<LPAD>(g3, Pq, emit);
+            // LPAD is a multiple of 8: every store covers 8 columns at an
             // 8-aligned column offset.
-            const uint32_t col = aAddr + (uint32_t)(u * 2 * P.lPad + h * P.lPad);
+            const uint32_t col = aAddr + (uint32_t)(u * 2 * LPAD + h * LPAD);
 #pragma unroll
-            for (int pc = 0; pc < kMaxGridN / 8; ++pc)
-              if (pc * 8 < P.lPad) tmem_st8(col + pc * 8, &words[pc * 8]);
+            for (int pc = 0; pc < LPAD / 8; ++pc) tmem_st8(col + pc * 8, &words[pc * 8]);
           }
         } else {
           uint32_t words[kTableChunk / 2];
@@ -309,7 +300,6 @@ __global__ void __launch_bounds__((TEAMS * kTeamWarps + 2) * 32, 1)
         if (lane == 0) mbar_arrive(&bars->full[sc]);
       }
       if (!ok) break;
-      if (team != 0) continue;
 
       // ---------------------------------------------------------- epilogue
       if (!mbar_wait_warp(&bars->acc_full, accPh, abort_flag)) { ok = false; break; }
@@ -344,19 +334,25 @@ __global__ void __launch_bounds__((TEAMS * kTeamWarps + 2) * 32, 1)
   if (warp == kMmaWarp) tmem_dealloc(tbase, kTmemCols);
 }
 
-template <int GEN, int PREC, int TEAMS>
+template <int GEN, int PREC, int LPAD>
 cudaError_t launch_one(const TcArgs& args, size_t smem, int grid, cudaStream_t st) {
-  auto fn = rf_tc_kernel<GEN, PREC, TEAMS>;
+  auto fn = rf_tc_kernel<GEN, PREC, LPAD>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  fn<<<grid, (TEAMS * kTeamWarps + 2) * 32, smem, st>>>(args);
+  fn<<<grid, kThreads, smem, st>>>(args);
   return cudaGetLastError();
 }
 
-template <int GEN, int PREC>
-cudaError_t launch_teams(const TcArgs& args, int teams, size_t smem, int grid, cudaStream_t st) {
-  if (teams == 2) return launch_one<GEN, PREC, 2>(args, smem, grid, st);
-  return launch_one<GEN, PREC, 1>(args, smem, grid, st);
+template <int PREC>
+cudaError_t launch_prec(const Plan& P, const TcArgs& args, size_t smem, int grid, cudaStream_t st) {
+  if (P.gen != GEN_GRID3) return launch_one<GEN_TABLE, PREC, 0>(args, smem, grid, st);
+  switch (P.lPad) {
+    case 8: return launch_one<GEN_GRID3, PREC, 8>(args, smem, grid, st);
+    case 16: return launch_one<GEN_GRID3, PREC, 16>(args, smem, grid, st);
+    case 24: return launch_one<GEN_GRID3, PREC, 24>(args, smem, grid, st);
+    case 32: return launch_one<GEN_GRID3, PREC, 32>(args, smem, grid, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace
@@ -398,15 +394,9 @@ cudaError_t launch_tc(const Plan& P, const double* dX, const void* dB, const dou
   args.stages = stages;
   const int64_t tiles = (rows + kTileM - 1) / kTileM;
   const int grid = (int)(tiles < numSMs ? tiles : numSMs);
-  const int teams = P.teams == 2 ? 2 : 1;
-  if (P.gen == GEN_GRID3) {
-    if (P.prec == PREC_FP16) return launch_teams<GEN_GRID3, PREC_FP16>(args, teams, smem, grid, st);
-    if (P.prec == PREC_BF16_FAST) return launch_teams<GEN_GRID3, PREC_BF16_FAST>(args, teams, smem, grid, st);
-    return launch_teams<GEN_GRID3, PREC_BF16>(args, teams, smem, grid, st);
-  }
-  if (P.prec == PREC_FP16) return launch_teams<GEN_TABLE, PREC_FP16>(args, teams, smem, grid, st);
-  if (P.prec == PREC_BF16_FAST) return launch_teams<GEN_TABLE, PREC_BF16_FAST>(args, teams, smem, grid, st);
-  return launch_teams<GEN_TABLE, PREC_BF16>(args, teams, smem, grid, st);
+  if (P.prec == PREC_FP16) return launch_prec<PREC_FP16>(P, args, smem, grid, st);
+  if (P.prec == PREC_BF16_FAST) return launch_prec<PREC_BF16_FAST>(P, args, smem, grid, st);
+  return launch_prec<PREC_BF16>(P, args, smem, grid, st);
 }
 
 }  // namespace rfb
