@@ -175,50 +175,50 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
     __syncwarp();
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------- MMA issuer
-    if (lane == 0) {
-      // The hi/lo amplitude rows sit one above the other in each B stage, so
-      // one MMA with N = bRows computes both products into 2*nmcPad
-      // accumulator columns; the epilogue adds the halves.  Descriptors are
-      // advanced by plain adds of the start address field (it cannot
-      // overflow: shared memory is below 256 KB).
-      const uint32_t idesc = make_idesc(PREC == PREC_FP16 ? 0u : 1u, 128u, (uint32_t)P.bRows);
-      const uint32_t lbo = (uint32_t)P.bRows * 16u, sbo = 128u;
-      const uint64_t desc0 = make_sdesc(smem_u32(sB), lbo, sbo);
-      const uint64_t sStep = (uint64_t)(P.stageBytes >> 4);
-      const uint64_t jStep = (uint64_t)((2u * lbo) >> 4);
-      uint32_t s = 0, ph = 0, accPh = 0;
-      bool ok = true, ready = false;  // ready: full[s] of the next stage already observed
-      for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
-        if (!mbar_wait(&bars->acc_empty, accPh ^ 1, abort_flag)) { ok = false; break; }
+    // The whole warp runs the loop (its state stays warp-uniform; every
+    // branch condition is made uniform by a warp vote, so that the warp stays
+    // converged for elect.sync); one elected lane issues each MMA and commit.  The hi/lo amplitude rows sit
+    // one above the other in each B stage, so one MMA with N = bRows computes
+    // both products into 2*nmcPad accumulator columns; the epilogue adds the
+    // halves.  Descriptors are advanced by plain adds of the start address
+    // field (it cannot overflow: shared memory is below 256 KB).
+    const uint32_t idesc = make_idesc(PREC == PREC_FP16 ? 0u : 1u, 128u, (uint32_t)P.bRows);
+    const uint32_t lbo = (uint32_t)P.bRows * 16u, sbo = 128u;
+    const uint64_t desc0 = make_sdesc(smem_u32(sB), lbo, sbo);
+    const uint64_t sStep = (uint64_t)(P.stageBytes >> 4);
+    const uint64_t jStep = (uint64_t)((2u * lbo) >> 4);
+    uint32_t s = 0, ph = 0, accPh = 0;
+    bool ok = true, ready = false;  // ready: full[s] of the next stage already observed
+    for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
+      if (!mbar_wait_warp(&bars->acc_empty, accPh ^ 1, abort_flag)) { ok = false; break; }
+      tc_fence_after();
+      for (int64_t ch = 0; ch < nChunks; ++ch) {
+        if (!ready && !mbar_wait_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
         tc_fence_after();
-        for (int64_t ch = 0; ch < nChunks; ++ch) {
-          if (!ready && !mbar_wait(&bars->full[s], ph, abort_flag)) { ok = false; break; }
-          tc_fence_after();
-          const uint32_t aBase = tbase + aCol0 + s * aStride;
-          const uint64_t d0 = desc0 + sStep * s;
-          const uint32_t sn = (s + 1 == (uint32_t)S) ? 0u : s + 1;
-          const uint32_t phn = (s + 1 == (uint32_t)S) ? ph ^ 1 : ph;
-          const bool more = (ch + 1 < nChunks) || (tile + gridDim.x < numTiles);
-          mma_ts(tbase, aBase, d0, idesc, ch != 0 ? 1u : 0u);  // the tile's first MMA overwrites D
+        const uint32_t aBase = tbase + aCol0 + s * aStride;
+        const uint64_t d0 = desc0 + sStep * s;
+        const uint32_t sn = (s + 1 == (uint32_t)S) ? 0u : s + 1;
+        const uint32_t phn = (s + 1 == (uint32_t)S) ? ph ^ 1 : ph;
+        const bool more = (ch + 1 < nChunks) || (tile + gridDim.x < numTiles);
+        mma_ts_elect(tbase, aBase, d0, idesc, ch != 0 ? 1u : 0u);  // the tile's first MMA overwrites D
 #pragma unroll
-          for (int j = 1; j < STEPS - 1; ++j) mma_ts(tbase, aBase + 8u * j, d0 + jStep * j, idesc, 1u);
-          // probe the next stage while this stage's last MMA is queued
-          ready = more && mbar_test_wait(&bars->full[sn], phn);
-          mma_ts(tbase, aBase + 8u * (STEPS - 1), d0 + jStep * (STEPS - 1), idesc, 1u);
-          mma_commit(&bars->empty[s]);
-          s = sn;
-          ph = phn;
-        }
-        if (!ok) break;
-        mma_commit(&bars->acc_full);
-        accPh ^= 1;
+        for (int j = 1; j < STEPS - 1; ++j) mma_ts_elect(tbase, aBase + 8u * j, d0 + jStep * j, idesc, 1u);
+        // probe the next stage while this stage's last MMA is queued
+        ready = __all_sync(0xffffffffu, more && mbar_test_wait(&bars->full[sn], phn));
+        mma_ts_elect(tbase, aBase + 8u * (STEPS - 1), d0 + jStep * (STEPS - 1), idesc, 1u);
+        mma_commit_elect(&bars->empty[s]);
+        s = sn;
+        ph = phn;
       }
-      if (!ok) raise_abort(bars, a.err);
-      // Drain every MMA this thread issued before TMEM is released.
-      mma_commit(&bars->done);
-      volatile int never = 0;
-      mbar_wait(&bars->done, 0, &never);
+      if (!ok) break;
+      mma_commit_elect(&bars->acc_full);
+      accPh ^= 1;
     }
+    if (!ok && lane == 0) raise_abort(bars, a.err);
+    // Drain every MMA the elected lane issued before TMEM is released.
+    mma_commit_elect(&bars->done);
+    volatile int never = 0;
+    mbar_wait(&bars->done, 0, &never);
     __syncwarp();
   } else {
     // ------------------------------------------------- generators + epilogue
