@@ -132,26 +132,17 @@ __device__ __forceinline__ void mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_
       "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
-// mma_ts issued by one elected lane of the calling warp, which must be
-// converged (all 32 lanes call).  Running the issue loop on the whole warp
-// keeps its state warp-uniform; elect.sync picks the same lane every time, so
-// that lane's tcgen05.commit covers all the MMAs.
-__device__ __forceinline__ void mma_ts_elect(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
-                                             uint32_t accumulate) {
+// One lane of a converged warp (elect.sync over all 32 lanes), for code that
+// runs a loop on the whole warp and issues single-thread instructions from
+// the elected lane.
+__device__ __forceinline__ bool elect_one() {
+  uint32_t e;
   asm volatile(
-      "{\n\t.reg .pred p, e;\n\t.reg .b32 l;\n\t"
-      "elect.sync l|e, 0xffffffff;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "@e tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-__device__ __forceinline__ void mma_commit_elect(uint64_t* bar) {
-  asm volatile(
-      "{\n\t.reg .pred e;\n\t.reg .b32 l;\n\t"
-      "elect.sync l|e, 0xffffffff;\n\t"
-      "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}" ::"r"(smem_u32(bar))
-      : "memory");
+      "{\n\t.reg .pred p;\n\t.reg .b32 l;\n\t"
+      "elect.sync l|p, 0xffffffff;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(e));
+  return e != 0;
 }
 // Arrive once on `bar` when all prior tcgen05 async ops of this thread finish.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {

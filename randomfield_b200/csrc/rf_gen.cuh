@@ -95,6 +95,41 @@ __device__ __forceinline__ float2 grid3_outer(const Plan& P, const float2* e12, 
   return make_float2(e1.x * e2.x - e1.y * e2.y, e1.x * e2.y + e1.y * e2.x);
 }
 
+// Outer phasor P = E1(i1) * E2(i2)^{s2} walked group by group in registers,
+// for the tensor-core forms: E1 by the recurrence E1(i1+1) = E1(i1) * E1(1),
+// restarted at E1(0) = 1 on every wrap of i1 (at most n1 - 1 <= 31 FP32
+// complex products, relative error below 4e-6, far under the BF16/FP16
+// rounding of the tile); E2(i2) from an FP64-reduced phase at each wrap.
+// The FP32 plain form keeps the accurate per-axis tables (grid3_outer).
+struct Grid3Walk {
+  float2 e1, e1step, e2;
+  int i1, i2, s2;
+  __device__ __forceinline__ void init(const Plan& P, const double* x) {
+    i1 = i2 = s2 = 0;
+    e1 = make_float2(1.f, 0.f);
+    e2 = e1;
+    e1step = axis_phasor(P.kDelta[0], 1, x[0]);
+  }
+  __device__ __forceinline__ float2 outer() const {
+    const float e2y = s2 ? -e2.y : e2.y;
+    return make_float2(e1.x * e2.x - e1.y * e2y, e1.x * e2y + e1.y * e2.x);
+  }
+  // Advance one group; the wrap test is uniform across the warp.
+  __device__ __forceinline__ void next(const Plan& P, const double* x) {
+    if (++i1 == P.kNStep[0]) {
+      i1 = 0;
+      e1 = make_float2(1.f, 0.f);
+      if (++i2 == P.kNStep[1]) {
+        i2 = 0;
+        ++s2;
+      }
+      e2 = axis_phasor(P.kDelta[1], i2, x[1]);
+    } else {
+      e1 = make_float2(e1.x * e1step.x - e1.y * e1step.y, e1.x * e1step.y + e1.y * e1step.x);
+    }
+  }
+};
+
 // The 2*LH (cos, sin) pairs of one half-stage: for t < LH, pair 2t is
 // P*E3(t) (s3 = +) and pair 2t+1 is P*conj(E3(t)) (s3 = -).  With P = a+ib
 // and E3 = c+id, both signs share a*c and b*c:

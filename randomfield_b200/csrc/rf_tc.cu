@@ -8,13 +8,14 @@
 //                                         x B (16 x Nmc, amplitude/phase in SMEM)
 //
 // Warp roles (320 threads, one CTA per SM):
-//   warps 0-7   generators: build the trig tile of each stage straight into
-//               TMEM (tcgen05.st), lane = point, two warps per lane quarter
-//               split the columns; after the last stage of a tile they run
-//               the fused epilogue (tcgen05.ld, ampMult, marginal map, FP64
-//               stores);
-//   warp 8      MMA issuer (one thread): tcgen05.mma kind::f16, A from TMEM,
-//               B by descriptor from SMEM; tcgen05.commit frees stages;
+//   warp 0      MMA issuer: the warp runs the stage loop, one elected lane
+//               issues tcgen05.mma kind::f16 (A from TMEM, B by descriptor
+//               from SMEM) and tcgen05.commit, which frees stages;
+//   warps 1-8   generators: build the trig tile of each stage straight into
+//               TMEM (tcgen05.st), lane = point; the two warps of a TMEM lane
+//               quarter split the columns; after the last stage of a tile they
+//               run the fused epilogue (tcgen05.ld, ampMult, marginal map,
+//               FP64 stores);
 //   warp 9      producer (one thread): 1-D bulk copies (TMA) of B stages from
 //               HBM/L2 into SMEM; no multicast.
 // The issuing thread can run only about one MMA ahead of the tensor core, so
@@ -25,6 +26,10 @@
 // code (the kernel is specialised on the padded axis-3 length LPAD, which
 // fixes the MMAs per stage; a runtime-guarded unrolled loop cost a branch
 // resolution per MMA and halved the tensor throughput).
+// Measured balance (128^3 workload, BF16): the MMAs of a stage take about
+// 770 cycles; the generators of the three sub-partitions without a service
+// warp need about 750, those sharing a sub-partition with the issuer about
+// 880, which sets the stage period (about 1130 cycles with the barriers).
 // TMEM: accumulator columns [0, bRows), then A stages of chunkK columns.
 // Every wait is bounded (globaltimer); on expiry the kernel raises an error
 // word, drains its own async work, frees TMEM and returns.
@@ -36,10 +41,11 @@ namespace rfb {
 
 namespace {
 
-constexpr int kTeamWarps = 8;  // generator warps
-constexpr int kGenWarps = kTeamWarps;
-constexpr int kMmaWarp = kGenWarps;
-constexpr int kProdWarp = kGenWarps + 1;
+constexpr int kMmaWarp = 0;
+constexpr int kGenWarp0 = 1;   // generators: warps 1-8
+constexpr int kGenWarps = 8;
+constexpr int kTeamWarps = kGenWarps;
+constexpr int kProdWarp = kGenWarp0 + kGenWarps;
 constexpr int kThreads = (kProdWarp + 1) * 32;
 constexpr int kMaxStages = 8;
 constexpr uint32_t kTmemCols = 512;
@@ -52,8 +58,6 @@ struct Bars {
   uint64_t acc_full;
   uint64_t acc_empty;
   uint64_t done;
-  uint64_t e12_free;
-  uint64_t e12_ready;
   uint32_t tmem_base;
   int abort_flag;
 };
@@ -97,7 +101,6 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
   Bars* bars = reinterpret_cast<Bars*>(smem);
   unsigned char* sB = smem + kHeaderBytes;
   double* sK = reinterpret_cast<double*>(sB + (size_t)a.stages * P.stageBytes);
-  float2* e12 = reinterpret_cast<float2*>(sK + (GEN == GEN_TABLE ? a.stages * 3 * kTableChunk : 0));
   volatile int* abort_flag = &bars->abort_flag;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -114,8 +117,6 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
     mbar_init(&bars->acc_full, 1);
     mbar_init(&bars->acc_empty, kTeamWarps);
     mbar_init(&bars->done, 1);
-    mbar_init(&bars->e12_free, kGenWarps);
-    mbar_init(&bars->e12_ready, kTeamWarps);
     bars->abort_flag = 0;
     mbar_fence_init();
   }
@@ -176,12 +177,16 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
   } else if (warp == kMmaWarp) {
     // ---------------------------------------------------------- MMA issuer
     // The whole warp runs the loop (its state stays warp-uniform; every
-    // branch condition is made uniform by a warp vote, so that the warp stays
-    // converged for elect.sync); one elected lane issues each MMA and commit.  The hi/lo amplitude rows sit
-    // one above the other in each B stage, so one MMA with N = bRows computes
-    // both products into 2*nmcPad accumulator columns; the epilogue adds the
-    // halves.  Descriptors are advanced by plain adds of the start address
-    // field (it cannot overflow: shared memory is below 256 KB).
+    // branch condition is made uniform by a warp vote); the lane elected once
+    // here issues every MMA and commit, so that its commits cover its MMAs.
+    // One elect for the kernel, not one per MMA: a warp-collective
+    // instruction per MMA slowed the generator warps sharing this warp's
+    // sub-partition by a fifth.  The hi/lo amplitude rows sit one above the
+    // other in each B stage, so one MMA with N = bRows computes both products
+    // into 2*nmcPad accumulator columns; the epilogue adds the halves.
+    // Descriptors are advanced by plain adds of the start address field (it
+    // cannot overflow: shared memory is below 256 KB).
+    const bool leader = elect_one();
     const uint32_t idesc = make_idesc(PREC == PREC_FP16 ? 0u : 1u, 128u, (uint32_t)P.bRows);
     const uint32_t lbo = (uint32_t)P.bRows * 16u, sbo = 128u;
     const uint64_t desc0 = make_sdesc(smem_u32(sB), lbo, sbo);
@@ -200,32 +205,41 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
         const uint32_t sn = (s + 1 == (uint32_t)S) ? 0u : s + 1;
         const uint32_t phn = (s + 1 == (uint32_t)S) ? ph ^ 1 : ph;
         const bool more = (ch + 1 < nChunks) || (tile + gridDim.x < numTiles);
-        mma_ts_elect(tbase, aBase, d0, idesc, ch != 0 ? 1u : 0u);  // the tile's first MMA overwrites D
+        if (leader) {
+          mma_ts(tbase, aBase, d0, idesc, ch != 0 ? 1u : 0u);  // the tile's first MMA overwrites D
 #pragma unroll
-        for (int j = 1; j < STEPS - 1; ++j) mma_ts_elect(tbase, aBase + 8u * j, d0 + jStep * j, idesc, 1u);
-        // probe the next stage while this stage's last MMA is queued
+          for (int j = 1; j < STEPS - 1; ++j) mma_ts(tbase, aBase + 8u * j, d0 + jStep * j, idesc, 1u);
+        }
+        // probe the next stage while this stage's last MMAs are queued
         ready = __all_sync(0xffffffffu, more && mbar_test_wait(&bars->full[sn], phn));
-        mma_ts_elect(tbase, aBase + 8u * (STEPS - 1), d0 + jStep * (STEPS - 1), idesc, 1u);
-        mma_commit_elect(&bars->empty[s]);
+        if (leader) {
+          mma_ts(tbase, aBase + 8u * (STEPS - 1), d0 + jStep * (STEPS - 1), idesc, 1u);
+          mma_commit(&bars->empty[s]);
+        }
+        __syncwarp();
         s = sn;
         ph = phn;
       }
       if (!ok) break;
-      mma_commit_elect(&bars->acc_full);
+      if (leader) mma_commit(&bars->acc_full);
+      __syncwarp();
       accPh ^= 1;
     }
     if (!ok && lane == 0) raise_abort(bars, a.err);
     // Drain every MMA the elected lane issued before TMEM is released.
-    mma_commit_elect(&bars->done);
+    if (leader) mma_commit(&bars->done);
+    __syncwarp();
     volatile int never = 0;
     mbar_wait(&bars->done, 0, &never);
     __syncwarp();
   } else {
     // ------------------------------------------------- generators + epilogue
-    const int q = warp & 3, h = warp >> 2;
+    // TMEM lane quarter = warp % 4 (the sub-partition's lanes); the two
+    // generator warps of each quarter take the two column halves.
+    const int q = warp & 3, h = (warp - kGenWarp0) >> 2;
     const int row = q * 32 + lane;
     const uint32_t laneOff = (uint32_t)(q * 32) << 16;
-    uint32_t s = 0, ph = 0, accPh = 0, ePh = 0;
+    uint32_t s = 0, ph = 0, accPh = 0;
     bool ok = true;
     for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
       const int64_t p = a.row0 + tile * kTileM + row;
@@ -238,35 +252,26 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
       }
 
       Grid3Thread g3;
+      Grid3Walk walk;
       if (GEN == GEN_GRID3) {
         grid3_thread_setup<LPAD>(g3, P, h, x);
-        // The shared axis-1/axis-2 phasor table is rewritten per tile: every
-        // generator warp first declares it is done with the previous tile's
-        // table, then writes its part (half 0: axis 1, half 1: axis 2), then
-        // all read.  Bounded mbarrier rendezvous, not named barriers, so that
-        // an aborting warp cannot leave the others blocked.
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&bars->e12_free);
-        if (!mbar_wait_warp(&bars->e12_free, ePh, abort_flag)) { ok = false; break; }
-        if (h == 0) {
-          for (int i = 0; i < P.kNStep[0]; ++i) e12[i * kTileM + row] = axis_phasor(P.kDelta[0], i, x[0]);
-        } else {
-          for (int i = 0; i < P.kNStep[1]; ++i) e12[(P.kNStep[0] + i) * kTileM + row] = axis_phasor(P.kDelta[1], i, x[1]);
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&bars->e12_ready);
-        if (!mbar_wait_warp(&bars->e12_ready, ePh, abort_flag)) { ok = false; break; }
-        ePh ^= 1;
+        walk.init(P, x);
       }
 
-      Grid3Outer outer;
+      // A full barrier wait costs a warp a couple of hundred cycles even when
+      // the phase is already complete, so lane 0 probes the next stage's
+      // slot at the start of the current stage and the answer is read after
+      // the stage's work; the wait proper runs only when the probe failed.
+      bool freeSeen = false;
       for (int64_t ch = 0; ch < nChunks; ++ch) {
         const uint32_t sc = s, phc = ph;
         if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
-        bool w = mbar_wait_warp(&bars->empty[sc], phc ^ 1, abort_flag);
+        bool w = freeSeen || mbar_wait_warp(&bars->empty[sc], phc ^ 1, abort_flag);
         if (GEN == GEN_TABLE) w = w && mbar_wait_warp(&bars->kfull[sc], phc, abort_flag, true);
         if (!w) { ok = false; break; }
         tc_fence_after();
+        uint32_t probe = 0;
+        if (lane == 0 && ch + 1 < nChunks) probe = mbar_test_wait(&bars->empty[s], ph ^ 1) ? 1u : 0u;
         const uint32_t aAddr = tbase + laneOff + aCol0 + sc * aStride;
         if (GEN == GEN_GRID3) {
 #pragma unroll
@@ -275,8 +280,8 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
             auto emit = [&](int idx, float c, float sn) {
               words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
             };
-            const float2 Pq = grid3_outer(P, e12, row, outer);
-            outer.next(P.kNStep[0], P.kNStep[1]);
+            const float2 Pq = walk.outer();
+            walk.next(P, x);
             grid3_pairs<LPAD>(g3, Pq, emit);
             // LPAD is a multiple of 8: every store covers 8 columns at an
             // 8-aligned column offset.
@@ -294,6 +299,7 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
           tmem_st8(col, &words[0]);
           tmem_st8(col + 8, &words[8]);
         }
+        freeSeen = __shfl_sync(0xffffffffu, probe, 0) != 0;
         tmem_st_wait();
         tc_fence_before();
         __syncwarp();
@@ -358,7 +364,6 @@ cudaError_t launch_prec(const Plan& P, const TcArgs& args, size_t smem, int grid
 }  // namespace
 
 size_t tc_smem_bytes(const Plan& P, int* stages) {
-  const size_t e12 = (P.gen == GEN_GRID3) ? (size_t)(P.kNStep[0] + P.kNStep[1]) * kTileM * sizeof(float2) : 0;
   const size_t perStage = (size_t)P.stageBytes + (P.gen == GEN_TABLE ? kKtabStageBytes : 0);
   const size_t limit = 227 * 1024;
   // A stages live in TMEM after the bRows accumulator columns
@@ -368,7 +373,7 @@ size_t tc_smem_bytes(const Plan& P, int* stages) {
   // an SM: asking for more than half of the SM's shared memory guarantees it.
   const size_t floor = 120 * 1024;
   for (int s = maxS; s >= 2; --s) {
-    const size_t total = kHeaderBytes + s * perStage + e12;
+    const size_t total = kHeaderBytes + s * perStage;
     if (total <= limit) {
       if (stages) *stages = s;
       return total < floor ? floor : total;
