@@ -140,6 +140,49 @@ int rf_context_set_timing(rf_context* ctx, int enable);
 int rf_context_last_times(rf_context* ctx, double* tables_ms, double* contract_ms, double* post_ms,
                           int32_t* kernel_launches);
 
+/*
+ * Batches.  No counterpart in the reference, whose driver (sample_RF.f90,
+ * single_realization :348) generates one field per call; these entry points
+ * generate many independent requests in one grouped launch: a persistent
+ * tcgen05 kernel whose CTAs run (request realization block, 128-point tile)
+ * work items of all requests, balanced across the SMs, replayed from a
+ * captured CUDA graph.  Each request carries the arguments of
+ * rf_create_standard_gaussian_field_unstruct; its field equals the single-call
+ * field within the precision form's tolerance.  Tensor-core forms only (the
+ * plain FP32 form runs request by request); literal mode is not supported in
+ * a batch (RF_ENOTSUP).  The realization block of the grouped launch is
+ * chosen by a tuner on the first batch of each precision form (every
+ * candidate computes the same field).
+ */
+typedef struct rf_request {
+  const double* xPoints;  /* nDim x n: host memory (rf_generate_batch) or device memory (_device) */
+  double* randField;      /* n x Nmc, the same kind of memory */
+  int64_t n;
+  int32_t nDim, corrMod, margiFirst, Nmc, method;
+  int32_t reserved0;
+  double corrL[3];
+  double fieldAvg, fieldVar;
+  rf_options opt;         /* precision and device must agree across a batch */
+} rf_request;
+
+typedef struct rf_batch_stats {
+  double tables_ms;           /* device time of the grouped table build */
+  double contract_ms;         /* device time of the grouped contraction */
+  int64_t units;              /* realization blocks of all requests */
+  int64_t work_items;         /* (unit, tile) items */
+  int32_t realization_block;  /* chosen by the tuner */
+  int32_t stages;             /* pipeline depth of the grouped kernel */
+  int32_t graph_replayed;     /* 1: the launch replayed a captured CUDA graph */
+  int32_t tuned;              /* 1: this call ran the tuner */
+} rf_batch_stats;
+
+/* Host buffers; returns when every field has been copied back. */
+int rf_generate_batch(rf_context* ctx, const rf_request* reqs, int32_t count);
+/* Device buffers; queued on `stream` (0 = the context's stream). */
+int rf_generate_batch_device(rf_context* ctx, const rf_request* reqs, int32_t count, void* stream);
+/* Statistics of the last batch on the context (waits for it). */
+int rf_batch_last_stats(rf_context* ctx, rf_batch_stats* out);
+
 /* Problem geometry exactly as the generator will use it (host only, no GPU):
  * K wavevectors, kNStep, kDelta, ampMult (randomFieldND.f90:260-266). */
 int rf_query_geometry(const double* xPoints, int nDim, int64_t n, int corrMod,

@@ -19,7 +19,8 @@ import numpy as np
 
 __all__ = [
     "RandomFieldError", "Options", "Context", "lib", "create_standard_gaussian_field_unstruct",
-    "query_geometry", "generate_device_noalloc", "ISOTROPIC", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
+    "query_geometry", "generate_device_noalloc", "Request", "BatchStats", "make_request", "generate_batch",
+    "ISOTROPIC", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
     "PREC_BF16", "PREC_FP16", "PREC_FP32", "PREC_BF16_FAST", "LIB_PATH", "STATUS",
 ]
 
@@ -48,6 +49,7 @@ EXPORTS = [
     "rf_options_init", "rf_create_standard_gaussian_field_unstruct", "rf_context_create", "rf_context_destroy",
     "rf_generate_device", "rf_context_synchronize", "rf_query_geometry", "rf_last_error", "rf_abi_version",
     "rf_context_set_timing", "rf_context_last_times", "rf_generate_device_noalloc",
+    "rf_generate_batch", "rf_generate_batch_device", "rf_batch_last_stats",
 ]
 
 
@@ -95,6 +97,44 @@ class Options(C.Structure):
         return o
 
 
+class Request(C.Structure):
+    """rf_request (include/randomfield_b200.h): one request of a batch."""
+
+    _fields_ = [
+        ("xPoints", C.c_void_p),
+        ("randField", C.c_void_p),
+        ("n", C.c_int64),
+        ("nDim", C.c_int32),
+        ("corrMod", C.c_int32),
+        ("margiFirst", C.c_int32),
+        ("Nmc", C.c_int32),
+        ("method", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("corrL", C.c_double * 3),
+        ("fieldAvg", C.c_double),
+        ("fieldVar", C.c_double),
+        ("opt", Options),
+    ]
+
+
+class BatchStats(C.Structure):
+    """rf_batch_stats: the last grouped launch of a context."""
+
+    _fields_ = [
+        ("tables_ms", C.c_double),
+        ("contract_ms", C.c_double),
+        ("units", C.c_int64),
+        ("work_items", C.c_int64),
+        ("realization_block", C.c_int32),
+        ("stages", C.c_int32),
+        ("graph_replayed", C.c_int32),
+        ("tuned", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -123,6 +163,9 @@ def lib() -> C.CDLL:
                                                  P(Options), C.c_void_p]
         L.rf_query_geometry.argtypes = [P(d), i32, i64, i32, P(d), i32, P(Options), P(i64), P(C.c_int32), P(d),
                                         P(d)]
+        L.rf_generate_batch.argtypes = [C.c_void_p, P(Request), C.c_int32]
+        L.rf_generate_batch_device.argtypes = [C.c_void_p, P(Request), C.c_int32, C.c_void_p]
+        L.rf_batch_last_stats.argtypes = [C.c_void_p, P(BatchStats)]
         _lib = L
     return _lib
 
@@ -219,6 +262,43 @@ def generate_device_noalloc(d_x, nDim, n, corrMod, margiFirst, corrL, fieldAvg, 
                                             int(Nmc), int(method), C.c_void_p(ptr(d_out)), C.byref(o), C.c_void_p(s)))
 
 
+def make_request(xPoints, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, randField,
+                 options=None, **kw) -> Request:
+    """An rf_request over buffers the caller keeps alive until the batch
+    returns: ``xPoints``/``randField`` are device pointers (ints or objects
+    with ``data_ptr()``) for the device batch, or numpy arrays (nDim x n and
+    Fortran-ordered n x Nmc float64) for the host batch."""
+    r = Request()
+    if isinstance(xPoints, np.ndarray):
+        if xPoints.dtype != np.float64 or not xPoints.flags.f_contiguous:
+            raise RandomFieldError(-9, "xPoints must be a Fortran-ordered float64 nDim x n array")
+        nDim, n = xPoints.shape
+        if (randField.dtype != np.float64 or not randField.flags.f_contiguous
+                or randField.shape != (n, int(Nmc))):
+            raise RandomFieldError(-9, "randField must be a Fortran-ordered float64 n x Nmc array")
+        r.xPoints, r.randField = xPoints.ctypes.data, randField.ctypes.data
+    else:
+        nDim, n = kw.pop("nDim"), kw.pop("n")
+        r.xPoints, r.randField = Context._ptr(xPoints), Context._ptr(randField)
+    r.n, r.nDim = int(n), int(nDim)
+    r.corrMod = _id(corrMod, _CORRMOD, "corrMod")
+    r.margiFirst = _id(margiFirst, _MARGI, "margiFirst")
+    cl = list(np.asarray(corrL, dtype=np.float64).reshape(-1))
+    for i in range(3):
+        r.corrL[i] = float(cl[i]) if i < len(cl) else 1.0
+    r.fieldAvg, r.fieldVar = float(fieldAvg), float(fieldVar)
+    r.Nmc, r.method = int(Nmc), int(method)
+    r.opt = _opts(options if options is not None else (kw or None))
+    return r
+
+
+def generate_batch(ctx: "Context", requests) -> None:
+    """rf_generate_batch: host-buffer requests (see :func:`make_request`),
+    one grouped launch; returns when every randField is filled."""
+    arr = (Request * len(requests))(*requests)
+    _check(lib().rf_generate_batch(ctx._h, arr, len(requests)))
+
+
 class Context:
     """rf_context: device-resident generation on a CUDA stream.
 
@@ -264,6 +344,17 @@ class Context:
 
     def set_timing(self, enable: bool = True) -> None:
         _check(lib().rf_context_set_timing(self._h, int(bool(enable))))
+
+    def generate_batch_device(self, requests, stream=0) -> None:
+        """rf_generate_batch_device: device-buffer requests, queued on the stream."""
+        s = stream if isinstance(stream, int) else int(getattr(stream, "cuda_stream", 0))
+        arr = (Request * len(requests))(*requests)
+        _check(lib().rf_generate_batch_device(self._h, arr, len(requests), C.c_void_p(s)))
+
+    def batch_stats(self) -> dict:
+        st = BatchStats()
+        _check(lib().rf_batch_last_stats(self._h, C.byref(st)))
+        return st.as_dict()
 
     def last_times(self):
         """(tables_ms, contract_ms, post_ms, kernel_launches) of the last call."""

@@ -1,0 +1,463 @@
+// rf_batch.cu -- batches: many independent requests in one grouped launch.
+//
+// Each request (the arguments of createStandardGaussianFieldUnstruct,
+// README.md:58-92) is planned exactly as a single call (validation, geometry,
+// seeds: rf_host.cu) and split into realization blocks ("units").  Every
+// unit's 128-point tiles become work items; a longest-processing-time-first
+// assignment spreads the items over one persistent CTA per SM, and two
+// kernels run the batch: the grouped table builder and the grouped tcgen05
+// contraction (rf_tc.cu, rf_group_kernel), which picks the generator per tile
+// (GEN_GRID3 for 3-D Shinozuka grids of 24 wavenumbers on the last axis after
+// padding, GEN_TABLE otherwise).  Both kernels read every per-batch quantity
+// from one descriptor buffer in device memory, so the pair is captured once
+// as a CUDA graph per layout and replayed for every later batch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <queue>
+#include <utility>
+#include <vector>
+
+#include "rf_internal.h"
+
+using namespace rfb;
+using namespace rfh;
+
+namespace {
+
+constexpr size_t kAlign = 256;
+size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+
+// Relative device cost of one stage by generator (cycles per stage measured
+// on the 128^3 Shinozuka workload and the 200k-point isotropic config); only
+// the ratio matters, for the balance of the CTAs.
+double stage_cost(const Plan& P) {
+  const double n = (double)P.bRows / 128.0;
+  return P.gen == GEN_GRID3 ? 1130.0 * std::max(0.6, n) : 600.0 * std::max(0.6, n);
+}
+
+struct DescLayout {
+  size_t subs, prefix, cta, items, total;
+  size_t capUnits, capItems;
+};
+
+DescLayout desc_layout(size_t capUnits, size_t capItems, int numSMs) {
+  DescLayout d;
+  d.capUnits = capUnits;
+  d.capItems = capItems;
+  d.subs = kAlign;  // header: the unit count
+  d.prefix = d.subs + align_up(capUnits * sizeof(GroupSub));
+  d.cta = d.prefix + align_up((capUnits + 1) * sizeof(int64_t));
+  d.items = d.cta + align_up((size_t)(numSMs + 1) * sizeof(int32_t));
+  d.total = d.items + align_up(capItems * sizeof(GroupItem));
+  return d;
+}
+
+struct BatchState {
+  std::vector<Plan> plans;         // per request, before the realization split
+  std::vector<const double*> dx;   // device points per request
+  std::vector<double*> dout;       // device fields per request
+};
+
+struct GroupRun {
+  int prec = 0;
+  int rblk = 0;
+  SlotLayout L{};
+  size_t smem = 0;
+  int64_t units = 0, items = 0;
+  bool replayed = false;
+};
+
+// Realization-block candidates of the tuner: the MMA N of a unit is
+// 2*block (BF16 hi/lo) or block; more columns amortise the trig tile over
+// more realizations, fewer waste less on requests with small Nmc.
+std::vector<int> block_candidates(int prec) {
+  if (prec == PREC_BF16) return {64, 32};
+  return {128, 64};
+}
+
+int destroy_graphs(rf_context* c) {
+  for (auto& g : c->graphs) cudaGraphExecDestroy(g.second);
+  c->graphs.clear();
+  return RF_OK;
+}
+
+// Builds the units, operands, schedule and descriptors of one grouped run
+// with realization block `rblk`, and launches it (graph replay when one is
+// cached for the layout).  Timing events bev[0..2] bracket the two kernels.
+int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream_t st, GroupRun& run) {
+  run.prec = prec;
+  run.rblk = rblk;
+  // ---- units
+  std::vector<GroupSub> subs;
+  std::vector<int64_t> elems;
+  std::vector<double> tileCost;
+  std::vector<int64_t> tiles;
+  int32_t maxBRows = 0;
+  int64_t maxStage = 0;
+  size_t arena = 0;
+  for (size_t i = 0; i < B.plans.size(); ++i) {
+    Plan P0 = B.plans[i];
+    if (P0.gen == GEN_GRID3 && P0.lPad != kGroupLPad) P0.forceTable = 1;
+    for (int32_t r0 = 0; r0 < P0.Nmc; r0 += rblk) {
+      Plan P = P0;
+      P.rOff = r0;
+      P.nmcBlk = std::min(rblk, P0.Nmc - r0);
+      if (int rc = layout(P)) return rc;
+      GroupSub g;
+      memset(&g, 0, sizeof(g));
+      g.P = P;
+      g.x = B.dx[i];
+      g.out = B.dout[i];
+      subs.push_back(g);
+      elems.push_back(P.nChunks * P.chunkK * P.nmcPad);
+      tiles.push_back((P.n + kTileM - 1) / kTileM);
+      tileCost.push_back((double)P.nChunks * stage_cost(P));
+      maxBRows = std::max(maxBRows, P.bRows);
+      maxStage = std::max(maxStage, P.stageBytes);
+      arena += align_up((size_t)(P.nChunks * P.stageBytes));
+      if (P.gen == GEN_TABLE) arena += align_up((size_t)P.nChunks * 3 * kTableChunk * sizeof(double));
+    }
+  }
+  const size_t nU = subs.size();
+  run.units = (int64_t)nU;
+  run.smem = group_layout(maxBRows, maxStage, 0, &run.L);
+  if (run.smem == 0) return fail(RF_ENOTSUP, "grouped launch: stages of %lld bytes do not fit", (long long)maxStage);
+
+  // ---- operands in the arena
+  if (int rc = ensure(c->dArena, c->capArena, std::max<size_t>(arena, kAlign), "batch operands")) return rc;
+  size_t off = 0;
+  for (auto& g : subs) {
+    g.B = c->dArena + off;
+    off += align_up((size_t)(g.P.nChunks * g.P.stageBytes));
+    if (g.P.gen == GEN_TABLE) {
+      g.ktab = reinterpret_cast<double*>(c->dArena + off);
+      off += align_up((size_t)g.P.nChunks * 3 * kTableChunk * sizeof(double));
+    }
+  }
+
+  // ---- schedule: LPT over the tiles, longest units first
+  const int nCta = c->numSMs;
+  std::vector<size_t> order(nU);
+  for (size_t u = 0; u < nU; ++u) order[u] = u;
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return tileCost[a] > tileCost[b]; });
+  using Load = std::pair<double, int>;
+  std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+  for (int b = 0; b < nCta; ++b) heap.push({0.0, b});
+  std::vector<std::vector<GroupItem>> perCta(nCta);
+  int64_t nItems = 0;
+  for (size_t u : order) {
+    for (int64_t t = 0; t < tiles[u]; ++t) {
+      Load l = heap.top();
+      heap.pop();
+      perCta[l.second].push_back(GroupItem{(int32_t)u, (int32_t)t});
+      l.first += tileCost[u];
+      heap.push(l);
+    }
+    nItems += tiles[u];
+  }
+  run.items = nItems;
+
+  // ---- descriptors (pinned staging -> device).  Their capacities only
+  // grow, so the offsets inside the buffer stay those of the cached graphs.
+  size_t capU = std::max<size_t>(c->descCapU, 1024), capI = std::max<size_t>(c->descCapI, (size_t)1 << 16);
+  while (capU < nU) capU *= 2;
+  while (capI < (size_t)nItems) capI *= 2;
+  const DescLayout D = desc_layout(capU, capI, nCta);
+  if (capU != c->descCapU || capI != c->descCapI || !c->dDesc) {
+    RF_CUDA(cudaStreamSynchronize(st), "batch sync");
+    destroy_graphs(c);  // the graphs point into the old layout
+    if (c->dDesc) cudaFree(c->dDesc);
+    c->dDesc = nullptr;
+    c->capDesc = 0;
+    if (int rc = ensure(c->dDesc, c->capDesc, D.total, "batch descriptors")) return rc;
+    c->descCapU = capU;
+    c->descCapI = capI;
+  }
+  if (int rc = ensure_host(c->hDesc, c->capHDesc, D.total, "batch descriptor staging")) return rc;
+  RF_CUDA(cudaStreamSynchronize(st), "batch staging sync");  // the staging buffer may still feed a copy
+  unsigned char* h = c->hDesc;
+  *reinterpret_cast<int32_t*>(h) = (int32_t)nU;
+  memcpy(h + D.subs, subs.data(), nU * sizeof(GroupSub));
+  int64_t* pre = reinterpret_cast<int64_t*>(h + D.prefix);
+  pre[0] = 0;
+  for (size_t u = 0; u < nU; ++u) pre[u + 1] = pre[u] + elems[u];
+  int32_t* cta = reinterpret_cast<int32_t*>(h + D.cta);
+  GroupItem* it = reinterpret_cast<GroupItem*>(h + D.items);
+  int32_t pos = 0;
+  for (int b = 0; b < nCta; ++b) {
+    cta[b] = pos;
+    memcpy(it + pos, perCta[b].data(), perCta[b].size() * sizeof(GroupItem));
+    pos += (int32_t)perCta[b].size();
+  }
+  cta[nCta] = pos;
+  RF_CUDA(cudaMemcpyAsync(c->dDesc, h, D.items + (size_t)nItems * sizeof(GroupItem), cudaMemcpyHostToDevice, st),
+          "batch descriptor copy");
+
+  // ---- launch: tables, contraction (graph per layout)
+  GroupArgs g;
+  g.subs = reinterpret_cast<const GroupSub*>(c->dDesc + D.subs);
+  g.items = reinterpret_cast<const GroupItem*>(c->dDesc + D.items);
+  g.ctaStart = reinterpret_cast<const int32_t*>(c->dDesc + D.cta);
+  g.err = c->dErr;
+  g.L = run.L;
+  const GroupSub* dSubs = g.subs;
+  const int64_t* dPrefix = reinterpret_cast<const int64_t*>(c->dDesc + D.prefix);
+  const int32_t* dCount = reinterpret_cast<const int32_t*>(c->dDesc);
+  for (auto& e : c->bev)
+    if (!e) RF_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+  RF_CUDA(group_set_smem(prec, run.smem), "grouped kernel attributes");
+  rf_context::GraphKey key{prec, run.L.S, run.L.aCol0, run.L.slotBytes, c->dDesc};
+  auto found = c->graphs.find(key);
+  cudaGraphExec_t exec = nullptr;
+  if (found != c->graphs.end()) {
+    exec = found->second;
+    run.replayed = true;
+  } else {
+    cudaGraph_t graph = nullptr;
+    RF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture");
+    cudaError_t e1 = cudaEventRecordWithFlags(c->bev[0], st, cudaEventRecordExternal);
+    cudaError_t e2 = launch_group_tables(dSubs, dPrefix, dCount, jump_table(), nCta * 8, st);
+    cudaError_t e3 = cudaEventRecordWithFlags(c->bev[1], st, cudaEventRecordExternal);
+    cudaError_t e4 = launch_group(prec, g, run.smem, nCta, st);
+    cudaError_t e5 = cudaEventRecordWithFlags(c->bev[2], st, cudaEventRecordExternal);
+    cudaError_t ee = cudaStreamEndCapture(st, &graph);
+    for (cudaError_t e : {e1, e2, e3, e4, e5, ee})
+      if (e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return cuda_fail(e, "capture of the grouped launch");
+      }
+    cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate");
+    c->graphs[key] = exec;
+  }
+  RF_CUDA(cudaGraphLaunch(exec, st), "cudaGraphLaunch");
+  c->launches += 2;
+  return RF_OK;
+}
+
+int batch_times(rf_context* c, double* tables, double* contract) {
+  RF_CUDA(cudaEventSynchronize(c->bev[2]), "cudaEventSynchronize");
+  float a = 0, b = 0;
+  RF_CUDA(cudaEventElapsedTime(&a, c->bev[0], c->bev[1]), "cudaEventElapsedTime");
+  RF_CUDA(cudaEventElapsedTime(&b, c->bev[1], c->bev[2]), "cudaEventElapsedTime");
+  *tables = a;
+  *contract = b;
+  return RF_OK;
+}
+
+// Plans every request (extents from `ext`), then runs the grouped launch,
+// tuning the realization block on the first batch of a precision form.
+int run_batch(rf_context* c, const rf_request* reqs, int32_t count, const std::vector<Request>& rq,
+              const std::vector<double>& ext, BatchState& B, cudaStream_t st) {
+  const int prec = rq[0].opt.precision;
+  B.plans.resize(count);
+  for (int32_t i = 0; i < count; ++i)
+    if (int rc = build_plan(rq[i], &ext[3 * i], B.plans[i])) return rc;
+  (void)reqs;
+  GroupRun run;
+  rf_batch_stats stats{};
+  if (c->tunedBlock[prec] == 0) {
+    double best = 1e300;
+    int bestBlk = 0;
+    for (int blk : block_candidates(prec)) {
+      GroupRun r;
+      if (int rc = group_run(c, B, prec, blk, st, r)) return rc;
+      double t = 0, k = 0;
+      if (int rc = batch_times(c, &t, &k)) return rc;
+      if (t + k < best) {
+        best = t + k;
+        bestBlk = blk;
+      }
+    }
+    c->tunedBlock[prec] = bestBlk;
+    stats.tuned = 1;
+  }
+  if (int rc = group_run(c, B, prec, c->tunedBlock[prec], st, run)) return rc;
+  stats.units = run.units;
+  stats.work_items = run.items;
+  stats.realization_block = run.rblk;
+  stats.stages = run.L.S;
+  stats.graph_replayed = run.replayed ? 1 : 0;
+  // normalisation passes (per request, after the contraction)
+  for (int32_t i = 0; i < count; ++i) {
+    const Plan& P = B.plans[i];
+    if (!P.normalize) continue;
+    if ((size_t)2 * P.Nmc * sizeof(double) > c->capWork)
+      if (int rc = ensure(c->dWork, c->capWork, (size_t)2 * P.Nmc * sizeof(double), "moments")) return rc;
+    RF_CUDA(launch_normalize_and_map(P, B.dout[i], P.Nmc, c->dWork, st), "normalisation kernels");
+    c->launches += 3;
+  }
+  c->last = stats;
+  return RF_OK;
+}
+
+int check_batch(const rf_request* reqs, int32_t count, std::vector<Request>& rq) {
+  if (!reqs || count < 1) return fail(RF_EINVAL_ARG, "empty batch");
+  rq.resize(count);
+  for (int32_t i = 0; i < count; ++i) {
+    const rf_request& r = reqs[i];
+    if (!r.xPoints || !r.randField) return fail(RF_EINVAL_ARG, "request %d: null pointer", i);
+    rq[i] = make_request(r.nDim, r.n, r.corrMod, r.margiFirst, r.corrL, r.fieldAvg, r.fieldVar, r.Nmc, r.method,
+                         &r.opt);
+    if (int rc = validate(rq[i])) return fail(rc, "request %d: %s", i, g_err.c_str());
+    if (rq[i].opt.precision != rq[0].opt.precision)
+      return fail(RF_EINVAL_ARG, "request %d: all requests of a batch need the same precision form", i);
+    if (rq[i].opt.device != rq[0].opt.device)
+      return fail(RF_EINVAL_ARG, "request %d: all requests of a batch need the same device", i);
+    if (rq[i].opt.literal) return fail(RF_ENOTSUP, "request %d: literal mode is not available in a batch", i);
+  }
+  return RF_OK;
+}
+
+bool needs_extent(const Request& r) {
+  for (int d = 0; d < r.nDim; ++d)
+    if (!(r.opt.x_range[d] > 0.0)) return true;
+  return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rf_generate_batch(rf_context* ctx, const rf_request* reqs, int32_t count) {
+  g_err.clear();
+  if (!ctx) return fail(RF_EINVAL_ARG, "null context");
+  std::vector<Request> rq;
+  if (int rc = check_batch(reqs, count, rq)) return rc;
+  if (rq[0].opt.precision == RF_PREC_FP32) {
+    // the plain form has no grouped kernel: request by request
+    for (int32_t i = 0; i < count; ++i) {
+      const rf_request& r = reqs[i];
+      rf_options o = rq[i].opt;
+      if (int rc = rf_create_standard_gaussian_field_unstruct(r.xPoints, r.nDim, r.n, r.corrMod, r.margiFirst, r.corrL,
+                                                              r.fieldAvg, r.fieldVar, r.Nmc, r.method, r.randField,
+                                                              &o))
+        return rc;
+    }
+    return RF_OK;
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  cudaStream_t st = ctx->stream;
+  ctx->launches = 0;
+  // host extents, arena for points and fields after the operands
+  std::vector<double> ext(3 * count, 0.0);
+  size_t io = 0;
+  for (int32_t i = 0; i < count; ++i) {
+    const rf_request& r = reqs[i];
+    if (needs_extent(rq[i]))
+      for (int d = 0; d < r.nDim; ++d) {
+        double lo = r.xPoints[d], hi = r.xPoints[d];
+        for (int64_t k = 1; k < r.n; ++k) {
+          lo = std::min(lo, r.xPoints[k * r.nDim + d]);
+          hi = std::max(hi, r.xPoints[k * r.nDim + d]);
+        }
+        ext[3 * i + d] = hi - lo;
+      }
+    io += align_up(sizeof(double) * (size_t)r.n * r.nDim) + align_up(sizeof(double) * (size_t)r.n * r.Nmc);
+  }
+  if (int rc = ensure(ctx->dX, ctx->capX, io, "batch points and fields")) return rc;
+  BatchState B;
+  B.dx.resize(count);
+  B.dout.resize(count);
+  unsigned char* base = reinterpret_cast<unsigned char*>(ctx->dX);
+  size_t off = 0;
+  for (int32_t i = 0; i < count; ++i) {
+    const rf_request& r = reqs[i];
+    const size_t xb = sizeof(double) * (size_t)r.n * r.nDim, ob = sizeof(double) * (size_t)r.n * r.Nmc;
+    B.dx[i] = reinterpret_cast<double*>(base + off);
+    off += align_up(xb);
+    B.dout[i] = reinterpret_cast<double*>(base + off);
+    off += align_up(ob);
+    RF_CUDA(cudaMemcpyAsync(const_cast<double*>(B.dx[i]), r.xPoints, xb, cudaMemcpyHostToDevice, st),
+            "copy of xPoints");
+  }
+  if (int rc = run_batch(ctx, reqs, count, rq, ext, B, st)) return rc;
+  for (int32_t i = 0; i < count; ++i) {
+    const rf_request& r = reqs[i];
+    RF_CUDA(cudaMemcpyAsync(r.randField, B.dout[i], sizeof(double) * (size_t)r.n * r.Nmc, cudaMemcpyDeviceToHost,
+                            st),
+            "copy of randField");
+  }
+  RF_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  return check_device_error(ctx);
+}
+
+int rf_generate_batch_device(rf_context* ctx, const rf_request* reqs, int32_t count, void* stream) {
+  g_err.clear();
+  if (!ctx) return fail(RF_EINVAL_ARG, "null context");
+  std::vector<Request> rq;
+  if (int rc = check_batch(reqs, count, rq)) return rc;
+  if (rq[0].opt.precision == RF_PREC_FP32) {
+    for (int32_t i = 0; i < count; ++i) {
+      const rf_request& r = reqs[i];
+      rf_options o = rq[i].opt;
+      if (int rc = rf_generate_device(ctx, r.xPoints, r.nDim, r.n, r.corrMod, r.margiFirst, r.corrL, r.fieldAvg,
+                                      r.fieldVar, r.Nmc, r.method, r.randField, &o, stream))
+        return rc;
+    }
+    return RF_OK;
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
+  ctx->launches = 0;
+  // device extents: one reduction per request that needs it, one copy back
+  std::vector<double> ext(3 * count, 0.0);
+  int32_t nx = 0;
+  for (int32_t i = 0; i < count; ++i) nx += needs_extent(rq[i]) ? 1 : 0;
+  if (nx > 0) {
+    const size_t per = (size_t)6 * kExtentBlocks;
+    if (int rc = ensure(ctx->dExt, ctx->capExt, sizeof(double) * per * nx, "batch extents")) return rc;
+    if (int rc = ensure_host(ctx->hExt, ctx->capHExt, sizeof(double) * per * nx, "batch extents")) return rc;
+    int32_t k = 0;
+    for (int32_t i = 0; i < count; ++i)
+      if (needs_extent(rq[i])) launch_extent(reqs[i].xPoints, reqs[i].n, reqs[i].nDim, ctx->dExt + per * k++, st);
+    RF_CUDA(cudaGetLastError(), "extent kernels");
+    ctx->launches += nx;
+    RF_CUDA(cudaMemcpyAsync(ctx->hExt, ctx->dExt, sizeof(double) * per * nx, cudaMemcpyDeviceToHost, st),
+            "extent copy");
+    RF_CUDA(cudaStreamSynchronize(st), "extent sync");
+    k = 0;
+    for (int32_t i = 0; i < count; ++i) {
+      if (!needs_extent(rq[i])) continue;
+      const double* part = ctx->hExt + per * k++;
+      for (int d = 0; d < reqs[i].nDim; ++d) {
+        double lo = INFINITY, hi = -INFINITY;
+        for (int b = 0; b < kExtentBlocks; ++b) {
+          lo = std::min(lo, part[b * 6 + d]);
+          hi = std::max(hi, part[b * 6 + 3 + d]);
+        }
+        ext[3 * i + d] = hi - lo;
+      }
+    }
+  }
+  BatchState B;
+  B.dx.resize(count);
+  B.dout.resize(count);
+  for (int32_t i = 0; i < count; ++i) {
+    B.dx[i] = reqs[i].xPoints;
+    B.dout[i] = reqs[i].randField;
+  }
+  return run_batch(ctx, reqs, count, rq, ext, B, st);
+}
+
+int rf_batch_last_stats(rf_context* ctx, rf_batch_stats* out) {
+  g_err.clear();
+  if (!ctx || !out) return fail(RF_EINVAL_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  *out = ctx->last;
+  if (ctx->bev[2]) {
+    if (int rc = batch_times(ctx, &out->tables_ms, &out->contract_ms)) return rc;
+  }
+  return RF_OK;
+}
+
+}  // extern "C"

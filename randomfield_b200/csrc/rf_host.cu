@@ -17,13 +17,14 @@
 
 #include "../../include/randomfield_b200.h"
 #include "rf_device.cuh"
+#include "rf_internal.h"
 #include "rf_launch.h"
 #include "rf_plan.h"
 
 using namespace rfb;
 
 // ------------------------------------------------------------------ errors
-namespace {
+namespace rfh {
 thread_local std::string g_err;
 
 int fail(int code, const char* fmt, ...) {
@@ -42,12 +43,6 @@ int cuda_fail(cudaError_t e, const char* where) {
     return fail(RF_ENODEV, "%s: %s", where, cudaGetErrorString(e));
   return fail(RF_ECUDA, "%s: %s", where, cudaGetErrorString(e));
 }
-
-#define RF_CUDA(call, where)                   \
-  do {                                         \
-    cudaError_t e_ = (call);                   \
-    if (e_ != cudaSuccess) return cuda_fail(e_, where); \
-  } while (0)
 
 // rnglib jump table: a^(2^j) mod m (rnglib.f90:548-659 multipliers).
 const JumpTable& jump_table() {
@@ -70,15 +65,6 @@ const JumpTable& jump_table() {
 double kmax_nd(int nDim) { return nDim == 1 ? 6.457 : (nDim == 2 ? 7.035 : 7.355); }
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
-
-struct Request {
-  int nDim;
-  int64_t n;
-  int corrMod, margiFirst, Nmc, method;
-  double corrL[3];
-  double fieldAvg, fieldVar;
-  rf_options opt;
-};
 
 // type_inputRF.f90:1159-1206, randomFieldND.f90:162-166, constants_RF.f90:12-21
 int validate(const Request& r) {
@@ -183,7 +169,7 @@ int seeds(int64_t seedStart, Plan& P) {
 int layout(Plan& P) {
   const bool tc = P.prec != PREC_FP32;
   P.gen = GEN_TABLE;
-  if (P.method == RF_SHINOZUKA && P.nDim == 3 && !P.literal && P.kNStep[0] <= kMaxGridN &&
+  if (P.method == RF_SHINOZUKA && P.nDim == 3 && !P.literal && !P.forceTable && P.kNStep[0] <= kMaxGridN &&
       P.kNStep[1] <= kMaxGridN && P.kNStep[2] <= kMaxGridN)
     P.gen = GEN_GRID3;
   if (P.gen == GEN_GRID3) {
@@ -192,13 +178,11 @@ int layout(Plan& P) {
     // columns): more MMAs per barrier wait of the issuing thread.  The number
     // of groups, n1*n2*2, is always even.
     P.gps = (tc && 4 * P.lPad <= kMaxStageCols) ? 2 : 1;
-    P.teams = 1;  // a second generator team measured slower (it competes with the MMA issuer)
     P.chunkK = 2 * P.lPad * P.gps;
     P.nChunks = (int64_t)P.kNStep[0] * P.kNStep[1] * 2 / P.gps;
   } else {
     P.lPad = 0;
     P.gps = 1;
-    P.teams = 1;
     P.chunkK = kTableChunk;
     P.nChunks = (P.K + kTableChunk - 1) / kTableChunk;
   }
@@ -285,52 +269,7 @@ __global__ void rf_extent_kernel(const double* __restrict__ x, int64_t n, int nD
     }
 }
 
-}  // namespace
-
 // ---------------------------------------------------------------- context
-struct rf_context {
-  int device = 0;
-  int numSMs = 0;
-  cudaStream_t stream = nullptr;
-  std::mutex mu;
-  void* dB = nullptr;
-  size_t capB = 0;
-  double* dKtab = nullptr;
-  size_t capK = 0;
-  double* dWork = nullptr;  // extent partials and moments
-  size_t capWork = 0;
-  double* hWork = nullptr;  // pinned mirror of dWork
-  uint32_t* dErr = nullptr;
-  double* dX = nullptr;     // flat API staging of the points
-  size_t capX = 0;
-  double* dOut = nullptr;   // flat API result buffer
-  size_t capOut = 0;
-  bool timing = false;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  bool evValid = false;
-  int32_t launches = 0;     // kernels launched by the last generation
-};
-
-namespace {
-
-template <typename T>
-int ensure(T*& p, size_t& cap, size_t bytes, const char* what) {
-  if (bytes <= cap && p) return RF_OK;
-  if (p) cudaFree(p);
-  p = nullptr;
-  cap = 0;
-  void* q = nullptr;
-  cudaError_t e = cudaMalloc(&q, bytes);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return fail(RF_ENOMEM, "cannot allocate %zu bytes of device memory for %s", bytes, what);
-  }
-  p = reinterpret_cast<T*>(q);
-  cap = bytes;
-  return RF_OK;
-}
-
-constexpr int kExtentBlocks = 128;
 
 int context_init(rf_context* c, int device) {
   int count = 0;
@@ -367,12 +306,24 @@ void context_free(rf_context* c) {
   if (c->hWork) cudaFreeHost(c->hWork);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : c->bev)
+    if (e) cudaEventDestroy(e);
+  for (auto& g : c->graphs) cudaGraphExecDestroy(g.second);
+  cudaFree(c->dArena);
+  cudaFree(c->dDesc);
+  cudaFree(c->dExt);
+  if (c->hDesc) cudaFreeHost(c->hDesc);
+  if (c->hExt) cudaFreeHost(c->hExt);
   if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+void launch_extent(const double* dX, int64_t n, int nDim, double* part, cudaStream_t st) {
+  rf_extent_kernel<<<kExtentBlocks, 256, 0, st>>>(dX, n, nDim, part);
 }
 
 // Extent of the device-resident points per axis (needed for xRange).
 int device_extent(rf_context* c, const double* dX, int nDim, int64_t n, cudaStream_t st, double* ext) {
-  rf_extent_kernel<<<kExtentBlocks, 256, 0, st>>>(dX, n, nDim, c->dWork);
+  launch_extent(dX, n, nDim, c->dWork, st);
   RF_CUDA(cudaGetLastError(), "extent kernel");
   ++c->launches;
   RF_CUDA(cudaMemcpyAsync(c->hWork, c->dWork, sizeof(double) * 6 * kExtentBlocks, cudaMemcpyDeviceToHost, st),
@@ -518,7 +469,9 @@ Request make_request(int nDim, int64_t n, int corrMod, int margiFirst, const dou
   return r;
 }
 
-}  // namespace
+}  // namespace rfh
+
+using namespace rfh;
 
 // ------------------------------------------------- planning for other units
 // Thin wrappers over the validation and planning above for entry points

@@ -1,0 +1,143 @@
+// rf_internal.h -- host-side internals shared by the C-ABI translation units
+// (rf_host.cu: single requests; rf_batch.cu: batches and the serving loop).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/randomfield_b200.h"
+#include "rf_device.cuh"
+#include "rf_launch.h"
+#include "rf_plan.h"
+
+// Device state of one context: streams, reusable buffers, timing events,
+// and the grouped-launch state of the batch entry points.
+struct rf_context {
+  int device = 0;
+  int numSMs = 0;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  void* dB = nullptr;
+  size_t capB = 0;
+  double* dKtab = nullptr;
+  size_t capK = 0;
+  double* dWork = nullptr;  // extent partials and moments
+  size_t capWork = 0;
+  double* hWork = nullptr;  // pinned mirror of dWork
+  uint32_t* dErr = nullptr;
+  double* dX = nullptr;     // flat API staging of the points
+  size_t capX = 0;
+  double* dOut = nullptr;   // flat API result buffer
+  size_t capOut = 0;
+  bool timing = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool evValid = false;
+  int32_t launches = 0;     // kernels launched by the last generation
+
+  // ---- grouped launches (rf_batch.cu)
+  unsigned char* dArena = nullptr;  // operands, and points/fields of host batches
+  size_t capArena = 0;
+  unsigned char* dDesc = nullptr;   // units, prefix, CTA slices, work items
+  size_t capDesc = 0;
+  size_t descCapU = 0, descCapI = 0;  // unit and item capacities of its layout
+  unsigned char* hDesc = nullptr;   // pinned staging of dDesc
+  size_t capHDesc = 0;
+  double* dExt = nullptr;           // extent partials of device batches
+  size_t capExt = 0;
+  double* hExt = nullptr;
+  size_t capHExt = 0;
+  cudaEvent_t bev[3] = {nullptr, nullptr, nullptr};
+  struct GraphKey {
+    int prec, S, aCol0;
+    int64_t slotBytes;
+    const void* desc;
+    bool operator<(const GraphKey& o) const {
+      if (prec != o.prec) return prec < o.prec;
+      if (S != o.S) return S < o.S;
+      if (aCol0 != o.aCol0) return aCol0 < o.aCol0;
+      if (slotBytes != o.slotBytes) return slotBytes < o.slotBytes;
+      return desc < o.desc;
+    }
+  };
+  std::map<GraphKey, cudaGraphExec_t> graphs;
+  int tunedBlock[4] = {0, 0, 0, 0};  // realization block chosen by the tuner, per precision form
+  rf_batch_stats last{};
+};
+
+namespace rfh {
+
+extern thread_local std::string g_err;
+int fail(int code, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* where);
+
+#define RF_CUDA(call, where)                                     \
+  do {                                                           \
+    cudaError_t e_ = (call);                                     \
+    if (e_ != cudaSuccess) return rfh::cuda_fail(e_, where);     \
+  } while (0)
+
+struct Request {
+  int nDim;
+  int64_t n;
+  int corrMod, margiFirst, Nmc, method;
+  double corrL[3];
+  double fieldAvg, fieldVar;
+  rf_options opt;
+};
+
+constexpr int kExtentBlocks = 128;
+
+const rfb::JumpTable& jump_table();
+int64_t round_up(int64_t v, int64_t m);
+int validate(const Request& r);
+int layout(rfb::Plan& P);
+int build_plan(const Request& rq, const double* ext, rfb::Plan& P);
+int32_t realization_block(const rfb::Plan& P);
+int device_extent(rf_context* c, const double* dX, int nDim, int64_t n, cudaStream_t st, double* ext);
+int run_plan(rf_context* c, const rfb::Plan& P0, const double* dX, double* dOut, cudaStream_t st);
+int check_device_error(rf_context* c);
+int default_context(int device, rf_context** out);
+Request make_request(int nDim, int64_t n, int corrMod, int margiFirst, const double* corrL, double fieldAvg,
+                     double fieldVar, int Nmc, int method, const rf_options* opt);
+void launch_extent(const double* dX, int64_t n, int nDim, double* part, cudaStream_t st);
+
+// Grows a device buffer to at least `bytes` (contents are not kept).
+template <typename T>
+int ensure(T*& p, size_t& cap, size_t bytes, const char* what) {
+  if (bytes <= cap && p) return RF_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(RF_ENOMEM, "cannot allocate %zu bytes of device memory for %s", bytes, what);
+  }
+  p = reinterpret_cast<T*>(q);
+  cap = bytes;
+  return RF_OK;
+}
+
+// Grows a pinned host buffer to at least `bytes` (contents are not kept).
+template <typename T>
+int ensure_host(T*& p, size_t& cap, size_t bytes, const char* what) {
+  if (bytes <= cap && p) return RF_OK;
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  cap = 0;
+  void* q = nullptr;
+  cudaError_t e = cudaMallocHost(&q, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(RF_ENOMEM, "cannot allocate %zu bytes of pinned host memory for %s", bytes, what);
+  }
+  p = reinterpret_cast<T*>(q);
+  cap = bytes;
+  return RF_OK;
+}
+
+}  // namespace rfh

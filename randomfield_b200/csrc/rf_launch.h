@@ -31,6 +31,32 @@ cudaError_t launch_normalize_and_map(const Plan& P, double* dOut, int32_t ncols,
 // Shared-memory bytes the tcgen05 kernel needs for this plan (0 if it
 // cannot fit).
 size_t tc_smem_bytes(const Plan& P, int* stages);
+
+// Grouped launch (rf_tc.cu): every CTA b runs the work items
+// items[ctaStart[b] .. ctaStart[b+1]) of the units `subs`, all with the
+// shared slot layout L.  GEN_GRID3 units must have lPad == kGroupLPad; the
+// others run GEN_TABLE.
+constexpr int kGroupLPad = 24;
+struct GroupArgs {
+  const GroupSub* subs;
+  const GroupItem* items;
+  const int32_t* ctaStart;
+  uint32_t* err;
+  SlotLayout L;
+};
+// Slot layout for units with at most maxBRows B rows and maxStageBytes per
+// stage, at most maxStages deep; returns the shared-memory bytes (0: none fits).
+size_t group_layout(int32_t maxBRows, int64_t maxStageBytes, int32_t maxStages, SlotLayout* L);
+// Sets the grouped kernel's shared-memory size (outside any stream capture),
+// then launch_group queues it.
+cudaError_t group_set_smem(int prec, size_t smem);
+cudaError_t launch_group(int prec, const GroupArgs& g, size_t smem, int grid, cudaStream_t st);
+
+// Grouped table builder: B (and the wavevector chunks) of every unit; the
+// element range of unit u is [prefix[u], prefix[u+1]) of prefix[*nsubs]
+// (all three in device memory, read when the kernel runs).
+cudaError_t launch_group_tables(const GroupSub* subs, const int64_t* prefix, const int32_t* nsubs,
+                                const JumpTable& jt, int blocks, cudaStream_t st);
 size_t fp32_smem_bytes(const Plan& P);
 
 }  // namespace rfb

@@ -19,6 +19,7 @@ constexpr double kR8Scale = 4.656613057E-10;  // rnglib.f90:1517
 enum Generator : int32_t {
   GEN_TABLE = 0,  // explicit wavevector table, one FP64 phase + SFU sincos per (point, k)
   GEN_GRID3 = 1,  // 3-D tensor-grid wavevectors: per-axis tables and angle addition
+  GEN_MIXED = 2,  // kernel variant only: the generator is chosen per tile (grouped launch)
 };
 
 enum Precision : int32_t { PREC_BF16 = 0, PREC_FP16 = 1, PREC_FP32 = 2, PREC_BF16_FAST = 3 };
@@ -51,7 +52,7 @@ struct Plan {
   int32_t chunkK;             // k-values per stage
   int32_t lPad;               // GEN_GRID3: inner (axis 3) length padded to a multiple of 8
   int32_t gps;                // GEN_GRID3: outer groups (i1, i2, s2) per stage
-  int32_t teams;              // tcgen05 path: generator teams of 8 warps (1 or 2)
+  int32_t forceTable;         // 1: GEN_TABLE even where GEN_GRID3 applies
   int64_t nChunks;            // stages per tile
   int64_t stageBytes;         // bytes of one B stage
   int32_t bScaleLog2;         // FP16: B stored times 2^bScaleLog2
@@ -60,6 +61,34 @@ struct Plan {
   int32_t applyMarginal;      // 0 when a normalisation pass follows
   int32_t lognormal;
   double margSd, margAvg;
+};
+
+// Shared-memory and TMEM slot layout of one tcgen05 launch: B slot s at
+// byte slotBytes*s of the slot area, its wavevector chunk (GEN_TABLE) at
+// ktabOff + s*768, its A tile at TMEM column aCol0 + s*aStride (the
+// accumulator occupies the columns below aCol0).
+struct SlotLayout {
+  int32_t S;
+  int32_t aCol0;
+  int32_t aStride;
+  int32_t ktabOff;
+  int64_t slotBytes;
+};
+
+// One unit of a grouped launch: a request's realization block with its own
+// plan, operands and output (device pointers).
+struct GroupSub {
+  Plan P;
+  const double* x;      // n x nDim points
+  double* out;          // Nmc x n field (realization-major)
+  unsigned char* B;     // contraction operand, nChunks stages
+  double* ktab;         // GEN_TABLE wavevector chunks
+};
+
+// Work item of a grouped launch: tile `tile` (128 points) of unit `sub`.
+struct GroupItem {
+  int32_t sub;
+  int32_t tile;
 };
 
 }  // namespace rfb

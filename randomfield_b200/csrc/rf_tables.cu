@@ -111,10 +111,12 @@ __device__ __forceinline__ int64_t tc_b_offset(int32_t bRows, int32_t row, int32
   return (int64_t)(kel >> 3) * (bRows * 16) + (row >> 3) * 128 + (row & 7) * 16 + (kel & 7) * 2;
 }
 
-__global__ void rf_tables_kernel(const Plan P, const JumpTable jt, void* __restrict__ B, double* __restrict__ ktab,
-                                 int64_t literalSlab, int64_t nSlab) {
+// Element tid = kk * nmcPad + r of the operand: B rows of wavevector kk (in
+// kernel order) for realization column r, and the wavevector itself (r = 0).
+__device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt, void* __restrict__ B,
+                                              double* __restrict__ ktab, int64_t literalSlab, int64_t nSlab,
+                                              int64_t tid) {
   const int64_t total = P.nChunks * P.chunkK;
-  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int r = (int)(tid % P.nmcPad);
   const int64_t kk = tid / P.nmcPad;
   if (kk >= total) return;
@@ -177,6 +179,35 @@ __global__ void rf_tables_kernel(const Plan P, const JumpTable jt, void* __restr
     *reinterpret_cast<__nv_bfloat16*>(b + tc_b_offset(P.bRows, P.nmcPad + r, 2 * c)) = lc;
     *reinterpret_cast<__nv_bfloat16*>(b + tc_b_offset(P.bRows, P.nmcPad + r, 2 * c + 1)) = ls;
   }
+}
+
+__global__ void rf_tables_kernel(const Plan P, const JumpTable jt, void* __restrict__ B, double* __restrict__ ktab,
+                                 int64_t literalSlab, int64_t nSlab) {
+  table_element(P, jt, B, ktab, literalSlab, nSlab, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Grouped builder: a grid-stride loop over the concatenated elements of all
+// units (a fixed grid, so that the launch can sit in a captured graph).
+__global__ void rf_group_tables_kernel(const GroupSub* __restrict__ subs, const int64_t* __restrict__ prefix,
+                                       const int32_t* __restrict__ nsubsPtr, const JumpTable jt) {
+  const int32_t nsubs = *nsubsPtr;
+  const int64_t total = prefix[nsubs];
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int32_t lo = 0, hi = nsubs - 1;  // last unit whose prefix <= t
+    while (lo < hi) {
+      const int32_t mid = (lo + hi + 1) >> 1;
+      if (prefix[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const GroupSub& u = subs[lo];
+    table_element(u.P, jt, u.B, u.ktab, -1, 1, t - prefix[lo]);
+  }
+}
+
+cudaError_t launch_group_tables(const GroupSub* subs, const int64_t* prefix, const int32_t* nsubs,
+                                const JumpTable& jt, int blocks, cudaStream_t st) {
+  rf_group_tables_kernel<<<blocks, 256, 0, st>>>(subs, prefix, nsubs, jt);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_tables(const Plan& P, const JumpTable& jt, void* dB, double* dKtab, int64_t literalSlab,

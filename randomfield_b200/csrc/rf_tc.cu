@@ -7,6 +7,11 @@
 //   D (128 points x Nmc, FP32 in TMEM) += A (128 x 16, trig tile in TMEM)
 //                                         x B (16 x Nmc, amplitude/phase in SMEM)
 //
+// Two launches share one pipeline body: rf_tc_kernel runs the tiles of one
+// request, rf_group_kernel runs a list of (request block, tile) work items of
+// many requests per CTA (the batched and serving forms), choosing the
+// generator per tile.
+//
 // Warp roles (320 threads, one CTA per SM):
 //   warp 0      MMA issuer: the warp runs the stage loop, one elected lane
 //               issues tcgen05.mma kind::f16 (A from TMEM, B by descriptor
@@ -30,7 +35,7 @@
 // 770 cycles; the generators of the three sub-partitions without a service
 // warp need about 750, those sharing a sub-partition with the issuer about
 // 880, which sets the stage period (about 1130 cycles with the barriers).
-// TMEM: accumulator columns [0, bRows), then A stages of chunkK columns.
+// TMEM: accumulator columns [0, aCol0), then the A slots (SlotLayout).
 // Every wait is bounded (globaltimer); on expiry the kernel raises an error
 // word, drains its own async work, frees TMEM and returns.
 #include "rf_device.cuh"
@@ -42,14 +47,14 @@ namespace rfb {
 namespace {
 
 constexpr int kMmaWarp = 0;
-constexpr int kGenWarp0 = 1;   // generators: warps 1-8
+constexpr int kGenWarp0 = 1;  // generators: warps 1-8
 constexpr int kGenWarps = 8;
-constexpr int kTeamWarps = kGenWarps;
 constexpr int kProdWarp = kGenWarp0 + kGenWarps;
 constexpr int kThreads = (kProdWarp + 1) * 32;
 constexpr int kMaxStages = 8;
 constexpr uint32_t kTmemCols = 512;
 constexpr int kKtabStageBytes = 3 * kTableChunk * 8;
+constexpr int kTableSteps = kTableChunk / 8;  // MMAs (K = 16) per GEN_TABLE stage
 
 struct Bars {
   uint64_t full[kMaxStages];   // generators (8 warps) + producer (bytes)
@@ -72,7 +77,56 @@ struct TcArgs {
   double* out;
   uint32_t* err;
   int64_t row0, rows;
-  int stages;
+  SlotLayout L;
+};
+
+// One tile of work as every role sees it.
+struct TileView {
+  const Plan* P;
+  const double* x;
+  double* out;
+  const unsigned char* B;
+  const double* ktab;
+  int64_t row0, rows;  // point range of the request covered by the launch
+  int64_t tile;        // tile (128 points) inside that range
+};
+
+// The tiles blockIdx.x, blockIdx.x + gridDim.x, ... of one request.
+struct SingleWork {
+  const TcArgs* a;
+  int64_t numTiles;
+  __device__ __forceinline__ int64_t count() const {
+    return (int64_t)blockIdx.x < numTiles ? (numTiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  }
+  __device__ __forceinline__ void get(int64_t i, TileView& v) const {
+    v.P = &a->P;
+    v.x = a->x;
+    v.out = a->out;
+    v.B = a->B;
+    v.ktab = a->ktab;
+    v.row0 = a->row0;
+    v.rows = a->rows;
+    v.tile = blockIdx.x + i * gridDim.x;
+  }
+};
+
+// This CTA's slice [ctaStart[b], ctaStart[b+1]) of a grouped work list.
+struct GroupWork {
+  const GroupArgs* g;
+  int64_t begin, end;
+  __device__ __forceinline__ int64_t count() const { return end - begin; }
+  __device__ __forceinline__ void get(int64_t i, TileView& v) const {
+    const GroupItem it = g->items[begin + i];
+    const GroupSub& s = g->subs[it.sub];
+    v.P = &s.P;
+    v.x = s.x;
+    v.out = s.out;
+    v.B = s.B;
+    v.ktab = s.ktab;
+    v.row0 = 0;
+    v.rows = s.P.n;
+    v.tile = it.tile;
+  }
 };
 
 __device__ __forceinline__ void raise_abort(Bars* bars, uint32_t* err) {
@@ -91,31 +145,51 @@ __device__ __forceinline__ double finish_value(const Plan& P, float acc) {
   return v;
 }
 
-// LPAD: GEN_GRID3 axis-3 length padded to 8/16/24/32 (0 for GEN_TABLE).
-template <int GEN, int PREC, int LPAD>
-__global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constant__ TcArgs a) {
-  // MMAs (K = 16) per stage: two groups of 2*LPAD columns, or one table chunk
-  constexpr int STEPS = (GEN == GEN_GRID3) ? LPAD / 2 : kTableChunk / 8;
+// The MMAs of one stage from the elected lane, with the probe of the next
+// stage's full barrier between the last two; returns the probe (warp-uniform).
+template <int STEPS>
+__device__ __forceinline__ bool issue_stage(bool leader, uint32_t tbase, uint32_t aBase, uint64_t d0, uint64_t jStep,
+                                            uint32_t idesc, uint32_t acc0, bool more, uint64_t* fullNext,
+                                            uint32_t phn, uint64_t* emptyBar) {
+  if (leader) {
+    mma_ts(tbase, aBase, d0, idesc, acc0);  // the tile's first MMA overwrites D
+#pragma unroll
+    for (int j = 1; j < STEPS - 1; ++j) mma_ts(tbase, aBase + 8u * j, d0 + jStep * j, idesc, 1u);
+  }
+  const bool ready = __all_sync(0xffffffffu, more && mbar_test_wait(fullNext, phn));
+  if (leader) {
+    mma_ts(tbase, aBase + 8u * (STEPS - 1), d0 + jStep * (STEPS - 1), idesc, 1u);
+    mma_commit(emptyBar);
+  }
+  __syncwarp();
+  return ready;
+}
+
+// The pipeline of one CTA over the work items of `w`.
+// GEN: GEN_TABLE, GEN_GRID3 (axis-3 length padded to LPAD) or GEN_MIXED
+// (chosen per tile; its GEN_GRID3 tiles have lPad == LPAD).
+template <int GEN, int PREC, int LPAD, class Work>
+__device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint32_t* err) {
+  constexpr bool kHasGrid = GEN != GEN_TABLE;
+  constexpr bool kHasTable = GEN != GEN_GRID3;
   extern __shared__ __align__(1024) unsigned char smem[];
-  const Plan& P = a.P;
   Bars* bars = reinterpret_cast<Bars*>(smem);
   unsigned char* sB = smem + kHeaderBytes;
-  double* sK = reinterpret_cast<double*>(sB + (size_t)a.stages * P.stageBytes);
+  double* sK = reinterpret_cast<double*>(sB + L.ktabOff);
   volatile int* abort_flag = &bars->abort_flag;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int S = a.stages;
-  const uint32_t aCol0 = (uint32_t)P.bRows;     // first A column (accumulator below)
-  const uint32_t aStride = (uint32_t)P.chunkK;  // TMEM columns per A stage
+  const int S = L.S;
+  const int64_t count = w.count();
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
-      mbar_init(&bars->full[s], kTeamWarps + 1);
+      mbar_init(&bars->full[s], kGenWarps + 1);
       mbar_init(&bars->kfull[s], 1);
       mbar_init(&bars->empty[s], 1);
     }
     mbar_init(&bars->acc_full, 1);
-    mbar_init(&bars->acc_empty, kTeamWarps);
+    mbar_init(&bars->acc_empty, kGenWarps);
     mbar_init(&bars->done, 1);
     bars->abort_flag = 0;
     mbar_fence_init();
@@ -129,45 +203,48 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
   tc_fence_after();
   const uint32_t tbase = bars->tmem_base;
 
-  const int64_t numTiles = (a.rows + kTileM - 1) / kTileM;
-  const int64_t nChunks = P.nChunks;
-
   if (warp == kProdWarp) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
       uint32_t s = 0, ph = 0;
+      uint32_t ktabSlots = 0;  // slots whose last copy carried a wavevector chunk
       int64_t issued = 0;
-      for (int64_t tile = blockIdx.x; tile < numTiles && !*abort_flag; tile += gridDim.x) {
+      TileView v;
+      for (int64_t i = 0; i < count && !*abort_flag; ++i) {
+        w.get(i, v);
+        const Plan& P = *v.P;
+        const bool table = kHasTable && (GEN == GEN_TABLE || P.gen != GEN_GRID3);
+        const int64_t nChunks = P.nChunks;
         for (int64_t ch = 0; ch < nChunks; ++ch) {
           if (!mbar_wait(&bars->empty[s], ph ^ 1, abort_flag)) {
-            raise_abort(bars, a.err);
+            raise_abort(bars, err);
             break;
           }
           mbar_arrive_expect_tx(&bars->full[s], (uint32_t)P.stageBytes);
-          bulk_g2s(sB + (size_t)s * P.stageBytes, a.B + ch * P.stageBytes, (uint32_t)P.stageBytes, &bars->full[s]);
-          if (GEN == GEN_TABLE) {
+          bulk_g2s(sB + (size_t)s * L.slotBytes, v.B + ch * P.stageBytes, (uint32_t)P.stageBytes, &bars->full[s]);
+          if (table) {
             mbar_arrive_expect_tx(&bars->kfull[s], (uint32_t)kKtabStageBytes);
-            bulk_g2s(sK + s * 3 * kTableChunk, a.ktab + ch * 3 * kTableChunk, kKtabStageBytes, &bars->kfull[s]);
+            bulk_g2s(sK + s * 3 * kTableChunk, v.ktab + ch * 3 * kTableChunk, kKtabStageBytes, &bars->kfull[s]);
+            ktabSlots |= 1u << s;
+          } else {
+            ktabSlots &= ~(1u << s);
           }
           ++issued;
           if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
         }
-        if (*abort_flag) break;
       }
       if (*abort_flag) {
         // Drain: wait (bounded, ignoring the abort flag) for the copies still
-        // in flight so that no bulk copy lands after the CTA exits.  A stage's
-        // copies are done once its kfull phase (table) has completed, and its
-        // B bytes once the full phase could complete: wait on both with the
-        // phase of the last use of each slot.
+        // in flight so that no bulk copy lands after the CTA exits.  A slot's
+        // wavevector copy is done once its kfull phase completes; the B
+        // copies complete_tx on full[s], whose generator arrivals may never
+        // come, so those are waited for by time.
         volatile int never = 0;
-        for (int i = 0; i < S && issued > 0; ++i, --issued) {
+        for (int k = 0; k < S && issued > 0; ++k, --issued) {
           if (s == 0) { s = S; ph ^= 1; }
           --s;
-          if (GEN == GEN_TABLE) mbar_wait(&bars->kfull[s], ph, &never);
+          if (ktabSlots & (1u << s)) mbar_wait(&bars->kfull[s], ph, &never);
         }
-        // the B copies complete_tx on full[s]; the generators' arrivals may
-        // never come, so wait for the transfer by time instead
         const uint64_t t0 = globaltimer_ns();
         while (globaltimer_ns() - t0 < 1000000ull) {
         }
@@ -187,36 +264,36 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
     // Descriptors are advanced by plain adds of the start address field (it
     // cannot overflow: shared memory is below 256 KB).
     const bool leader = elect_one();
-    const uint32_t idesc = make_idesc(PREC == PREC_FP16 ? 0u : 1u, 128u, (uint32_t)P.bRows);
-    const uint32_t lbo = (uint32_t)P.bRows * 16u, sbo = 128u;
-    const uint64_t desc0 = make_sdesc(smem_u32(sB), lbo, sbo);
-    const uint64_t sStep = (uint64_t)(P.stageBytes >> 4);
-    const uint64_t jStep = (uint64_t)((2u * lbo) >> 4);
+    const uint64_t sStep = (uint64_t)(L.slotBytes >> 4);
     uint32_t s = 0, ph = 0, accPh = 0;
     bool ok = true, ready = false;  // ready: full[s] of the next stage already observed
-    for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
+    TileView v;
+    for (int64_t i = 0; i < count && ok; ++i) {
+      w.get(i, v);
+      const Plan& P = *v.P;
+      const bool grid = kHasGrid && (GEN == GEN_GRID3 || P.gen == GEN_GRID3);
+      const uint32_t idesc = make_idesc(PREC == PREC_FP16 ? 0u : 1u, 128u, (uint32_t)P.bRows);
+      const uint32_t lbo = (uint32_t)P.bRows * 16u, sbo = 128u;
+      const uint64_t desc0 = make_sdesc(smem_u32(sB), lbo, sbo);
+      const uint64_t jStep = (uint64_t)((2u * lbo) >> 4);
+      const int64_t nChunks = P.nChunks;
       if (!mbar_wait_warp(&bars->acc_empty, accPh ^ 1, abort_flag)) { ok = false; break; }
       tc_fence_after();
       for (int64_t ch = 0; ch < nChunks; ++ch) {
         if (!ready && !mbar_wait_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
         tc_fence_after();
-        const uint32_t aBase = tbase + aCol0 + s * aStride;
+        const uint32_t aBase = tbase + (uint32_t)L.aCol0 + s * (uint32_t)L.aStride;
         const uint64_t d0 = desc0 + sStep * s;
         const uint32_t sn = (s + 1 == (uint32_t)S) ? 0u : s + 1;
         const uint32_t phn = (s + 1 == (uint32_t)S) ? ph ^ 1 : ph;
-        const bool more = (ch + 1 < nChunks) || (tile + gridDim.x < numTiles);
-        if (leader) {
-          mma_ts(tbase, aBase, d0, idesc, ch != 0 ? 1u : 0u);  // the tile's first MMA overwrites D
-#pragma unroll
-          for (int j = 1; j < STEPS - 1; ++j) mma_ts(tbase, aBase + 8u * j, d0 + jStep * j, idesc, 1u);
-        }
-        // probe the next stage while this stage's last MMAs are queued
-        ready = __all_sync(0xffffffffu, more && mbar_test_wait(&bars->full[sn], phn));
-        if (leader) {
-          mma_ts(tbase, aBase + 8u * (STEPS - 1), d0 + jStep * (STEPS - 1), idesc, 1u);
-          mma_commit(&bars->empty[s]);
-        }
-        __syncwarp();
+        const bool more = (ch + 1 < nChunks) || (i + 1 < count);
+        const uint32_t acc0 = ch != 0 ? 1u : 0u;
+        if (kHasGrid && grid)
+          ready = issue_stage<(LPAD > 0 ? LPAD / 2 : 2)>(leader, tbase, aBase, d0, jStep, idesc, acc0, more,
+                                                           &bars->full[sn], phn, &bars->empty[s]);
+        else
+          ready = issue_stage<kTableSteps>(leader, tbase, aBase, d0, jStep, idesc, acc0, more, &bars->full[sn], phn,
+                                           &bars->empty[s]);
         s = sn;
         ph = phn;
       }
@@ -225,7 +302,7 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
       __syncwarp();
       accPh ^= 1;
     }
-    if (!ok && lane == 0) raise_abort(bars, a.err);
+    if (!ok && lane == 0) raise_abort(bars, err);
     // Drain every MMA the elected lane issued before TMEM is released.
     if (leader) mma_commit(&bars->done);
     __syncwarp();
@@ -241,19 +318,24 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
     const uint32_t laneOff = (uint32_t)(q * 32) << 16;
     uint32_t s = 0, ph = 0, accPh = 0;
     bool ok = true;
-    for (int64_t tile = blockIdx.x; tile < numTiles && ok; tile += gridDim.x) {
-      const int64_t p = a.row0 + tile * kTileM + row;
-      const bool valid = (p < a.row0 + a.rows);
+    TileView v;
+    for (int64_t i = 0; i < count && ok; ++i) {
+      w.get(i, v);
+      const Plan& P = *v.P;
+      const bool grid = kHasGrid && (GEN == GEN_GRID3 || P.gen == GEN_GRID3);
+      const int64_t nChunks = P.nChunks;
+      const int64_t p = v.row0 + v.tile * kTileM + row;
+      const bool valid = (p < v.row0 + v.rows);
       double x[3] = {0.0, 0.0, 0.0};
       if (valid) {
 #pragma unroll
         for (int d = 0; d < 3; ++d)
-          if (d < P.nDim) x[d] = a.x[p * P.nDim + d] / P.corrL[d];
+          if (d < P.nDim) x[d] = v.x[p * P.nDim + d] / P.corrL[d];
       }
 
       Grid3Thread g3;
       Grid3Walk walk;
-      if (GEN == GEN_GRID3) {
+      if (kHasGrid && grid) {
         grid3_thread_setup<LPAD>(g3, P, h, x);
         walk.init(P, x);
       }
@@ -266,14 +348,14 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
       for (int64_t ch = 0; ch < nChunks; ++ch) {
         const uint32_t sc = s, phc = ph;
         if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
-        bool w = freeSeen || mbar_wait_warp(&bars->empty[sc], phc ^ 1, abort_flag);
-        if (GEN == GEN_TABLE) w = w && mbar_wait_warp(&bars->kfull[sc], phc, abort_flag, true);
-        if (!w) { ok = false; break; }
+        bool wt = freeSeen || mbar_wait_warp(&bars->empty[sc], phc ^ 1, abort_flag);
+        if (kHasTable && !grid) wt = wt && mbar_wait_warp(&bars->kfull[sc], phc, abort_flag, true);
+        if (!wt) { ok = false; break; }
         tc_fence_after();
         uint32_t probe = 0;
         if (lane == 0 && ch + 1 < nChunks) probe = mbar_test_wait(&bars->empty[s], ph ^ 1) ? 1u : 0u;
-        const uint32_t aAddr = tbase + laneOff + aCol0 + sc * aStride;
-        if (GEN == GEN_GRID3) {
+        const uint32_t aAddr = tbase + laneOff + (uint32_t)L.aCol0 + sc * (uint32_t)L.aStride;
+        if (kHasGrid && grid) {
 #pragma unroll
           for (int u = 0; u < 2; ++u) {  // two groups per stage
             uint32_t words[LPAD > 0 ? LPAD : 1];
@@ -289,7 +371,7 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
 #pragma unroll
             for (int pc = 0; pc < LPAD / 8; ++pc) tmem_st8(col + pc * 8, &words[pc * 8]);
           }
-        } else {
+        } else if (kHasTable) {
           uint32_t words[kTableChunk / 2];
           auto emit = [&](int idx, float c, float sn) {
             words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
@@ -312,17 +394,17 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
       tc_fence_after();
       const int half = P.nmcPad / 2;
       for (int cb = h * half; cb < (h + 1) * half; cb += 8) {
-        uint32_t v[8], lo[8];
-        tmem_ld8(tbase + laneOff + cb, v);
+        uint32_t va[8], lo[8];
+        tmem_ld8(tbase + laneOff + cb, va);
         if (PREC == PREC_BF16) tmem_ld8(tbase + laneOff + P.nmcPad + cb, lo);
         tmem_ld_wait();
         if (valid) {
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             const int r = cb + j;
-            float acc = __uint_as_float(v[j]);
+            float acc = __uint_as_float(va[j]);
             if (PREC == PREC_BF16) acc += __uint_as_float(lo[j]);
-            if (r < P.nmcBlk) a.out[(int64_t)(P.rOff + r) * P.n + p] = finish_value(P, acc);
+            if (r < P.nmcBlk) v.out[(int64_t)(P.rOff + r) * P.n + p] = finish_value(P, acc);
           }
         }
       }
@@ -331,13 +413,26 @@ __global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constan
       if (lane == 0) mbar_arrive(&bars->acc_empty);
       accPh ^= 1;
     }
-    if (!ok) raise_abort(bars, a.err);
+    if (!ok) raise_abort(bars, err);
   }
 
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   if (warp == kMmaWarp) tmem_dealloc(tbase, kTmemCols);
+}
+
+// LPAD: GEN_GRID3 axis-3 length padded to 8/16/24/32 (0 for GEN_TABLE).
+template <int GEN, int PREC, int LPAD>
+__global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constant__ TcArgs a) {
+  const SingleWork w{&a, (a.rows + kTileM - 1) / kTileM};
+  tc_body<GEN, PREC, LPAD>(w, a.L, a.err);
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(kThreads, 1) rf_group_kernel(const __grid_constant__ GroupArgs g) {
+  const GroupWork w{&g, g.ctaStart[blockIdx.x], g.ctaStart[blockIdx.x + 1]};
+  tc_body<GEN_MIXED, PREC, kGroupLPad>(w, g.L, g.err);
 }
 
 template <int GEN, int PREC, int LPAD>
@@ -361,25 +456,46 @@ cudaError_t launch_prec(const Plan& P, const TcArgs& args, size_t smem, int grid
   }
 }
 
+template <int PREC>
+cudaError_t launch_group_prec(const GroupArgs& g, size_t smem, int grid, cudaStream_t st) {
+  rf_group_kernel<PREC><<<grid, kThreads, smem, st>>>(g);
+  return cudaGetLastError();
+}
+
+// Shared-memory bytes of a layout (with the wavevector slots when `table`).
+size_t layout_bytes(const SlotLayout& L, bool table) {
+  return (size_t)kHeaderBytes + (size_t)L.S * (size_t)L.slotBytes + (table ? (size_t)L.S * kKtabStageBytes : 0);
+}
+
+// Deepest pipeline (2..maxS stages) that fits TMEM and shared memory; S = 0
+// when none does.  The kernel allocates all 512 TMEM columns, so two CTAs
+// must never share an SM: asking for more than half of the SM's shared
+// memory guarantees it.
+size_t fit_layout(SlotLayout& L, bool table, int maxS = kMaxStages) {
+  const size_t limit = 227 * 1024, floor = 120 * 1024;
+  int tmemS = (int)((kTmemCols - (uint32_t)L.aCol0) / (uint32_t)L.aStride);
+  if (maxS > tmemS) maxS = tmemS;
+  if (maxS > kMaxStages) maxS = kMaxStages;
+  for (int s = maxS; s >= 2; --s) {
+    L.S = s;
+    L.ktabOff = (int32_t)((size_t)s * (size_t)L.slotBytes);
+    const size_t total = layout_bytes(L, table);
+    if (total <= limit) return total < floor ? floor : total;
+  }
+  L.S = 0;
+  return 0;
+}
+
 }  // namespace
 
 size_t tc_smem_bytes(const Plan& P, int* stages) {
-  const size_t perStage = (size_t)P.stageBytes + (P.gen == GEN_TABLE ? kKtabStageBytes : 0);
-  const size_t limit = 227 * 1024;
-  // A stages live in TMEM after the bRows accumulator columns
-  int maxS = (int)((kTmemCols - (uint32_t)P.bRows) / (uint32_t)P.chunkK);
-  if (maxS > kMaxStages) maxS = kMaxStages;
-  // The kernel allocates all 512 TMEM columns, so two CTAs must never share
-  // an SM: asking for more than half of the SM's shared memory guarantees it.
-  const size_t floor = 120 * 1024;
-  for (int s = maxS; s >= 2; --s) {
-    const size_t total = kHeaderBytes + s * perStage;
-    if (total <= limit) {
-      if (stages) *stages = s;
-      return total < floor ? floor : total;
-    }
-  }
-  return 0;
+  SlotLayout L;
+  L.aCol0 = P.bRows;
+  L.aStride = P.chunkK;
+  L.slotBytes = P.stageBytes;
+  const size_t smem = fit_layout(L, P.gen == GEN_TABLE);
+  if (stages) *stages = L.S;
+  return smem;
 }
 
 cudaError_t launch_tc(const Plan& P, const double* dX, const void* dB, const double* dKtab, double* dOut,
@@ -393,15 +509,39 @@ cudaError_t launch_tc(const Plan& P, const double* dX, const void* dB, const dou
   args.err = dErr;
   args.row0 = row0;
   args.rows = rows;
-  int stages = 0;
-  const size_t smem = tc_smem_bytes(P, &stages);
+  args.L.aCol0 = P.bRows;
+  args.L.aStride = P.chunkK;
+  args.L.slotBytes = P.stageBytes;
+  const size_t smem = fit_layout(args.L, P.gen == GEN_TABLE);
   if (smem == 0) return cudaErrorInvalidValue;
-  args.stages = stages;
   const int64_t tiles = (rows + kTileM - 1) / kTileM;
   const int grid = (int)(tiles < numSMs ? tiles : numSMs);
   if (P.prec == PREC_FP16) return launch_prec<PREC_FP16>(P, args, smem, grid, st);
   if (P.prec == PREC_BF16_FAST) return launch_prec<PREC_BF16_FAST>(P, args, smem, grid, st);
   return launch_prec<PREC_BF16>(P, args, smem, grid, st);
+}
+
+size_t group_layout(int32_t maxBRows, int64_t maxStageBytes, int32_t maxStages, SlotLayout* L) {
+  L->aCol0 = maxBRows;
+  L->aStride = 2 * (2 * kGroupLPad);  // a GEN_GRID3 stage (two groups); GEN_TABLE stages use 32 of its columns
+  L->slotBytes = maxStageBytes;
+  return fit_layout(*L, true, maxStages > 0 ? maxStages : kMaxStages);
+}
+
+cudaError_t group_set_smem(int prec, size_t smem) {
+  const int b = (int)smem;
+  if (prec == PREC_FP16) return cudaFuncSetAttribute(rf_group_kernel<PREC_FP16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (prec == PREC_BF16_FAST)
+    return cudaFuncSetAttribute(rf_group_kernel<PREC_BF16_FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (prec == PREC_BF16) return cudaFuncSetAttribute(rf_group_kernel<PREC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_group(int prec, const GroupArgs& g, size_t smem, int grid, cudaStream_t st) {
+  if (prec == PREC_FP16) return launch_group_prec<PREC_FP16>(g, smem, grid, st);
+  if (prec == PREC_BF16_FAST) return launch_group_prec<PREC_BF16_FAST>(g, smem, grid, st);
+  if (prec == PREC_BF16) return launch_group_prec<PREC_BF16>(g, smem, grid, st);
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace rfb
