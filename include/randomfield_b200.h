@@ -183,6 +183,50 @@ int rf_generate_batch_device(rf_context* ctx, const rf_request* reqs, int32_t co
 /* Statistics of the last batch on the context (waits for it). */
 int rf_batch_last_stats(rf_context* ctx, rf_batch_stats* out);
 
+/*
+ * Serving loop.  No counterpart in the reference.  A server owns a worker
+ * thread and two batch slots (each a context with its own stream): requests
+ * submitted from any thread queue in FIFO order; the worker admits queued
+ * requests into a free slot while their device footprint (points, field,
+ * operands) fits the slot's share of the HBM budget, launches the slot's
+ * grouped batch, and admits the next arrivals into the other slot while the
+ * first runs (continuous batching: a request waits for at most the batch in
+ * flight).  Points are copied in and fields out through pinned staging, so a
+ * request's host buffers must stay valid until rf_server_wait returns.
+ * Latency is measured from rf_server_submit to the field being in the
+ * caller's buffer.  A request larger than a slot's share fails with
+ * RF_ENOMEM_ADMISSION.  The result of a request does not depend on the
+ * requests batched with it (each request's tables come from its own seed).
+ */
+typedef struct rf_server rf_server;
+typedef struct rf_server_config {
+  int32_t size;              /* sizeof(rf_server_config) */
+  int32_t device;
+  int32_t precision;         /* RF_PREC_BF16 / FP16 / BF16_FAST */
+  int32_t max_batch;         /* requests per grouped launch (0: 512) */
+  int64_t hbm_budget_bytes;  /* device memory for requests in flight (0: half the free memory) */
+  int32_t reserved[8];
+} rf_server_config;
+typedef struct rf_server_stats {
+  int64_t submitted, completed, failed, batches;
+  int64_t admission_waits;   /* batches closed early because the budget was full */
+  int64_t peak_bytes;        /* largest footprint admitted to one slot */
+  double field_values;       /* sum of n * Nmc over completed requests */
+  double busy_ms;            /* device time of the grouped launches */
+  double p50_ms, p99_ms, max_ms, mean_ms;  /* submit -> field in the caller's buffer */
+} rf_server_stats;
+
+void rf_server_config_init(rf_server_config* cfg);
+int rf_server_create(const rf_server_config* cfg, rf_server** out);
+/* Queues a request (host buffers); *ticket identifies it for rf_server_wait. */
+int rf_server_submit(rf_server* srv, const rf_request* req, int64_t* ticket);
+/* Waits (timeout_s < 0: forever) for a request; returns its status
+ * (RF_ETIMEDOUT when the wait timed out) and its latency in milliseconds. */
+int rf_server_wait(rf_server* srv, int64_t ticket, double timeout_s, double* latency_ms);
+int rf_server_get_stats(rf_server* srv, rf_server_stats* out);
+/* Drains the queue, stops the worker and frees the server. */
+int rf_server_destroy(rf_server* srv);
+
 /* Problem geometry exactly as the generator will use it (host only, no GPU):
  * K wavevectors, kNStep, kDelta, ampMult (randomFieldND.f90:260-266). */
 int rf_query_geometry(const double* xPoints, int nDim, int64_t n, int corrMod,

@@ -20,7 +20,7 @@ import numpy as np
 __all__ = [
     "RandomFieldError", "Options", "Context", "lib", "create_standard_gaussian_field_unstruct",
     "query_geometry", "generate_device_noalloc", "Request", "BatchStats", "make_request", "generate_batch",
-    "ISOTROPIC", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
+    "Server", "ServerConfig", "ServerStats", "ISOTROPIC", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
     "PREC_BF16", "PREC_FP16", "PREC_FP32", "PREC_BF16_FAST", "LIB_PATH", "STATUS",
 ]
 
@@ -50,6 +50,8 @@ EXPORTS = [
     "rf_generate_device", "rf_context_synchronize", "rf_query_geometry", "rf_last_error", "rf_abi_version",
     "rf_context_set_timing", "rf_context_last_times", "rf_generate_device_noalloc",
     "rf_generate_batch", "rf_generate_batch_device", "rf_batch_last_stats",
+    "rf_server_config_init", "rf_server_create", "rf_server_submit", "rf_server_wait", "rf_server_get_stats",
+    "rf_server_destroy",
 ]
 
 
@@ -135,6 +137,33 @@ class BatchStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerConfig(C.Structure):
+    """rf_server_config."""
+
+    _fields_ = [
+        ("size", C.c_int32),
+        ("device", C.c_int32),
+        ("precision", C.c_int32),
+        ("max_batch", C.c_int32),
+        ("hbm_budget_bytes", C.c_int64),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
+class ServerStats(C.Structure):
+    """rf_server_stats."""
+
+    _fields_ = [
+        ("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64), ("batches", C.c_int64),
+        ("admission_waits", C.c_int64), ("peak_bytes", C.c_int64), ("field_values", C.c_double),
+        ("busy_ms", C.c_double), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
+        ("mean_ms", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -166,6 +195,13 @@ def lib() -> C.CDLL:
         L.rf_generate_batch.argtypes = [C.c_void_p, P(Request), C.c_int32]
         L.rf_generate_batch_device.argtypes = [C.c_void_p, P(Request), C.c_int32, C.c_void_p]
         L.rf_batch_last_stats.argtypes = [C.c_void_p, P(BatchStats)]
+        L.rf_server_config_init.argtypes = [P(ServerConfig)]
+        L.rf_server_config_init.restype = None
+        L.rf_server_create.argtypes = [P(ServerConfig), P(C.c_void_p)]
+        L.rf_server_submit.argtypes = [C.c_void_p, P(Request), P(i64)]
+        L.rf_server_wait.argtypes = [C.c_void_p, i64, d, P(d)]
+        L.rf_server_get_stats.argtypes = [C.c_void_p, P(ServerStats)]
+        L.rf_server_destroy.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -297,6 +333,57 @@ def generate_batch(ctx: "Context", requests) -> None:
     one grouped launch; returns when every randField is filled."""
     arr = (Request * len(requests))(*requests)
     _check(lib().rf_generate_batch(ctx._h, arr, len(requests)))
+
+
+class Server:
+    """rf_server: the serving loop (continuous batching, HBM admission).
+
+    ``submit(request)`` takes a host-buffer :class:`Request` (keep its arrays
+    alive until ``wait`` returns) and returns a ticket; ``wait(ticket)``
+    returns the request's latency in milliseconds or raises its error.
+    """
+
+    def __init__(self, device=0, precision="bf16", max_batch=512, hbm_budget_bytes=0):
+        cfg = ServerConfig()
+        lib().rf_server_config_init(C.byref(cfg))
+        cfg.device = int(device)
+        cfg.precision = _PREC[precision] if isinstance(precision, str) else int(precision)
+        cfg.max_batch = int(max_batch)
+        cfg.hbm_budget_bytes = int(hbm_budget_bytes)
+        h = C.c_void_p()
+        _check(lib().rf_server_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, request: Request, keep=None) -> int:
+        t = C.c_int64()
+        _check(lib().rf_server_submit(self._h, C.byref(request), C.byref(t)))
+        self._keep[t.value] = (request, keep)
+        return t.value
+
+    def wait(self, ticket: int, timeout_s: float = -1.0) -> float:
+        lat = C.c_double()
+        try:
+            _check(lib().rf_server_wait(self._h, int(ticket), float(timeout_s), C.byref(lat)))
+        finally:
+            self._keep.pop(int(ticket), None)
+        return lat.value
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().rf_server_get_stats(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            lib().rf_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Context:

@@ -297,6 +297,41 @@ int run_batch(rf_context* c, const rf_request* reqs, int32_t count, const std::v
   return RF_OK;
 }
 
+}  // namespace
+
+namespace rfh {
+
+int batch_run_device(rf_context* c, const std::vector<Request>& rq, const std::vector<const double*>& dx,
+                     const std::vector<double*>& dout, const std::vector<double>& ext, cudaStream_t st) {
+  BatchState B;
+  B.dx = dx;
+  B.dout = dout;
+  return run_batch(c, nullptr, (int32_t)rq.size(), rq, ext, B, st);
+}
+
+int request_footprint(const Request& rq, const double* ext, int rblk, size_t* bytes) {
+  Plan P0;
+  if (int rc = build_plan(rq, ext, P0)) return rc;
+  if (P0.gen == GEN_GRID3 && P0.lPad != kGroupLPad) P0.forceTable = 1;
+  size_t b = align_up(sizeof(double) * (size_t)rq.n * rq.nDim) + align_up(sizeof(double) * (size_t)rq.n * rq.Nmc);
+  for (int32_t r0 = 0; r0 < P0.Nmc; r0 += rblk) {
+    Plan P = P0;
+    P.rOff = r0;
+    P.nmcBlk = std::min(rblk, P0.Nmc - r0);
+    if (int rc = layout(P)) return rc;
+    b += align_up((size_t)(P.nChunks * P.stageBytes));
+    if (P.gen == GEN_TABLE) b += align_up((size_t)P.nChunks * 3 * kTableChunk * sizeof(double));
+  }
+  *bytes = b;
+  return RF_OK;
+}
+
+int default_block(int prec) { return block_candidates(prec)[0]; }
+
+}  // namespace rfh
+
+namespace {
+
 int check_batch(const rf_request* reqs, int32_t count, std::vector<Request>& rq) {
   if (!reqs || count < 1) return fail(RF_EINVAL_ARG, "empty batch");
   rq.resize(count);

@@ -104,6 +104,19 @@ Request make_request(int nDim, int64_t n, int corrMod, int margiFirst, const dou
                      double fieldVar, int Nmc, int method, const rf_options* opt);
 void launch_extent(const double* dX, int64_t n, int nDim, double* part, cudaStream_t st);
 
+// rf_batch.cu: plan and run a batch whose points and fields are in device
+// memory (queued on st; returns without waiting).
+int batch_run_device(rf_context* c, const std::vector<Request>& rq, const std::vector<const double*>& dx,
+                     const std::vector<double*>& dout, const std::vector<double>& ext, cudaStream_t st);
+// Device bytes a request holds in a batch with realization block rblk:
+// points, field, operands.
+int request_footprint(const Request& rq, const double* ext, int rblk, size_t* bytes);
+// Realization block of the grouped launch before the tuner has run.
+int default_block(int prec);
+// rf_host.cu: create / free a context.
+int context_init(rf_context* c, int device);
+void context_free(rf_context* c);
+
 // Grows a device buffer to at least `bytes` (contents are not kept).
 template <typename T>
 int ensure(T*& p, size_t& cap, size_t bytes, const char* what) {
