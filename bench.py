@@ -191,6 +191,191 @@ def end_to_end(args, rf, torch, dist, xh, n, opts, world, local):
     return e2e
 
 
+# ----------------------------------------------------------------- batched / serving
+BATCH_REQUESTS = 512
+SERVE_RATE = 200.0
+
+
+def draw_request(rs, large_frac=0.0):
+    """One request of the batched mix: n log-uniform in [1e3, 1e6] points
+    uniform in a box of side U[1, 20], Nmc U{1..128}, method 1 or 2 (p = .5),
+    corrL per axis U[0.5, 4], gaussian or lognormal marginal (p = .5).  The
+    wavevector count is fixed per method: Shinozuka 24^3 x 4, isotropic
+    64 radii x 64 directions (the reference rule would give up to ~6e5
+    wavevectors at side 20 and corrL 0.5).  With probability large_frac the
+    request is a 256^3 structured grid (spacing 0.05) with Nmc = 16."""
+    method = 1 if rs.uniform() < 0.5 else 2
+    marg = "lognormal" if rs.uniform() < 0.5 else "gaussian"
+    corrL = tuple(float(v) for v in rs.uniform(0.5, 4.0, 3))
+    if large_frac and rs.uniform() < large_frac:
+        ax = np.arange(256, dtype=np.float64) * 0.05
+        z, y, x = np.meshgrid(ax, ax, ax, indexing="ij")
+        pts = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+        Nmc, kind = 16, "grid256"
+    else:
+        n = int(np.exp(rs.uniform(np.log(1e3), np.log(1e6))))
+        side = rs.uniform(1.0, 20.0)
+        pts = rs.uniform(0.0, side, size=(n, 3)).astype(np.float32).astype(np.float64)
+        Nmc, kind = int(rs.randint(1, 129)), "box"
+    opts = dict(k_nstep=(KN, KN, KN)) if method == 2 else dict(iso_n_radial=64, iso_n_dir=64)
+    avg, var = (1.0, 0.25) if marg == "lognormal" else (0.0, 1.0)
+    return dict(points=pts, Nmc=Nmc, method=method, marg=marg, corrL=corrL, avg=avg, var=var, opts=opts, kind=kind)
+
+
+def bench_batched(args, rf, torch, local):
+    """512 requests in one grouped launch (rf_generate_batch_device, CUDA
+    graph replay after the first batch), device-resident buffers; e2e through
+    rf_generate_batch with host buffers when host memory allows."""
+    rs = np.random.RandomState(2024)
+    mix = [draw_request(rs) for _ in range(BATCH_REQUESTS)]
+    values = float(sum(m["points"].shape[0] * m["Nmc"] for m in mix))
+    ctx = rf.Context(local)
+    keep, reqs = [], []
+    for i, m in enumerate(mix):
+        dx = torch.from_numpy(m["points"]).cuda(local)
+        dout = torch.empty((m["Nmc"], m["points"].shape[0]), dtype=torch.float64, device=f"cuda:{local}")
+        keep.append((dx, dout))
+        reqs.append(rf.make_request(dx, "gaussian", m["marg"], m["corrL"], m["avg"], m["var"], m["Nmc"], m["method"],
+                                    dout, precision="bf16", seed_start=i, nDim=3, n=m["points"].shape[0],
+                                    **m["opts"]))
+    stream = torch.cuda.Stream(device=local)
+    for _ in range(max(2, args.warmup)):  # the first batch runs the tuner
+        ctx.generate_batch_device(reqs, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    steps = max(2, min(args.steps, 3))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for a, b in ev:
+            a.record(stream)
+            ctx.generate_batch_device(reqs, stream=stream.cuda_stream)
+            b.record(stream)
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    st = ctx.batch_stats()
+    out = {"workload": f"{BATCH_REQUESTS} requests: n log-uniform 1e3-1e6 in a box of side U[1,20], Nmc U{{1..128}}, "
+                       "method 1|2, corrL U[0.5,4]^3, gaussian|lognormal; Shinozuka 24^3x4, isotropic 64x64",
+           "field_values_per_batch": values, "value": values * steps / (sum(ms) / 1e3), "unit": "field values/s",
+           "ms_per_batch": float(np.mean(ms)), "p50_ms": float(np.percentile(ms, 50)),
+           "p99_ms": float(np.percentile(ms, 99)),
+           "latency_note": "one grouped launch: every request of a batch completes with it",
+           "grouped_launch": st, "precision": "bf16"}
+    # end to end with host buffers (needs about 2x the fields in host memory)
+    need = 8.0 * values + sum(m["points"].nbytes for m in mix)
+    try:
+        import psutil
+        avail = float(psutil.virtual_memory().available)
+    except Exception:
+        avail = 0.0
+    del keep
+    torch.cuda.empty_cache()
+    if avail > 2.0 * need and not args.no_e2e:
+        hx = [np.asfortranarray(m["points"].T) for m in mix]
+        ho = [np.empty((m["points"].shape[0], m["Nmc"]), order="F") for m in mix]
+        hreqs = [rf.make_request(hx[i], "gaussian", m["marg"], m["corrL"], m["avg"], m["var"], m["Nmc"], m["method"],
+                                 ho[i], precision="bf16", seed_start=i, **m["opts"]) for i, m in enumerate(mix)]
+        rf.generate_batch(ctx, hreqs)
+        t0 = time.perf_counter()
+        rf.generate_batch(ctx, hreqs)
+        dt = time.perf_counter() - t0
+        out["e2e"] = {"value": values / dt, "unit": "field values/s", "ms_per_batch": dt * 1e3,
+                      "h2d_bytes_per_step": int(sum(m["points"].nbytes for m in mix)),
+                      "d2h_bytes_per_step": int(8 * values), "api": "rf_generate_batch (pageable host buffers)"}
+        del hx, ho
+    else:
+        out["e2e"] = {"value": None, "reason": f"host memory available {avail / 1e9:.0f} GB < 2x {need / 1e9:.0f} GB"}
+    ctx.close()
+    return out
+
+
+def bench_serving(args, rf, torch, local):
+    """Poisson arrivals at 200 requests/s into the serving loop for
+    --serve-seconds: request sizes as in the batched mix plus 5% 256^3 grids
+    with Nmc = 16.  A pool of 96 clients with page-locked buffers issues the
+    arrivals (an arrival takes the next idle client; when none is idle the
+    arrival is delayed, and the delay is reported)."""
+    import threading
+
+    rs = np.random.RandomState(77)
+    pool = []
+    for i in range(96):
+        m = draw_request(rs, large_frac=0.05)
+        n = m["points"].shape[0]
+        hx = torch.from_numpy(np.ascontiguousarray(m["points"])).pin_memory()
+        ho = torch.empty((m["Nmc"], n), dtype=torch.float64).pin_memory()
+        xa, oa = hx.numpy().T, ho.numpy().T  # Fortran views: 3 x n, n x Nmc
+        req = rf.make_request(xa, "gaussian", m["marg"], m["corrL"], m["avg"], m["var"], m["Nmc"], m["method"], oa,
+                              seed_start=1000 + i, **m["opts"])
+        pool.append(dict(req=req, keep=(hx, ho, xa, oa), values=float(n * m["Nmc"]), kind=m["kind"]))
+    srv = rf.Server(device=local, precision="bf16")
+    # warm the two slots (tuner, graphs) outside the measured window
+    for c in pool[:4]:
+        srv.wait(srv.submit(c["req"]))
+    busy = [False] * len(pool)
+    lock = threading.Lock()
+    pending = []
+    done_evt = threading.Event()
+
+    def waiter():
+        while True:
+            with lock:
+                item = pending.pop(0) if pending else None
+            if item is None:
+                if done_evt.is_set():
+                    return
+                time.sleep(0.0005)
+                continue
+            t, k = item
+            srv.wait(t)
+            with lock:
+                busy[k] = False
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    base = srv.stats()
+    T = float(args.serve_seconds)
+    gaps = rs.exponential(1.0 / SERVE_RATE, size=int(SERVE_RATE * T * 1.5) + 16)
+    arrivals = np.cumsum(gaps)
+    arrivals = arrivals[arrivals < T]
+    blocked_s, offered, nxt = 0.0, 0.0, 0
+    t0 = time.perf_counter()
+    for ta in arrivals:
+        while time.perf_counter() - t0 < ta:
+            time.sleep(0.0002)
+        k = None
+        while k is None:
+            with lock:
+                for j in range(len(pool)):
+                    c = (nxt + j) % len(pool)
+                    if not busy[c]:
+                        k = c
+                        busy[c] = True
+                        break
+            if k is None:
+                tb = time.perf_counter()
+                time.sleep(0.0005)
+                blocked_s += time.perf_counter() - tb
+        nxt = k + 1
+        t = srv.submit(pool[k]["req"])
+        offered += pool[k]["values"]
+        with lock:
+            pending.append((t, k))
+    done_evt.set()
+    th.join()
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    completed = st["completed"] - base["completed"]
+    vals = st["field_values"] - base["field_values"]
+    return {"workload": f"Poisson {SERVE_RATE:.0f} req/s for {T:.0f} s; sizes as the batched mix plus 5% 256^3 "
+                        "grids with Nmc 16 (single domain: the 8-subdomain blend is a separate entry point)",
+            "requests": int(completed), "value": vals / wall, "unit": "field values/s",
+            "offered_field_values_per_s": offered / T, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "max_ms": st["max_ms"], "batches": st["batches"] - base["batches"],
+            "arrivals_delayed_s": blocked_s, "failed": st["failed"], "duration_s": wall,
+            "latency": "submit -> field in the caller's page-locked buffer; statistics over the whole run "
+                       "including the four warm-up requests"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -201,6 +386,10 @@ def main():
     ap.add_argument("--no-forms", action="store_true", help="skip the other precision forms")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 512-request batched form")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop form")
+    ap.add_argument("--serve-seconds", type=float, default=20.0,
+                    help="duration of the Poisson arrival stream (the serving config names 60 s)")
     ap.add_argument("--grid", default="128,128,128",
                     help="grid points per axis; a smaller grid (e.g. 32,32,18 = one wave of 144 tiles) "
                          "keeps profiler captures short; the headline workload is 128,128,128")
@@ -338,6 +527,13 @@ def main():
     if world > 1:
         dist.barrier()
     ctx.close()
+    del dx, dout, flush
+    torch.cuda.empty_cache()
+    batched = serving = None
+    if rank == 0 and world == 1 and not args.no_batched and args.precision != "fp32":
+        batched = bench_batched(args, rf, torch, local)
+    if rank == 0 and world == 1 and not args.no_serve and args.precision != "fp32":
+        serving = bench_serving(args, rf, torch, local)
     if rank == 0:
         line = {
             "metric": "field values/s", "value": value, "unit": "field values/s", "n_gpus": world,
@@ -355,6 +551,8 @@ def main():
             "e2e": e2e,
             "accuracy": acc,
             "forms": forms,
+            "batched": batched,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

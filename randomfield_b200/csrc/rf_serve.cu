@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdint>
 #include <cstring>
 #include <deque>
 #include <thread>
@@ -57,7 +58,7 @@ struct Slot {
   std::vector<Pending> batch;
   unsigned char* hStage = nullptr;  // pinned: points then fields of the batch
   size_t capStage = 0;
-  std::vector<size_t> outOff;       // field offsets inside hStage
+  std::vector<size_t> outOff;       // field offsets inside hStage (SIZE_MAX: copied straight to the caller)
   int status = RF_OK;
   std::string error;
 };
@@ -85,18 +86,34 @@ namespace {
 
 // Launches the slot's batch: points into staging and onto the device, the
 // grouped generation, fields back into staging, completion event.
+bool pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 int launch_slot(rf_server* s, Slot& sl) {
   rf_context* c = sl.ctx;
   cudaStream_t st = c->stream;
   RF_CUDA(cudaSetDevice(c->device), "cudaSetDevice");
   const size_t n = sl.batch.size();
   size_t stage = 0, io = 0;
-  for (const Pending& p : sl.batch) {
+  // callers' page-locked buffers are copied to and from directly; pageable
+  // ones go through the slot's pinned staging
+  std::vector<char> pinX(n), pinO(n);
+  for (size_t i = 0; i < n; ++i) {
+    const Pending& p = sl.batch[i];
     const size_t xb = sizeof(double) * (size_t)p.rq.n * p.rq.nDim, ob = sizeof(double) * (size_t)p.rq.n * p.rq.Nmc;
-    stage += align_up(xb) + align_up(ob);
+    pinX[i] = pinned(p.req.xPoints);
+    pinO[i] = pinned(p.req.randField);
+    stage += (pinX[i] ? 0 : align_up(xb)) + (pinO[i] ? 0 : align_up(ob));
     io += align_up(xb) + align_up(ob);
   }
-  if (int rc = ensure_host(sl.hStage, sl.capStage, stage, "serving staging")) return rc;
+  if (stage > 0)
+    if (int rc = ensure_host(sl.hStage, sl.capStage, stage, "serving staging")) return rc;
   if (int rc = ensure(c->dX, c->capX, io, "serving points and fields")) return rc;
   std::vector<Request> rq(n);
   std::vector<const double*> dx(n);
@@ -104,17 +121,27 @@ int launch_slot(rf_server* s, Slot& sl) {
   std::vector<double> ext(3 * n);
   sl.outOff.assign(n, 0);
   unsigned char* dbase = reinterpret_cast<unsigned char*>(c->dX);
-  size_t off = 0;
+  size_t off = 0, soff = 0;
   for (size_t i = 0; i < n; ++i) {
     const Pending& p = sl.batch[i];
     const size_t xb = sizeof(double) * (size_t)p.rq.n * p.rq.nDim, ob = sizeof(double) * (size_t)p.rq.n * p.rq.Nmc;
-    memcpy(sl.hStage + off, p.req.xPoints, xb);
+    const void* src = p.req.xPoints;
+    if (!pinX[i]) {
+      memcpy(sl.hStage + soff, p.req.xPoints, xb);
+      src = sl.hStage + soff;
+      soff += align_up(xb);
+    }
     dx[i] = reinterpret_cast<const double*>(dbase + off);
-    RF_CUDA(cudaMemcpyAsync(dbase + off, sl.hStage + off, xb, cudaMemcpyHostToDevice, st), "copy of xPoints");
+    RF_CUDA(cudaMemcpyAsync(dbase + off, src, xb, cudaMemcpyHostToDevice, st), "copy of xPoints");
     off += align_up(xb);
     dout[i] = reinterpret_cast<double*>(dbase + off);
-    sl.outOff[i] = off;
     off += align_up(ob);
+    if (pinO[i]) {
+      sl.outOff[i] = SIZE_MAX;
+    } else {
+      sl.outOff[i] = soff;
+      soff += align_up(ob);
+    }
     rq[i] = p.rq;
     for (int d = 0; d < 3; ++d) ext[3 * i + d] = p.ext[d];
   }
@@ -122,7 +149,8 @@ int launch_slot(rf_server* s, Slot& sl) {
   for (size_t i = 0; i < n; ++i) {
     const Pending& p = sl.batch[i];
     const size_t ob = sizeof(double) * (size_t)p.rq.n * p.rq.Nmc;
-    RF_CUDA(cudaMemcpyAsync(sl.hStage + sl.outOff[i], dout[i], ob, cudaMemcpyDeviceToHost, st), "copy of randField");
+    void* dst = sl.outOff[i] == SIZE_MAX ? (void*)p.req.randField : (void*)(sl.hStage + sl.outOff[i]);
+    RF_CUDA(cudaMemcpyAsync(dst, dout[i], ob, cudaMemcpyDeviceToHost, st), "copy of randField");
   }
   RF_CUDA(cudaEventRecord(sl.evDone, st), "cudaEventRecord");
   (void)s;
@@ -144,7 +172,8 @@ void finish_slot(rf_server* s, Slot& sl) {
         busy = a + b;
       for (size_t i = 0; i < sl.batch.size(); ++i) {
         const Pending& p = sl.batch[i];
-        memcpy(p.req.randField, sl.hStage + sl.outOff[i], sizeof(double) * (size_t)p.rq.n * p.rq.Nmc);
+        if (sl.outOff[i] != SIZE_MAX)
+          memcpy(p.req.randField, sl.hStage + sl.outOff[i], sizeof(double) * (size_t)p.rq.n * p.rq.Nmc);
       }
     }
   }
