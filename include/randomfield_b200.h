@@ -184,6 +184,45 @@ int rf_generate_batch_device(rf_context* ctx, const rf_request* reqs, int32_t co
 int rf_batch_last_stats(rf_context* ctx, rf_batch_stats* out);
 
 /*
+ * Localization blend (localization_RF.f90:199-263, 705-857; calls_RF.f90:
+ * 209-213, 324-369; topography_RF.f90:49-52): one field on a structured group
+ * grid assembled from nFields[0] x nFields[1] x nFields[2] overlapping
+ * subdomains.  The overlap (units of corrL) is rounded to the grid as the
+ * reference does; overlapNPoints = nint((overlap*corrL - 2*xStep)/xStep) + 1
+ * points are shared by neighbouring subdomains, each of
+ * (xNStep + (nFields-1)*overlapNPoints)/nFields points per axis (this must be
+ * an integer: rf_blend_layout reports the subdomain size or RF_EINVAL_RANGE).
+ * Subdomain f (fieldNumber 1.., axis 1 fastest) is generated with seed
+ * seed_start + fieldNumber (sample_RF.f90:311) on its own grid, multiplied by
+ * its cosine partition of unity (all faces ramped) and added into the group
+ * field in the grouped launch's epilogue; the group's border faces are then
+ * divided by the group's partition (border correction) and the marginal map
+ * applied.  randField is xNStep[0]*xNStep[1]*xNStep[2] x Nmc, axis 1 fastest.
+ * Tensor-core forms only; the border correction applies to every
+ * realization (the reference corrects column 1 only).
+ */
+typedef struct rf_blend_grid {
+  int32_t nDim;
+  int32_t xNStep[3];   /* group grid points per axis */
+  int32_t nFields[3];  /* subdomains per axis */
+  int32_t reserved0;
+  double xMin[3];
+  double xStep[3];
+  double overlap;      /* in units of corrL (the reference's IPT%overlap) */
+  int32_t reserved[8];
+} rf_blend_grid;
+/* Subdomain points per axis and overlapNPoints per axis of a blend grid. */
+int rf_blend_layout(const rf_blend_grid* grid, const double* corrL, int32_t* subNStep, int32_t* overlapNPoints);
+/* Host randField; returns when it is filled. */
+int rf_generate_blended(rf_context* ctx, const rf_blend_grid* grid, int corrMod, int margiFirst, const double* corrL,
+                        double fieldAvg, double fieldVar, int Nmc, int method, double* randField,
+                        const rf_options* opt);
+/* Device randField, queued on `stream` (0 = the context's stream). */
+int rf_generate_blended_device(rf_context* ctx, const rf_blend_grid* grid, int corrMod, int margiFirst,
+                               const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method,
+                               double* d_randField, const rf_options* opt, void* stream);
+
+/*
  * Serving loop.  No counterpart in the reference.  A server owns a worker
  * thread and two batch slots (each a context with its own stream): requests
  * submitted from any thread queue in FIFO order; the worker admits queued

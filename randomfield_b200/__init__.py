@@ -20,7 +20,7 @@ import numpy as np
 __all__ = [
     "RandomFieldError", "Options", "Context", "lib", "create_standard_gaussian_field_unstruct",
     "query_geometry", "generate_device_noalloc", "Request", "BatchStats", "make_request", "generate_batch",
-    "Server", "ServerConfig", "ServerStats", "ISOTROPIC", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
+    "Server", "ServerConfig", "ServerStats", "BlendGrid", "blend_layout", "ISOTROPIC", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
     "PREC_BF16", "PREC_FP16", "PREC_FP32", "PREC_BF16_FAST", "LIB_PATH", "STATUS",
 ]
 
@@ -51,7 +51,7 @@ EXPORTS = [
     "rf_context_set_timing", "rf_context_last_times", "rf_generate_device_noalloc",
     "rf_generate_batch", "rf_generate_batch_device", "rf_batch_last_stats",
     "rf_server_config_init", "rf_server_create", "rf_server_submit", "rf_server_wait", "rf_server_get_stats",
-    "rf_server_destroy",
+    "rf_server_destroy", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
 ]
 
 
@@ -137,6 +137,43 @@ class BatchStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BlendGrid(C.Structure):
+    """rf_blend_grid: a structured group grid split into overlapping subdomains."""
+
+    _fields_ = [
+        ("nDim", C.c_int32),
+        ("xNStep", C.c_int32 * 3),
+        ("nFields", C.c_int32 * 3),
+        ("reserved0", C.c_int32),
+        ("xMin", C.c_double * 3),
+        ("xStep", C.c_double * 3),
+        ("overlap", C.c_double),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+    @classmethod
+    def make(cls, xNStep, xStep, nFields, overlap, xMin=None) -> "BlendGrid":
+        g = cls()
+        nd = len(xNStep)
+        g.nDim = nd
+        for d in range(3):
+            g.xNStep[d] = int(xNStep[d]) if d < nd else 1
+            g.nFields[d] = int(nFields[d]) if d < nd else 1
+            g.xStep[d] = float(xStep[d]) if d < nd else 0.0
+            g.xMin[d] = float(xMin[d]) if (xMin is not None and d < nd) else 0.0
+        g.overlap = float(overlap)
+        return g
+
+
+def blend_layout(grid: "BlendGrid", corrL):
+    """(subdomain points per axis, overlapNPoints per axis) of a blend grid."""
+    cl = np.ascontiguousarray(np.asarray(list(corrL) + [1.0] * (3 - len(corrL)), dtype=np.float64))
+    L = (C.c_int32 * 3)()
+    O = (C.c_int32 * 3)()
+    _check(lib().rf_blend_layout(C.byref(grid), cl.ctypes.data_as(C.POINTER(C.c_double)), L, O))
+    return list(L), list(O)
+
+
 class ServerConfig(C.Structure):
     """rf_server_config."""
 
@@ -202,6 +239,11 @@ def lib() -> C.CDLL:
         L.rf_server_wait.argtypes = [C.c_void_p, i64, d, P(d)]
         L.rf_server_get_stats.argtypes = [C.c_void_p, P(ServerStats)]
         L.rf_server_destroy.argtypes = [C.c_void_p]
+        L.rf_blend_layout.argtypes = [P(BlendGrid), P(d), P(C.c_int32), P(C.c_int32)]
+        L.rf_generate_blended.argtypes = [C.c_void_p, P(BlendGrid), i32, i32, P(d), d, d, i32, i32, P(d),
+                                          P(Options)]
+        L.rf_generate_blended_device.argtypes = [C.c_void_p, P(BlendGrid), i32, i32, P(d), d, d, i32, i32,
+                                                 C.c_void_p, P(Options), C.c_void_p]
         _lib = L
     return _lib
 
@@ -437,6 +479,33 @@ class Context:
         s = stream if isinstance(stream, int) else int(getattr(stream, "cuda_stream", 0))
         arr = (Request * len(requests))(*requests)
         _check(lib().rf_generate_batch_device(self._h, arr, len(requests), C.c_void_p(s)))
+
+    def generate_blended(self, grid: "BlendGrid", corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method,
+                         randField=None, options=None, **kw):
+        """rf_generate_blended: the blended field on the group grid, returned
+        (or written into randField) as a Fortran-ordered G x Nmc array."""
+        G = int(np.prod([grid.xNStep[d] for d in range(grid.nDim)]))
+        if randField is None:
+            randField = np.empty((G, int(Nmc)), dtype=np.float64, order="F")
+        cl = np.ascontiguousarray(np.asarray(corrL, dtype=np.float64).reshape(-1))
+        o = _opts(options if options is not None else (kw or None))
+        P = C.POINTER(C.c_double)
+        _check(lib().rf_generate_blended(self._h, C.byref(grid), _id(corrMod, _CORRMOD, "corrMod"),
+                                         _id(margiFirst, _MARGI, "margiFirst"), cl.ctypes.data_as(P),
+                                         float(fieldAvg), float(fieldVar), int(Nmc), int(method),
+                                         randField.ctypes.data_as(P), C.byref(o)))
+        return randField
+
+    def generate_blended_device(self, grid: "BlendGrid", corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc,
+                                method, d_out, options=None, stream=0, **kw) -> None:
+        cl = np.ascontiguousarray(np.asarray(corrL, dtype=np.float64).reshape(-1))
+        o = _opts(options if options is not None else (kw or None))
+        s = stream if isinstance(stream, int) else int(getattr(stream, "cuda_stream", 0))
+        _check(lib().rf_generate_blended_device(self._h, C.byref(grid), _id(corrMod, _CORRMOD, "corrMod"),
+                                                _id(margiFirst, _MARGI, "margiFirst"),
+                                                cl.ctypes.data_as(C.POINTER(C.c_double)), float(fieldAvg),
+                                                float(fieldVar), int(Nmc), int(method), C.c_void_p(self._ptr(d_out)),
+                                                C.byref(o), C.c_void_p(s)))
 
     def batch_stats(self) -> dict:
         st = BatchStats()

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -56,11 +57,31 @@ DescLayout desc_layout(size_t capUnits, size_t capItems, int numSMs) {
   return d;
 }
 
+// A request that is a subdomain of a localization blend (rf_blend.cuh).
+struct BlendSpec {
+  int32_t bDims[3], bOrigin[3], gDims[3], bRamp[3];
+  int64_t gTotal;
+};
+
 struct BatchState {
   std::vector<Plan> plans;         // per request, before the realization split
   std::vector<const double*> dx;   // device points per request
-  std::vector<double*> dout;       // device fields per request
+  std::vector<double*> dout;       // device fields per request (the group field for blend subdomains)
+  std::vector<BlendSpec> blend;    // empty, or one per request
+  bool accumulate = false;         // the launch adds into its outputs: run it once (no tuning runs)
 };
+
+void apply_blend(Plan& P, const BlendSpec& b) {
+  P.blend = 1;
+  for (int d = 0; d < 3; ++d) {
+    P.bDims[d] = b.bDims[d];
+    P.bOrigin[d] = b.bOrigin[d];
+    P.gDims[d] = b.gDims[d];
+    P.bRamp[d] = b.bRamp[d];
+  }
+  P.gTotal = b.gTotal;
+  P.applyMarginal = 0;  // the marginal map follows the border correction
+}
 
 struct GroupRun {
   int prec = 0;
@@ -107,6 +128,7 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
       P.rOff = r0;
       P.nmcBlk = std::min(rblk, P0.Nmc - r0);
       if (int rc = layout(P)) return rc;
+      if (!B.blend.empty()) apply_blend(P, B.blend[i]);
       GroupSub g;
       memset(&g, 0, sizeof(g));
       g.P = P;
@@ -262,7 +284,7 @@ int run_batch(rf_context* c, const rf_request* reqs, int32_t count, const std::v
   (void)reqs;
   GroupRun run;
   rf_batch_stats stats{};
-  if (c->tunedBlock[prec] == 0) {
+  if (c->tunedBlock[prec] == 0 && !B.accumulate) {
     double best = 1e300;
     int bestBlk = 0;
     for (int blk : block_candidates(prec)) {
@@ -278,7 +300,8 @@ int run_batch(rf_context* c, const rf_request* reqs, int32_t count, const std::v
     c->tunedBlock[prec] = bestBlk;
     stats.tuned = 1;
   }
-  if (int rc = group_run(c, B, prec, c->tunedBlock[prec], st, run)) return rc;
+  const int blk = c->tunedBlock[prec] ? c->tunedBlock[prec] : block_candidates(prec)[0];
+  if (int rc = group_run(c, B, prec, blk, st, run)) return rc;
   stats.units = run.units;
   stats.work_items = run.items;
   stats.realization_block = run.rblk;
@@ -356,9 +379,162 @@ bool needs_extent(const Request& r) {
   return false;
 }
 
+// topography_RF.f90:49-52 (overlap rounded to the grid, at least two steps
+// where the axis is split) and localization_RF.f90:746 (overlapNPoints);
+// subdomains of L points start every L - overlapNPoints points.
+int blend_geometry(const rf_blend_grid* g, const double* corrL, int32_t* L, int32_t* O) {
+  if (!g || !corrL) return fail(RF_EINVAL_ARG, "null pointer argument");
+  if (g->nDim < 1 || g->nDim > 3) return fail(RF_EINVAL_NDIM, "nDim must be 1, 2 or 3 (got %d)", g->nDim);
+  for (int d = 0; d < 3; ++d) {
+    L[d] = 1;
+    O[d] = 0;
+    if (d >= g->nDim) continue;
+    const int32_t N = g->xNStep[d], F = g->nFields[d];
+    const double h = g->xStep[d];
+    if (N < 2 || F < 1 || !(h > 0.0) || !(corrL[d] > 0.0))
+      return fail(RF_EINVAL_ARG, "blend axis %d: xNStep >= 2, nFields >= 1, xStep > 0, corrL > 0 needed", d + 1);
+    double ov = F == 1 ? 0.0 : g->overlap;
+    ov = std::nearbyint(ov * corrL[d] / h) * h / corrL[d];
+    if (F != 1 && ov < 2.0 * h / corrL[d]) ov = 2.0 * h / corrL[d];
+    O[d] = (int32_t)std::lround((ov * corrL[d] - 2.0 * h) / h) + 1;
+    const int32_t shared = (F - 1) * std::max(O[d], 0);
+    if ((N + shared) % F != 0)
+      return fail(RF_EINVAL_RANGE,
+                  "blend axis %d: %d points do not split into %d subdomains sharing %d points (N + (F-1)*O "
+                  "must be a multiple of F)",
+                  d + 1, N, F, O[d]);
+    L[d] = (N + shared) / F;
+    if (F > 1 && L[d] <= O[d]) return fail(RF_EINVAL_RANGE, "blend axis %d: overlap wider than a subdomain", d + 1);
+  }
+  return RF_OK;
+}
+
+// The blended field of `grid` into the device array dOut (group points x Nmc).
+int run_blended(rf_context* c, const rf_blend_grid* grid, const Request& base, double* dOut, cudaStream_t st) {
+  int32_t L[3], O[3];
+  if (int rc = blend_geometry(grid, base.corrL, L, O)) return rc;
+  if (base.opt.precision == RF_PREC_FP32) return fail(RF_ENOTSUP, "the blend runs the tensor-core forms");
+  if (base.opt.literal) return fail(RF_ENOTSUP, "literal mode is not available for the blend");
+  const int nd = grid->nDim;
+  int32_t F[3] = {1, 1, 1}, G[3] = {1, 1, 1};
+  for (int d = 0; d < nd; ++d) {
+    F[d] = grid->nFields[d];
+    G[d] = grid->xNStep[d];
+  }
+  const int64_t gTotal = (int64_t)G[0] * G[1] * G[2];
+  const int64_t sub = (int64_t)L[0] * L[1] * L[2];
+  const int nSub = F[0] * F[1] * F[2];
+  int64_t seed0 = base.opt.seed_start;
+  if (seed0 < 0) {  // one stochastic seed, then + fieldNumber (sample_RF.f90:316-317)
+    const auto t = std::chrono::steady_clock::now().time_since_epoch().count();
+    seed0 = (int64_t)((uint64_t)t % 100000000ull);
+  }
+  if (int rc = ensure(c->dX, c->capX, sizeof(double) * (size_t)sub * nd * nSub, "subdomain points")) return rc;
+  RF_CUDA(cudaMemsetAsync(dOut, 0, sizeof(double) * (size_t)gTotal * base.Nmc, st), "clear of randField");
+  BatchState B;
+  std::vector<Request> rq(nSub);
+  std::vector<double> ext(3 * nSub, 0.0);
+  B.dx.resize(nSub);
+  B.dout.assign(nSub, dOut);
+  B.blend.resize(nSub);
+  B.accumulate = true;
+  for (int f = 0; f < nSub; ++f) {
+    const int32_t fi[3] = {f % F[0], (f / F[0]) % F[1], f / (F[0] * F[1])};
+    BlendSpec& b = B.blend[f];
+    double x0[3] = {0, 0, 0}, h[3] = {0, 0, 0};
+    for (int d = 0; d < 3; ++d) {
+      b.bDims[d] = L[d];
+      b.bOrigin[d] = d < nd ? fi[d] * (L[d] - std::max(O[d], 0)) : 0;
+      b.gDims[d] = G[d];
+      b.bRamp[d] = d < nd ? O[d] : 0;
+      if (d < nd) {
+        h[d] = grid->xStep[d];
+        x0[d] = grid->xMin[d] + (double)b.bOrigin[d] * h[d];
+      }
+    }
+    b.gTotal = gTotal;
+    double* dx = c->dX + (size_t)f * sub * nd;
+    RF_CUDA(launch_grid_points(dx, nd, L, x0, h, st), "subdomain points kernel");
+    c->launches += 1;
+    B.dx[f] = dx;
+    rq[f] = base;
+    rq[f].n = sub;
+    rq[f].opt.seed_start = seed0 + f + 1;  // fieldNumber = f + 1
+    rq[f].opt.normalize = 0;
+    for (int d = 0; d < nd; ++d) rq[f].opt.x_range[d] = (double)(L[d] - 1) * grid->xStep[d];
+  }
+  if (int rc = run_batch(c, nullptr, nSub, rq, ext, B, st)) return rc;
+  // the group: border correction, then the marginal map (or normalisation)
+  Plan Gp;
+  if (int rc = build_plan(rq[0], &ext[0], Gp)) return rc;
+  Gp.nDim = nd;
+  Gp.n = gTotal;
+  Gp.gTotal = gTotal;
+  for (int d = 0; d < 3; ++d) {
+    Gp.gDims[d] = G[d];
+    Gp.bRamp[d] = d < nd ? O[d] : 0;
+  }
+  const bool norm = base.opt.normalize != 0;
+  RF_CUDA(launch_blend_finish(Gp, dOut, norm ? 0 : 1, st), "border correction kernel");
+  c->launches += 1;
+  if (norm) {
+    if ((size_t)2 * Gp.Nmc * sizeof(double) > c->capWork)
+      if (int rc = ensure(c->dWork, c->capWork, (size_t)2 * Gp.Nmc * sizeof(double), "moments")) return rc;
+    RF_CUDA(launch_normalize_and_map(Gp, dOut, Gp.Nmc, c->dWork, st), "normalisation kernels");
+    c->launches += 3;
+  }
+  return RF_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int rf_blend_layout(const rf_blend_grid* grid, const double* corrL, int32_t* subNStep, int32_t* overlapNPoints) {
+  g_err.clear();
+  int32_t L[3], O[3];
+  if (int rc = blend_geometry(grid, corrL, L, O)) return rc;
+  for (int d = 0; d < 3; ++d) {
+    if (subNStep) subNStep[d] = L[d];
+    if (overlapNPoints) overlapNPoints[d] = O[d];
+  }
+  return RF_OK;
+}
+
+int rf_generate_blended_device(rf_context* ctx, const rf_blend_grid* grid, int corrMod, int margiFirst,
+                               const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method,
+                               double* d_randField, const rf_options* opt, void* stream) {
+  g_err.clear();
+  if (!ctx || !grid || !corrL || !d_randField) return fail(RF_EINVAL_ARG, "null pointer argument");
+  Request rq = make_request(grid->nDim, 1, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
+  if (int rc = validate(rq)) return rc;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
+  ctx->launches = 0;
+  return run_blended(ctx, grid, rq, d_randField, st);
+}
+
+int rf_generate_blended(rf_context* ctx, const rf_blend_grid* grid, int corrMod, int margiFirst, const double* corrL,
+                        double fieldAvg, double fieldVar, int Nmc, int method, double* randField,
+                        const rf_options* opt) {
+  g_err.clear();
+  if (!ctx || !grid || !corrL || !randField) return fail(RF_EINVAL_ARG, "null pointer argument");
+  Request rq = make_request(grid->nDim, 1, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
+  if (int rc = validate(rq)) return rc;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  cudaStream_t st = ctx->stream;
+  ctx->launches = 0;
+  int64_t gTotal = 1;
+  for (int d = 0; d < grid->nDim && d < 3; ++d) gTotal *= std::max(grid->xNStep[d], 1);
+  const size_t bytes = sizeof(double) * (size_t)gTotal * Nmc;
+  if (int rc = ensure(ctx->dOut, ctx->capOut, bytes, "blended field")) return rc;
+  if (int rc = run_blended(ctx, grid, rq, ctx->dOut, st)) return rc;
+  RF_CUDA(cudaMemcpyAsync(randField, ctx->dOut, bytes, cudaMemcpyDeviceToHost, st), "copy of randField");
+  RF_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  return check_device_error(ctx);
+}
 
 int rf_generate_batch(rf_context* ctx, const rf_request* reqs, int32_t count) {
   g_err.clear();

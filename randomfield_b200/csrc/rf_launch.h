@@ -28,6 +28,14 @@ cudaError_t launch_fp32(const Plan& P, const double* dX, const void* dB, const d
 cudaError_t launch_normalize_and_map(const Plan& P, double* dOut, int32_t ncols, double* dWork,
                                      cudaStream_t st);
 
+// Grid points x0 + i*h of an L[0] x L[1] x L[2] box (axis 1 fastest).
+cudaError_t launch_grid_points(double* dX, int32_t nDim, const int32_t* L, const double* x0, const double* h,
+                               cudaStream_t st);
+
+// Border correction of a blended group field, then (applyMarginal) the
+// marginal map; G carries nDim, Nmc, gDims, gTotal, bRamp and the marginal.
+cudaError_t launch_blend_finish(const Plan& G, double* dOut, int32_t applyMarginal, cudaStream_t st);
+
 // Shared-memory bytes the tcgen05 kernel needs for this plan (0 if it
 // cannot fit).
 size_t tc_smem_bytes(const Plan& P, int* stages);

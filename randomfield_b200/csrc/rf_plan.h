@@ -61,6 +61,16 @@ struct Plan {
   int32_t applyMarginal;      // 0 when a normalisation pass follows
   int32_t lognormal;
   double margSd, margAvg;
+  // localization blend (localization_RF.f90:199-263, 705-857): the request
+  // is subdomain of a structured group grid; its points are the subdomain's
+  // grid points (axis 1 fastest) and the epilogue adds the partition-of-unity
+  // weight times the Gaussian field into the group field at bOrigin
+  int32_t blend;
+  int32_t bDims[3];           // subdomain grid points per axis
+  int32_t bOrigin[3];         // subdomain origin in group grid indices
+  int32_t gDims[3];           // group grid points per axis
+  int32_t bRamp[3];           // overlapNPoints per axis (< 1: no ramp)
+  int64_t gTotal;             // group grid points
 };
 
 // Shared-memory and TMEM slot layout of one tcgen05 launch: B slot s at

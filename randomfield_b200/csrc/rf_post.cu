@@ -4,6 +4,7 @@
 // for normalisation; otherwise the map is fused into the contraction
 // epilogue.  Sums are FP64: column mean, then the mean square of the
 // centred column, exactly the two reductions of the reference.
+#include "rf_blend.cuh"
 #include "rf_device.cuh"
 #include "rf_launch.h"
 
@@ -58,7 +59,62 @@ __global__ void rf_apply_kernel(double* __restrict__ f, int64_t n, int32_t ncols
   }
 }
 
+// Border correction of a blended group field (calls_RF.f90:324-369): a
+// group without neighbours divides by its partition of unity built with
+// `reverse`, i.e. the ramps of every outer face (the subdomains ramped their
+// faces on the group border too); then the marginal map unless a
+// normalisation pass follows.  P describes the group: gDims, bRamp, nDim.
+__global__ void rf_blend_finish_kernel(double* __restrict__ f, const Plan P, int32_t applyMarginal) {
+  const int col = blockIdx.y;
+  double* c = f + (int64_t)col * P.gTotal;
+  for (int64_t g = (int64_t)blockIdx.x * kThreads + threadIdx.x; g < P.gTotal; g += (int64_t)gridDim.x * kThreads) {
+    const int32_t i1 = (int32_t)(g % P.gDims[0]);
+    const int64_t t = g / P.gDims[0];
+    const int32_t i2 = (int32_t)(t % P.gDims[1]), i3 = (int32_t)(t / P.gDims[1]);
+    double w = blend_ramp(i1, P.gDims[0], P.bRamp[0]);
+    if (P.nDim > 1) w = w * blend_ramp(i2, P.gDims[1], P.bRamp[1]);
+    if (P.nDim > 2) w = w * blend_ramp(i3, P.gDims[2], P.bRamp[2]);
+    double v = c[g] / w;
+    if (applyMarginal) {
+      v = v * P.margSd + P.margAvg;
+      if (P.lognormal) v = exp(v);
+    }
+    c[g] = v;
+  }
+}
+
+// Grid points of a box: x_d = x0_d + i_d * h_d, axis 1 fastest (setGrid,
+// math_RF.f90:16-92), point-major (the coordinates of a point contiguous).
+__global__ void rf_grid_points_kernel(double* __restrict__ x, int32_t nDim, int32_t L0, int32_t L1, int32_t L2,
+                                      double x0, double x1, double x2, double h0, double h1, double h2) {
+  const int64_t total = (int64_t)L0 * L1 * L2;
+  for (int64_t p = (int64_t)blockIdx.x * kThreads + threadIdx.x; p < total; p += (int64_t)gridDim.x * kThreads) {
+    const int32_t i0 = (int32_t)(p % L0);
+    const int64_t t = p / L0;
+    const int32_t i1 = (int32_t)(t % L1), i2 = (int32_t)(t / L1);
+    x[p * nDim] = x0 + (double)i0 * h0;
+    if (nDim > 1) x[p * nDim + 1] = x1 + (double)i1 * h1;
+    if (nDim > 2) x[p * nDim + 2] = x2 + (double)i2 * h2;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_grid_points(double* dX, int32_t nDim, const int32_t* L, const double* x0, const double* h,
+                               cudaStream_t st) {
+  const int64_t total = (int64_t)L[0] * L[1] * L[2];
+  const int64_t want = (total + kThreads - 1) / kThreads;
+  const unsigned bx = (unsigned)(want < 1184 ? want : 1184);
+  rf_grid_points_kernel<<<bx, kThreads, 0, st>>>(dX, nDim, L[0], L[1], L[2], x0[0], x0[1], x0[2], h[0], h[1], h[2]);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_blend_finish(const Plan& G, double* dOut, int32_t applyMarginal, cudaStream_t st) {
+  const int64_t want = (G.gTotal + kThreads - 1) / kThreads;
+  const unsigned bx = (unsigned)(want < 296 ? want : 296);
+  rf_blend_finish_kernel<<<dim3(bx, G.Nmc), kThreads, 0, st>>>(dOut, G, applyMarginal);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_normalize_and_map(const Plan& P, double* dOut, int32_t ncols, double* dWork, cudaStream_t st) {
   double* sum = dWork;

@@ -20,7 +20,8 @@
 //               TMEM (tcgen05.st), lane = point; the two warps of a TMEM lane
 //               quarter split the columns; after the last stage of a tile they
 //               run the fused epilogue (tcgen05.ld, ampMult, marginal map,
-//               FP64 stores);
+//               FP64 stores; or the localization blend's weighted add into
+//               the group field);
 //   warp 9      producer (one thread): 1-D bulk copies (TMA) of B stages from
 //               HBM/L2 into SMEM; no multicast.
 // The issuing thread can run only about one MMA ahead of the tensor core, so
@@ -38,6 +39,7 @@
 // TMEM: accumulator columns [0, aCol0), then the A slots (SlotLayout).
 // Every wait is bounded (globaltimer); on expiry the kernel raises an error
 // word, drains its own async work, frees TMEM and returns.
+#include "rf_blend.cuh"
 #include "rf_device.cuh"
 #include "rf_gen.cuh"
 #include "rf_launch.h"
@@ -393,6 +395,9 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
       if (!mbar_wait_warp(&bars->acc_full, accPh, abort_flag)) { ok = false; break; }
       tc_fence_after();
       const int half = P.nmcPad / 2;
+      double bw = 0.0;  // localization blend: weight and group index of this point
+      int64_t bg = 0;
+      if (P.blend && valid) bw = blend_weight(P, p, &bg);
       for (int cb = h * half; cb < (h + 1) * half; cb += 8) {
         uint32_t va[8], lo[8];
         tmem_ld8(tbase + laneOff + cb, va);
@@ -404,7 +409,11 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
             const int r = cb + j;
             float acc = __uint_as_float(va[j]);
             if (PREC == PREC_BF16) acc += __uint_as_float(lo[j]);
-            if (r < P.nmcBlk) v.out[(int64_t)(P.rOff + r) * P.n + p] = finish_value(P, acc);
+            if (r >= P.nmcBlk) continue;
+            if (P.blend)
+              atomicAdd(&v.out[(int64_t)(P.rOff + r) * P.gTotal + bg], bw * ((double)acc * P.outScale));
+            else
+              v.out[(int64_t)(P.rOff + r) * P.n + p] = finish_value(P, acc);
           }
         }
       }

@@ -143,3 +143,20 @@ def test_no_gpu_fails_loudly():
     x = grid(4, 0.5).T
     rc, msg = call(x)
     assert rc == -25 and "device" in msg
+
+
+def test_blend_layout_rounds_overlap_and_checks_the_split():
+    """rf_blend_layout (host only): topography_RF.f90:49-52 overlap rounding
+    and localization_RF.f90:746 overlapNPoints; subdomains share O points."""
+    g = rf.BlendGrid.make((21, 21, 21), (0.1, 0.1, 0.1), (2, 2, 2), 0.4)
+    assert rf.blend_layout(g, (1.0, 1.0, 1.0)) == ([12, 12, 12], [3, 3, 3])
+    # overlap below two steps on a split axis is raised to two steps: O = 1
+    g = rf.BlendGrid.make((21, 21), (0.1, 0.1), (2, 1), 0.05)
+    L, O = rf.blend_layout(g, (1.0, 1.0))
+    assert O[0] == 1 and L[0] == 11 and L[1] == 21 and O[1] < 1
+    g = rf.BlendGrid.make((256, 256, 256), (0.05,) * 3, (2, 2, 2), 0.65)
+    assert rf.blend_layout(g, (1.0, 1.0, 1.0)) == ([134, 134, 134], [12, 12, 12])
+    g = rf.BlendGrid.make((20, 20, 20), (0.1,) * 3, (2, 2, 2), 0.4)
+    with pytest.raises(rf.RandomFieldError) as e:
+        rf.blend_layout(g, (1.0, 1.0, 1.0))
+    assert e.value.code == -8
