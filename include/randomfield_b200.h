@@ -259,6 +259,10 @@ void rf_server_config_init(rf_server_config* cfg);
 int rf_server_create(const rf_server_config* cfg, rf_server** out);
 /* Queues a request (host buffers); *ticket identifies it for rf_server_wait. */
 int rf_server_submit(rf_server* srv, const rf_request* req, int64_t* ticket);
+/* Queues a localization blend (rf_generate_blended's arguments, host randField). */
+int rf_server_submit_blended(rf_server* srv, const rf_blend_grid* grid, int corrMod, int margiFirst,
+                             const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method,
+                             double* randField, const rf_options* opt, int64_t* ticket);
 /* Waits (timeout_s < 0: forever) for a request; returns its status
  * (RF_ETIMEDOUT when the wait timed out) and its latency in milliseconds. */
 int rf_server_wait(rf_server* srv, int64_t ticket, double timeout_s, double* latency_ms);

@@ -51,7 +51,7 @@ EXPORTS = [
     "rf_context_set_timing", "rf_context_last_times", "rf_generate_device_noalloc",
     "rf_generate_batch", "rf_generate_batch_device", "rf_batch_last_stats",
     "rf_server_config_init", "rf_server_create", "rf_server_submit", "rf_server_wait", "rf_server_get_stats",
-    "rf_server_destroy", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
+    "rf_server_destroy", "rf_server_submit_blended", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
 ]
 
 
@@ -240,6 +240,8 @@ def lib() -> C.CDLL:
         L.rf_server_get_stats.argtypes = [C.c_void_p, P(ServerStats)]
         L.rf_server_destroy.argtypes = [C.c_void_p]
         L.rf_blend_layout.argtypes = [P(BlendGrid), P(d), P(C.c_int32), P(C.c_int32)]
+        L.rf_server_submit_blended.argtypes = [C.c_void_p, P(BlendGrid), i32, i32, P(d), d, d, i32, i32, P(d),
+                                               P(Options), P(i64)]
         L.rf_generate_blended.argtypes = [C.c_void_p, P(BlendGrid), i32, i32, P(d), d, d, i32, i32, P(d),
                                           P(Options)]
         L.rf_generate_blended_device.argtypes = [C.c_void_p, P(BlendGrid), i32, i32, P(d), d, d, i32, i32,
@@ -401,6 +403,21 @@ class Server:
         t = C.c_int64()
         _check(lib().rf_server_submit(self._h, C.byref(request), C.byref(t)))
         self._keep[t.value] = (request, keep)
+        return t.value
+
+    def submit_blended(self, grid: "BlendGrid", corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method,
+                       randField, options=None, **kw) -> int:
+        """Queues a localization blend; randField is a Fortran-ordered
+        float64 (group points x Nmc) array kept alive until ``wait``."""
+        cl = np.ascontiguousarray(np.asarray(corrL, dtype=np.float64).reshape(-1))
+        o = _opts(options if options is not None else (kw or None))
+        t = C.c_int64()
+        P = C.POINTER(C.c_double)
+        _check(lib().rf_server_submit_blended(self._h, C.byref(grid), _id(corrMod, _CORRMOD, "corrMod"),
+                                              _id(margiFirst, _MARGI, "margiFirst"), cl.ctypes.data_as(P),
+                                              float(fieldAvg), float(fieldVar), int(Nmc), int(method),
+                                              randField.ctypes.data_as(P), C.byref(o), C.byref(t)))
+        self._keep[t.value] = (grid, randField, cl, o)
         return t.value
 
     def wait(self, ticket: int, timeout_s: float = -1.0) -> float:

@@ -57,12 +57,6 @@ DescLayout desc_layout(size_t capUnits, size_t capItems, int numSMs) {
   return d;
 }
 
-// A request that is a subdomain of a localization blend (rf_blend.cuh).
-struct BlendSpec {
-  int32_t bDims[3], bOrigin[3], gDims[3], bRamp[3];
-  int64_t gTotal;
-};
-
 struct BatchState {
   std::vector<Plan> plans;         // per request, before the realization split
   std::vector<const double*> dx;   // device points per request
@@ -128,7 +122,7 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
       P.rOff = r0;
       P.nmcBlk = std::min(rblk, P0.Nmc - r0);
       if (int rc = layout(P)) return rc;
-      if (!B.blend.empty()) apply_blend(P, B.blend[i]);
+      if (!B.blend.empty() && B.blend[i].gTotal > 0) apply_blend(P, B.blend[i]);
       GroupSub g;
       memset(&g, 0, sizeof(g));
       g.P = P;
@@ -325,10 +319,15 @@ int run_batch(rf_context* c, const rf_request* reqs, int32_t count, const std::v
 namespace rfh {
 
 int batch_run_device(rf_context* c, const std::vector<Request>& rq, const std::vector<const double*>& dx,
-                     const std::vector<double*>& dout, const std::vector<double>& ext, cudaStream_t st) {
+                     const std::vector<double*>& dout, const std::vector<double>& ext, cudaStream_t st,
+                     const std::vector<BlendSpec>* blend) {
   BatchState B;
   B.dx = dx;
   B.dout = dout;
+  if (blend && !blend->empty()) {
+    B.blend = *blend;
+    B.accumulate = true;
+  }
   return run_batch(c, nullptr, (int32_t)rq.size(), rq, ext, B, st);
 }
 
@@ -409,8 +408,22 @@ int blend_geometry(const rf_blend_grid* g, const double* corrL, int32_t* L, int3
   return RF_OK;
 }
 
-// The blended field of `grid` into the device array dOut (group points x Nmc).
-int run_blended(rf_context* c, const rf_blend_grid* grid, const Request& base, double* dOut, cudaStream_t st) {
+}  // namespace
+
+namespace rfh {
+
+int blend_points_bytes(const rf_blend_grid* grid, const double* corrL, size_t* bytes) {
+  int32_t L[3], O[3];
+  if (int rc = blend_geometry(grid, corrL, L, O)) return rc;
+  int nSub = 1;
+  for (int d = 0; d < grid->nDim; ++d) nSub *= grid->nFields[d];
+  *bytes = sizeof(double) * (size_t)L[0] * L[1] * L[2] * grid->nDim * nSub;
+  return RF_OK;
+}
+
+int blend_expand(const rf_blend_grid* grid, const Request& base, double* dOut, double* dPoints, cudaStream_t st,
+                 std::vector<Request>& rq, std::vector<const double*>& dx, std::vector<double*>& dout,
+                 std::vector<BlendSpec>& spec, Plan* groupPlan) {
   int32_t L[3], O[3];
   if (int rc = blend_geometry(grid, base.corrL, L, O)) return rc;
   if (base.opt.precision == RF_PREC_FP32) return fail(RF_ENOTSUP, "the blend runs the tensor-core forms");
@@ -429,18 +442,10 @@ int run_blended(rf_context* c, const rf_blend_grid* grid, const Request& base, d
     const auto t = std::chrono::steady_clock::now().time_since_epoch().count();
     seed0 = (int64_t)((uint64_t)t % 100000000ull);
   }
-  if (int rc = ensure(c->dX, c->capX, sizeof(double) * (size_t)sub * nd * nSub, "subdomain points")) return rc;
   RF_CUDA(cudaMemsetAsync(dOut, 0, sizeof(double) * (size_t)gTotal * base.Nmc, st), "clear of randField");
-  BatchState B;
-  std::vector<Request> rq(nSub);
-  std::vector<double> ext(3 * nSub, 0.0);
-  B.dx.resize(nSub);
-  B.dout.assign(nSub, dOut);
-  B.blend.resize(nSub);
-  B.accumulate = true;
   for (int f = 0; f < nSub; ++f) {
     const int32_t fi[3] = {f % F[0], (f / F[0]) % F[1], f / (F[0] * F[1])};
-    BlendSpec& b = B.blend[f];
+    BlendSpec b;
     double x0[3] = {0, 0, 0}, h[3] = {0, 0, 0};
     for (int d = 0; d < 3; ++d) {
       b.bDims[d] = L[d];
@@ -453,20 +458,22 @@ int run_blended(rf_context* c, const rf_blend_grid* grid, const Request& base, d
       }
     }
     b.gTotal = gTotal;
-    double* dx = c->dX + (size_t)f * sub * nd;
-    RF_CUDA(launch_grid_points(dx, nd, L, x0, h, st), "subdomain points kernel");
-    c->launches += 1;
-    B.dx[f] = dx;
-    rq[f] = base;
-    rq[f].n = sub;
-    rq[f].opt.seed_start = seed0 + f + 1;  // fieldNumber = f + 1
-    rq[f].opt.normalize = 0;
-    for (int d = 0; d < nd; ++d) rq[f].opt.x_range[d] = (double)(L[d] - 1) * grid->xStep[d];
+    double* px = dPoints + (size_t)f * sub * nd;
+    RF_CUDA(launch_grid_points(px, nd, L, x0, h, st), "subdomain points kernel");
+    Request r = base;
+    r.n = sub;
+    r.opt.seed_start = seed0 + f + 1;  // fieldNumber = f + 1
+    r.opt.normalize = 0;
+    for (int d = 0; d < nd; ++d) r.opt.x_range[d] = (double)(L[d] - 1) * grid->xStep[d];
+    rq.push_back(r);
+    dx.push_back(px);
+    dout.push_back(dOut);
+    spec.push_back(b);
   }
-  if (int rc = run_batch(c, nullptr, nSub, rq, ext, B, st)) return rc;
-  // the group: border correction, then the marginal map (or normalisation)
-  Plan Gp;
-  if (int rc = build_plan(rq[0], &ext[0], Gp)) return rc;
+  // the group plan: marginal parameters of the request, group geometry
+  const double zero[3] = {0, 0, 0};
+  if (int rc = build_plan(rq.back(), zero, *groupPlan)) return rc;
+  Plan& Gp = *groupPlan;
   Gp.nDim = nd;
   Gp.n = gTotal;
   Gp.gTotal = gTotal;
@@ -474,16 +481,41 @@ int run_blended(rf_context* c, const rf_blend_grid* grid, const Request& base, d
     Gp.gDims[d] = G[d];
     Gp.bRamp[d] = d < nd ? O[d] : 0;
   }
-  const bool norm = base.opt.normalize != 0;
-  RF_CUDA(launch_blend_finish(Gp, dOut, norm ? 0 : 1, st), "border correction kernel");
+  Gp.normalize = base.opt.normalize ? 1 : 0;
+  return RF_OK;
+}
+
+int blend_finish(rf_context* c, const Plan& Gp, double* dOut, cudaStream_t st) {
+  RF_CUDA(launch_blend_finish(Gp, dOut, Gp.normalize ? 0 : 1, st), "border correction kernel");
   c->launches += 1;
-  if (norm) {
+  if (Gp.normalize) {
     if ((size_t)2 * Gp.Nmc * sizeof(double) > c->capWork)
       if (int rc = ensure(c->dWork, c->capWork, (size_t)2 * Gp.Nmc * sizeof(double), "moments")) return rc;
     RF_CUDA(launch_normalize_and_map(Gp, dOut, Gp.Nmc, c->dWork, st), "normalisation kernels");
     c->launches += 3;
   }
   return RF_OK;
+}
+
+}  // namespace rfh
+
+namespace {
+
+// The blended field of `grid` into the device array dOut (group points x Nmc).
+int run_blended(rf_context* c, const rf_blend_grid* grid, const Request& base, double* dOut, cudaStream_t st) {
+  size_t pb = 0;
+  if (int rc = blend_points_bytes(grid, base.corrL, &pb)) return rc;
+  if (int rc = ensure(c->dX, c->capX, pb, "subdomain points")) return rc;
+  std::vector<Request> rq;
+  std::vector<const double*> dx;
+  std::vector<double*> dout;
+  std::vector<BlendSpec> spec;
+  Plan Gp;
+  if (int rc = blend_expand(grid, base, dOut, c->dX, st, rq, dx, dout, spec, &Gp)) return rc;
+  c->launches += (int32_t)rq.size();
+  const std::vector<double> ext(3 * rq.size(), 0.0);
+  if (int rc = batch_run_device(c, rq, dx, dout, ext, st, &spec)) return rc;
+  return blend_finish(c, Gp, dOut, st);
 }
 
 }  // namespace

@@ -104,10 +104,27 @@ Request make_request(int nDim, int64_t n, int corrMod, int margiFirst, const dou
                      double fieldVar, int Nmc, int method, const rf_options* opt);
 void launch_extent(const double* dX, int64_t n, int nDim, double* part, cudaStream_t st);
 
+// A request that is a subdomain of a localization blend (rf_blend.cuh);
+// gTotal == 0 marks a plain request in a batch that mixes both.
+struct BlendSpec {
+  int32_t bDims[3], bOrigin[3], gDims[3], bRamp[3];
+  int64_t gTotal;
+};
+
 // rf_batch.cu: plan and run a batch whose points and fields are in device
-// memory (queued on st; returns without waiting).
+// memory (queued on st; returns without waiting).  With `blend`, one spec per
+// request.
 int batch_run_device(rf_context* c, const std::vector<Request>& rq, const std::vector<const double*>& dx,
-                     const std::vector<double*>& dout, const std::vector<double>& ext, cudaStream_t st);
+                     const std::vector<double*>& dout, const std::vector<double>& ext, cudaStream_t st,
+                     const std::vector<BlendSpec>* blend = nullptr);
+// Blend requests (rf_generate_blended): bytes of the subdomain points; the
+// subdomain requests (appended, points generated into dPoints, dOut
+// cleared) and the group plan; the border correction and marginal map.
+int blend_points_bytes(const rf_blend_grid* grid, const double* corrL, size_t* bytes);
+int blend_expand(const rf_blend_grid* grid, const Request& base, double* dOut, double* dPoints, cudaStream_t st,
+                 std::vector<Request>& rq, std::vector<const double*>& dx, std::vector<double*>& dout,
+                 std::vector<BlendSpec>& spec, rfb::Plan* groupPlan);
+int blend_finish(rf_context* c, const rfb::Plan& Gp, double* dOut, cudaStream_t st);
 // Device bytes a request holds in a batch with realization block rblk:
 // points, field, operands.
 int request_footprint(const Request& rq, const double* ext, int rblk, size_t* bytes);

@@ -42,6 +42,12 @@ struct Pending {
   double ext[3];
   size_t bytes;    // device footprint in a batch
   double tSubmit;
+  bool blended = false;  // a localization blend on `grid` (rq.n unused; the field has gPoints points)
+  rf_blend_grid grid;
+  int64_t gPoints = 0;
+  size_t pointBytes = 0;  // subdomain points of a blend
+  // the number of field values and the input bytes the request moves
+  int64_t fieldPoints() const { return blended ? gPoints : rq.n; }
 };
 
 struct Result {
@@ -106,8 +112,9 @@ int launch_slot(rf_server* s, Slot& sl) {
   std::vector<char> pinX(n), pinO(n);
   for (size_t i = 0; i < n; ++i) {
     const Pending& p = sl.batch[i];
-    const size_t xb = sizeof(double) * (size_t)p.rq.n * p.rq.nDim, ob = sizeof(double) * (size_t)p.rq.n * p.rq.Nmc;
-    pinX[i] = pinned(p.req.xPoints);
+    const size_t ob = sizeof(double) * (size_t)p.fieldPoints() * p.rq.Nmc;
+    const size_t xb = p.blended ? p.pointBytes : sizeof(double) * (size_t)p.rq.n * p.rq.nDim;
+    pinX[i] = p.blended ? 1 : pinned(p.req.xPoints);
     pinO[i] = pinned(p.req.randField);
     stage += (pinX[i] ? 0 : align_up(xb)) + (pinO[i] ? 0 : align_up(ob));
     io += align_up(xb) + align_up(ob);
@@ -115,42 +122,60 @@ int launch_slot(rf_server* s, Slot& sl) {
   if (stage > 0)
     if (int rc = ensure_host(sl.hStage, sl.capStage, stage, "serving staging")) return rc;
   if (int rc = ensure(c->dX, c->capX, io, "serving points and fields")) return rc;
-  std::vector<Request> rq(n);
-  std::vector<const double*> dx(n);
-  std::vector<double*> dout(n);
-  std::vector<double> ext(3 * n);
+  std::vector<Request> rq;
+  std::vector<const double*> dx;
+  std::vector<double*> dout, fieldOut(n);
+  std::vector<double> ext;
+  std::vector<BlendSpec> spec;
+  std::vector<std::pair<size_t, Plan>> groups;  // blended requests: index, group plan
   sl.outOff.assign(n, 0);
   unsigned char* dbase = reinterpret_cast<unsigned char*>(c->dX);
   size_t off = 0, soff = 0;
   for (size_t i = 0; i < n; ++i) {
     const Pending& p = sl.batch[i];
-    const size_t xb = sizeof(double) * (size_t)p.rq.n * p.rq.nDim, ob = sizeof(double) * (size_t)p.rq.n * p.rq.Nmc;
-    const void* src = p.req.xPoints;
-    if (!pinX[i]) {
-      memcpy(sl.hStage + soff, p.req.xPoints, xb);
-      src = sl.hStage + soff;
-      soff += align_up(xb);
-    }
-    dx[i] = reinterpret_cast<const double*>(dbase + off);
-    RF_CUDA(cudaMemcpyAsync(dbase + off, src, xb, cudaMemcpyHostToDevice, st), "copy of xPoints");
-    off += align_up(xb);
-    dout[i] = reinterpret_cast<double*>(dbase + off);
+    const size_t ob = sizeof(double) * (size_t)p.fieldPoints() * p.rq.Nmc;
+    double* pts = reinterpret_cast<double*>(dbase + off);
+    off += align_up(p.blended ? p.pointBytes : sizeof(double) * (size_t)p.rq.n * p.rq.nDim);
+    double* fld = reinterpret_cast<double*>(dbase + off);
     off += align_up(ob);
+    fieldOut[i] = fld;
     if (pinO[i]) {
       sl.outOff[i] = SIZE_MAX;
     } else {
       sl.outOff[i] = soff;
       soff += align_up(ob);
     }
-    rq[i] = p.rq;
-    for (int d = 0; d < 3; ++d) ext[3 * i + d] = p.ext[d];
+    if (p.blended) {
+      Plan Gp;
+      if (int rc = blend_expand(&p.grid, p.rq, fld, pts, st, rq, dx, dout, spec, &Gp)) return rc;
+      while (ext.size() < 3 * rq.size()) ext.push_back(0.0);
+      groups.push_back({i, Gp});
+      continue;
+    }
+    const size_t xb = sizeof(double) * (size_t)p.rq.n * p.rq.nDim;
+    const void* src = p.req.xPoints;
+    if (!pinX[i]) {
+      memcpy(sl.hStage + soff, p.req.xPoints, xb);
+      src = sl.hStage + soff;
+      soff += align_up(xb);
+    }
+    RF_CUDA(cudaMemcpyAsync(pts, src, xb, cudaMemcpyHostToDevice, st), "copy of xPoints");
+    rq.push_back(p.rq);
+    dx.push_back(pts);
+    dout.push_back(fld);
+    for (int d = 0; d < 3; ++d) ext.push_back(p.ext[d]);
+    BlendSpec none;
+    memset(&none, 0, sizeof(none));
+    spec.push_back(none);
   }
-  if (int rc = batch_run_device(c, rq, dx, dout, ext, st)) return rc;
+  if (int rc = batch_run_device(c, rq, dx, dout, ext, st, groups.empty() ? nullptr : &spec)) return rc;
+  for (auto& g : groups)
+    if (int rc = blend_finish(c, g.second, fieldOut[g.first], st)) return rc;
   for (size_t i = 0; i < n; ++i) {
     const Pending& p = sl.batch[i];
-    const size_t ob = sizeof(double) * (size_t)p.rq.n * p.rq.Nmc;
+    const size_t ob = sizeof(double) * (size_t)p.fieldPoints() * p.rq.Nmc;
     void* dst = sl.outOff[i] == SIZE_MAX ? (void*)p.req.randField : (void*)(sl.hStage + sl.outOff[i]);
-    RF_CUDA(cudaMemcpyAsync(dst, dout[i], ob, cudaMemcpyDeviceToHost, st), "copy of randField");
+    RF_CUDA(cudaMemcpyAsync(dst, fieldOut[i], ob, cudaMemcpyDeviceToHost, st), "copy of randField");
   }
   RF_CUDA(cudaEventRecord(sl.evDone, st), "cudaEventRecord");
   (void)s;
@@ -173,7 +198,7 @@ void finish_slot(rf_server* s, Slot& sl) {
       for (size_t i = 0; i < sl.batch.size(); ++i) {
         const Pending& p = sl.batch[i];
         if (sl.outOff[i] != SIZE_MAX)
-          memcpy(p.req.randField, sl.hStage + sl.outOff[i], sizeof(double) * (size_t)p.rq.n * p.rq.Nmc);
+          memcpy(p.req.randField, sl.hStage + sl.outOff[i], sizeof(double) * (size_t)p.fieldPoints() * p.rq.Nmc);
       }
     }
   }
@@ -188,7 +213,7 @@ void finish_slot(rf_server* s, Slot& sl) {
       if (status != RF_OK) r.error = sl.error.empty() ? g_err : sl.error;
       if (status == RF_OK) {
         s->st.completed += 1;
-        s->st.field_values += (double)p.rq.n * (double)p.rq.Nmc;
+        s->st.field_values += (double)p.fieldPoints() * (double)p.rq.Nmc;
         s->latencies.push_back(r.latency_ms);
       } else {
         s->st.failed += 1;
@@ -362,6 +387,52 @@ int rf_server_submit(rf_server* s, const rf_request* req, int64_t* ticket) {
     p.ext[d] = hi - lo;
   }
   if (int rc = request_footprint(p.rq, p.ext, s->block, &p.bytes)) return rc;
+  p.tSubmit = now_s();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return fail(RF_EINVAL_ARG, "the server is stopping");
+    p.ticket = s->nextTicket++;
+    *ticket = p.ticket;
+    s->results[p.ticket] = Result{};
+    s->st.submitted += 1;
+    s->queue.push_back(std::move(p));
+  }
+  s->cvWork.notify_one();
+  return RF_OK;
+}
+
+int rf_server_submit_blended(rf_server* s, const rf_blend_grid* grid, int corrMod, int margiFirst,
+                             const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method,
+                             double* randField, const rf_options* opt, int64_t* ticket) {
+  g_err.clear();
+  if (!s || !grid || !corrL || !randField || !ticket) return fail(RF_EINVAL_ARG, "null pointer argument");
+  Pending p;
+  memset(&p.req, 0, sizeof(p.req));
+  p.req.randField = randField;
+  p.rq = make_request(grid->nDim, 1, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
+  p.rq.opt.precision = s->cfg.precision;
+  p.rq.opt.device = s->cfg.device;
+  if (int rc = validate(p.rq)) return rc;
+  if (p.rq.opt.literal) return fail(RF_ENOTSUP, "literal mode is not available in the serving loop");
+  p.blended = true;
+  p.grid = *grid;
+  if (int rc = blend_points_bytes(grid, p.rq.corrL, &p.pointBytes)) return rc;
+  p.gPoints = 1;
+  for (int d = 0; d < grid->nDim; ++d) p.gPoints *= grid->xNStep[d];
+  // footprint: points, group field, the operands of every subdomain
+  int32_t L[3], O[3];
+  if (int rc = rf_blend_layout(grid, p.rq.corrL, L, O)) return rc;
+  Request sub = p.rq;
+  sub.n = (int64_t)L[0] * L[1] * L[2];
+  for (int d = 0; d < grid->nDim; ++d) sub.opt.x_range[d] = (double)(L[d] - 1) * grid->xStep[d];
+  size_t subBytes = 0;
+  const double zero[3] = {0, 0, 0};
+  if (int rc = request_footprint(sub, zero, s->block, &subBytes)) return rc;
+  int nSub = 1;
+  for (int d = 0; d < grid->nDim; ++d) nSub *= grid->nFields[d];
+  const size_t subIO = sizeof(double) * (size_t)sub.n * (sub.nDim + sub.Nmc);
+  p.bytes = p.pointBytes + sizeof(double) * (size_t)p.gPoints * Nmc + (size_t)nSub * (subBytes > subIO ? subBytes - subIO : 0);
+  for (int d = 0; d < 3; ++d) p.ext[d] = 0.0;
   p.tSubmit = now_s();
   {
     std::lock_guard<std::mutex> lk(s->mu);

@@ -105,3 +105,31 @@ def test_admission_rejects_oversized_request():
         assert st["failed"] == 1 and st["completed"] == 1
     finally:
         srv.close()
+
+
+def test_blended_request_in_the_mix():
+    """A localization blend submitted among plain requests gives the field of
+    rf_generate_blended alone (FP64 atomic adds make the order of the
+    subdomain contributions vary: relative difference <= 1e-12)."""
+    grid = rf.BlendGrid.make((21, 21, 21), (0.1, 0.1, 0.1), (2, 2, 2), 0.4)
+    ctx = rf.Context(0)
+    alone = ctx.generate_blended(grid, "gaussian", "lognormal", (1.0, 1.0, 1.0), 1.0, 0.25, 3, 2, precision="bf16",
+                                 seed_start=8, k_nstep=(24, 24, 24))
+    ctx.close()
+    srv = rf.Server(precision="bf16")
+    try:
+        tickets = []
+        for i, (x, Nmc, method, seed, marg) in enumerate(_mix()[:5]):
+            r, xf, out = _req(x, Nmc, method, seed, marg)
+            tickets.append(srv.submit(r, keep=(xf, out)))
+            if i == 2:
+                mixed = np.full(alone.shape, np.nan, order="F")
+                tb = srv.submit_blended(grid, "gaussian", "lognormal", (1.0, 1.0, 1.0), 1.0, 0.25, 3, 2, mixed,
+                                        seed_start=8, k_nstep=(24, 24, 24))
+        srv.wait(tb)
+        for t in tickets:
+            srv.wait(t)
+        assert np.isfinite(mixed).all()
+        assert errors(np.log(mixed), np.log(alone))[1] <= 1e-12
+    finally:
+        srv.close()
