@@ -26,6 +26,7 @@ extern "C" {
 /* Methods, correlation models and marginals: constants_RF.f90:12-21. */
 #define RF_ISOTROPIC 1
 #define RF_SHINOZUKA 2
+#define RF_RANDOMIZATION 3  /* Shinozuka sum over uniformly random wavevectors (randomFieldND.f90:343-361) */
 #define RF_CM_GAUSSIAN 1
 #define RF_CM_COS 2
 #define RF_FOM_GAUSSIAN 1
@@ -43,7 +44,7 @@ extern "C" {
 #define RF_EINVAL_NDIM -2       /* nDim outside 1..3, or < 2 for isotropic                   */
 #define RF_EINVAL_CORRL -3      /* corrL(i) <= 0               (type_inputRF.f90:1159-1206) */
 #define RF_EINVAL_LOGNORMAL -4  /* lognormal with fieldAvg <= 0 (randomFieldND.f90:162-166) */
-#define RF_EINVAL_METHOD -5     /* method not 1 or 2                                        */
+#define RF_EINVAL_METHOD -5     /* method not 1, 2 or 3                                     */
 #define RF_EINVAL_CORRMOD -6    /* corrMod not 1 or 2; cm_COS with 6 or fewer wavevectors    */
 #define RF_EINVAL_MARGINAL -7   /* margiFirst not 1 or 2                                    */
 #define RF_EINVAL_RANGE -8      /* zero extent along an axis (kDelta would be infinite)      */

@@ -18,7 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librfo.so")
 
-ISOTROPIC, SHINOZUKA = 1, 2
+ISOTROPIC, SHINOZUKA, RANDOMIZATION = 1, 2, 3
 CM_GAUSSIAN, CM_COS = 1, 2
 FOM_GAUSSIAN, FOM_LOGNORMAL = 1, 2
 

@@ -243,7 +243,7 @@ int32_t rfo_validate(const rfo_request* rq) {
   if (rq->corrMod != RFO_CM_GAUSSIAN && rq->corrMod != RFO_CM_COS) return RFO_EINVAL;
   if (rq->margiFirst != RFO_FOM_GAUSSIAN && rq->margiFirst != RFO_FOM_LOGNORMAL) return RFO_EINVAL;
   if (rq->margiFirst == RFO_FOM_LOGNORMAL && rq->fieldAvg <= 0.0) return RFO_EINVAL;
-  if (rq->method != RFO_SHINOZUKA && rq->method != RFO_ISOTROPIC) return RFO_EINVAL;
+  if (rq->method != RFO_SHINOZUKA && rq->method != RFO_ISOTROPIC && rq->method != RFO_RANDOMIZATION) return RFO_EINVAL;
   if (rq->method == RFO_ISOTROPIC && rq->nDim < 2) return RFO_EINVAL;
   if (rq->method == RFO_ISOTROPIC && rq->literal) return RFO_EINVAL;
   if (rq->seedStart < 0) return RFO_EINVAL;
@@ -274,7 +274,8 @@ int32_t rfo_geometry_of(const rfo_request* rq, rfo_geometry* g) {
     if (!(ext > 0.0)) return RFO_EINVAL; /* degenerate extent: kDelta = +inf */
     g->xRangeNorm[d] = ext / rq->corrL[d];
   }
-  if (rq->method == RFO_SHINOZUKA) {
+  if (rq->method != RFO_ISOTROPIC) {
+    /* Shinozuka and randomization share the grid sizes (spectra_RF.f90:87-124) */
     int64_t kn = 1;
     double prodDelta = 1.0;
     for (d = 0; d < rq->nDim; ++d) {
@@ -289,6 +290,13 @@ int32_t rfo_geometry_of(const rfo_request* rq, rfo_geometry* g) {
     }
     g->K = kn * ((int64_t)1 << (rq->nDim - 1));
     g->ampMult = 2.0 * sqrt(prodDelta / pow(2.0 * PI, (double)rq->nDim));
+    if (rq->method == RFO_RANDOMIZATION) {
+      /* randomFieldND.f90:262: 2*sqrt(1/(kNTotal*(2 PI)^nDim)) (literal).  A
+       * random wavevector of one quadrant represents kMax^nDim / kn of the
+       * spectral volume, which the intended amplitude restores. */
+      if (rq->literal) g->ampMult = 2.0 * sqrt(1.0 / ((double)g->K * pow(2.0 * PI, (double)rq->nDim)));
+      else g->ampMult = 2.0 * sqrt(pow(g->kMax, (double)rq->nDim) / ((double)kn * pow(2.0 * PI, (double)rq->nDim)));
+    }
   } else {
     double r2 = 0.0, kd;
     int32_t nr, nd;
@@ -329,25 +337,37 @@ int32_t rfo_kpoints(const rfo_request* rq, double* kPoints, double* amp, double*
   if (rc) return rc;
   K = g.K;
   if (rq->corrMod == RFO_CM_COS && K <= 6) return RFO_EINVAL; /* spectra_RF.f90:218 */
-  if (rq->method == RFO_SHINOZUKA) {
+  if (rq->method != RFO_ISOTROPIC) {
     int32_t nq = 1 << (rq->nDim - 1), q;
     int64_t kn = K / nq, b;
     double sign[4 * 3];
+    double* ubase = NULL;
     ksign(rq->nDim, sign);
+    if (rq->method == RFO_RANDOMIZATION) {
+      /* random_number(kPoints_base) then * kMax per axis (spectra_RF.f90:
+       * 119-124): nDim x kn draws, axis fastest, before the phases */
+      rfo_rnglib rng;
+      int64_t t;
+      ubase = (double*)malloc(sizeof(double) * kn * rq->nDim);
+      if (!ubase) return RFO_EINVAL;
+      if (rfo_rng_seed(&rng, rq->seedStart)) { free(ubase); return RFO_EINVAL; }
+      for (t = 0; t < kn * rq->nDim; ++t) ubase[t] = rfo_rng_r8_uni_01(&rng);
+    }
     for (q = 0; q < nq; ++q) {
       for (b = 0; b < kn; ++b) {
         int64_t rem = b;
         k = q * kn + b;
         for (d = 0; d < rq->nDim; ++d) {
           int64_t i = rem % g.kNStep[d];
-          rem /= g.kNStep[d];
           /* setGrid from 0 (spectra_RF.f90:118), then the sign copy :127-133
            * which starts at quadrant 2: the first quadrant stays unwritten. */
-          double base = 0.0 + g.kDelta[d] * (double)i;
+          double base = ubase ? ubase[b * rq->nDim + d] * g.kMax : 0.0 + g.kDelta[d] * (double)i;
+          rem /= g.kNStep[d];
           kPoints[k * rq->nDim + d] = (rq->literal && q == 0) ? 0.0 : base * sign[q * rq->nDim + d];
         }
       }
     }
+    free(ubase);
     for (k = 0; k < K; ++k) {
       double s;
       if (rq->corrMod == RFO_CM_GAUSSIAN) s = spectrum_gauss(&kPoints[k * rq->nDim], rq->nDim);
@@ -419,7 +439,9 @@ static int32_t draws(const rfo_request* rq, const rfo_geometry* g, double* phi, 
   int64_t K = g->K, k;
   int32_t r;
   if (rfo_rng_seed(&rng, rq->seedStart)) return RFO_EINVAL;
-  if (rq->method == RFO_SHINOZUKA) {
+  if (rq->method != RFO_ISOTROPIC) {
+    if (rq->method == RFO_RANDOMIZATION) /* the wavevector draws come first */
+      for (k = 0; k < (K >> (rq->nDim - 1)) * rq->nDim; ++k) (void)rfo_rng_i4_uni(&rng);
     for (r = 0; r < rq->Nmc; ++r)
       for (k = 0; k < K; ++k) {
         phi[k + K * r] = 2.0 * PI * rfo_rng_r8_uni_01(&rng);
@@ -576,7 +598,7 @@ int32_t rfo_generate(const rfo_request* rq, const int64_t* rows, int64_t nrows,
     for (d = 0; d < D; ++d) x[d] = rq->xPoints[i * D + d] / rq->corrL[d];
     for (r = 0; r < rq->Nmc; ++r) {
       double acc = 0.0;
-      if (rq->method == RFO_SHINOZUKA) {
+      if (rq->method != RFO_ISOTROPIC) {
         int64_t slab = i / t.g.xSlab + 1;
         int64_t tt = (int64_t)r * nSlab + slab;
         for (k = 0; k < K; ++k) {

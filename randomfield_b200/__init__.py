@@ -20,7 +20,7 @@ import numpy as np
 __all__ = [
     "RandomFieldError", "Options", "Context", "lib", "create_standard_gaussian_field_unstruct",
     "query_geometry", "generate_device_noalloc", "Request", "BatchStats", "make_request", "generate_batch",
-    "Server", "ServerConfig", "ServerStats", "BlendGrid", "blend_layout", "ISOTROPIC", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
+    "Server", "ServerConfig", "ServerStats", "BlendGrid", "blend_layout", "ISOTROPIC", "RANDOMIZATION", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
     "PREC_BF16", "PREC_FP16", "PREC_FP32", "PREC_BF16_FAST", "LIB_PATH", "STATUS",
 ]
 
@@ -28,7 +28,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librf_b200.so")
 
 # constants_RF.f90:12-21
-ISOTROPIC, SHINOZUKA = 1, 2
+ISOTROPIC, SHINOZUKA, RANDOMIZATION = 1, 2, 3
 CM_GAUSSIAN, CM_COS = 1, 2
 FOM_GAUSSIAN, FOM_LOGNORMAL = 1, 2
 PREC_BF16, PREC_FP16, PREC_FP32, PREC_BF16_FAST = 0, 1, 2, 3

@@ -73,8 +73,9 @@ int validate(const Request& r) {
   if (r.Nmc < 1) return fail(RF_EINVAL_NMC, "Nmc must be >= 1 (got %d)", r.Nmc);
   for (int d = 0; d < r.nDim; ++d)
     if (!(r.corrL[d] > 0.0)) return fail(RF_EINVAL_CORRL, "corrL(%d) must be > 0", d + 1);
-  if (r.method != RF_ISOTROPIC && r.method != RF_SHINOZUKA)
-    return fail(RF_EINVAL_METHOD, "method must be 1 (isotropic) or 2 (Shinozuka), got %d", r.method);
+  if (r.method != RF_ISOTROPIC && r.method != RF_SHINOZUKA && r.method != RF_RANDOMIZATION)
+    return fail(RF_EINVAL_METHOD, "method must be 1 (isotropic), 2 (Shinozuka) or 3 (randomization), got %d",
+                r.method);
   if (r.method == RF_ISOTROPIC && r.nDim < 2)
     return fail(RF_EINVAL_NDIM, "the isotropic method needs nDim 2 or 3");
   if (r.corrMod != RF_CM_GAUSSIAN && r.corrMod != RF_CM_COS)
@@ -86,8 +87,8 @@ int validate(const Request& r) {
   const rf_options& o = r.opt;
   if (o.precision < RF_PREC_BF16 || o.precision > RF_PREC_BF16_FAST)
     return fail(RF_EINVAL_ARG, "unknown precision form %d", o.precision);
-  if (o.literal && r.method != RF_SHINOZUKA)
-    return fail(RF_EINVAL_ARG, "literal mode exists for the Shinozuka method only");
+  if (o.literal && r.method == RF_ISOTROPIC)
+    return fail(RF_EINVAL_ARG, "literal mode exists for the Shinozuka and randomization methods only");
   for (int d = 0; d < 3; ++d)
     if (o.k_nstep[d] < 0 || o.k_nstep[d] == 1) return fail(RF_EINVAL_ARG, "k_nstep must be 0 or >= 2");
   if (o.iso_n_radial < 0 || o.iso_n_radial == 1 || o.iso_n_dir < 0)
@@ -120,7 +121,7 @@ int geometry(const Request& r, const double* ext, Plan& P) {
       return fail(RF_EINVAL_RANGE, "zero extent along axis %d: kDelta = 2 pi/(1.1 xRange) is infinite", d + 1);
     xr[d] = e / r.corrL[d];  // randomFieldND.f90:72
   }
-  if (r.method == RF_SHINOZUKA) {
+  if (r.method != RF_ISOTROPIC) {  // Shinozuka grid; randomization shares its sizes (spectra_RF.f90:87-124)
     int64_t kn = 1;
     double prod = 1.0;
     for (int d = 0; d < r.nDim; ++d) {
@@ -134,6 +135,13 @@ int geometry(const Request& r, const double* ext, Plan& P) {
     }
     P.K = kn * ((int64_t)1 << (r.nDim - 1));
     P.ampMult = 2.0 * std::sqrt(prod / std::pow(2.0 * kRefPi, (double)r.nDim));
+    if (r.method == RF_RANDOMIZATION) {
+      // randomFieldND.f90:262 (literal); intended: a random wavevector of a
+      // quadrant stands for kMax^nDim / kn of the spectral volume
+      if (o.literal) P.ampMult = 2.0 * std::sqrt(1.0 / ((double)P.K * std::pow(2.0 * kRefPi, (double)r.nDim)));
+      else
+        P.ampMult = 2.0 * std::sqrt(std::pow(P.kMax, (double)r.nDim) / ((double)kn * std::pow(2.0 * kRefPi, (double)r.nDim)));
+    }
   } else {
     double r2 = 0.0;
     for (int d = 0; d < r.nDim; ++d) r2 += xr[d] * xr[d];

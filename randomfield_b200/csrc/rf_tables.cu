@@ -51,17 +51,22 @@ __device__ KVal kvalue(const Plan& P, const JumpTable& jt, int64_t kk) {
       const double base = 0.0 + P.kDelta[d] * (double)idx[d];
       v.k[d] = sg[d] ? base * -1.0 : base * 1.0;
     }
-  } else if (P.method == 2) {  // Shinozuka through the table
+  } else if (P.method != 1) {  // Shinozuka through the table, or randomization
     if (kk >= P.K) return v;
     v.ref = kk;
     int64_t kn = 1;
     for (int d = 0; d < P.nDim; ++d) kn *= P.kNStep[d];
     const int q = (int)(kk / kn);
-    int64_t rem = kk % kn;
+    const int64_t b = kk % kn;
+    int64_t rem = b;
     for (int d = 0; d < P.nDim; ++d) {
       const int64_t i = rem % P.kNStep[d];
       rem /= P.kNStep[d];
-      const double base = 0.0 + P.kDelta[d] * (double)i;
+      // randomization: kPoints_base = random_number * kMax, axis fastest,
+      // the first nDim*kn draws of the stream (spectra_RF.f90:119-124)
+      const double base =
+          (P.method == 3) ? r8_uni_at(jt, P.ig1, P.ig2, (uint64_t)(b * P.nDim + d + 1)) * P.kMax
+                          : 0.0 + P.kDelta[d] * (double)i;
       // B2 in literal mode: the first quadrant is never written.
       v.k[d] = (P.literal && q == 0) ? 0.0 : base * (d == 0 ? 1.0 : quad_sign(q, d, P.nDim));
     }
@@ -134,8 +139,10 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
     const int64_t rg = (int64_t)P.rOff + r;  // realization index in the request
     double phi, gam = 1.0, amp = v.amp;
     const int64_t s1 = P.ig1, s2 = P.ig2;
-    if (P.method == 2) {
-      phi = 2.0 * kRefPi * r8_uni_at(jt, s1, s2, (uint64_t)(rg * P.K + v.ref + 1));
+    if (P.method != 1) {
+      // randomization: the phases follow the nDim*kn wavevector draws
+      const int64_t skip = (P.method == 3) ? (P.K >> (P.nDim - 1)) * P.nDim : 0;
+      phi = 2.0 * kRefPi * r8_uni_at(jt, s1, s2, (uint64_t)(skip + rg * P.K + v.ref + 1));
       if (P.literal && literalSlab >= 0) {
         // B1: slab m of realization n uses S^(1/2^t), t = (n-1)*nSlab + m
         // (randomFieldND.f90:312 inside the loops :276 and :284).

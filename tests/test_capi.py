@@ -63,8 +63,9 @@ def call(x, nDim=3, n=None, corrMod=1, margiFirst=1, corrL=(1.0, 1.0, 1.0), fiel
     (dict(corrL=(1.0, 1.0, -2.0)), -3),
     (dict(margiFirst=2, fieldAvg=0.0), -4),
     (dict(margiFirst=2, fieldAvg=-1.0), -4),
-    (dict(method=3), -5),
     (dict(method=4), -5),
+    (dict(method=0), -5),
+    (dict(method=1, opts=rf.Options.make(literal=True)), -9),
     (dict(corrMod=3), -6),
     (dict(margiFirst=0), -7),
     (dict(out=False), -9),

@@ -248,3 +248,25 @@ def test_device_api_matches_flat_api():
     ctx.synchronize()
     np.testing.assert_array_equal(dout.cpu().numpy(), np.asarray(flat).T)
     ctx.close()
+
+
+# --------------------------------------------------- randomization (method 3)
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+@pytest.mark.parametrize("nDim", [2, 3])
+def test_randomization_method(prec, nDim):
+    """Method 3: uniformly random wavevectors (drawn before the phases), the
+    Shinozuka sum over them, through GEN_TABLE."""
+    x = uniform_points(4000, 5.0, nDim=nDim, seed=31)
+    kw = dict(Nmc=6, method=3, k_nstep=(10, 10, 10)[:nDim] + (0,) * (3 - nDim), seed_start=4)
+    rows = np.random.RandomState(2).choice(x.shape[0], 200, replace=False)
+    ref = oracle(x, rows=rows, **kw)
+    got = gpu(x, prec, **kw)
+    check(prec, got[:, rows], ref)
+
+
+def test_randomization_literal_mode():
+    x = uniform_points(3000, 4.0, seed=8)
+    kw = dict(Nmc=3, method=3, k_nstep=(8, 8, 8), seed_start=2, literal=True)
+    ref = oracle(x, **kw)
+    got = gpu(x, "fp32", **kw)
+    check("fp32", got, ref)

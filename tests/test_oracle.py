@@ -280,3 +280,52 @@ def test_baseline_matches_generate():
     out, t = rq.baseline(100, 400, 1, 2, nthreads=2)
     assert t > 0
     np.testing.assert_allclose(out, full[1:3, 100:500], rtol=0, atol=1e-12)
+
+
+# ------------------------------------------------------- randomization (3)
+def test_randomization_wavevectors_are_the_first_draws():
+    """Method 3 (gen_Std_Gauss_Randomization, randomFieldND.f90:343-361):
+    kPoints_base = random_number * kMax (spectra_RF.f90:119-124), axis
+    fastest, drawn before the phases, then the set_kSign copies."""
+    x = grid(6, 0.2)
+    rq = O.OracleRequest(x, Nmc=2, method=O.RANDOMIZATION, kNStep=(4, 3, 5), seedStart=3)
+    g = rq.geometry()
+    kn = 4 * 3 * 5
+    assert g.K == 4 * kn
+    kp, amp, S = rq.kpoints()
+    r = O.rng(3)
+    u = np.array([O.lib().rfo_rng_r8_uni_01(C.byref(r)) for _ in range(3 * kn)]).reshape(kn, 3)
+    np.testing.assert_array_equal(kp[:kn], u * g.kMax)
+    signs = [(1, 1, 1), (1, 1, -1), (1, -1, 1), (1, -1, -1)]
+    for q, sg in enumerate(signs):
+        np.testing.assert_array_equal(kp[q * kn:(q + 1) * kn], u * g.kMax * np.array(sg))
+    np.testing.assert_allclose(amp, np.sqrt(np.prod(np.exp(-kp ** 2 / (4 * 3.1415926535898)), axis=1)), rtol=1e-13)
+    # the phases follow the 3*kn wavevector draws
+    Bc, Bs = rq.phase_matrix()  # [r, k]
+    phi0 = np.arctan2(-Bs[0], Bc[0])
+    r = O.rng(3)
+    for _ in range(3 * kn):
+        O.lib().rfo_rng_i4_uni(C.byref(r))
+    u0 = np.array([O.lib().rfo_rng_r8_uni_01(C.byref(r)) for _ in range(g.K)])
+    ref = np.angle(np.exp(1j * 2 * 3.1415926535898 * u0))
+    nz = amp > 1e-12
+    np.testing.assert_allclose(np.angle(np.exp(1j * phi0[nz])), ref[nz], atol=1e-9)
+
+
+def test_randomization_amplitude_unit_variance_and_literal_ampmult():
+    """Intended: a random wavevector of a quadrant stands for kMax^D/kn of the
+    spectral volume, so ampMult = 2 sqrt(kMax^D/(kn (2 pi)^D)) and the
+    ensemble variance ampMult^2/2 * sum S is 1 (up to the kMax truncation and
+    the Monte Carlo error of K random wavevectors).  Literal: the reference's
+    2 sqrt(1/(K (2 pi)^D)) (randomFieldND.f90:262)."""
+    x = grid(4, 0.3)
+    PI = 3.1415926535898
+    rq = O.OracleRequest(x, Nmc=1, method=O.RANDOMIZATION, kNStep=(16, 16, 16), seedStart=1)
+    g = rq.geometry()
+    kn = 16 ** 3
+    assert math.isclose(g.ampMult, 2 * math.sqrt(g.kMax ** 3 / (kn * (2 * PI) ** 3)), rel_tol=1e-14)
+    _, amp, S = rq.kpoints()
+    var = g.ampMult ** 2 / 2 * S.sum()
+    assert abs(var - 0.99) < 0.05, var
+    lit = O.OracleRequest(x, Nmc=1, method=O.RANDOMIZATION, kNStep=(16, 16, 16), seedStart=1, literal=True)
+    assert math.isclose(lit.geometry().ampMult, 2 * math.sqrt(1 / (4 * kn * (2 * PI) ** 3)), rel_tol=1e-14)
