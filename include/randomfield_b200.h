@@ -132,6 +132,13 @@ int rf_generate_device_noalloc(const double* d_xPoints, int nDim, int64_t n, int
 /* Waits for the context's queued work; reports a device-side timeout. */
 int rf_context_synchronize(rf_context* ctx);
 
+/* Failure-detection self test: launches a kernel whose bounded device wait
+ * (the waits every generation kernel uses) can never complete, on a phase
+ * nothing arrives on; after limit_ms the kernel raises the context's error
+ * word and returns, and the call reports RF_ETIMEDOUT, as a generation whose
+ * wait expired would.  No fault, trap or hang; the context stays usable. */
+int rf_context_selftest_timeout(rf_context* ctx, double limit_ms);
+
 /* Phase timers.  With timing enabled the context records CUDA events on the
  * launching stream around each phase of a generation; rf_context_last_times
  * waits for the last one and returns the device milliseconds of the table
