@@ -7,7 +7,8 @@
 ! include/randomfield_b200.h through iso_c_binding.  Arrays keep the
 ! reference's layouts: xPoints(nDim, n), randField(n, Nmc).  corrMod and
 ! margiFirst are the README's strings ("gaussian"; "gaussian" or
-! "lognormal"); method is 1 (isotropic) or 2 (Shinozuka-Deodatis).
+! "lognormal"); method is 1 (isotropic), 2 (Shinozuka-Deodatis) or 3
+! (randomization).
 !
 ! Errors: with the optional `status` argument present the C status code is
 ! returned (0 = success, negative RF_E* codes otherwise); without it an error
@@ -22,7 +23,7 @@ module rf_gpu
   private
 
   ! constants_RF.f90:12-21
-  integer, parameter, public :: RF_ISOTROPIC = 1, RF_SHINOZUKA = 2
+  integer, parameter, public :: RF_ISOTROPIC = 1, RF_SHINOZUKA = 2, RF_RANDOMIZATION = 3
   integer, parameter, public :: RF_CM_GAUSSIAN = 1, RF_CM_COS = 2
   integer, parameter, public :: RF_FOM_GAUSSIAN = 1, RF_FOM_LOGNORMAL = 2
   ! precision forms of the contraction
