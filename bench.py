@@ -527,10 +527,20 @@ def main():
     if os.path.exists(tp) and GRID == (128, 128, 128):
         with open(tp) as f:
             traffic = json.load(f).get(args.precision)
+    # the three bounds of the step: tensor MMA, SFU sincos, HBM bytes (the SFU
+    # rate is measured live by a MUFU microbenchmark kernel of the library)
+    sfu = rf.measure_sfu_rate(local)
+    pairs = float(n) * 3 * KN  # GEN_GRID3: per-axis phasors only
+    hbm_bytes = 8.0 * n * NMC + 24.0 * n + 2.0 * (2 * K) * (2 * NMC)
+    bounds = {"tensor_ms": flops / (peak * 1e12) * 1e3, "sfu_ms": pairs / sfu * 1e3,
+              "hbm_ms": hbm_bytes / (pk.get("hbm_gbs", 6650.0) * 1e9) * 1e3}
     roof = {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s", "frac": tflops / peak,
             "traffic": traffic, "kernel": "rf_tc_kernel (tcgen05 contraction + fused epilogue)",
             "kernel_ms": kern_ms, "peak_source": f"bf16_tflops_sustained, {src}",
-            "algorithmic_flops_per_launch": flops}
+            "algorithmic_flops_per_launch": flops, "bounds": bounds,
+            "sfu_pairs_per_s": sfu, "sfu_pairs_per_launch": pairs,
+            "note": "the slowest of the three bounds is the tensor MMA; GEN_GRID3 needs sincos only for the "
+                    "per-axis phasors (n1 + n2 + n3 per point), GEN_TABLE one pair per (point, wavevector)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -139,6 +139,10 @@ int rf_context_synchronize(rf_context* ctx);
  * wait expired would.  No fault, trap or hang; the context stays usable. */
 int rf_context_selftest_timeout(rf_context* ctx, double limit_ms);
 
+/* Measured MUFU (sin, cos) pair rate of the device: the SFU bound of the
+ * GEN_TABLE generator (one pair per point and wavevector). */
+int rf_measure_sfu_rate(int device, double* pairs_per_second);
+
 /* Phase timers.  With timing enabled the context records CUDA events on the
  * launching stream around each phase of a generation; rf_context_last_times
  * waits for the last one and returns the device milliseconds of the table

@@ -51,7 +51,7 @@ EXPORTS = [
     "rf_context_set_timing", "rf_context_last_times", "rf_generate_device_noalloc",
     "rf_generate_batch", "rf_generate_batch_device", "rf_batch_last_stats",
     "rf_server_config_init", "rf_server_create", "rf_server_submit", "rf_server_wait", "rf_server_get_stats",
-    "rf_server_destroy", "rf_server_submit_blended", "rf_context_selftest_timeout", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
+    "rf_server_destroy", "rf_server_submit_blended", "rf_context_selftest_timeout", "rf_measure_sfu_rate", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
 ]
 
 
@@ -240,6 +240,7 @@ def lib() -> C.CDLL:
         L.rf_server_get_stats.argtypes = [C.c_void_p, P(ServerStats)]
         L.rf_server_destroy.argtypes = [C.c_void_p]
         L.rf_context_selftest_timeout.argtypes = [C.c_void_p, d]
+        L.rf_measure_sfu_rate.argtypes = [i32, P(d)]
         L.rf_blend_layout.argtypes = [P(BlendGrid), P(d), P(C.c_int32), P(C.c_int32)]
         L.rf_server_submit_blended.argtypes = [C.c_void_p, P(BlendGrid), i32, i32, P(d), d, d, i32, i32, P(d),
                                                P(Options), P(i64)]
@@ -341,6 +342,13 @@ def generate_device_noalloc(d_x, nDim, n, corrMod, margiFirst, corrL, fieldAvg, 
                                             _id(margiFirst, _MARGI, "margiFirst"),
                                             cl.ctypes.data_as(C.POINTER(C.c_double)), float(fieldAvg), float(fieldVar),
                                             int(Nmc), int(method), C.c_void_p(ptr(d_out)), C.byref(o), C.c_void_p(s)))
+
+
+def measure_sfu_rate(device: int = 0) -> float:
+    """MUFU (sin, cos) pairs per second of the device (rf_measure_sfu_rate)."""
+    v = C.c_double()
+    _check(lib().rf_measure_sfu_rate(int(device), C.byref(v)))
+    return v.value
 
 
 def make_request(xPoints, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, randField,

@@ -1,4 +1,5 @@
-// rf_selftest.cu -- failure-detection self test of the bounded device waits.
+// rf_selftest.cu -- failure-detection self test of the bounded device waits,
+// and the SFU (MUFU sin/cos) rate used by the roofline of GEN_TABLE.
 //
 // Every wait of the generation kernels is bounded (mbar_wait: globaltimer
 // limit, abort flag); on expiry a kernel raises the context's error word,
@@ -31,7 +32,55 @@ __global__ void rf_wait_timeout_kernel(uint32_t* err, uint64_t limitNs) {
   if (!ok && (threadIdx.x & 31) == 0) atomicOr(err, kErrTimeout);
 }
 
+// MUFU sin/cos throughput: every thread runs 8 independent chains of
+// __sincosf on arguments kept in [-pi, pi] (the reduced phases of GEN_TABLE),
+// `iters` steps each; one step is one (sin, cos) pair.
+__global__ void rf_sfu_rate_kernel(float* sink, int iters) {
+  float a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = 0.1f * (float)(threadIdx.x & 31) + 0.37f * (float)j - 1.5f;
+  float acc = 0.f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      float s, c;
+      __sincosf(a[j], &s, &c);
+      a[j] = s + c * 0.5f;  // stays in [-1.5, 1.5]
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc += a[j];
+  if (acc == 12345.678f) sink[threadIdx.x] = acc;
+}
+
 }  // namespace
+
+extern "C" int rf_measure_sfu_rate(int device, double* pairs_per_second) {
+  g_err.clear();
+  if (!pairs_per_second) return fail(RF_EINVAL_ARG, "null output pointer");
+  RF_CUDA(cudaSetDevice(device), "cudaSetDevice");
+  int sms = 0;
+  RF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+  float* sink = nullptr;
+  RF_CUDA(cudaMalloc(&sink, 1024 * sizeof(float)), "cudaMalloc");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks = sms * 4, threads = 512, iters = 4096;
+  rf_sfu_rate_kernel<<<blocks, threads>>>(sink, 64);  // warm-up
+  cudaEventRecord(e0);
+  rf_sfu_rate_kernel<<<blocks, threads>>>(sink, iters);
+  cudaEventRecord(e1);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  if (e != cudaSuccess) return cuda_fail(e, "SFU rate kernel");
+  *pairs_per_second = (double)blocks * threads * iters * 8.0 / ((double)ms * 1e-3);
+  return RF_OK;
+}
 
 extern "C" int rf_context_selftest_timeout(rf_context* ctx, double limit_ms) {
   g_err.clear();
