@@ -395,7 +395,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="bf16", choices=["bf16", "fp16", "bf16_fast", "fp32"])
+    ap.add_argument("--precision", default="bf16", choices=["bf16", "fp16", "bf16_fast", "fp8", "fp32"])
     ap.add_argument("--no-forms", action="store_true", help="skip the other precision forms")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
@@ -501,7 +501,7 @@ def main():
     # other precision forms, same workload (fewer steps)
     forms = {}
     if not args.no_forms:
-        for prec in ("fp16", "bf16_fast", "fp32"):
+        for prec in ("fp16", "bf16_fast", "fp8", "fp32"):
             if prec == args.precision:
                 continue
             ns = 2 if prec == "fp32" else max(3, args.steps // 2)
@@ -564,7 +564,7 @@ def main():
             "metric": "field values/s", "value": value, "unit": "field values/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": {"bf16": "bf16", "fp16": "f16", "bf16_fast": "bf16", "fp32": "f32"}[args.precision],
+            "dtype": {"bf16": "bf16", "fp16": "f16", "bf16_fast": "bf16", "fp8": "e4m3", "fp32": "f32"}[args.precision],
             "data": "synthetic",
             "config": {"workload": WORKLOAD if GRID == (128, 128, 128) else f"{WORKLOAD} on a {GRID} grid", "n_points": n, "Nmc": NMC, "K": K, "precision": args.precision,
                        "l2": "flushed between timed steps (256 MiB write); output 1 GiB per step",

@@ -21,7 +21,7 @@ __all__ = [
     "RandomFieldError", "Options", "Context", "lib", "create_standard_gaussian_field_unstruct",
     "query_geometry", "generate_device_noalloc", "Request", "BatchStats", "make_request", "generate_batch",
     "Server", "ServerConfig", "ServerStats", "BlendGrid", "blend_layout", "ISOTROPIC", "RANDOMIZATION", "SHINOZUKA", "CM_GAUSSIAN", "CM_COS", "FOM_GAUSSIAN", "FOM_LOGNORMAL",
-    "PREC_BF16", "PREC_FP16", "PREC_FP32", "PREC_BF16_FAST", "LIB_PATH", "STATUS",
+    "PREC_BF16", "PREC_FP16", "PREC_FP32", "PREC_BF16_FAST", "PREC_FP8", "LIB_PATH", "STATUS",
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -31,7 +31,7 @@ LIB_PATH = os.path.join(HERE, "librf_b200.so")
 ISOTROPIC, SHINOZUKA, RANDOMIZATION = 1, 2, 3
 CM_GAUSSIAN, CM_COS = 1, 2
 FOM_GAUSSIAN, FOM_LOGNORMAL = 1, 2
-PREC_BF16, PREC_FP16, PREC_FP32, PREC_BF16_FAST = 0, 1, 2, 3
+PREC_BF16, PREC_FP16, PREC_FP32, PREC_BF16_FAST, PREC_FP8 = 0, 1, 2, 3, 4
 
 STATUS = {
     0: "RF_OK", -1: "RF_EINVAL_NMC", -2: "RF_EINVAL_NDIM", -3: "RF_EINVAL_CORRL", -4: "RF_EINVAL_LOGNORMAL",
@@ -42,7 +42,7 @@ STATUS = {
 
 _CORRMOD = {"gaussian": CM_GAUSSIAN, "cos": CM_COS, "cm_gaussian": CM_GAUSSIAN, "cm_cos": CM_COS}
 _MARGI = {"gaussian": FOM_GAUSSIAN, "lognormal": FOM_LOGNORMAL}
-_PREC = {"bf16": PREC_BF16, "fp16": PREC_FP16, "fp32": PREC_FP32, "bf16_fast": PREC_BF16_FAST}
+_PREC = {"bf16": PREC_BF16, "fp16": PREC_FP16, "fp32": PREC_FP32, "bf16_fast": PREC_BF16_FAST, "fp8": PREC_FP8}
 
 # Every symbol include/randomfield_b200.h declares.
 EXPORTS = [

@@ -90,7 +90,7 @@ struct GroupRun {
 // 2*block (BF16 hi/lo) or block; more columns amortise the trig tile over
 // more realizations, fewer waste less on requests with small Nmc.
 std::vector<int> block_candidates(int prec) {
-  if (prec == PREC_BF16) return {64, 32};
+  if (prec_hilo(prec)) return {64, 32};
   return {128, 64};
 }
 

@@ -147,6 +147,17 @@ __device__ __forceinline__ bool elect_one() {
       : "=r"(e));
   return e != 0;
 }
+// D[tmem] (+)= A[tmem] x B[smem descriptor], kind::f8f6f4 (A and B e4m3,
+// K = 32 per instruction), FP32 accumulate.
+__device__ __forceinline__ void mma_ts_f8(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
 // Arrive once on `bar` when all prior tcgen05 async ops of this thread finish.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -210,6 +221,14 @@ __device__ __forceinline__ double reduce_2pi(double x) {
 __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<uint32_t*>(&v);
+}
+// Four e4m3 values (round to nearest, saturating) in K order: byte 0 = c0,
+// byte 1 = s0, byte 2 = c1, byte 3 = s1.
+__device__ __forceinline__ uint32_t pack_e4m3x4(float c0, float s0, float c1, float s1) {
+  uint16_t lo, hi;
+  asm("cvt.rn.satfinite.e4m3x2.f32 %0, %1, %2;" : "=h"(lo) : "f"(s0), "f"(c0));
+  asm("cvt.rn.satfinite.e4m3x2.f32 %0, %1, %2;" : "=h"(hi) : "f"(s1), "f"(c1));
+  return (uint32_t)lo | ((uint32_t)hi << 16);
 }
 __device__ __forceinline__ uint32_t pack_f16x2(float lo, float hi) {
   __half2 v = __floats2half2_rn(lo, hi);

@@ -85,7 +85,7 @@ int validate(const Request& r) {
   if (r.margiFirst == RF_FOM_LOGNORMAL && r.fieldAvg <= 0.0)
     return fail(RF_EINVAL_LOGNORMAL, "when using lognormal fieldAvg should be a positive number");
   const rf_options& o = r.opt;
-  if (o.precision < RF_PREC_BF16 || o.precision > RF_PREC_BF16_FAST)
+  if (o.precision < RF_PREC_BF16 || o.precision > RF_PREC_FP8)
     return fail(RF_EINVAL_ARG, "unknown precision form %d", o.precision);
   if (o.literal && r.method == RF_ISOTROPIC)
     return fail(RF_EINVAL_ARG, "literal mode exists for the Shinozuka and randomization methods only");
@@ -197,15 +197,15 @@ int layout(Plan& P) {
   if (P.nmcBlk <= 0) {
     // the first realization block: one MMA holds at most 256 accumulator
     // columns and the hi/lo form uses two per realization
-    const int32_t blk = P.prec == PREC_FP32 ? P.Nmc : (P.prec == PREC_BF16 ? kMaxNmcPad / 2 : kMaxNmcPad);
+    const int32_t blk = P.prec == PREC_FP32 ? P.Nmc : (prec_hilo(P.prec) ? kMaxNmcPad / 2 : kMaxNmcPad);
     P.nmcBlk = std::min(P.Nmc, blk);
   }
   if (tc) {
     P.nmcPad = (int32_t)round_up(P.nmcBlk, 16);
-    P.bRows = P.prec == PREC_BF16 ? 2 * P.nmcPad : P.nmcPad;
+    P.bRows = prec_hilo(P.prec) ? 2 * P.nmcPad : P.nmcPad;
     // one MMA covers all bRows (N <= 256); the accumulator uses bRows columns
     if (P.bRows > kMaxNmcPad) return fail(RF_ENOTSUP, "realization block too large for one MMA");
-    P.stageBytes = (int64_t)2 * P.chunkK * P.bRows * 2;
+    P.stageBytes = (int64_t)2 * P.chunkK * P.bRows * (P.prec == PREC_FP8 ? 1 : 2);
   } else {
     int rpt = 1;
     while (rpt < 8 && 8 * rpt < P.nmcBlk) rpt *= 2;
@@ -213,9 +213,10 @@ int layout(Plan& P) {
     P.bRows = P.nmcPad;
     P.stageBytes = (int64_t)2 * P.chunkK * P.nmcPad * 4;
   }
-  // FP16 operand side: scale B by 2^s so that the largest |B| sits near 2^15.
+  // FP16 / FP8 operand side: scale B by 2^s so that the largest |B| sits near
+  // 2^15 (FP16, max 65504) or 240 (e4m3, max 448).
   P.bScaleLog2 = 0;
-  if (P.prec == PREC_FP16) {
+  if (P.prec == PREC_FP16 || P.prec == PREC_FP8) {
     double bound = 1.0;  // Shinozuka: sqrt(S) <= 1
     if (P.method == RF_ISOTROPIC) {
       bound = 0.0;
@@ -229,7 +230,7 @@ int layout(Plan& P) {
       }
       if (bound <= 0.0) bound = 1.0;
     }
-    P.bScaleLog2 = (int32_t)std::floor(std::log2(32768.0 / bound));
+    P.bScaleLog2 = (int32_t)std::floor(std::log2((P.prec == PREC_FP8 ? 240.0 : 32768.0) / bound));
   }
   P.outScale = P.ampMult * std::ldexp(1.0, -P.bScaleLog2);
   // multiVariateTransformation (randomFieldND.f90:139-178)
@@ -358,7 +359,7 @@ int build_plan(const Request& rq, const double* ext, Plan& P) {
 // and the hi/lo form uses two per realization.
 int32_t realization_block(const Plan& P) {
   if (P.prec == PREC_FP32) return P.Nmc;
-  return P.prec == PREC_BF16 ? kMaxNmcPad / 2 : kMaxNmcPad;
+  return prec_hilo(P.prec) ? kMaxNmcPad / 2 : kMaxNmcPad;
 }
 
 int run_block(rf_context* c, const Plan& P, const double* dX, double* dOut, cudaStream_t st);

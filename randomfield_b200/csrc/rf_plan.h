@@ -22,7 +22,10 @@ enum Generator : int32_t {
   GEN_MIXED = 2,  // kernel variant only: the generator is chosen per tile (grouped launch)
 };
 
-enum Precision : int32_t { PREC_BF16 = 0, PREC_FP16 = 1, PREC_FP32 = 2, PREC_BF16_FAST = 3 };
+enum Precision : int32_t { PREC_BF16 = 0, PREC_FP16 = 1, PREC_FP32 = 2, PREC_BF16_FAST = 3, PREC_FP8 = 4 };
+
+// Forms whose amplitude side is split into hi and lo rows (N = 2 * nmcPad).
+inline bool prec_hilo(int32_t prec) { return prec == PREC_BF16 || prec == PREC_FP8; }
 
 constexpr int kTileM = 128;        // points per tile (MMA M)
 constexpr int kStageCols = 64;     // max k-values (TMEM columns) per GEN_GRID3 group or FP32 stage
@@ -100,5 +103,9 @@ struct GroupItem {
   int32_t sub;
   int32_t tile;
 };
+
+// TMEM columns of one stage's A tile: one 32-bit column holds a (cos, sin)
+// pair of 16-bit values, or two pairs of 8-bit values.
+inline int32_t a_cols(const Plan& P) { return P.prec == PREC_FP8 ? P.chunkK / 2 : P.chunkK; }
 
 }  // namespace rfb

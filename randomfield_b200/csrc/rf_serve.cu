@@ -337,7 +337,7 @@ int rf_server_create(const rf_server_config* cfg, rf_server** out) {
     s->cfg.size = sizeof(rf_server_config);
   }
   if (s->cfg.max_batch <= 0) s->cfg.max_batch = 512;
-  if (s->cfg.precision != RF_PREC_BF16 && s->cfg.precision != RF_PREC_FP16 && s->cfg.precision != RF_PREC_BF16_FAST) {
+  if (s->cfg.precision == RF_PREC_FP32 || s->cfg.precision < RF_PREC_BF16 || s->cfg.precision > RF_PREC_FP8) {
     delete s;
     return fail(RF_EINVAL_ARG, "the serving loop runs the tensor-core forms (BF16, FP16, BF16 fast)");
   }

@@ -11,6 +11,8 @@
 // draw for draw.  Draw order follows the reference: Shinozuka K phases per
 // realization in k order (:278-279); isotropic direction blocks then, per
 // realization, a gamma block and a psi block (:460-468 restated).
+#include <cuda_fp8.h>
+
 #include "rf_device.cuh"
 #include "rf_gen.cuh"
 #include "rf_launch.h"
@@ -115,6 +117,17 @@ __device__ KVal kvalue(const Plan& P, const JumpTable& jt, int64_t kk) {
 __device__ __forceinline__ int64_t tc_b_offset(int32_t bRows, int32_t row, int32_t kel) {
   return (int64_t)(kel >> 3) * (bRows * 16) + (row >> 3) * 128 + (row & 7) * 16 + (kel & 7) * 2;
 }
+// The same core-matrix layout for 8-bit elements (16 elements per 16-byte row).
+__device__ __forceinline__ int64_t tc_b_offset8(int32_t bRows, int32_t row, int32_t kel) {
+  return (int64_t)(kel >> 4) * (bRows * 16) + (row >> 3) * 128 + (row & 7) * 16 + (kel & 15);
+}
+
+__device__ __forceinline__ unsigned char to_e4m3(double v) {
+  return (unsigned char)__nv_cvt_double_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
+}
+__device__ __forceinline__ double from_e4m3(unsigned char b) {
+  return (double)__half2float(__half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)b, __NV_E4M3)));
+}
 
 // Element tid = kk * nmcPad + r of the operand: B rows of wavevector kk (in
 // kernel order) for realization column r, and the wavevector itself (r = 0).
@@ -171,6 +184,15 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
     return;
   }
   unsigned char* b = reinterpret_cast<unsigned char*>(B) + stage * P.stageBytes;
+  if (P.prec == PREC_FP8) {  // scaled e4m3, hi and lo rows
+    const double sc = ldexp(1.0, P.bScaleLog2);
+    const unsigned char hc = to_e4m3(bc * sc), hs = to_e4m3(bs * sc);
+    b[tc_b_offset8(P.bRows, r, 2 * c)] = hc;
+    b[tc_b_offset8(P.bRows, r, 2 * c + 1)] = hs;
+    b[tc_b_offset8(P.bRows, P.nmcPad + r, 2 * c)] = to_e4m3(bc * sc - from_e4m3(hc));
+    b[tc_b_offset8(P.bRows, P.nmcPad + r, 2 * c + 1)] = to_e4m3(bs * sc - from_e4m3(hs));
+    return;
+  }
   if (P.prec == PREC_FP16) {
     const double sc = ldexp(1.0, P.bScaleLog2);
     *reinterpret_cast<__half*>(b + tc_b_offset(P.bRows, r, 2 * c)) = __double2half(bc * sc);

@@ -149,18 +149,27 @@ __device__ __forceinline__ double finish_value(const Plan& P, float acc) {
 
 // The MMAs of one stage from the elected lane, with the probe of the next
 // stage's full barrier between the last two; returns the probe (warp-uniform).
-template <int STEPS>
+// F8: kind::f8f6f4 (e4m3, K = 32 per MMA) instead of kind::f16 (K = 16); both
+// consume 8 TMEM columns of A and 32 bytes of each B row per MMA.
+template <bool F8>
+__device__ __forceinline__ void mma_one(uint32_t tbase, uint32_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  if (F8) mma_ts_f8(tbase, a, b, idesc, acc);
+  else mma_ts(tbase, a, b, idesc, acc);
+}
+
+template <int STEPS, bool F8>
 __device__ __forceinline__ bool issue_stage(bool leader, uint32_t tbase, uint32_t aBase, uint64_t d0, uint64_t jStep,
                                             uint32_t idesc, uint32_t acc0, bool more, uint64_t* fullNext,
                                             uint32_t phn, uint64_t* emptyBar) {
+  static_assert(STEPS >= 2, "a stage holds at least two MMAs");
   if (leader) {
-    mma_ts(tbase, aBase, d0, idesc, acc0);  // the tile's first MMA overwrites D
+    mma_one<F8>(tbase, aBase, d0, idesc, acc0);  // the tile's first MMA overwrites D
 #pragma unroll
-    for (int j = 1; j < STEPS - 1; ++j) mma_ts(tbase, aBase + 8u * j, d0 + jStep * j, idesc, 1u);
+    for (int j = 1; j < STEPS - 1; ++j) mma_one<F8>(tbase, aBase + 8u * j, d0 + jStep * j, idesc, 1u);
   }
   const bool ready = __all_sync(0xffffffffu, more && mbar_test_wait(fullNext, phn));
   if (leader) {
-    mma_ts(tbase, aBase + 8u * (STEPS - 1), d0 + jStep * (STEPS - 1), idesc, 1u);
+    mma_one<F8>(tbase, aBase + 8u * (STEPS - 1), d0 + jStep * (STEPS - 1), idesc, 1u);
     mma_commit(emptyBar);
   }
   __syncwarp();
@@ -174,6 +183,12 @@ template <int GEN, int PREC, int LPAD, class Work>
 __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint32_t* err) {
   constexpr bool kHasGrid = GEN != GEN_TABLE;
   constexpr bool kHasTable = GEN != GEN_GRID3;
+  constexpr bool kF8 = PREC == PREC_FP8;
+  constexpr bool kHiLo = PREC == PREC_BF16 || PREC == PREC_FP8;
+  // MMAs per stage: a GEN_GRID3 stage holds 2 groups x 2*LPAD (cos, sin) pairs,
+  // a GEN_TABLE stage kTableChunk pairs; K = 16 (16-bit) or 32 (e4m3) per MMA
+  constexpr int kGridSteps = (LPAD > 0 ? LPAD / 2 : 4) / (kF8 ? 2 : 1);
+  constexpr int kTabSteps = kTableSteps / (kF8 ? 2 : 1);
   extern __shared__ __align__(1024) unsigned char smem[];
   Bars* bars = reinterpret_cast<Bars*>(smem);
   unsigned char* sB = smem + kHeaderBytes;
@@ -274,7 +289,8 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
       w.get(i, v);
       const Plan& P = *v.P;
       const bool grid = kHasGrid && (GEN == GEN_GRID3 || P.gen == GEN_GRID3);
-      const uint32_t idesc = make_idesc(PREC == PREC_FP16 ? 0u : 1u, 128u, (uint32_t)P.bRows);
+      // A/B type field: F16 (0) or BF16 (1) for kind::f16, E4M3 (0) for kind::f8f6f4
+      const uint32_t idesc = make_idesc((PREC == PREC_FP16 || kF8) ? 0u : 1u, 128u, (uint32_t)P.bRows);
       const uint32_t lbo = (uint32_t)P.bRows * 16u, sbo = 128u;
       const uint64_t desc0 = make_sdesc(smem_u32(sB), lbo, sbo);
       const uint64_t jStep = (uint64_t)((2u * lbo) >> 4);
@@ -291,11 +307,11 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
         const bool more = (ch + 1 < nChunks) || (i + 1 < count);
         const uint32_t acc0 = ch != 0 ? 1u : 0u;
         if (kHasGrid && grid)
-          ready = issue_stage<(LPAD > 0 ? LPAD / 2 : 2)>(leader, tbase, aBase, d0, jStep, idesc, acc0, more,
-                                                           &bars->full[sn], phn, &bars->empty[s]);
+          ready = issue_stage<kGridSteps, kF8>(leader, tbase, aBase, d0, jStep, idesc, acc0, more, &bars->full[sn],
+                                               phn, &bars->empty[s]);
         else
-          ready = issue_stage<kTableSteps>(leader, tbase, aBase, d0, jStep, idesc, acc0, more, &bars->full[sn], phn,
-                                           &bars->empty[s]);
+          ready = issue_stage<kTabSteps, kF8>(leader, tbase, aBase, d0, jStep, idesc, acc0, more, &bars->full[sn],
+                                              phn, &bars->empty[s]);
         s = sn;
         ph = phn;
       }
@@ -360,28 +376,56 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
         if (kHasGrid && grid) {
 #pragma unroll
           for (int u = 0; u < 2; ++u) {  // two groups per stage
-            uint32_t words[LPAD > 0 ? LPAD : 1];
+            // one TMEM column per (cos, sin) pair, or per two pairs for e4m3
+            constexpr int NW = kF8 ? (LPAD > 0 ? LPAD / 2 : 1) : (LPAD > 0 ? LPAD : 1);
+            uint32_t words[NW];
+            float pc0 = 0.f, ps0 = 0.f;  // e4m3: the even pair waits for the odd one
             auto emit = [&](int idx, float c, float sn) {
-              words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
+              if (kF8) {
+                if ((idx & 1) == 0) {
+                  pc0 = c;
+                  ps0 = sn;
+                } else {
+                  words[idx >> 1] = pack_e4m3x4(pc0, ps0, c, sn);
+                }
+              } else {
+                words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
+              }
             };
             const float2 Pq = walk.outer();
             walk.next(P, x);
             grid3_pairs<LPAD>(g3, Pq, emit);
-            // LPAD is a multiple of 8: every store covers 8 columns at an
-            // 8-aligned column offset.
-            const uint32_t col = aAddr + (uint32_t)(u * 2 * LPAD + h * LPAD);
+            // LPAD is a multiple of 8: 16-bit stores cover 8 columns at
+            // 8-aligned offsets, e4m3 stores 4 columns at 4-aligned offsets.
+            const uint32_t col = aAddr + (uint32_t)(u * 2 * NW + h * NW);
+            if (kF8) {
 #pragma unroll
-            for (int pc = 0; pc < LPAD / 8; ++pc) tmem_st8(col + pc * 8, &words[pc * 8]);
+              for (int pc = 0; pc < NW / 4; ++pc) tmem_st4(col + pc * 4, &words[pc * 4]);
+            } else {
+#pragma unroll
+              for (int pc = 0; pc < NW / 8; ++pc) tmem_st8(col + pc * 8, &words[pc * 8]);
+            }
           }
         } else if (kHasTable) {
-          uint32_t words[kTableChunk / 2];
+          constexpr int NW = kF8 ? kTableChunk / 4 : kTableChunk / 2;
+          uint32_t words[NW];
+          float pc0 = 0.f, ps0 = 0.f;
           auto emit = [&](int idx, float c, float sn) {
-            words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
+            if (kF8) {
+              if ((idx & 1) == 0) {
+                pc0 = c;
+                ps0 = sn;
+              } else {
+                words[idx >> 1] = pack_e4m3x4(pc0, ps0, c, sn);
+              }
+            } else {
+              words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
+            }
           };
           table_pairs(sK + sc * 3 * kTableChunk, h, x, emit);
-          const uint32_t col = aAddr + (uint32_t)(h * (kTableChunk / 2));
-          tmem_st8(col, &words[0]);
-          tmem_st8(col + 8, &words[8]);
+          const uint32_t col = aAddr + (uint32_t)(h * NW);
+#pragma unroll
+          for (int pc = 0; pc < NW / 8; ++pc) tmem_st8(col + pc * 8, &words[pc * 8]);
         }
         freeSeen = __shfl_sync(0xffffffffu, probe, 0) != 0;
         tmem_st_wait();
@@ -401,14 +445,14 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
       for (int cb = h * half; cb < (h + 1) * half; cb += 8) {
         uint32_t va[8], lo[8];
         tmem_ld8(tbase + laneOff + cb, va);
-        if (PREC == PREC_BF16) tmem_ld8(tbase + laneOff + P.nmcPad + cb, lo);
+        if (kHiLo) tmem_ld8(tbase + laneOff + P.nmcPad + cb, lo);
         tmem_ld_wait();
         if (valid) {
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             const int r = cb + j;
             float acc = __uint_as_float(va[j]);
-            if (PREC == PREC_BF16) acc += __uint_as_float(lo[j]);
+            if (kHiLo) acc += __uint_as_float(lo[j]);
             if (r >= P.nmcBlk) continue;
             if (P.blend)
               atomicAdd(&v.out[(int64_t)(P.rOff + r) * P.gTotal + bg], bw * ((double)acc * P.outScale));
@@ -500,7 +544,7 @@ size_t fit_layout(SlotLayout& L, bool table, int maxS = kMaxStages) {
 size_t tc_smem_bytes(const Plan& P, int* stages) {
   SlotLayout L;
   L.aCol0 = P.bRows;
-  L.aStride = P.chunkK;
+  L.aStride = a_cols(P);
   L.slotBytes = P.stageBytes;
   const size_t smem = fit_layout(L, P.gen == GEN_TABLE);
   if (stages) *stages = L.S;
@@ -519,7 +563,7 @@ cudaError_t launch_tc(const Plan& P, const double* dX, const void* dB, const dou
   args.row0 = row0;
   args.rows = rows;
   args.L.aCol0 = P.bRows;
-  args.L.aStride = P.chunkK;
+  args.L.aStride = a_cols(P);
   args.L.slotBytes = P.stageBytes;
   const size_t smem = fit_layout(args.L, P.gen == GEN_TABLE);
   if (smem == 0) return cudaErrorInvalidValue;
@@ -527,6 +571,7 @@ cudaError_t launch_tc(const Plan& P, const double* dX, const void* dB, const dou
   const int grid = (int)(tiles < numSMs ? tiles : numSMs);
   if (P.prec == PREC_FP16) return launch_prec<PREC_FP16>(P, args, smem, grid, st);
   if (P.prec == PREC_BF16_FAST) return launch_prec<PREC_BF16_FAST>(P, args, smem, grid, st);
+  if (P.prec == PREC_FP8) return launch_prec<PREC_FP8>(P, args, smem, grid, st);
   return launch_prec<PREC_BF16>(P, args, smem, grid, st);
 }
 
@@ -543,6 +588,7 @@ cudaError_t group_set_smem(int prec, size_t smem) {
   if (prec == PREC_BF16_FAST)
     return cudaFuncSetAttribute(rf_group_kernel<PREC_BF16_FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   if (prec == PREC_BF16) return cudaFuncSetAttribute(rf_group_kernel<PREC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (prec == PREC_FP8) return cudaFuncSetAttribute(rf_group_kernel<PREC_FP8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
   return cudaErrorInvalidValue;
 }
 
@@ -550,6 +596,7 @@ cudaError_t launch_group(int prec, const GroupArgs& g, size_t smem, int grid, cu
   if (prec == PREC_FP16) return launch_group_prec<PREC_FP16>(g, smem, grid, st);
   if (prec == PREC_BF16_FAST) return launch_group_prec<PREC_BF16_FAST>(g, smem, grid, st);
   if (prec == PREC_BF16) return launch_group_prec<PREC_BF16>(g, smem, grid, st);
+  if (prec == PREC_FP8) return launch_group_prec<PREC_FP8>(g, smem, grid, st);
   return cudaErrorInvalidValue;
 }
 

@@ -6,6 +6,7 @@ Tolerances (stated here and in the bench):
   BF16 form (hi/lo B)  relative-L2 <= 2e-3 per realization
   FP16 form            relative-L2 <= 2e-3 per realization
   BF16 fast form       relative-L2 <= 3e-3 (single BF16 amplitude side)
+  FP8 e4m3 form        relative-L2 <= 5e-2 (stated option: 3 significand bits in the trig tile)
 Full-size workloads are checked on oracle row subsets plus size-independent
 properties (moments of the whole field, determinism).
 """
@@ -22,7 +23,7 @@ from tests.helpers import errors, grid, per_realization_errors, uniform_points
 pytestmark = pytest.mark.gpu
 
 FP32_MAXABS = 1e-5
-REL_L2 = {"bf16": 2e-3, "fp16": 2e-3, "bf16_fast": 3e-3}
+REL_L2 = {"bf16": 2e-3, "fp16": 2e-3, "bf16_fast": 3e-3, "fp8": 5e-2}
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
@@ -270,3 +271,26 @@ def test_randomization_literal_mode():
     ref = oracle(x, **kw)
     got = gpu(x, "fp32", **kw)
     check("fp32", got, ref)
+
+
+# ---------------------------------------------------------- FP8 e4m3 option
+@pytest.mark.parametrize("kind", ["grid3", "table", "isotropic"])
+def test_fp8_form(kind):
+    """kind::f8f6f4 MMAs on e4m3 trig tiles and hi/lo e4m3 amplitude rows:
+    GEN_GRID3 (24 wavenumbers on axis 3), GEN_TABLE (Shinozuka 2-D) and the
+    isotropic table, against the oracle within the option's stated bound."""
+    if kind == "grid3":
+        x = grid(24, 0.1)
+        kw = dict(Nmc=64, k_nstep=(24, 24, 24), seed_start=2)
+    elif kind == "table":
+        x = uniform_points(5000, 4.0, nDim=2, seed=5)
+        kw = dict(Nmc=20, k_nstep=(32, 32, 0), seed_start=3)
+    else:
+        x = uniform_points(8000, 8.0, seed=6)
+        kw = dict(Nmc=33, method=1, iso_n_radial=40, iso_n_dir=40, seed_start=4)
+    rows = np.random.RandomState(3).choice(x.shape[0], 160, replace=False)
+    ref = oracle(x, rows=rows, **kw)
+    got = gpu(x, "fp8", **kw)
+    check("fp8", got[:, rows], ref)
+    # the form is an option: its error is well above the BF16 form's
+    assert errors(got[:, rows], ref)[1] > 2e-3
