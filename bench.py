@@ -222,6 +222,59 @@ def draw_request(rs, large_frac=0.0):
     return dict(points=pts, Nmc=Nmc, method=method, marg=marg, corrL=corrL, avg=avg, var=var, opts=opts, kind=kind)
 
 
+def bench_configs(args, rf, torch, local, sfu_rate, peak_tflops):
+    """The other single-request configs, device-resident, each timed with
+    CUDA events over a few calls: config 1 (Shinozuka 32^3, spacing 0.1,
+    Nmc 4, 16^3 x 4 wavevectors) and config 2 (isotropic, 200k points uniform
+    in [0, 10]^3, lognormal avg 1 var 0.25, Nmc 64, 64 x 64 wavevectors),
+    in the BF16 form and the plain FP32 form.  Config 2 runs GEN_TABLE, whose
+    bound is the SFU: one (sin, cos) pair per point and wavevector."""
+    out = {}
+    rs = np.random.RandomState(12)
+    ax = np.arange(32, dtype=np.float64) * 0.1
+    z, y, x = np.meshgrid(ax, ax, ax, indexing="ij")
+    c1 = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1)
+    c2 = rs.uniform(0.0, 10.0, size=(200000, 3)).astype(np.float32).astype(np.float64)
+    cases = {
+        "cfg1_shinozuka_32cubed": (c1, 4, 2, "gaussian", 0.0, 1.0, dict(k_nstep=(16, 16, 16))),
+        "cfg2_isotropic_200k": (c2, 64, 1, "lognormal", 1.0, 0.25, dict(iso_n_radial=64, iso_n_dir=64)),
+    }
+    ctx = rf.Context(local)
+    ctx.set_timing(True)
+    for name, (pts, Nmc, method, marg, avg, var, o) in cases.items():
+        n = pts.shape[0]
+        dx = torch.from_numpy(np.ascontiguousarray(pts)).cuda(local)
+        dout = torch.empty((Nmc, n), dtype=torch.float64, device=f"cuda:{local}")
+        res = {"n_points": n, "Nmc": Nmc}
+        for prec in ("bf16", "fp32"):
+            def call():
+                ctx.generate(dx, 3, n, 1, marg, (1.0, 1.0, 1.0), avg, var, Nmc, method, dout, precision=prec, **o)
+            for _ in range(2):
+                call()
+            ctx.synchronize()
+            reps = 5 if prec == "bf16" else 2
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            kms = []
+            a.record()
+            for _ in range(reps):
+                call()
+                kms.append(ctx.last_times()[1])
+            b.record()
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b) / reps
+            res[prec] = {"value": n * Nmc / (ms / 1e3), "unit": "field values/s", "ms_per_call": ms,
+                         "contract_ms": float(np.mean(kms))}
+        K = 4 * 16 ** 3 if method == 2 else 64 * 64
+        flops = 2.0 * n * 2 * K * Nmc
+        res["bounds_ms"] = {"tensor": flops / (peak_tflops * 1e12) * 1e3,
+                            "sfu": (n * K if method == 1 else n * 48) / sfu_rate * 1e3}
+        res["bf16_over_fp32_plain"] = res["bf16"]["value"] / res["fp32"]["value"]
+        out[name] = res
+        del dx, dout
+    ctx.close()
+    return out
+
+
 def bench_batched(args, rf, torch, local):
     """512 requests in one grouped launch (rf_generate_batch_device, CUDA
     graph replay after the first batch), device-resident buffers; e2e through
@@ -287,7 +340,7 @@ def bench_batched(args, rf, torch, local):
     return out
 
 
-def bench_serving(args, rf, torch, local):
+def bench_serving(args, rf, torch, local, rate=SERVE_RATE, seconds=None):
     """Poisson arrivals at 200 requests/s into the serving loop for
     --serve-seconds: request sizes as in the batched mix plus 5% 256^3 grids
     with Nmc = 16.  A pool of 96 clients with page-locked buffers issues the
@@ -343,8 +396,8 @@ def bench_serving(args, rf, torch, local):
     th = threading.Thread(target=waiter)
     th.start()
     base = srv.stats()
-    T = float(args.serve_seconds)
-    gaps = rs.exponential(1.0 / SERVE_RATE, size=int(SERVE_RATE * T * 1.5) + 16)
+    T = float(seconds if seconds is not None else args.serve_seconds)
+    gaps = rs.exponential(1.0 / rate, size=int(rate * T * 1.5) + 16)
     arrivals = np.cumsum(gaps)
     arrivals = arrivals[arrivals < T]
     blocked_s, offered, nxt = 0.0, 0.0, 0
@@ -378,7 +431,7 @@ def bench_serving(args, rf, torch, local):
     completed = st["completed"] - base["completed"]
     vals = st["field_values"] - base["field_values"]
     n_large = sum(1 for c in pool if c["kind"] == "grid256")
-    return {"workload": f"Poisson {SERVE_RATE:.0f} req/s for {T:.0f} s; sizes as the batched mix plus 5% 256^3 "
+    return {"workload": f"Poisson {rate:.0f} req/s for {T:.0f} s; sizes as the batched mix plus 5% 256^3 "
                         "grids with Nmc 16, each the localization blend of 8 subdomains (134^3, 12 shared points)",
             "client_pool": f"{len(pool)} clients, {n_large} of them 256^3 blends",
             "requests": int(completed), "value": vals / wall, "unit": "field values/s",
@@ -401,6 +454,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
     ap.add_argument("--no-batched", action="store_true", help="skip the 512-request batched form")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop form")
+    ap.add_argument("--serve-low-rate", type=float, default=30.0,
+                    help="second serving run at this arrival rate (requests/s), below the device's capacity")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="duration of the Poisson arrival stream (the serving config names 60 s)")
     ap.add_argument("--grid", default="128,128,128",
@@ -554,11 +609,15 @@ def main():
     ctx.close()
     del dx, dout, flush
     torch.cuda.empty_cache()
-    batched = serving = None
+    batched = serving = configs = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        configs = bench_configs(args, rf, torch, local, sfu, peak)
     if rank == 0 and world == 1 and not args.no_batched and args.precision != "fp32":
         batched = bench_batched(args, rf, torch, local)
     if rank == 0 and world == 1 and not args.no_serve and args.precision != "fp32":
         serving = bench_serving(args, rf, torch, local)
+        # the same loop at an arrival rate the device sustains, for the latency of an unsaturated loop
+        serving["at_sustainable_rate"] = bench_serving(args, rf, torch, local, rate=args.serve_low_rate, seconds=10.0)
     if rank == 0:
         line = {
             "metric": "field values/s", "value": value, "unit": "field values/s", "n_gpus": world,
@@ -576,6 +635,7 @@ def main():
             "e2e": e2e,
             "accuracy": acc,
             "forms": forms,
+            "configs": configs,
             "batched": batched,
             "serving": serving,
         }
