@@ -60,6 +60,7 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
       if (d < P.nDim) x[d] = a.x[p * P.nDim + d] / P.corrL[d];
   }
 
+  const bool fastPhase = table_fast_phase(x, P.kMax);
   Grid3Thread g3;
   if (GEN == GEN_GRID3) {
     grid3_thread_setup<LPAD>(g3, P, h, x);
@@ -101,10 +102,12 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
       });
     } else {
       const int col0 = h * (kTableChunk / 2);
-      table_pairs(sK, h, x, [&](int idx, float c, float sn) {
+      auto put = [&](int idx, float c, float sn) {
         As[(2 * (col0 + idx)) * kTileM + row] = c;
         As[(2 * (col0 + idx) + 1) * kTileM + row] = sn;
-      });
+      };
+      if (fastPhase) table_pairs<true, kTableChunk / 2>(sK, h, x, put);
+      else table_pairs<false, kTableChunk / 2>(sK, h, x, put);
     }
     __syncthreads();
 

@@ -2,8 +2,8 @@
 //
 // A trig tile holds, for 128 points and a stage of wavevectors, the pair
 // (cos(k.x), sin(k.x)) of every (point, k).  Two generators:
-//   GEN_TABLE  explicit wavevector table: FP64 phase k.x, Cody-Waite reduction
-//              to [-pi, pi], SFU sincos (one MUFU sin + cos per pair);
+//   GEN_TABLE  explicit wavevector table: FP64 phase k.x in turns, reduced
+//              modulo one turn, SFU sincos (one MUFU sin + cos per pair);
 //   GEN_GRID3  3-D tensor-grid wavevectors k = (i1 d1, s2 i2 d2, s3 i3 d3)
 //              (spectra_RF.f90:87-133): per-axis FP64-reduced tables
 //              E_d(i) = exp(i k_d(i) x_d) per point and angle addition
@@ -156,23 +156,59 @@ __device__ __forceinline__ void grid3_pairs(const Grid3Thread& g, float2 Pq, Emi
   }
 }
 
-// GEN_TABLE: (cos, sin) of k_j . x for the 16 wavevectors j = h*16 + t of a
-// stage; kt = [3][kTableChunk] FP64.  The phase accumulates x.k from zero in
-// axis order as DGEMM 'T' does (BLAS/dgemm.f90:246-249).
-template <typename Emit>
+// GEN_TABLE: (cos, sin) of k_j . x for the T wavevectors j = h * T + t,
+// t < T, of a stage (column part h); kt = [3][kTableChunk] FP64
+// wavevector components in turns (k / 2 pi).  The phase accumulates x.k in
+// FP64 from the first axis, as DGEMM 'T' does (BLAS/dgemm.f90:246-249).
+//
+// Reduction modulo one turn.  FAST (the caller's bound |x.k| < 2^18 turns):
+// adding 1.5 * 2^20 puts the phase on the FP64 grid of 2^-32 turns, so the
+// low word of the sum is the phase modulo one turn as a signed 32-bit
+// fixed-point number; an arithmetic shift keeps 2^-23 turns (the shift
+// constant carries the half unit that rounds), and the integer becomes a
+// float exactly through the exponent of 1.5 * 2^23.  One FP64 add and no
+// conversion instruction: the conversion unit is the one the SFU sincos
+// also needs.  Otherwise the integer part is removed with rint (exact).
+// Both keep the angle within 2^-24 turns of the FP64 phase, inside
+// [-pi, pi], where __sincosf is accurate to 2^-21.4.
+template <bool FAST, int T, typename Emit>
 __device__ __forceinline__ void table_pairs(const double* kt, int h, const double* x, Emit&& emit) {
+  static_assert(T % 2 == 0 && T <= kTableChunk, "pairs of wavevectors per thread");
+  constexpr double kShift = 1572864.0 + 0x1p-24;         // 1.5 * 2^20 + half a unit of 2^-23
+  constexpr float kUnit = 6.283185307179586f * 0x1p-23f;  // radians per 2^-23 turn
+  float r[T];
 #pragma unroll
-  for (int t = 0; t < kTableChunk / 2; ++t) {
-    const int j = h * (kTableChunk / 2) + t;
-    double th = 0.0;
-    th = th + x[0] * kt[j];
-    th = th + x[1] * kt[kTableChunk + j];
-    th = th + x[2] * kt[2 * kTableChunk + j];
-    const float r = (float)reduce_2pi(th);
+  for (int t = 0; t < T; t += 2) {
+    const int j = h * T + t;
+    const double2 k0 = *reinterpret_cast<const double2*>(kt + j);
+    const double2 k1 = *reinterpret_cast<const double2*>(kt + kTableChunk + j);
+    const double2 k2 = *reinterpret_cast<const double2*>(kt + 2 * kTableChunk + j);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      double th = 0.0;
+      th = th + x[0] * (e ? k0.y : k0.x);
+      th = th + x[1] * (e ? k1.y : k1.x);
+      th = th + x[2] * (e ? k2.y : k2.x);
+      if (FAST) {
+        const int32_t q = __double2loint(th + kShift) >> 9;
+        r[t + e] = (__int_as_float(0x4B400000 + q) - 12582912.0f) * kUnit;
+      } else {
+        r[t + e] = (float)(th - rint(th)) * 6.283185307179586f;
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
     float s, c;
-    __sincosf(r, &s, &c);
+    __sincosf(r[t], &s, &c);
     emit(t, c, s);
   }
+}
+
+// Whether a point may take the FAST reduction of table_pairs: |x.k| / 2 pi is
+// below 2^18 turns for every |k_d| <= kMax (every table's bound).
+__device__ __forceinline__ bool table_fast_phase(const double* x, double kMax) {
+  return (fabs(x[0]) + fabs(x[1]) + fabs(x[2])) * kMax < 0x1p18 * 6.283185307179586;
 }
 
 }  // namespace rfb

@@ -30,7 +30,7 @@ inline bool prec_hilo(int32_t prec) { return prec == PREC_BF16 || prec == PREC_F
 constexpr int kTileM = 128;        // points per tile (MMA M)
 constexpr int kStageCols = 64;     // max k-values (TMEM columns) per GEN_GRID3 group or FP32 stage
 constexpr int kMaxStageCols = 128; // max k-values per tcgen05 stage (two groups)
-constexpr int kTableChunk = 32;    // k-values per stage for GEN_TABLE
+constexpr int kTableChunk = 64;    // k-values per stage for GEN_TABLE
 constexpr int kMaxGridN = 32;      // GEN_GRID3: max wavenumbers per axis
 constexpr int kMaxNmcPad = 256;    // realizations per launch (MMA N <= 256)
 

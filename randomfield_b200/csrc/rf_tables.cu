@@ -144,7 +144,8 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
 
   if (ktab && r == 0) {
     double* kt = ktab + stage * 3 * P.chunkK;
-    for (int d = 0; d < 3; ++d) kt[d * P.chunkK + c] = v.k[d];
+    // in turns: the generators reduce the phase x.k / 2 pi modulo one
+    for (int d = 0; d < 3; ++d) kt[d * P.chunkK + c] = v.k[d] / 6.283185307179586;
   }
 
   double bc = 0.0, bs = 0.0;

@@ -12,17 +12,17 @@
 // many requests per CTA (the batched and serving forms), choosing the
 // generator per tile.
 //
-// Warp roles (320 threads, one CTA per SM):
+// Warp roles (one CTA per SM; 320 threads, 576 for GEN_TABLE kernels):
 //   warp 0      MMA issuer: the warp runs the stage loop, one elected lane
 //               issues tcgen05.mma kind::f16 (A from TMEM, B by descriptor
 //               from SMEM) and tcgen05.commit, which frees stages;
-//   warps 1-8   generators: build the trig tile of each stage straight into
-//               TMEM (tcgen05.st), lane = point; the two warps of a TMEM lane
-//               quarter split the columns; after the last stage of a tile they
-//               run the fused epilogue (tcgen05.ld, ampMult, marginal map,
-//               FP64 stores; or the localization blend's weighted add into
-//               the group field);
-//   warp 9      producer (one thread): 1-D bulk copies (TMA) of B stages from
+//   warps 1-G   generators (G = 8, or 16 for GEN_TABLE): build the trig tile
+//               of each stage straight into TMEM (tcgen05.st), lane = point;
+//               the G/4 warps of a TMEM lane quarter split the columns; after
+//               the last stage of a tile they run the fused epilogue
+//               (tcgen05.ld, ampMult, marginal map, FP64 stores; or the
+//               localization blend's weighted add into the group field);
+//   warp G+1    producer (one thread): 1-D bulk copies (TMA) of B stages from
 //               HBM/L2 into SMEM; no multicast.
 // The issuing thread can run only about one MMA ahead of the tensor core, so
 // anything it does between MMAs idles the tensor pipe: it waits on one
@@ -49,10 +49,22 @@ namespace rfb {
 namespace {
 
 constexpr int kMmaWarp = 0;
-constexpr int kGenWarp0 = 1;  // generators: warps 1-8
-constexpr int kGenWarps = 8;
-constexpr int kProdWarp = kGenWarp0 + kGenWarps;
-constexpr int kThreads = (kProdWarp + 1) * 32;
+constexpr int kGenWarp0 = 1;  // generators: warps 1 .. Roles::kGen
+// Warp roles of a kernel variant.  GEN_TABLE kernels run 16 generator warps
+// (four per TMEM lane quarter, each a quarter of the stage's columns): their
+// generators are latency-bound on the FP64 -> SFU chain of each pair, and
+// four warps per sub-partition hide what two could not (200k points,
+// isotropic 64 x 64 wavevectors: 1.08 -> 0.96 ms).  GEN_GRID3 kernels keep 8: at 16 the
+// 128^3 workload ran 3 % slower (it is held at the 1000 W power cap, where
+// more warps only spend more energy per stage), and the grouped kernel holds
+// both generators' state, more registers than 576 threads have.
+template <int GEN>
+struct Roles {
+  static constexpr int kGen = GEN == GEN_TABLE ? 16 : 8;
+  static constexpr int kParts = kGen / 4;  // column parts per lane quarter
+  static constexpr int kProd = kGenWarp0 + kGen;
+  static constexpr int kThreads = (kProd + 1) * 32;
+};
 constexpr int kMaxStages = 8;
 constexpr uint32_t kTmemCols = 512;
 constexpr int kKtabStageBytes = 3 * kTableChunk * 8;
@@ -189,6 +201,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
   // a GEN_TABLE stage kTableChunk pairs; K = 16 (16-bit) or 32 (e4m3) per MMA
   constexpr int kGridSteps = (LPAD > 0 ? LPAD / 2 : 4) / (kF8 ? 2 : 1);
   constexpr int kTabSteps = kTableSteps / (kF8 ? 2 : 1);
+  constexpr int kGenWarps = Roles<GEN>::kGen, kParts = Roles<GEN>::kParts, kProdWarp = Roles<GEN>::kProd;
   extern __shared__ __align__(1024) unsigned char smem[];
   Bars* bars = reinterpret_cast<Bars*>(smem);
   unsigned char* sB = smem + kHeaderBytes;
@@ -329,8 +342,8 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
     __syncwarp();
   } else {
     // ------------------------------------------------- generators + epilogue
-    // TMEM lane quarter = warp % 4 (the sub-partition's lanes); the two
-    // generator warps of each quarter take the two column halves.
+    // TMEM lane quarter = warp % 4 (the sub-partition's lanes); the
+    // generator warps of each quarter take the column parts h.
     const int q = warp & 3, h = (warp - kGenWarp0) >> 2;
     const int row = q * 32 + lane;
     const uint32_t laneOff = (uint32_t)(q * 32) << 16;
@@ -351,10 +364,11 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
           if (d < P.nDim) x[d] = v.x[p * P.nDim + d] / P.corrL[d];
       }
 
+      const bool fastPhase = table_fast_phase(x, P.kMax);
       Grid3Thread g3;
       Grid3Walk walk;
       if (kHasGrid && grid) {
-        grid3_thread_setup<LPAD>(g3, P, h, x);
+        grid3_thread_setup<LPAD>(g3, P, kParts == 4 ? (h & 1) : h, x);
         walk.init(P, x);
       }
 
@@ -374,8 +388,14 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
         if (lane == 0 && ch + 1 < nChunks) probe = mbar_test_wait(&bars->empty[s], ph ^ 1) ? 1u : 0u;
         const uint32_t aAddr = tbase + laneOff + (uint32_t)L.aCol0 + sc * (uint32_t)L.aStride;
         if (kHasGrid && grid) {
+          // Two groups per stage.  With two column parts per lane quarter a
+          // thread takes its half (h) of both groups; with four, half h & 1
+          // of group h >> 1 only, and walks past the other group's phasor.
 #pragma unroll
-          for (int u = 0; u < 2; ++u) {  // two groups per stage
+          for (int u = 0; u < 2; ++u) {
+            const float2 Pq = walk.outer();
+            walk.next(P, x);
+            if (kParts == 4 && u != (h >> 1)) continue;
             // one TMEM column per (cos, sin) pair, or per two pairs for e4m3
             constexpr int NW = kF8 ? (LPAD > 0 ? LPAD / 2 : 1) : (LPAD > 0 ? LPAD : 1);
             uint32_t words[NW];
@@ -392,12 +412,10 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
                 words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
               }
             };
-            const float2 Pq = walk.outer();
-            walk.next(P, x);
             grid3_pairs<LPAD>(g3, Pq, emit);
             // LPAD is a multiple of 8: 16-bit stores cover 8 columns at
             // 8-aligned offsets, e4m3 stores 4 columns at 4-aligned offsets.
-            const uint32_t col = aAddr + (uint32_t)(u * 2 * NW + h * NW);
+            const uint32_t col = aAddr + (uint32_t)(u * 2 * NW + (kParts == 4 ? (h & 1) : h) * NW);
             if (kF8) {
 #pragma unroll
               for (int pc = 0; pc < NW / 4; ++pc) tmem_st4(col + pc * 4, &words[pc * 4]);
@@ -407,7 +425,8 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
             }
           }
         } else if (kHasTable) {
-          constexpr int NW = kF8 ? kTableChunk / 4 : kTableChunk / 2;
+          constexpr int T = kTableChunk / kParts;  // pairs of this thread
+          constexpr int NW = kF8 ? T / 2 : T;
           uint32_t words[NW];
           float pc0 = 0.f, ps0 = 0.f;
           auto emit = [&](int idx, float c, float sn) {
@@ -422,7 +441,8 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
               words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
             }
           };
-          table_pairs(sK + sc * 3 * kTableChunk, h, x, emit);
+          if (fastPhase) table_pairs<true, T>(sK + sc * 3 * kTableChunk, h, x, emit);
+          else table_pairs<false, T>(sK + sc * 3 * kTableChunk, h, x, emit);
           const uint32_t col = aAddr + (uint32_t)(h * NW);
 #pragma unroll
           for (int pc = 0; pc < NW / 8; ++pc) tmem_st8(col + pc * 8, &words[pc * 8]);
@@ -438,11 +458,10 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
       // ---------------------------------------------------------- epilogue
       if (!mbar_wait_warp(&bars->acc_full, accPh, abort_flag)) { ok = false; break; }
       tc_fence_after();
-      const int half = P.nmcPad / 2;
       double bw = 0.0;  // localization blend: weight and group index of this point
       int64_t bg = 0;
       if (P.blend && valid) bw = blend_weight(P, p, &bg);
-      for (int cb = h * half; cb < (h + 1) * half; cb += 8) {
+      for (int cb = h * 8; cb < P.nmcPad; cb += 8 * kParts) {  // 8-column blocks, round robin over the parts
         uint32_t va[8], lo[8];
         tmem_ld8(tbase + laneOff + cb, va);
         if (kHiLo) tmem_ld8(tbase + laneOff + P.nmcPad + cb, lo);
@@ -477,13 +496,13 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
 
 // LPAD: GEN_GRID3 axis-3 length padded to 8/16/24/32 (0 for GEN_TABLE).
 template <int GEN, int PREC, int LPAD>
-__global__ void __launch_bounds__(kThreads, 1) rf_tc_kernel(const __grid_constant__ TcArgs a) {
+__global__ void __launch_bounds__(Roles<GEN>::kThreads, 1) rf_tc_kernel(const __grid_constant__ TcArgs a) {
   const SingleWork w{&a, (a.rows + kTileM - 1) / kTileM};
   tc_body<GEN, PREC, LPAD>(w, a.L, a.err);
 }
 
 template <int PREC>
-__global__ void __launch_bounds__(kThreads, 1) rf_group_kernel(const __grid_constant__ GroupArgs g) {
+__global__ void __launch_bounds__(Roles<GEN_MIXED>::kThreads, 1) rf_group_kernel(const __grid_constant__ GroupArgs g) {
   const GroupWork w{&g, g.ctaStart[blockIdx.x], g.ctaStart[blockIdx.x + 1]};
   tc_body<GEN_MIXED, PREC, kGroupLPad>(w, g.L, g.err);
 }
@@ -493,7 +512,7 @@ cudaError_t launch_one(const TcArgs& args, size_t smem, int grid, cudaStream_t s
   auto fn = rf_tc_kernel<GEN, PREC, LPAD>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  fn<<<grid, kThreads, smem, st>>>(args);
+  fn<<<grid, Roles<GEN>::kThreads, smem, st>>>(args);
   return cudaGetLastError();
 }
 
@@ -511,7 +530,7 @@ cudaError_t launch_prec(const Plan& P, const TcArgs& args, size_t smem, int grid
 
 template <int PREC>
 cudaError_t launch_group_prec(const GroupArgs& g, size_t smem, int grid, cudaStream_t st) {
-  rf_group_kernel<PREC><<<grid, kThreads, smem, st>>>(g);
+  rf_group_kernel<PREC><<<grid, Roles<GEN_MIXED>::kThreads, smem, st>>>(g);
   return cudaGetLastError();
 }
 
