@@ -135,7 +135,7 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
       maxBRows = std::max(maxBRows, P.bRows);
       maxStage = std::max(maxStage, P.stageBytes);
       arena += align_up((size_t)(P.nChunks * P.stageBytes));
-      if (P.gen == GEN_TABLE) arena += align_up((size_t)P.nChunks * 3 * kTableChunk * sizeof(double));
+      if (P.gen == GEN_TABLE) arena += align_up((size_t)P.nChunks * kKtabStageBytes);
     }
   }
   const size_t nU = subs.size();
@@ -151,7 +151,7 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
     off += align_up((size_t)(g.P.nChunks * g.P.stageBytes));
     if (g.P.gen == GEN_TABLE) {
       g.ktab = reinterpret_cast<double*>(c->dArena + off);
-      off += align_up((size_t)g.P.nChunks * 3 * kTableChunk * sizeof(double));
+      off += align_up((size_t)g.P.nChunks * kKtabStageBytes);
     }
   }
 
@@ -342,7 +342,7 @@ int request_footprint(const Request& rq, const double* ext, int rblk, size_t* by
     P.nmcBlk = std::min(rblk, P0.Nmc - r0);
     if (int rc = layout(P)) return rc;
     b += align_up((size_t)(P.nChunks * P.stageBytes));
-    if (P.gen == GEN_TABLE) b += align_up((size_t)P.nChunks * 3 * kTableChunk * sizeof(double));
+    if (P.gen == GEN_TABLE) b += align_up((size_t)P.nChunks * kKtabStageBytes);
   }
   *bytes = b;
   return RF_OK;

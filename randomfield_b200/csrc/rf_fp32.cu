@@ -42,8 +42,8 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
   constexpr int NB = 8 * RPT;
   float* As = reinterpret_cast<float*>(smem);                 // [kMaxKel][128]
   float* Bs = As + kMaxKel * kTileM;                          // [kMaxKel][NB]
-  double* sK = reinterpret_cast<double*>(Bs + kMaxKel * NB);  // [3][kTableChunk]
-  float2* e12 = reinterpret_cast<float2*>(sK + 3 * kTableChunk);
+  double* sK = reinterpret_cast<double*>(Bs + kMaxKel * NB);  // one wavevector chunk
+  float2* e12 = reinterpret_cast<float2*>(sK + kKtabStageDoubles);
 
   const int tid = threadIdx.x;
   const int row = tid & (kTileM - 1), h = tid >> 7;
@@ -88,7 +88,8 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
       Bs[e * NB + c] = bsrc[(int64_t)e * P.nmcPad + c];
     }
     if (GEN == GEN_TABLE) {
-      for (int i = tid; i < 3 * kTableChunk; i += kThreads) sK[i] = a.ktab[ch * 3 * kTableChunk + i];
+      // the FP64 part of the chunk (the fixed-point arrays serve the tensor-core forms)
+      for (int i = tid; i < 3 * kTableChunk; i += kThreads) sK[i] = a.ktab[ch * kKtabStageDoubles + i];
       __syncthreads();
     }
     // trig tile: element 2c = cos, 2c+1 = sin of stage column c
@@ -106,6 +107,8 @@ __global__ void __launch_bounds__(kThreads) rf_fp32_kernel(const __grid_constant
         As[(2 * (col0 + idx)) * kTileM + row] = c;
         As[(2 * (col0 + idx) + 1) * kTileM + row] = sn;
       };
+      // FP64 phases: no tensor-core work here for FP64 to contend with, and
+      // the fixed-point form costs more instructions per pair
       if (fastPhase) table_pairs<true, kTableChunk / 2>(sK, h, x, put);
       else table_pairs<false, kTableChunk / 2>(sK, h, x, put);
     }
@@ -184,7 +187,7 @@ int rpt_of(const Plan& P) {
 size_t fp32_smem_bytes(const Plan& P) {
   const int nb = 8 * rpt_of(P);
   const size_t e12 = (P.gen == GEN_GRID3) ? (size_t)(P.kNStep[0] + P.kNStep[1]) * kTileM * sizeof(float2) : 0;
-  return (size_t)kMaxKel * kTileM * 4 + (size_t)kMaxKel * nb * 4 + 3 * kTableChunk * 8 + e12;
+  return (size_t)kMaxKel * kTileM * 4 + (size_t)kMaxKel * nb * 4 + kKtabStageBytes + e12;
 }
 
 cudaError_t launch_fp32(const Plan& P, const double* dX, const void* dB, const double* dKtab, double* dOut,

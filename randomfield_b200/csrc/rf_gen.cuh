@@ -205,6 +205,82 @@ __device__ __forceinline__ void table_pairs(const double* kt, int h, const doubl
   }
 }
 
+// GEN_TABLE for the tensor-core forms, without FP64 in the per-pair work.
+// FP64 instructions issue to the sub-partition pipe the tcgen05 MMAs also
+// occupy, so an FP64 phase per (point, wavevector) stalls behind the
+// contraction.  Fixed point instead: with x = a + b, a = A / 4 (A integer)
+// and |b| <= 1/8, and k / 2 pi = C 2^-30 + e (C integer, |e| <= 2^-31),
+//   x.k = 2 pi (sum_d A_d C_d) 2^-32 + sum_d b_d k_d + 2 pi sum_d a_d e_d.
+// The first term modulo 2 pi is the wrapped 32-bit integer sum (exact for
+// any magnitude), kept to 2^-23 turns; the second, below 1.6 rad
+// (|b| <= 1/8, |k_1| <= sqrt(3) kMax), is formed in FP32; the third is below
+// 2 pi |x|_1 2^-31 and is dropped: the point takes this path when
+// |x|_1 <= 128 (2^-24 turns).  The angle lies in [-1.51 pi, 1.51 pi] and
+// carries at most 9e-7 rad of error (rms 2.4e-7); __sincosf measured on this
+// range stays within 7.1e-7 of sin and cos (4.0e-7 on [-pi, pi]).  All of
+// it is far below the 16-bit rounding of the trig tile.  Other points take
+// the FP64 table_pairs, as does the plain FP32 form.
+struct FxpPoint {
+  int32_t A[3];
+  float b[3];
+  bool ok;
+};
+
+__device__ __forceinline__ FxpPoint fxp_point(const double* x, double kMax) {
+  FxpPoint f;
+  // |k / 2 pi| <= kMax / 2 pi < 2 keeps C within int32
+  f.ok = (fabs(x[0]) + fabs(x[1]) + fabs(x[2])) <= 128.0 && kMax < 4.0 * 3.141592653589793;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double a = f.ok ? rint(x[d] * 4.0) : 0.0;
+    f.A[d] = (int32_t)a;
+    f.b[d] = (float)(x[d] - 0.25 * a);
+  }
+  return f;
+}
+
+// The T pairs j = h * T + t of a stage (T a multiple of 4) from the fixed
+// point and FP32 arrays of the stage's wavevector chunk kt.
+template <int T, typename Emit>
+__device__ __forceinline__ void table_pairs_fxp(const double* kt, int h, const FxpPoint& f, Emit&& emit) {
+  static_assert(T % 4 == 0 && T <= kTableChunk, "pairs of wavevectors per thread");
+  const int32_t* kc = reinterpret_cast<const int32_t*>(kt + 3 * kTableChunk);
+  const float* kf = reinterpret_cast<const float*>(kc + 3 * kTableChunk);
+  constexpr float kUnit = 6.283185307179586f * 0x1p-23f;  // radians per 2^-23 turn
+  float r[T];
+#pragma unroll
+  for (int t = 0; t < T; t += 4) {
+    const int j = h * T + t;
+    const int4 c0 = *reinterpret_cast<const int4*>(kc + j);
+    const int4 c1 = *reinterpret_cast<const int4*>(kc + kTableChunk + j);
+    const int4 c2 = *reinterpret_cast<const int4*>(kc + 2 * kTableChunk + j);
+    const float4 f0 = *reinterpret_cast<const float4*>(kf + j);  // k in radians, FP32
+    const float4 f1 = *reinterpret_cast<const float4*>(kf + kTableChunk + j);
+    const float4 f2 = *reinterpret_cast<const float4*>(kf + 2 * kTableChunk + j);
+    const int32_t cc[3][4] = {{c0.x, c0.y, c0.z, c0.w}, {c1.x, c1.y, c1.z, c1.w}, {c2.x, c2.y, c2.z, c2.w}};
+    const float ff[3][4] = {{f0.x, f0.y, f0.z, f0.w}, {f1.x, f1.y, f1.z, f1.w}, {f2.x, f2.y, f2.z, f2.w}};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      // coarse term in units of 2^-32 turns, wrapping (unsigned arithmetic)
+      const uint32_t P = (uint32_t)f.A[0] * (uint32_t)cc[0][e] + (uint32_t)f.A[1] * (uint32_t)cc[1][e] +
+                         (uint32_t)f.A[2] * (uint32_t)cc[2][e];
+      // fine term in radians, plus half a unit of 2^-23 turn: the shift
+      // below truncates, so the sum rounds
+      const float s = fmaf(f.b[2], ff[2][e], fmaf(f.b[1], ff[1][e], fmaf(f.b[0], ff[0][e], 0.5f * kUnit)));
+      // to units of 2^-23 turns, as a float through the exponent of 1.5 * 2^23
+      const int32_t q = (int32_t)P >> 9;
+      const float qf = __int_as_float(0x4B400000 + q) - 12582912.0f;
+      r[t + e] = fmaf(qf, kUnit, s);
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    float s, c;
+    __sincosf(r[t], &s, &c);
+    emit(t, c, s);
+  }
+}
+
 // Whether a point may take the FAST reduction of table_pairs: |x.k| / 2 pi is
 // below 2^18 turns for every |k_d| <= kMax (every table's bound).
 __device__ __forceinline__ bool table_fast_phase(const double* x, double kMax) {

@@ -399,7 +399,7 @@ int run_block(rf_context* c, const Plan& P, const double* dX, double* dOut, cuda
   if (int rc = ensure(c->dB, c->capB, bBytes, "contraction operand")) return rc;
   double* ktab = nullptr;
   if (P.gen == GEN_TABLE) {
-    if (int rc = ensure(c->dKtab, c->capK, (size_t)P.nChunks * 3 * kTableChunk * sizeof(double), "wavevector table"))
+    if (int rc = ensure(c->dKtab, c->capK, (size_t)P.nChunks * kKtabStageBytes, "wavevector table"))
       return rc;
     ktab = c->dKtab;
   }

@@ -200,7 +200,7 @@ extern "C" int rf_generate_device_noalloc(const double* d_xPoints, int nDim, int
     Plan P = P0;
     if (int rc = host_block_layout(&P, r0, std::min(blk, P0.Nmc - r0))) return rc;
     const size_t opBytes = (size_t)P.nChunks * P.stageBytes;
-    const size_t tabBytes = P.gen == GEN_TABLE ? (size_t)P.nChunks * 3 * kTableChunk * sizeof(double) : 0;
+    const size_t tabBytes = P.gen == GEN_TABLE ? (size_t)P.nChunks * kKtabStageBytes : 0;
     if (opBytes > kOperandBytes || tabBytes > kTableBytes) {
       char buf[256];
       snprintf(buf, sizeof(buf),

@@ -31,6 +31,10 @@ constexpr int kTileM = 128;        // points per tile (MMA M)
 constexpr int kStageCols = 64;     // max k-values (TMEM columns) per GEN_GRID3 group or FP32 stage
 constexpr int kMaxStageCols = 128; // max k-values per tcgen05 stage (two groups)
 constexpr int kTableChunk = 64;    // k-values per stage for GEN_TABLE
+// The GEN_TABLE wavevector chunk of one stage: three [3][kTableChunk] arrays,
+// k / 2 pi in FP64, round(k / 2 pi * 2^30) in int32 and k in FP32.
+constexpr int kKtabStageDoubles = 6 * kTableChunk;
+constexpr int kKtabStageBytes = 8 * kKtabStageDoubles;
 constexpr int kMaxGridN = 32;      // GEN_GRID3: max wavenumbers per axis
 constexpr int kMaxNmcPad = 256;    // realizations per launch (MMA N <= 256)
 

@@ -143,9 +143,18 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
   const int32_t c = (int32_t)(kk % P.chunkK);
 
   if (ktab && r == 0) {
-    double* kt = ktab + stage * 3 * P.chunkK;
-    // in turns: the generators reduce the phase x.k / 2 pi modulo one
-    for (int d = 0; d < 3; ++d) kt[d * P.chunkK + c] = v.k[d] / 6.283185307179586;
+    // k / 2 pi in FP64 and as fixed point with 30 fraction bits (range
+    // |k / 2 pi| < 2; every table has |k_d| <= kMax <= 7.36 < 4 pi), and k in
+    // FP32 (radians).  GEN_TABLE plans have chunkK == kTableChunk.
+    double* kt = ktab + stage * kKtabStageDoubles;
+    int32_t* kc = reinterpret_cast<int32_t*>(kt + 3 * kTableChunk);
+    float* kf = reinterpret_cast<float*>(kc + 3 * kTableChunk);
+    for (int d = 0; d < 3; ++d) {
+      const double t = v.k[d] / 6.283185307179586;
+      kt[d * kTableChunk + c] = t;
+      kc[d * kTableChunk + c] = (fabs(t) < 2.0) ? (int32_t)llrint(t * 0x1p30) : 0;
+      kf[d * kTableChunk + c] = (float)v.k[d];
+    }
   }
 
   double bc = 0.0, bs = 0.0;

@@ -67,7 +67,6 @@ struct Roles {
 };
 constexpr int kMaxStages = 8;
 constexpr uint32_t kTmemCols = 512;
-constexpr int kKtabStageBytes = 3 * kTableChunk * 8;
 constexpr int kTableSteps = kTableChunk / 8;  // MMAs (K = 16) per GEN_TABLE stage
 
 struct Bars {
@@ -254,7 +253,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
           bulk_g2s(sB + (size_t)s * L.slotBytes, v.B + ch * P.stageBytes, (uint32_t)P.stageBytes, &bars->full[s]);
           if (table) {
             mbar_arrive_expect_tx(&bars->kfull[s], (uint32_t)kKtabStageBytes);
-            bulk_g2s(sK + s * 3 * kTableChunk, v.ktab + ch * 3 * kTableChunk, kKtabStageBytes, &bars->kfull[s]);
+            bulk_g2s(sK + s * kKtabStageDoubles, v.ktab + ch * kKtabStageDoubles, kKtabStageBytes, &bars->kfull[s]);
             ktabSlots |= 1u << s;
           } else {
             ktabSlots &= ~(1u << s);
@@ -365,6 +364,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
       }
 
       const bool fastPhase = table_fast_phase(x, P.kMax);
+      const FxpPoint fxp = fxp_point(x, P.kMax);
       Grid3Thread g3;
       Grid3Walk walk;
       if (kHasGrid && grid) {
@@ -441,8 +441,10 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
               words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
             }
           };
-          if (fastPhase) table_pairs<true, T>(sK + sc * 3 * kTableChunk, h, x, emit);
-          else table_pairs<false, T>(sK + sc * 3 * kTableChunk, h, x, emit);
+          const double* kt = sK + sc * kKtabStageDoubles;
+          if (fxp.ok) table_pairs_fxp<T>(kt, h, fxp, emit);
+          else if (fastPhase) table_pairs<true, T>(kt, h, x, emit);
+          else table_pairs<false, T>(kt, h, x, emit);
           const uint32_t col = aAddr + (uint32_t)(h * NW);
 #pragma unroll
           for (int pc = 0; pc < NW / 8; ++pc) tmem_st8(col + pc * 8, &words[pc * 8]);
