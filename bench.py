@@ -442,6 +442,44 @@ def bench_serving(args, rf, torch, local, rate=SERVE_RATE, seconds=None):
                        "including the four warm-up requests"}
 
 
+def run_iso_case(args):
+    """The isotropic request of config 2 alone (GEN_TABLE, BF16 unless
+    --precision): n points U[0,10]^3, 64 x 64 wavevectors, lognormal avg 1
+    var 0.25, Nmc 64; W untimed and K timed calls, device-resident."""
+    import torch
+
+    import randomfield_b200 as rf
+
+    torch.cuda.set_device(0)
+    rs = np.random.RandomState(12)
+    n = args.points
+    pts = rs.uniform(0.0, 10.0, size=(n, 3)).astype(np.float32).astype(np.float64)
+    ctx = rf.Context(0)
+    ctx.set_timing(True)
+    dx = torch.from_numpy(pts).cuda()
+    dout = torch.empty((64, n), dtype=torch.float64, device="cuda")
+
+    def call():
+        ctx.generate(dx, 3, n, 1, 2, (1.0, 1.0, 1.0), 1.0, 0.25, 64, 1, dout, precision=args.precision,
+                     iso_n_radial=64, iso_n_dir=64)
+
+    for _ in range(args.warmup):
+        call()
+    ctx.synchronize()
+    kms = []
+    for _ in range(args.steps):
+        call()
+        kms.append(ctx.last_times()[1])
+    ctx.synchronize()
+    if not torch.isfinite(dout).all().item():
+        raise RuntimeError("non-finite field values")
+    ms = float(np.mean(kms))
+    print(json.dumps({"case": "isotropic", "workload": f"{n} points U[0,10]^3, isotropic 64 x 64, Nmc 64, lognormal",
+                      "precision": args.precision, "contract_ms": ms, "value": n * 64 / (ms / 1e3),
+                      "unit": "field values/s", "steps": args.steps, "warmup": args.warmup}))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -458,6 +496,10 @@ def main():
                     help="second serving run at this arrival rate (requests/s), below the device's capacity")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="duration of the Poisson arrival stream (the serving config names 60 s)")
+    ap.add_argument("--case", default="headline", choices=["headline", "iso"],
+                    help="iso: only the isotropic request of config 2 (GEN_TABLE), on --points points, for "
+                         "profiler captures of that kernel; prints one JSON line of its own")
+    ap.add_argument("--points", type=int, default=200000, help="points of the --case iso request")
     ap.add_argument("--grid", default="128,128,128",
                     help="grid points per axis; a smaller grid (e.g. 32,32,18 = one wave of 144 tiles) "
                          "keeps profiler captures short; the headline workload is 128,128,128")
@@ -470,6 +512,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.case == "iso":
+        run_iso_case(args)
         return
 
     import torch
@@ -571,7 +616,6 @@ def main():
     if not args.no_e2e:
         e2e = end_to_end(args, rf, torch, dist, xh, n, opts, world, local)
 
-    pk, src = peaks()
     pk, src = peaks()
     K = 4 * KN ** 3
     flops = 2.0 * n * (2 * K) * NMC  # algorithmic: the hi/lo split's second MMA is not credited

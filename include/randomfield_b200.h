@@ -145,6 +145,39 @@ int rf_context_selftest_timeout(rf_context* ctx, double limit_ms);
  * GEN_TABLE generator (one pair per point and wavevector). */
 int rf_measure_sfu_rate(int device, double* pairs_per_second);
 
+/*
+ * Field statistics on the device (statistics_RF.f90), for a field already in
+ * device memory (rf_generate_device, rf_generate_batch_device): no copy of
+ * the field to the host.
+ *   - per realization r: mean and standard deviation over the n points
+ *     (calculate_average_and_stdVar_MPI, statistics_RF.f90:18-174, "by
+ *     event"), and their global values over all n * Nmc values;
+ *   - with a structured grid (xNStep, axis 1 fastest, n = prod xNStep): the
+ *     directional correlation of realization 1 normalised by the global mean
+ *     and deviation, lags 0 .. xNStep_d / 2 - 1 per axis (rebuild_Sk_FFT and
+ *     rebuild_Sk, :180-419: |FFT|^2 averaged over the lines, inverse FFT;
+ *     here the same circular autocorrelation summed directly), and the
+ *     correlation-length estimate 2 (sum R - (R_0 + R_last) / 2) xStep_d
+ *     (rebuild_corrL, :425-443).
+ * d_randField is n x Nmc column-major (FP64).  evnt_avg / evnt_std (host,
+ * Nmc entries each) may be null; with xNStep null only the moments are
+ * computed.  sk (host, sum_d xNStep_d / 2 entries, axis 1 first) and corrL_out
+ * (host, nDim entries) may be null.  Axis lengths above 4096 give RF_ENOTSUP.
+ * Runs on the context's stream and returns when the results are on the host.
+ * Sums are formed in FP64 in a fixed order: repeated calls give identical
+ * results.
+ */
+typedef struct rf_field_stats {
+  double global_avg;
+  double global_std;
+  int64_t n;
+  int32_t Nmc, nDim;
+} rf_field_stats;
+
+int rf_field_statistics(rf_context* ctx, const double* d_randField, int64_t n, int Nmc, int nDim,
+                        const int64_t* xNStep, const double* xStep, double* evnt_avg, double* evnt_std,
+                        double* sk, double* corrL_out, rf_field_stats* out);
+
 /* Phase timers.  With timing enabled the context records CUDA events on the
  * launching stream around each phase of a generation; rf_context_last_times
  * waits for the last one and returns the device milliseconds of the table

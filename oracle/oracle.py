@@ -228,3 +228,61 @@ def unity_partition(xNStep, overlapNPoints, faceMask=0xFFFFFFFF):
     lib().rfo_unity_partition(nd, a.ctypes.data_as(C.POINTER(C.c_int32)), b.ctypes.data_as(C.POINTER(C.c_int32)),
                               faceMask, _dptr(out))
     return out
+
+
+def field_statistics(field, xNStep=None, xStep=None):
+    """statistics_RF.f90 restated in FP64 with numpy's FFT, step by step.
+
+    field: n x Nmc (point index fastest within a realization).
+    Moments by event and global (calculate_average_and_stdVar_MPI,
+    statistics_RF.f90:62-63, :80-86).  With xNStep (axis 1 fastest): the
+    directional correlation of realization 1 as rebuild_Sk_FFT computes it
+    (:275 normalise by the global mean and deviation, forward FFT along the
+    axis, :350 divide by N, :360 times the conjugate, :380 mean over the
+    other axes, :395 unnormalised backward FFT, :405 real part), lags
+    0 .. N/2 - 1 as rebuild_Sk keeps them (:207), and the correlation length
+    of rebuild_corrL (:435).
+    """
+    f = np.asarray(field, dtype=np.float64)
+    n, Nmc = f.shape
+    S = f.sum(axis=0)
+    Q = (f * f).sum(axis=0)
+    evnt_avg = S / n
+    evnt_std = np.sqrt(Q / n - evnt_avg ** 2)
+    gavg = S.sum() / (n * Nmc)
+    gstd = np.sqrt(Q.sum() / (n * Nmc) - gavg ** 2)
+    out = {"evnt_avg": evnt_avg, "evnt_std": evnt_std, "global_avg": gavg, "global_std": gstd}
+    if xNStep is None:
+        return out
+    nd = len(xNStep)
+    a = ((f[:, 0] - gavg) / gstd).reshape(tuple(int(v) for v in reversed(xNStep)))  # a[i_nd, ..., i_1]
+    sk, cl = [], []
+    for d in range(nd):
+        ax = nd - 1 - d
+        N = int(xNStep[d])
+        F = np.fft.fft(a, axis=ax) / N
+        P = F * np.conj(F)
+        other = tuple(i for i in range(nd) if i != ax)
+        v = P.mean(axis=other) if other else P
+        R = (np.fft.ifft(v) * N).real[: N // 2]
+        sk.append(R)
+        if xStep is not None:
+            cl.append(2.0 * (R.sum() - (R[0] + R[-1]) / 2.0) * xStep[d])
+    out["sk"] = sk
+    if xStep is not None:
+        out["corrL"] = np.array(cl)
+    return out
+
+
+def circular_autocorrelation(field_col, xNStep):
+    """The same lags by the direct sum the device computes:
+    R(l) = mean over the lines along the axis of (1/N) sum_z g(z) g(z+l mod N)."""
+    nd = len(xNStep)
+    a = np.asarray(field_col, dtype=np.float64).reshape(tuple(int(v) for v in reversed(xNStep)))
+    out = []
+    for d in range(nd):
+        ax = nd - 1 - d
+        N = int(xNStep[d])
+        R = np.array([(a * np.roll(a, -l, axis=ax)).mean() for l in range(N // 2)])
+        out.append(R)
+    return out

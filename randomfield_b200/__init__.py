@@ -52,6 +52,7 @@ EXPORTS = [
     "rf_generate_batch", "rf_generate_batch_device", "rf_batch_last_stats",
     "rf_server_config_init", "rf_server_create", "rf_server_submit", "rf_server_wait", "rf_server_get_stats",
     "rf_server_destroy", "rf_server_submit_blended", "rf_context_selftest_timeout", "rf_measure_sfu_rate", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
+    "rf_field_statistics",
 ]
 
 
@@ -116,6 +117,18 @@ class Request(C.Structure):
         ("fieldAvg", C.c_double),
         ("fieldVar", C.c_double),
         ("opt", Options),
+    ]
+
+
+class FieldStats(C.Structure):
+    """rf_field_stats: global moments of a field (statistics_RF.f90:18-174)."""
+
+    _fields_ = [
+        ("global_avg", C.c_double),
+        ("global_std", C.c_double),
+        ("n", C.c_int64),
+        ("Nmc", C.c_int32),
+        ("nDim", C.c_int32),
     ]
 
 
@@ -241,6 +254,8 @@ def lib() -> C.CDLL:
         L.rf_server_destroy.argtypes = [C.c_void_p]
         L.rf_context_selftest_timeout.argtypes = [C.c_void_p, d]
         L.rf_measure_sfu_rate.argtypes = [i32, P(d)]
+        L.rf_field_statistics.argtypes = [C.c_void_p, C.c_void_p, i64, i32, i32, P(i64), P(d), P(d), P(d), P(d),
+                                          P(d), P(FieldStats)]
         L.rf_blend_layout.argtypes = [P(BlendGrid), P(d), P(C.c_int32), P(C.c_int32)]
         L.rf_server_submit_blended.argtypes = [C.c_void_p, P(BlendGrid), i32, i32, P(d), d, d, i32, i32, P(d),
                                                P(Options), P(i64)]
@@ -537,6 +552,43 @@ class Context:
                                                 cl.ctypes.data_as(C.POINTER(C.c_double)), float(fieldAvg),
                                                 float(fieldVar), int(Nmc), int(method), C.c_void_p(self._ptr(d_out)),
                                                 C.byref(o), C.c_void_p(s)))
+
+    def field_statistics(self, d_field, n: int, Nmc: int, nDim: int = 3, grid=None, step=None) -> dict:
+        """rf_field_statistics on a device field (n x Nmc column-major, e.g.
+        a torch tensor of shape (Nmc, n)): per-realization mean and standard
+        deviation, global mean and deviation, and with ``grid`` (points per
+        axis, axis 1 fastest) and ``step`` the directional correlation of
+        realization 1 (lags 0 .. N_d/2 - 1 per axis) and the correlation
+        length estimate per axis."""
+        P = C.POINTER(C.c_double)
+        avg = np.empty(int(Nmc))
+        std = np.empty(int(Nmc))
+        st = FieldStats()
+        out = {}
+        if grid is not None:
+            g = np.ascontiguousarray(np.asarray(grid, dtype=np.int64).reshape(-1)[:nDim])
+            h = np.ascontiguousarray(np.asarray(step, dtype=np.float64).reshape(-1)[:nDim]) if step is not None \
+                else None
+            sk = np.empty(int(sum(int(v) // 2 for v in g)))
+            cl = np.empty(int(nDim))
+            _check(lib().rf_field_statistics(self._h, C.c_void_p(self._ptr(d_field)), int(n), int(Nmc), int(nDim),
+                                             g.ctypes.data_as(C.POINTER(C.c_int64)),
+                                             h.ctypes.data_as(P) if h is not None else None, avg.ctypes.data_as(P),
+                                             std.ctypes.data_as(P), sk.ctypes.data_as(P),
+                                             cl.ctypes.data_as(P) if h is not None else None, C.byref(st)))
+            parts, o = [], 0
+            for v in g:
+                parts.append(sk[o:o + int(v) // 2])
+                o += int(v) // 2
+            out["sk"] = parts
+            if h is not None:
+                out["corrL"] = cl
+        else:
+            _check(lib().rf_field_statistics(self._h, C.c_void_p(self._ptr(d_field)), int(n), int(Nmc), int(nDim),
+                                             None, None, avg.ctypes.data_as(P), std.ctypes.data_as(P), None, None,
+                                             C.byref(st)))
+        out.update(evnt_avg=avg, evnt_std=std, global_avg=st.global_avg, global_std=st.global_std)
+        return out
 
     def batch_stats(self) -> dict:
         st = BatchStats()

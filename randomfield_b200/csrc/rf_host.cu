@@ -309,6 +309,8 @@ void context_free(rf_context* c) {
   cudaFree(c->dB);
   cudaFree(c->dKtab);
   cudaFree(c->dWork);
+  cudaFree(c->dStats);
+  if (c->hStats) cudaFreeHost(c->hStats);
   cudaFree(c->dErr);
   cudaFree(c->dX);
   cudaFree(c->dOut);

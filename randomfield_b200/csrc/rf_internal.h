@@ -27,6 +27,10 @@ struct rf_context {
   double* dWork = nullptr;  // extent partials and moments
   size_t capWork = 0;
   double* hWork = nullptr;  // pinned mirror of dWork
+  double* dStats = nullptr; // field statistics scratch (rf_stats.cu)
+  size_t capStats = 0;
+  double* hStats = nullptr;
+  size_t capHStats = 0;
   uint32_t* dErr = nullptr;
   double* dX = nullptr;     // flat API staging of the points
   size_t capX = 0;
