@@ -27,6 +27,7 @@ extern "C" {
 #define RF_ISOTROPIC 1
 #define RF_SHINOZUKA 2
 #define RF_RANDOMIZATION 3  /* Shinozuka sum over uniformly random wavevectors (randomFieldND.f90:343-361) */
+#define RF_FFT 4            /* spectral DCT on a structured grid: rf_generate_fft_grid (randomFieldND.f90:520-763) */
 #define RF_CM_GAUSSIAN 1
 #define RF_CM_COS 2
 #define RF_FOM_GAUSSIAN 1
@@ -177,6 +178,22 @@ typedef struct rf_field_stats {
 int rf_field_statistics(rf_context* ctx, const double* d_randField, int64_t n, int Nmc, int nDim,
                         const int64_t* xNStep, const double* xStep, double* evnt_avg, double* evnt_std,
                         double* sk, double* corrL_out, rf_field_stats* out);
+
+/*
+ * The FFT method (method 4; gen_Std_Gauss_FFT, randomFieldND.f90:520-763),
+ * which the reference runs on a structured mesh only: the grid has xNStep[d]
+ * points spaced xStep[d] along axis d (nDim 2 or 3, axis 1 fastest, 2 to
+ * 2048 points per axis).  Random amplitudes on the k grid of set_kPoints'
+ * FFT branch (spectra_RF.f90:135-160), the multi-dimensional DCT-III of
+ * FFTW's REDFT01 with the reference's scale, then the marginal map.  The
+ * reference fills realization 1 only; realization r here uses the rnglib
+ * stream of seed_start + r, so realization 1 is the reference's.
+ * d_randField (device) is prod(xNStep) x Nmc column-major.  Returns when
+ * the field is complete.
+ */
+int rf_generate_fft_grid(rf_context* ctx, int nDim, const int64_t* xNStep, const double* xStep, int corrMod,
+                         int margiFirst, const double* corrL, double fieldAvg, double fieldVar, int Nmc,
+                         double* d_randField, const rf_options* opt);
 
 /* Phase timers.  With timing enabled the context records CUDA events on the
  * launching stream around each phase of a generation; rf_context_last_times

@@ -286,3 +286,44 @@ def circular_autocorrelation(field_col, xNStep):
         R = np.array([(a * np.roll(a, -l, axis=ax)).mean() for l in range(N // 2)])
         out.append(R)
     return out
+
+
+PI_REF = 3.1415926535898  # constants_RF.f90: PI as the reference writes it
+
+
+def fft_method_field(xNStep, xStep, corrL, seedStart, corrMod=CM_GAUSSIAN):
+    """gen_Std_Gauss_FFT (randomFieldND.f90:520-763) restated with numpy and
+    scipy's DCT, single process, one realization; returns the standard
+    (pre-marginal) field on the grid, axis 1 fastest.
+
+    Coordinates and steps divided by corrL (gen_Std_Gauss :58-73); k grid of
+    set_kPoints' FFT branch (spectra_RF.f90:135-160): kNStep = grid points,
+    kDelta = 2 PI / (1.1 xRange), from 0, axis 1 fastest; S of set_SkVec
+    (:202-208 Gaussian, :210-220 cm_COS); draws :674-686 (gamma: K draws,
+    K - 1 skipped, phi: K draws); X = (gamma - 1/2) sqrt(S) cos(2 PI phi)
+    (:695-696); FFTW REDFT01 on every axis = scipy's DCT type 3, norm None
+    (:712-733); scale sqrt(prod xStep) in 2-D, 2 sqrt(prod xStep) in 3-D.
+    """
+    from scipy import fft as sfft
+
+    n = [int(v) for v in xNStep]
+    nd = len(n)
+    h = np.asarray(xStep, dtype=np.float64) / np.asarray(corrL, dtype=np.float64)[:nd]
+    xr = (np.asarray(n) - 1) * h
+    kd = 2.0 * PI_REF / (1.1 * xr)
+    K = int(np.prod(n))
+    r = rng(seedStart)
+    u = np.array([lib().rfo_rng_r8_uni_01(C.byref(r)) for _ in range(3 * K - 1)])
+    gamma, phi = u[:K], u[2 * K - 1:3 * K - 1]
+    idx = np.indices(tuple(reversed(n))).reshape(nd, -1)[::-1]  # idx[d] = i_d, axis 1 fastest
+    S = np.ones(K)
+    for d in range(nd):
+        k = 0.0 + kd[d] * idx[d]
+        S = S * 1.0 * np.exp(-((k * k) * 1.0) / (4.0 * PI_REF))
+    if corrMod == CM_COS:
+        S = np.zeros(K)
+        S[5] = 1.0
+    X = (gamma - 0.5) * np.sqrt(S) * np.cos(2.0 * PI_REF * phi)
+    Y = sfft.dctn(X.reshape(tuple(reversed(n))), type=3, norm=None)
+    scale = (2.0 if nd == 3 else 1.0) * np.sqrt(np.prod(h))
+    return Y.reshape(-1) * scale

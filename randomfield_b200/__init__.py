@@ -28,7 +28,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librf_b200.so")
 
 # constants_RF.f90:12-21
-ISOTROPIC, SHINOZUKA, RANDOMIZATION = 1, 2, 3
+ISOTROPIC, SHINOZUKA, RANDOMIZATION, FFT = 1, 2, 3, 4
 CM_GAUSSIAN, CM_COS = 1, 2
 FOM_GAUSSIAN, FOM_LOGNORMAL = 1, 2
 PREC_BF16, PREC_FP16, PREC_FP32, PREC_BF16_FAST, PREC_FP8 = 0, 1, 2, 3, 4
@@ -52,7 +52,7 @@ EXPORTS = [
     "rf_generate_batch", "rf_generate_batch_device", "rf_batch_last_stats",
     "rf_server_config_init", "rf_server_create", "rf_server_submit", "rf_server_wait", "rf_server_get_stats",
     "rf_server_destroy", "rf_server_submit_blended", "rf_context_selftest_timeout", "rf_measure_sfu_rate", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
-    "rf_field_statistics",
+    "rf_field_statistics", "rf_generate_fft_grid",
 ]
 
 
@@ -254,6 +254,8 @@ def lib() -> C.CDLL:
         L.rf_server_destroy.argtypes = [C.c_void_p]
         L.rf_context_selftest_timeout.argtypes = [C.c_void_p, d]
         L.rf_measure_sfu_rate.argtypes = [i32, P(d)]
+        L.rf_generate_fft_grid.argtypes = [C.c_void_p, i32, P(i64), P(d), i32, i32, P(d), d, d, i32, C.c_void_p,
+                                           P(Options)]
         L.rf_field_statistics.argtypes = [C.c_void_p, C.c_void_p, i64, i32, i32, P(i64), P(d), P(d), P(d), P(d),
                                           P(d), P(FieldStats)]
         L.rf_blend_layout.argtypes = [P(BlendGrid), P(d), P(C.c_int32), P(C.c_int32)]
@@ -552,6 +554,23 @@ class Context:
                                                 cl.ctypes.data_as(C.POINTER(C.c_double)), float(fieldAvg),
                                                 float(fieldVar), int(Nmc), int(method), C.c_void_p(self._ptr(d_out)),
                                                 C.byref(o), C.c_void_p(s)))
+
+    def generate_fft_grid(self, d_out, xNStep, xStep, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc,
+                          options=None, **kw) -> None:
+        """rf_generate_fft_grid: the FFT method (method 4) on a structured grid
+        of xNStep points spaced xStep per axis (2-D or 3-D, axis 1 fastest);
+        d_out holds prod(xNStep) x Nmc float64 column-major (e.g. a torch
+        tensor of shape (Nmc, prod(xNStep)))."""
+        nDim = len(xNStep)
+        g = np.ascontiguousarray(np.asarray(xNStep, dtype=np.int64).reshape(-1))
+        h = np.ascontiguousarray(np.asarray(xStep, dtype=np.float64).reshape(-1))
+        cl = np.ascontiguousarray(np.asarray(corrL, dtype=np.float64).reshape(-1))
+        o = _opts(options if options is not None else (kw or None))
+        P = C.POINTER(C.c_double)
+        _check(lib().rf_generate_fft_grid(self._h, int(nDim), g.ctypes.data_as(C.POINTER(C.c_int64)), h.ctypes.data_as(P),
+                                          _id(corrMod, _CORRMOD, "corrMod"), _id(margiFirst, _MARGI, "margiFirst"),
+                                          cl.ctypes.data_as(P), float(fieldAvg), float(fieldVar), int(Nmc),
+                                          C.c_void_p(self._ptr(d_out)), C.byref(o)))
 
     def field_statistics(self, d_field, n: int, Nmc: int, nDim: int = 3, grid=None, step=None) -> dict:
         """rf_field_statistics on a device field (n x Nmc column-major, e.g.

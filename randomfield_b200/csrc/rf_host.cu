@@ -310,6 +310,7 @@ void context_free(rf_context* c) {
   cudaFree(c->dKtab);
   cudaFree(c->dWork);
   cudaFree(c->dStats);
+  cudaFree(c->dFft);
   if (c->hStats) cudaFreeHost(c->hStats);
   cudaFree(c->dErr);
   cudaFree(c->dX);

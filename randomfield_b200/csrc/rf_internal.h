@@ -27,6 +27,8 @@ struct rf_context {
   double* dWork = nullptr;  // extent partials and moments
   size_t capWork = 0;
   double* hWork = nullptr;  // pinned mirror of dWork
+  double* dFft = nullptr;   // FFT method: amplitudes, pass buffer, cosine matrices (rf_fft.cu)
+  size_t capFft = 0;
   double* dStats = nullptr; // field statistics scratch (rf_stats.cu)
   size_t capStats = 0;
   double* hStats = nullptr;
@@ -99,6 +101,7 @@ int64_t round_up(int64_t v, int64_t m);
 int validate(const Request& r);
 int layout(rfb::Plan& P);
 int build_plan(const Request& rq, const double* ext, rfb::Plan& P);
+int seeds(int64_t seedStart, rfb::Plan& P);  // rnglib seed words of seed_start (< 0: from the clock)
 int32_t realization_block(const rfb::Plan& P);
 int device_extent(rf_context* c, const double* dX, int nDim, int64_t n, cudaStream_t st, double* ext);
 int run_plan(rf_context* c, const rfb::Plan& P0, const double* dX, double* dOut, cudaStream_t st);
