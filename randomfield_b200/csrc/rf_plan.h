@@ -37,6 +37,7 @@ constexpr int kKtabStageDoubles = 6 * kTableChunk;
 constexpr int kKtabStageBytes = 8 * kKtabStageDoubles;
 constexpr int kMaxGridN = 32;      // GEN_GRID3: max wavenumbers per axis
 constexpr int kMaxNmcPad = 256;    // realizations per launch (MMA N <= 256)
+constexpr int kLoMaskWords = 32;   // stages of a plan that can drop the lo rows: up to 1024
 
 struct Plan {
   // request
@@ -60,6 +61,11 @@ struct Plan {
   int32_t lPad;               // GEN_GRID3: inner (axis 3) length padded to a multiple of 8
   int32_t gps;                // GEN_GRID3: outer groups (i1, i2, s2) per stage
   int32_t forceTable;         // 1: GEN_TABLE even where GEN_GRID3 applies
+  // BF16 hi/lo, single GEN_GRID3 requests: with loSkip, B stage s carries
+  // the lo rows only where bit s of loMask is set (stage_has_lo); the other
+  // stages hold the hi rows alone (half the bytes, MMA N = nmcPad)
+  int32_t loSkip;
+  uint32_t loMask[kLoMaskWords];
   int64_t nChunks;            // stages per tile
   int64_t stageBytes;         // bytes of one B stage
   int32_t bScaleLog2;         // FP16: B stored times 2^bScaleLog2
@@ -79,6 +85,26 @@ struct Plan {
   int32_t bRamp[3];           // overlapNPoints per axis (< 1: no ramp)
   int64_t gTotal;             // group grid points
 };
+
+__host__ __device__ inline int popcount32(uint32_t x) {
+#ifdef __CUDA_ARCH__
+  return __popc(x);
+#else
+  return __builtin_popcount(x);
+#endif
+}
+// Whether B stage s of the plan carries the lo rows.
+__host__ __device__ inline bool stage_has_lo(const Plan& P, int64_t s) {
+  return !P.loSkip || ((P.loMask[s >> 5] >> (s & 31)) & 1u);
+}
+// Byte offset of B stage s: hi-only stages take half of stageBytes.
+__host__ __device__ inline int64_t stage_offset(const Plan& P, int64_t s) {
+  if (!P.loSkip) return s * P.stageBytes;
+  int64_t lo = 0;
+  for (int64_t w = 0; w < (s >> 5); ++w) lo += popcount32(P.loMask[w]);
+  if (s & 31) lo += popcount32(P.loMask[s >> 5] & ((1u << (s & 31)) - 1u));
+  return (s + lo) * (P.stageBytes / 2);
+}
 
 // Shared-memory and TMEM slot layout of one tcgen05 launch: B slot s at
 // byte slotBytes*s of the slot area, its wavevector chunk (GEN_TABLE) at

@@ -193,7 +193,7 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
     b[(int64_t)(2 * c + 1) * P.nmcPad + r] = (float)bs;
     return;
   }
-  unsigned char* b = reinterpret_cast<unsigned char*>(B) + stage * P.stageBytes;
+  unsigned char* b = reinterpret_cast<unsigned char*>(B) + stage_offset(P, stage);
   if (P.prec == PREC_FP8) {  // scaled e4m3, hi and lo rows
     const double sc = ldexp(1.0, P.bScaleLog2);
     const unsigned char hc = to_e4m3(bc * sc), hs = to_e4m3(bs * sc);
@@ -209,10 +209,13 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
     *reinterpret_cast<__half*>(b + tc_b_offset(P.bRows, r, 2 * c + 1)) = __double2half(bs * sc);
     return;
   }
+  // a stage without the lo rows is laid out for nmcPad rows
+  const bool lo = stage_has_lo(P, stage);
+  const int32_t rowsS = lo ? P.bRows : P.nmcPad;
   const __nv_bfloat16 hc = __double2bfloat16(bc), hs = __double2bfloat16(bs);
-  *reinterpret_cast<__nv_bfloat16*>(b + tc_b_offset(P.bRows, r, 2 * c)) = hc;
-  *reinterpret_cast<__nv_bfloat16*>(b + tc_b_offset(P.bRows, r, 2 * c + 1)) = hs;
-  if (P.prec == PREC_BF16) {  // hi/lo split of the amplitude side
+  *reinterpret_cast<__nv_bfloat16*>(b + tc_b_offset(rowsS, r, 2 * c)) = hc;
+  *reinterpret_cast<__nv_bfloat16*>(b + tc_b_offset(rowsS, r, 2 * c + 1)) = hs;
+  if (P.prec == PREC_BF16 && lo) {  // hi/lo split of the amplitude side
     const __nv_bfloat16 lc = __double2bfloat16(bc - (double)__bfloat162float(hc));
     const __nv_bfloat16 ls = __double2bfloat16(bs - (double)__bfloat162float(hs));
     *reinterpret_cast<__nv_bfloat16*>(b + tc_b_offset(P.bRows, P.nmcPad + r, 2 * c)) = lc;

@@ -244,13 +244,16 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
         const Plan& P = *v.P;
         const bool table = kHasTable && (GEN == GEN_TABLE || P.gen != GEN_GRID3);
         const int64_t nChunks = P.nChunks;
+        int64_t off = 0;  // byte offset of stage ch in B (hi-only stages are half size)
         for (int64_t ch = 0; ch < nChunks; ++ch) {
           if (!mbar_wait(&bars->empty[s], ph ^ 1, abort_flag)) {
             raise_abort(bars, err);
             break;
           }
-          mbar_arrive_expect_tx(&bars->full[s], (uint32_t)P.stageBytes);
-          bulk_g2s(sB + (size_t)s * L.slotBytes, v.B + ch * P.stageBytes, (uint32_t)P.stageBytes, &bars->full[s]);
+          const uint32_t bytes = (uint32_t)(stage_has_lo(P, ch) ? P.stageBytes : P.stageBytes / 2);
+          mbar_arrive_expect_tx(&bars->full[s], bytes);
+          bulk_g2s(sB + (size_t)s * L.slotBytes, v.B + off, bytes, &bars->full[s]);
+          off += bytes;
           if (table) {
             mbar_arrive_expect_tx(&bars->kfull[s], (uint32_t)kKtabStageBytes);
             bulk_g2s(sK + s * kKtabStageDoubles, v.ktab + ch * kKtabStageDoubles, kKtabStageBytes, &bars->kfull[s]);
@@ -302,10 +305,14 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
       const Plan& P = *v.P;
       const bool grid = kHasGrid && (GEN == GEN_GRID3 || P.gen == GEN_GRID3);
       // A/B type field: F16 (0) or BF16 (1) for kind::f16, E4M3 (0) for kind::f8f6f4
-      const uint32_t idesc = make_idesc((PREC == PREC_FP16 || kF8) ? 0u : 1u, 128u, (uint32_t)P.bRows);
+      const uint32_t idescAll = make_idesc((PREC == PREC_FP16 || kF8) ? 0u : 1u, 128u, (uint32_t)P.bRows);
       const uint32_t lbo = (uint32_t)P.bRows * 16u, sbo = 128u;
-      const uint64_t desc0 = make_sdesc(smem_u32(sB), lbo, sbo);
-      const uint64_t jStep = (uint64_t)((2u * lbo) >> 4);
+      const uint64_t descAll = make_sdesc(smem_u32(sB), lbo, sbo);
+      const uint64_t jStepAll = (uint64_t)((2u * lbo) >> 4);
+      // hi-only stages (loSkip): N = nmcPad rows laid out for nmcPad
+      const uint32_t idescHi = make_idesc((PREC == PREC_FP16 || kF8) ? 0u : 1u, 128u, (uint32_t)P.nmcPad);
+      const uint64_t descHi = make_sdesc(smem_u32(sB), (uint32_t)P.nmcPad * 16u, sbo);
+      const uint64_t jStepHi = (uint64_t)(((uint32_t)P.nmcPad * 32u) >> 4);
       const int64_t nChunks = P.nChunks;
       if (!mbar_wait_warp(&bars->acc_empty, accPh ^ 1, abort_flag)) { ok = false; break; }
       tc_fence_after();
@@ -313,7 +320,10 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
         if (!ready && !mbar_wait_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
         tc_fence_after();
         const uint32_t aBase = tbase + (uint32_t)L.aCol0 + s * (uint32_t)L.aStride;
-        const uint64_t d0 = desc0 + sStep * s;
+        const bool lo = stage_has_lo(P, ch);
+        const uint32_t idesc = lo ? idescAll : idescHi;
+        const uint64_t jStep = lo ? jStepAll : jStepHi;
+        const uint64_t d0 = (lo ? descAll : descHi) + sStep * s;
         const uint32_t sn = (s + 1 == (uint32_t)S) ? 0u : s + 1;
         const uint32_t phn = (s + 1 == (uint32_t)S) ? ph ^ 1 : ph;
         const bool more = (ch + 1 < nChunks) || (i + 1 < count);
