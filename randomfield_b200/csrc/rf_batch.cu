@@ -123,6 +123,7 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
       P.nmcBlk = std::min(rblk, P0.Nmc - r0);
       if (int rc = layout(P)) return rc;
       if (!B.blend.empty() && B.blend[i].gTotal > 0) apply_blend(P, B.blend[i]);
+      lo_layout(P);
       GroupSub g;
       memset(&g, 0, sizeof(g));
       g.P = P;

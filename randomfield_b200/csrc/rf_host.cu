@@ -367,9 +367,9 @@ int build_plan(const Request& rq, const double* ext, Plan& P) {
 // the hi term only: their BF16 rounding adds a relative error of about
 // 2^-9 sqrt(2 kLoDropShare / 3) = 5e-4 in quadrature to the trig tile's
 // 1.1e-3.  For the 128^3 workload (24^3 x 4 wavevectors) that drops the lo
-// rows of 347 of 576 stages: 30 % fewer MMAs and operand bytes.  Single
-// GEN_GRID3 requests of the Gaussian spectrum only (the grouped launch and
-// the other generators keep both terms everywhere).
+// rows of 347 of 576 stages: 30 % fewer MMAs and operand bytes.  GEN_GRID3
+// requests of the Gaussian spectrum, alone or in a grouped launch (not the
+// subdomains of a blend, nor the other generators, which keep both terms).
 constexpr double kLoDropShare = 0.10;
 
 void lo_layout(Plan& P) {

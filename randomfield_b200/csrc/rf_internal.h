@@ -101,7 +101,9 @@ int64_t round_up(int64_t v, int64_t m);
 int validate(const Request& r);
 int layout(rfb::Plan& P);
 int build_plan(const Request& rq, const double* ext, rfb::Plan& P);
-int seeds(int64_t seedStart, rfb::Plan& P);  // rnglib seed words of seed_start (< 0: from the clock)
+int seeds(int64_t seedStart, rfb::Plan& P);
+// BF16 GEN_GRID3 plans: the stages that keep only the hi term (rf_host.cu)
+void lo_layout(rfb::Plan& P);  // rnglib seed words of seed_start (< 0: from the clock)
 int32_t realization_block(const rfb::Plan& P);
 int device_extent(rf_context* c, const double* dX, int nDim, int64_t n, cudaStream_t st, double* ext);
 int run_plan(rf_context* c, const rfb::Plan& P0, const double* dX, double* dOut, cudaStream_t st);
