@@ -326,6 +326,9 @@ void context_free(rf_context* c) {
   cudaFree(c->dExt);
   if (c->hDesc) cudaFreeHost(c->hDesc);
   if (c->hExt) cudaFreeHost(c->hExt);
+  for (auto& e : c->slabEv)
+    if (e) cudaEventDestroy(e);
+  if (c->copyStream) cudaStreamDestroy(c->copyStream);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -477,6 +480,55 @@ int run_block(rf_context* c, const Plan& P, const double* dX, double* dOut, cuda
     }
     c->launches += 2;
   }
+  return RF_OK;
+}
+
+// The flat entry point's tail for large fields into page-locked host memory:
+// the contraction runs in point slabs on the context's stream and each
+// slab's n_slab x Nmc block goes to the host on a second stream while the
+// next slab computes (one 2-D copy per slab: Nmc rows of the slab's points).
+// Only the last slab's copy is left after the kernels.  Tensor-core forms,
+// one realization block, no literal slabs, no normalisation pass (which needs
+// the whole field first); returns RF_ENOTSUP otherwise so that the caller
+// takes the plain path.
+int run_plan_slabs(rf_context* c, const Plan& P0, const double* dX, double* dOut, double* hOut, cudaStream_t st) {
+  if (P0.prec == PREC_FP32 || P0.literal || P0.normalize || P0.Nmc > realization_block(P0)) return RF_ENOTSUP;
+  const int64_t tiles = (P0.n + kTileM - 1) / kTileM;
+  int nSlabs = (int)std::min<int64_t>(8, tiles / (8 * (int64_t)c->numSMs));
+  if (nSlabs < 2) return RF_ENOTSUP;
+  Plan P = P0;
+  P.rOff = 0;
+  P.nmcBlk = P0.Nmc;
+  if (int rc = layout(P)) return rc;
+  lo_layout(P);
+  if (tc_smem_bytes(P, nullptr) == 0)
+    return fail(RF_ENOTSUP, "stage too large for shared memory (Nmc or wavenumbers per axis too large)");
+  if (!c->copyStream) RF_CUDA(cudaStreamCreateWithFlags(&c->copyStream, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (auto& e : c->slabEv)
+    if (!e) RF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  if (int rc = ensure(c->dB, c->capB, (size_t)P.nChunks * P.stageBytes, "contraction operand")) return rc;
+  double* ktab = nullptr;
+  if (P.gen == GEN_TABLE) {
+    if (int rc = ensure(c->dKtab, c->capK, (size_t)P.nChunks * kKtabStageBytes, "wavevector table")) return rc;
+    ktab = c->dKtab;
+  }
+  RF_CUDA(launch_tables(P, jump_table(), c->dB, ktab, -1, 1, st), "table kernel");
+  const int64_t slabRows = round_up((P.n + nSlabs - 1) / nSlabs, kTileM);
+  const size_t pitch = sizeof(double) * (size_t)P.n;
+  int k = 0;
+  for (int64_t row0 = 0; row0 < P.n; row0 += slabRows, ++k) {
+    const int64_t rows = std::min(slabRows, P.n - row0);
+    RF_CUDA(launch_tc(P, dX, c->dB, ktab, dOut, row0, rows, c->dErr, c->numSMs, st), "tcgen05 contraction kernel");
+    RF_CUDA(cudaEventRecord(c->slabEv[k], st), "cudaEventRecord");
+    RF_CUDA(cudaStreamWaitEvent(c->copyStream, c->slabEv[k], 0), "cudaStreamWaitEvent");
+    RF_CUDA(cudaMemcpy2DAsync(hOut + row0, pitch, dOut + row0, pitch, sizeof(double) * (size_t)rows, (size_t)P.Nmc,
+                              cudaMemcpyDeviceToHost, c->copyStream),
+            "copy of a field slab");
+    c->launches += 1;
+  }
+  c->launches += 1;
+  RF_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  RF_CUDA(cudaStreamSynchronize(c->copyStream), "cudaStreamSynchronize");
   return RF_OK;
 }
 
@@ -715,6 +767,16 @@ int rf_create_standard_gaussian_field_unstruct(const double* xPoints, int nDim, 
     if (int rc = device_extent(c, c->dX, nDim, n, st, ext)) return rc;
   Plan P;
   if (int rc = build_plan(rq, ext, P)) return rc;
+  // page-locked destination: copy slabs out while the next ones compute
+  cudaPointerAttributes pa;
+  const bool pinned = cudaPointerGetAttributes(&pa, randField) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  if (!pinned) cudaGetLastError();
+  if (pinned && !c->timing) {
+    const int rc = run_plan_slabs(c, P, c->dX, c->dOut, randField, st);
+    if (rc == RF_OK) return check_device_error(c);
+    if (rc != RF_ENOTSUP) return rc;
+    g_err.clear();
+  }
   if (int rc = run_plan(c, P, c->dX, c->dOut, st)) return rc;
   RF_CUDA(cudaMemcpyAsync(randField, c->dOut, oBytes, cudaMemcpyDeviceToHost, st), "copy of randField");
   RF_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");

@@ -19,6 +19,8 @@ struct rf_context {
   int device = 0;
   int numSMs = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copyStream = nullptr;  // flat API: slab copies to the host beside the contraction
+  cudaEvent_t slabEv[8] = {};
   std::mutex mu;
   void* dB = nullptr;
   size_t capB = 0;
