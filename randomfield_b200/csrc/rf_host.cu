@@ -97,6 +97,14 @@ int validate(const Request& r) {
 }
 
 // Geometry of spectra_RF.f90:50-133 (Shinozuka grid, isotropic radial rule),
+// Whether axis d's extent enters the geometry: the Shinozuka/randomization
+// step along d when its wavenumber count is not given, the isotropic radial
+// step (from the diagonal) when the radial count is not given.
+bool extent_needed(const Request& r, int d) {
+  if (r.method == RF_ISOTROPIC) return !(r.opt.iso_n_radial > 0);
+  return !(r.opt.k_nstep[d] > 0);
+}
+
 // ampMult of randomFieldND.f90:260-266.  ext[d] is the physical extent.
 int geometry(const Request& r, const double* ext, Plan& P) {
   const rf_options& o = r.opt;
@@ -116,6 +124,7 @@ int geometry(const Request& r, const double* ext, Plan& P) {
   P.kMax = kmax_nd(r.nDim);
   double xr[3] = {0, 0, 0};
   for (int d = 0; d < r.nDim; ++d) {
+    if (!extent_needed(r, d)) continue;  // an explicit wavenumber count leaves xRange unused
     const double e = o.x_range[d] > 0.0 ? o.x_range[d] : ext[d];
     if (!(e > 0.0) || !std::isfinite(e))
       return fail(RF_EINVAL_RANGE, "zero extent along axis %d: kDelta = 2 pi/(1.1 xRange) is infinite", d + 1);
@@ -731,8 +740,8 @@ int rf_generate_device(rf_context* ctx, const double* d_xPoints, int nDim, int64
   ctx->launches = 0;
   ctx->evValid = false;
   double ext[3] = {0, 0, 0};
-  bool need = false;
-  for (int d = 0; d < nDim; ++d) need = need || !(rq.opt.x_range[d] > 0.0);
+  bool need = false;  // the extent pass (and its host read-back) only where the geometry uses it
+  for (int d = 0; d < nDim; ++d) need = need || (!(rq.opt.x_range[d] > 0.0) && extent_needed(rq, d));
   if (need)
     if (int rc = device_extent(ctx, d_xPoints, nDim, n, st, ext)) return rc;
   Plan P;
@@ -761,8 +770,8 @@ int rf_create_standard_gaussian_field_unstruct(const double* xPoints, int nDim, 
   cudaStream_t st = c->stream;
   RF_CUDA(cudaMemcpyAsync(c->dX, xPoints, xBytes, cudaMemcpyHostToDevice, st), "copy of xPoints");
   double ext[3] = {0, 0, 0};
-  bool need = false;
-  for (int d = 0; d < nDim; ++d) need = need || !(rq.opt.x_range[d] > 0.0);
+  bool need = false;  // the extent pass (and its host read-back) only where the geometry uses it
+  for (int d = 0; d < nDim; ++d) need = need || (!(rq.opt.x_range[d] > 0.0) && extent_needed(rq, d));
   if (need)
     if (int rc = device_extent(c, c->dX, nDim, n, st, ext)) return rc;
   Plan P;
