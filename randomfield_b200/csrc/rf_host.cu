@@ -337,7 +337,10 @@ void context_free(rf_context* c) {
   if (c->hExt) cudaFreeHost(c->hExt);
   for (auto& e : c->slabEv)
     if (e) cudaEventDestroy(e);
+  for (auto& e : c->h2dEv)
+    if (e) cudaEventDestroy(e);
   if (c->copyStream) cudaStreamDestroy(c->copyStream);
+  if (c->h2dStream) cudaStreamDestroy(c->h2dStream);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -496,14 +499,17 @@ int run_block(rf_context* c, const Plan& P, const double* dX, double* dOut, cuda
 // the contraction runs in point slabs on the context's stream and each
 // slab's n_slab x Nmc block goes to the host on a second stream while the
 // next slab computes (one 2-D copy per slab: Nmc rows of the slab's points).
-// Only the last slab's copy is left after the kernels.  Tensor-core forms,
+// Only the last slab's copy is left after the kernels.  With hX (the points
+// still on the host) the slabs' points go up on a third stream, each ahead
+// of its slab's kernel, behind the first slab's copy only.  Tensor-core forms,
 // one realization block, no literal slabs, no normalisation pass (which needs
 // the whole field first); returns RF_ENOTSUP otherwise so that the caller
 // takes the plain path.
-int run_plan_slabs(rf_context* c, const Plan& P0, const double* dX, double* dOut, double* hOut, cudaStream_t st) {
+int run_plan_slabs(rf_context* c, const Plan& P0, double* dX, double* dOut, double* hOut, cudaStream_t st,
+                   const double* hX) {
   if (P0.prec == PREC_FP32 || P0.literal || P0.normalize || P0.Nmc > realization_block(P0)) return RF_ENOTSUP;
   const int64_t tiles = (P0.n + kTileM - 1) / kTileM;
-  int nSlabs = (int)std::min<int64_t>(8, tiles / (8 * (int64_t)c->numSMs));
+  int nSlabs = (int)std::min<int64_t>(16, tiles / (8 * (int64_t)c->numSMs));
   if (nSlabs < 2) return RF_ENOTSUP;
   Plan P = P0;
   P.rOff = 0;
@@ -513,7 +519,10 @@ int run_plan_slabs(rf_context* c, const Plan& P0, const double* dX, double* dOut
   if (tc_smem_bytes(P, nullptr) == 0)
     return fail(RF_ENOTSUP, "stage too large for shared memory (Nmc or wavenumbers per axis too large)");
   if (!c->copyStream) RF_CUDA(cudaStreamCreateWithFlags(&c->copyStream, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (!c->h2dStream) RF_CUDA(cudaStreamCreateWithFlags(&c->h2dStream, cudaStreamNonBlocking), "cudaStreamCreate");
   for (auto& e : c->slabEv)
+    if (!e) RF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+  for (auto& e : c->h2dEv)
     if (!e) RF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
   if (int rc = ensure(c->dB, c->capB, (size_t)P.nChunks * P.stageBytes, "contraction operand")) return rc;
   double* ktab = nullptr;
@@ -524,9 +533,21 @@ int run_plan_slabs(rf_context* c, const Plan& P0, const double* dX, double* dOut
   RF_CUDA(launch_tables(P, jump_table(), c->dB, ktab, -1, 1, st), "table kernel");
   const int64_t slabRows = round_up((P.n + nSlabs - 1) / nSlabs, kTileM);
   const size_t pitch = sizeof(double) * (size_t)P.n;
+  if (hX) {
+    int j = 0;
+    for (int64_t row0 = 0; row0 < P.n; row0 += slabRows, ++j) {
+      const int64_t rows = std::min(slabRows, P.n - row0);
+      const size_t pb = sizeof(double) * (size_t)P.nDim;
+      RF_CUDA(cudaMemcpyAsync(dX + row0 * P.nDim, hX + row0 * P.nDim, pb * (size_t)rows, cudaMemcpyHostToDevice,
+                              c->h2dStream),
+              "copy of a point slab");
+      RF_CUDA(cudaEventRecord(c->h2dEv[j], c->h2dStream), "cudaEventRecord");
+    }
+  }
   int k = 0;
   for (int64_t row0 = 0; row0 < P.n; row0 += slabRows, ++k) {
     const int64_t rows = std::min(slabRows, P.n - row0);
+    if (hX) RF_CUDA(cudaStreamWaitEvent(st, c->h2dEv[k], 0), "cudaStreamWaitEvent");
     RF_CUDA(launch_tc(P, dX, c->dB, ktab, dOut, row0, rows, c->dErr, c->numSMs, st), "tcgen05 contraction kernel");
     RF_CUDA(cudaEventRecord(c->slabEv[k], st), "cudaEventRecord");
     RF_CUDA(cudaStreamWaitEvent(c->copyStream, c->slabEv[k], 0), "cudaStreamWaitEvent");
@@ -538,6 +559,7 @@ int run_plan_slabs(rf_context* c, const Plan& P0, const double* dX, double* dOut
   c->launches += 1;
   RF_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   RF_CUDA(cudaStreamSynchronize(c->copyStream), "cudaStreamSynchronize");
+  if (hX) RF_CUDA(cudaStreamSynchronize(c->h2dStream), "cudaStreamSynchronize");
   return RF_OK;
 }
 
@@ -768,24 +790,29 @@ int rf_create_standard_gaussian_field_unstruct(const double* xPoints, int nDim, 
   if (int rc = ensure(c->dX, c->capX, xBytes, "points")) return rc;
   if (int rc = ensure(c->dOut, c->capOut, oBytes, "field")) return rc;
   cudaStream_t st = c->stream;
-  RF_CUDA(cudaMemcpyAsync(c->dX, xPoints, xBytes, cudaMemcpyHostToDevice, st), "copy of xPoints");
   double ext[3] = {0, 0, 0};
   bool need = false;  // the extent pass (and its host read-back) only where the geometry uses it
   for (int d = 0; d < nDim; ++d) need = need || (!(rq.opt.x_range[d] > 0.0) && extent_needed(rq, d));
-  if (need)
+  bool onDevice = false;  // points copied up
+  if (need) {
+    RF_CUDA(cudaMemcpyAsync(c->dX, xPoints, xBytes, cudaMemcpyHostToDevice, st), "copy of xPoints");
+    onDevice = true;
     if (int rc = device_extent(c, c->dX, nDim, n, st, ext)) return rc;
+  }
   Plan P;
   if (int rc = build_plan(rq, ext, P)) return rc;
-  // page-locked destination: copy slabs out while the next ones compute
+  // page-locked destination: copy slabs out while the next ones compute (and,
+  // when the points are still on the host, copy them up slab by slab)
   cudaPointerAttributes pa;
   const bool pinned = cudaPointerGetAttributes(&pa, randField) == cudaSuccess && pa.type == cudaMemoryTypeHost;
   if (!pinned) cudaGetLastError();
   if (pinned && !c->timing) {
-    const int rc = run_plan_slabs(c, P, c->dX, c->dOut, randField, st);
+    const int rc = run_plan_slabs(c, P, c->dX, c->dOut, randField, st, onDevice ? nullptr : xPoints);
     if (rc == RF_OK) return check_device_error(c);
     if (rc != RF_ENOTSUP) return rc;
     g_err.clear();
   }
+  if (!onDevice) RF_CUDA(cudaMemcpyAsync(c->dX, xPoints, xBytes, cudaMemcpyHostToDevice, st), "copy of xPoints");
   if (int rc = run_plan(c, P, c->dX, c->dOut, st)) return rc;
   RF_CUDA(cudaMemcpyAsync(randField, c->dOut, oBytes, cudaMemcpyDeviceToHost, st), "copy of randField");
   RF_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");

@@ -20,7 +20,9 @@ struct rf_context {
   int numSMs = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t copyStream = nullptr;  // flat API: slab copies to the host beside the contraction
-  cudaEvent_t slabEv[8] = {};
+  cudaStream_t h2dStream = nullptr;   // flat API: slab copies of the points ahead of the contraction
+  cudaEvent_t slabEv[16] = {};
+  cudaEvent_t h2dEv[16] = {};
   std::mutex mu;
   void* dB = nullptr;
   size_t capB = 0;
