@@ -195,6 +195,25 @@ int rf_generate_fft_grid(rf_context* ctx, int nDim, const int64_t* xNStep, const
                          int margiFirst, const double* corrL, double fieldAvg, double fieldVar, int Nmc,
                          double* d_randField, const rf_options* opt);
 
+/*
+ * The Shinozuka field (method 2) on a structured grid: the points
+ * x_d = xMin[d] + j xStep[d], j < xNStep[d], axis 1 fastest (setGrid,
+ * math_RF.f90:16-92, as set_XPoints builds them, mesh_RF.f90:17-64), the
+ * same field that rf_generate_device computes when given those points in
+ * that order (same wavevectors, phases, extent rule and marginal map; the
+ * extent is max - min of the coordinates).  Because both the wavevectors
+ * and the points are tensor grids, the sum is evaluated axis by axis in
+ * FP64 (n1 n2 n3 N3 + n1 n2 N2 N3 + n1 N1 N2 N3 work per realization
+ * instead of 4 n1 n2 n3 N1 N2 N3), so the result matches the reference's
+ * FP64 sum to rounding whatever opt->precision says.  Limits: method 2, at
+ * most 32 wavenumbers per axis, no literal mode (RF_ENOTSUP otherwise:
+ * rf_generate_device covers those).  d_randField (device) is
+ * prod(xNStep) x Nmc column-major; queued on `stream` (0 = the context's).
+ */
+int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double* xStep, const int64_t* xNStep,
+                     int corrMod, int margiFirst, const double* corrL, double fieldAvg, double fieldVar, int Nmc,
+                     int method, double* d_randField, const rf_options* opt, void* stream);
+
 /* Phase timers.  With timing enabled the context records CUDA events on the
  * launching stream around each phase of a generation; rf_context_last_times
  * waits for the last one and returns the device milliseconds of the table

@@ -52,7 +52,7 @@ EXPORTS = [
     "rf_generate_batch", "rf_generate_batch_device", "rf_batch_last_stats",
     "rf_server_config_init", "rf_server_create", "rf_server_submit", "rf_server_wait", "rf_server_get_stats",
     "rf_server_destroy", "rf_server_submit_blended", "rf_context_selftest_timeout", "rf_measure_sfu_rate", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
-    "rf_field_statistics", "rf_generate_fft_grid",
+    "rf_field_statistics", "rf_generate_fft_grid", "rf_generate_grid",
 ]
 
 
@@ -256,6 +256,8 @@ def lib() -> C.CDLL:
         L.rf_measure_sfu_rate.argtypes = [i32, P(d)]
         L.rf_generate_fft_grid.argtypes = [C.c_void_p, i32, P(i64), P(d), i32, i32, P(d), d, d, i32, C.c_void_p,
                                            P(Options)]
+        L.rf_generate_grid.argtypes = [C.c_void_p, i32, P(d), P(d), P(i64), i32, i32, P(d), d, d, i32, i32,
+                                       C.c_void_p, P(Options), C.c_void_p]
         L.rf_field_statistics.argtypes = [C.c_void_p, C.c_void_p, i64, i32, i32, P(i64), P(d), P(d), P(d), P(d),
                                           P(d), P(FieldStats)]
         L.rf_blend_layout.argtypes = [P(BlendGrid), P(d), P(C.c_int32), P(C.c_int32)]
@@ -571,6 +573,28 @@ class Context:
                                           _id(corrMod, _CORRMOD, "corrMod"), _id(margiFirst, _MARGI, "margiFirst"),
                                           cl.ctypes.data_as(P), float(fieldAvg), float(fieldVar), int(Nmc),
                                           C.c_void_p(self._ptr(d_out)), C.byref(o)))
+
+    def generate_grid(self, d_out, xMin, xStep, xNStep, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc,
+                      method=SHINOZUKA, options=None, stream=0, **kw) -> None:
+        """rf_generate_grid: the Shinozuka field on the structured grid
+        xMin + j * xStep (xNStep points per axis, axis 1 fastest), evaluated
+        axis by axis in FP64; d_out holds prod(xNStep) x Nmc float64
+        column-major (e.g. a torch tensor of shape (Nmc, prod(xNStep)))."""
+        nDim = len(xNStep)
+        a = np.ascontiguousarray(np.asarray(xMin, dtype=np.float64).reshape(-1))
+        h = np.ascontiguousarray(np.asarray(xStep, dtype=np.float64).reshape(-1))
+        g = np.ascontiguousarray(np.asarray(xNStep, dtype=np.int64).reshape(-1))
+        cl = np.ascontiguousarray(np.asarray(corrL, dtype=np.float64).reshape(-1))
+        if not (len(a) == len(h) == len(cl) == nDim):
+            raise ValueError("xMin, xStep, xNStep and corrL need one entry per axis")
+        o = _opts(options if options is not None else (kw or None))
+        s = stream if isinstance(stream, int) else int(getattr(stream, "cuda_stream", 0))
+        P = C.POINTER(C.c_double)
+        _check(lib().rf_generate_grid(self._h, int(nDim), a.ctypes.data_as(P), h.ctypes.data_as(P),
+                                      g.ctypes.data_as(C.POINTER(C.c_int64)), _id(corrMod, _CORRMOD, "corrMod"),
+                                      _id(margiFirst, _MARGI, "margiFirst"), cl.ctypes.data_as(P), float(fieldAvg),
+                                      float(fieldVar), int(Nmc), int(method), C.c_void_p(self._ptr(d_out)),
+                                      C.byref(o), C.c_void_p(s)))
 
     def field_statistics(self, d_field, n: int, Nmc: int, nDim: int = 3, grid=None, step=None) -> dict:
         """rf_field_statistics on a device field (n x Nmc column-major, e.g.

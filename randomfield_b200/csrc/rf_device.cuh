@@ -246,11 +246,12 @@ __device__ __forceinline__ int64_t mulmod(int64_t a, int64_t b, int64_t m) {
   return (int64_t)(((unsigned long long)a * (unsigned long long)b) % (unsigned long long)m);
 }
 
-// i4_uni value of the p-th call (p >= 1) of generator 1 seeded (s1, s2):
-// cg = a^p * s mod m for each component (rnglib.f90:600-619), then
-// z = cg1 - cg2 folded to 1..m1-1 (:627-631).
-__device__ __forceinline__ int32_t i4_uni_at(const JumpTable& jt, int64_t s1, int64_t s2, uint64_t p) {
-  int64_t c1 = s1, c2 = s2;
+// State (cg1, cg2) of generator 1 seeded (s1, s2) after p calls:
+// cg = a^p * s mod m for each component (rnglib.f90:600-619).
+__device__ __forceinline__ void uni_state_at(const JumpTable& jt, int64_t s1, int64_t s2, uint64_t p, int64_t& c1,
+                                             int64_t& c2) {
+  c1 = s1;
+  c2 = s2;
   int j = 0;
   while (p) {
     if (p & 1ull) {
@@ -260,9 +261,24 @@ __device__ __forceinline__ int32_t i4_uni_at(const JumpTable& jt, int64_t s1, in
     p >>= 1;
     ++j;
   }
+}
+// One call further: cg = a * cg mod m (a = jt.p*[0]).
+__device__ __forceinline__ void uni_state_next(const JumpTable& jt, int64_t& c1, int64_t& c2) {
+  c1 = mulmod(jt.p1[0], c1, kM1);
+  c2 = mulmod(jt.p2[0], c2, kM2);
+}
+// i4_uni's value of a state: z = cg1 - cg2 folded to 1..m1-1 (:627-631).
+__device__ __forceinline__ int32_t uni_value(int64_t c1, int64_t c2) {
   int64_t z = c1 - c2;
   if (z < 1) z += kM1 - 1;
   return (int32_t)z;
+}
+
+// i4_uni value of the p-th call (p >= 1) of generator 1 seeded (s1, s2).
+__device__ __forceinline__ int32_t i4_uni_at(const JumpTable& jt, int64_t s1, int64_t s2, uint64_t p) {
+  int64_t c1, c2;
+  uni_state_at(jt, s1, s2, p, c1, c2);
+  return uni_value(c1, c2);
 }
 __device__ __forceinline__ double r8_uni_at(const JumpTable& jt, int64_t s1, int64_t s2, uint64_t p) {
   return (double)i4_uni_at(jt, s1, s2, p) * kR8Scale;

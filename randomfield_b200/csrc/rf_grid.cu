@@ -1,0 +1,471 @@
+// rf_grid.cu -- the Shinozuka sum on a structured grid, by separable stages.
+//
+// The reference evaluates f(x, r) = ampMult * sum_k a_k cos(k.x + phi_{k,r})
+// point by point (gen_Std_Gauss_Shinozuka, randomFieldND.f90:184-337) with
+// k on the tensor grid k = (i1 d1, s2 i2 d2, s3 i3 d3) of set_kPoints
+// (spectra_RF.f90:87-133; s2, s3 the sign rows of set_kSign, :267-286).
+// When the points themselves form a tensor grid x = (x1(j1), x2(j2), x3(j3))
+// (setGrid, math_RF.f90:16-92, as set_XPoints builds them, mesh_RF.f90:17-64)
+// the phasor factorises, exp(i k.x) = E1(i1, j1) E2(s2 i2, j2) E3(s3 i3, j3)
+// with E_d(i, j) = exp(i k_d(i) x_d(j)), and the sum runs axis by axis:
+//   C(k)            = a_k exp(i phi_{k,r})                      (coefficients)
+//   G(i1,i2,s2; j3) = sum_{i3,s3} C E3^{+-}  = sum_i3 P c3 + i Q s3   (axis 3)
+//   H(i1; j2, j3)   = sum_{i2,s2} G E2^{+-}  = sum_i2 u c2 + i v s2   (axis 2)
+//   f(j1, j2, j3)   = ampMult Re sum_i1 H E1 = sum_i1 Hr c1 - Hi s1   (axis 1)
+// where the two signs of an axis share one cosine and one sine:
+// P = C(s3=+) + C(s3=-), Q = C(s3=+) - C(s3=-), u = G(s2=+) + G(s2=-),
+// v = G(s2=+) - G(s2=-).  Per realization that is
+//   4 n1 n2 n3 N3 + 4 n1 n2 N2 N3 + 2 n1 N1 N2 N3
+// FP64 multiply-adds instead of the reference's N1 N2 N3 x 4 n1 n2 n3 cosines
+// (128^3 points, 24^3 x 4 wavevectors: 1.5e8 instead of 1.2e11), so the
+// whole computation stays in FP64: the field equals the reference's sum to
+// FP64 rounding, with no reduced-precision operand anywhere.
+//
+// Every stage is a small dense product whose tiles run through one register-
+// blocked FP64 routine (tile_fma): a 256-thread CTA computes a 64-row x 32J-
+// column tile, warp w rows 8w..8w+7, lane l columns l + 32j, operands in
+// shared memory (the row operand transposed, read as warp-wide broadcasts).
+//   rf_sep_phasors  E_d(i, j) for the three axes (FP64 sincos);
+//   rf_sep_coeffs   P, Q for every (r, s2, i2, i1, i3) from the rnglib stream;
+//   rf_sep_axis3    tiles (r, 64 rows j3, 32 pairs (i1,i2)) -> u, v;
+//   rf_sep_axes21   persistent: item (r, j3, 64 rows j2, 128 columns j1):
+//                   H into shared memory, then f, the marginal map and the
+//                   store of 64 x 128 field values.
+// Axes the request does not have are carried as length-1 axes with k = 0 and
+// one sign row, so 1-D and 2-D grids take the same kernels.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "rf_internal.h"
+
+using namespace rfb;
+using namespace rfh;
+
+namespace {
+
+constexpr int kSepThreads = 256;
+constexpr int kRows = 64;     // rows of a tile
+constexpr int kLdT = 66;      // row stride of a transposed operand (doubles): 16-byte aligned, conflict-free writes
+constexpr int kMaxSepN = 32;  // wavenumbers per axis
+constexpr size_t kSepScratch = (size_t)512 << 20;  // P/Q and u/v of one realization block
+
+struct SepSpec {
+  int32_t nDim;
+  int32_t N[3];   // grid points per axis (1 where the request has no axis)
+  int32_t kn[3];  // wavenumbers per axis (1 where absent)
+  int32_t S2, S3; // sign rows of axes 2 and 3
+  int32_t corrMod;
+  int32_t ig1, ig2;
+  int32_t r0, nr;  // realizations [r0, r0 + nr) of this block
+  int32_t applyMarginal, lognormal;
+  int64_t K, n;
+  double kDelta[3];
+  double xMin[3], xStep[3], corrL[3];
+  double ampMult, margSd, margAvg;
+};
+
+// acc[i][j] += sum_{k < K} AT[k][8 warp + i] * B[k][32 j + lane]
+// (AT row stride kLdT, B row stride ldb, both in shared memory; K even).
+template <int J>
+__device__ __forceinline__ void tile_fma(const double* __restrict__ AT, const double* __restrict__ B, int ldb,
+                                         int K, int warp, int lane, double (&acc)[8][J]) {
+  const double* a = AT + 8 * warp;
+  const double* b = B + lane;
+#pragma unroll 2
+  for (int k = 0; k < K; ++k) {
+    double av[8], bv[J];
+#pragma unroll
+    for (int i = 0; i < 8; i += 2) {
+      const double2 t = *reinterpret_cast<const double2*>(a + (int64_t)k * kLdT + i);
+      av[i] = t.x;
+      av[i + 1] = t.y;
+    }
+#pragma unroll
+    for (int j = 0; j < J; ++j) bv[j] = b[(int64_t)k * ldb + 32 * j];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < J; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+  }
+}
+
+// E_d(i, j) = (cos, sin)(k_d(i) x_d(j)), k_d(i) = 0 + kDelta_d i (setGrid from
+// 0, spectra_RF.f90:118), x_d(j) = (xMin_d + xStep_d j) / corrL_d
+// (randomFieldND.f90:58-73).  Table d holds kn_d x N_d entries, i major.
+__global__ void rf_sep_phasors(const SepSpec sp, double2* __restrict__ E) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t off = 0;
+  for (int d = 0; d < 3; ++d) {
+    const int64_t sz = (int64_t)sp.kn[d] * sp.N[d];
+    if (t < off + sz) {
+      const int64_t e = t - off;
+      const int32_t i = (int32_t)(e / sp.N[d]), j = (int32_t)(e % sp.N[d]);
+      double c = 1.0, s = 0.0;
+      if (d < sp.nDim) {
+        const double k = 0.0 + sp.kDelta[d] * (double)i;
+        const double x = (sp.xMin[d] + sp.xStep[d] * (double)j) / sp.corrL[d];
+        sincos(k * x, &s, &c);
+      }
+      E[t] = make_double2(c, s);
+      return;
+    }
+    off += sz;
+  }
+}
+
+// (Pr, Pi, Qr, Qi) of (rl, s2, i2, i1, i3), stored i3 fastest: C = a_k
+// exp(i phi) with phi_{k,r} = 2 pi U(r K + k + 1) (K draws per realization in
+// the reference's k order, randomFieldND.f90:278-279), the reference index
+// k = q kn + i1 + n1 (i2 + n2 i3) of sign row q = s2 S3 + s3, a_k from S(k)
+// (spectra_RF.f90:202-220).  One thread per (rl, s2, i2, i3) walks i1: the
+// draws of a run of i1 are consecutive calls of the generator, so each of the
+// two sign rows jumps ahead once and then steps.  Sign rows an axis does not
+// have are zero.
+__global__ void rf_sep_coeffs(const SepSpec sp, const JumpTable jt, double4* __restrict__ PQ) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t n1 = sp.kn[0], n2 = sp.kn[1], n3 = sp.kn[2];
+  const int64_t total = (int64_t)sp.nr * 2 * n2 * n3;
+  if (t >= total) return;
+  const int32_t i3 = (int32_t)(t % n3);
+  const int32_t i2 = (int32_t)((t / n3) % n2);
+  const int32_t s2 = (int32_t)((t / ((int64_t)n3 * n2)) % 2);
+  const int64_t rl = t / ((int64_t)n3 * n2 * 2);
+  const int64_t rg = sp.r0 + rl;
+  const int64_t kn = (int64_t)n1 * n2 * n3;
+  double4* o = PQ + ((rl * 2 + s2) * n2 + i2) * (int64_t)n1 * n3 + i3;
+  if (s2 >= sp.S2) {
+    for (int32_t i1 = 0; i1 < n1; ++i1) o[(int64_t)i1 * n3] = make_double4(0.0, 0.0, 0.0, 0.0);
+    return;
+  }
+  int64_t c1[2] = {0, 0}, c2[2] = {0, 0};
+  for (int s3 = 0; s3 < sp.S3; ++s3) {
+    const int64_t k0 = (int64_t)(s2 * sp.S3 + s3) * kn + (int64_t)n1 * (i2 + (int64_t)n2 * i3);
+    uni_state_at(jt, sp.ig1, sp.ig2, (uint64_t)(rg * sp.K + k0 + 1), c1[s3], c2[s3]);
+  }
+  for (int32_t i1 = 0; i1 < n1; ++i1) {
+    double cr[2] = {0.0, 0.0}, ci[2] = {0.0, 0.0};
+    for (int s3 = 0; s3 < sp.S3; ++s3) {
+      if (i1) uni_state_next(jt, c1[s3], c2[s3]);
+      const int64_t kref = (int64_t)(s2 * sp.S3 + s3) * kn + i1 + (int64_t)n1 * (i2 + (int64_t)n2 * i3);
+      double amp;
+      if (sp.corrMod == RF_CM_GAUSSIAN) {
+        const int32_t idx[3] = {i1, i2, i3};
+        double S = 1.0;
+        for (int d = 0; d < sp.nDim; ++d) {
+          const double base = 0.0 + sp.kDelta[d] * (double)idx[d];
+          const bool neg = (d == 1 && s2) || (d == 2 && s3);
+          const double k = neg ? base * -1.0 : base * 1.0;
+          S = S * 1.0 * exp(-((k * k) * 1.0) / (4.0 * kRefPi));  // spectra_RF.f90:202-208, corrL = 1
+        }
+        amp = sqrt(S);
+      } else {
+        amp = (kref == 5) ? 1.0 : 0.0;  // cm_COS, spectra_RF.f90:210-220
+      }
+      const double phi = 2.0 * kRefPi * ((double)uni_value(c1[s3], c2[s3]) * kR8Scale);
+      double sn, cs;
+      sincos(phi, &sn, &cs);
+      cr[s3] = amp * cs;
+      ci[s3] = amp * sn;
+    }
+    o[(int64_t)i1 * n3] = make_double4(cr[0] + cr[1], ci[0] + ci[1], cr[0] - cr[1], ci[0] - ci[1]);
+  }
+}
+
+// Axis 3.  Tile (rl, row block of 64 j3, block of 32 pairs m = i2 n1 + i1):
+// columns 32 (2 s2 + reim) + lane of the product are G_{s2}(m) real/imag,
+// from the k-rows 2 i3 (cos) and 2 i3 + 1 (sin):
+//   Gr = sum Pr c3 - Qi s3,  Gi = sum Pi c3 + Qr s3.
+// The epilogue folds the two signs of axis 2 into u = G+ + G-, v = G+ - G-
+// and stores UV[rl][j3][m] = (ur, ui, vr, vi).
+__global__ void __launch_bounds__(kSepThreads) rf_sep_axis3(const SepSpec sp, const double2* __restrict__ E3,
+                                                            const double4* __restrict__ PQ, double4* __restrict__ UV) {
+  extern __shared__ __align__(16) double sm[];
+  const int32_t n1 = sp.kn[0], n2 = sp.kn[1], n3 = sp.kn[2], N3 = sp.N[2];
+  const int K = 2 * n3;
+  double* AT = sm;              // [K][kLdT]
+  double* B = sm + K * kLdT;    // [K][128]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t pairs = (int64_t)n1 * n2;
+  const int64_t rowBlocks = (N3 + kRows - 1) / kRows, pairBlocks = (pairs + 31) / 32;
+  const int64_t tiles = (int64_t)sp.nr * rowBlocks * pairBlocks;
+  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int64_t pb = tile % pairBlocks;
+    const int64_t rb = (tile / pairBlocks) % rowBlocks;
+    const int64_t rl = tile / (pairBlocks * rowBlocks);
+    __syncthreads();  // the previous tile's operands are consumed
+    for (int e = threadIdx.x; e < n3 * kRows; e += kSepThreads) {
+      const int i3 = e / kRows, row = e % kRows;
+      const int64_t j3 = rb * kRows + row;
+      const double2 v = j3 < N3 ? E3[(int64_t)i3 * N3 + j3] : make_double2(0.0, 0.0);
+      AT[(2 * i3) * kLdT + row] = v.x;
+      AT[(2 * i3 + 1) * kLdT + row] = v.y;
+    }
+    for (int e = threadIdx.x; e < 2 * n3 * 32; e += kSepThreads) {
+      const int ml = e % 32, i3 = (e / 32) % n3, s2 = e / (32 * n3);
+      const int64_t m = pb * 32 + ml;
+      double4 pq = make_double4(0.0, 0.0, 0.0, 0.0);
+      if (m < pairs) {
+        const int64_t i2 = m / n1, i1 = m % n1;
+        pq = PQ[(((rl * 2 + s2) * n2 + i2) * n1 + i1) * n3 + i3];
+      }
+      double* c = B + (2 * i3) * 128 + (2 * s2) * 32 + ml;
+      c[0] = pq.x;         // Pr   -> Gr
+      c[32] = pq.y;        // Pi   -> Gi
+      c[128] = -pq.w;      // -Qi  -> Gr
+      c[128 + 32] = pq.z;  // Qr   -> Gi
+    }
+    __syncthreads();
+    double acc[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    tile_fma<4>(AT, B, 128, K, warp, lane, acc);
+    const int64_t m = pb * 32 + lane;
+    if (m < pairs) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int64_t j3 = rb * kRows + 8 * warp + i;
+        if (j3 < N3)
+          UV[(rl * N3 + j3) * pairs + m] = make_double4(acc[i][0] + acc[i][2], acc[i][1] + acc[i][3],
+                                                        acc[i][0] - acc[i][2], acc[i][1] - acc[i][3]);
+      }
+    }
+  }
+}
+
+struct Axes21Smem {
+  double* E2T;  // [2 n2][kLdT]  rows j2 of the current row block: (c2, s2) per i2
+  double* W;    // [2 n2][64]    u, v of the current (rl, j3) as the axis-2 operand
+  double* HT;   // [2 n1][kLdT]  H transposed: (Hr, Hi) per i1
+  double* E1;   // [2 n1][128]   ampMult (c1, -s1) of the current column block
+};
+
+// Axes 2 and 1, persistent over items (column block, row block, rl, j3),
+// the blocks outermost so that a CTA's consecutive items share E2T and E1.
+//   H (64 x 2 n1) = E2T^T (64 x 2 n2) * W (2 n2 x 2 n1),
+//     W[2 i2][2 i1 + {0,1}] = (ur, ui), W[2 i2 + 1][2 i1 + {0,1}] = (-vi, vr);
+//   f (64 x 128)  = H (64 x 2 n1) * E1 (2 n1 x 128).
+__global__ void __launch_bounds__(kSepThreads, 1) rf_sep_axes21(const SepSpec sp, const double2* __restrict__ E1g,
+                                                                const double2* __restrict__ E2g,
+                                                                const double4* __restrict__ UV,
+                                                                double* __restrict__ out) {
+  extern __shared__ __align__(16) double sm[];
+  const int32_t n1 = sp.kn[0], n2 = sp.kn[1], N1 = sp.N[0], N2 = sp.N[1], N3 = sp.N[2];
+  const int K2 = 2 * n2, K1 = 2 * n1;
+  Axes21Smem s;
+  s.E2T = sm;
+  s.W = s.E2T + K2 * kLdT;
+  s.HT = s.W + K2 * 64;
+  s.E1 = s.HT + K1 * kLdT;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t pairs = (int64_t)n1 * n2;
+  const int64_t rowBlocks = (N2 + kRows - 1) / kRows, colBlocks = (N1 + 127) / 128;
+  const int64_t inner = (int64_t)sp.nr * N3;
+  const int64_t items = colBlocks * rowBlocks * inner;
+  for (int e = threadIdx.x; e < K2 * 64; e += kSepThreads) s.W[e] = 0.0;  // columns >= 2 n1 stay zero
+  int64_t curBlock = -1;
+  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const int64_t blk = it / inner;
+    const int64_t cb = blk / rowBlocks, rb = blk % rowBlocks;
+    const int64_t rl = (it % inner) / N3, j3 = it % N3;
+    __syncthreads();  // the previous item is done with W, HT (and E2T, E1)
+    if (blk != curBlock) {
+      curBlock = blk;
+      for (int e = threadIdx.x; e < n2 * kRows; e += kSepThreads) {
+        const int i2 = e / kRows, row = e % kRows;
+        const int64_t j2 = rb * kRows + row;
+        const double2 v = j2 < N2 ? E2g[(int64_t)i2 * N2 + j2] : make_double2(0.0, 0.0);
+        s.E2T[(2 * i2) * kLdT + row] = v.x;
+        s.E2T[(2 * i2 + 1) * kLdT + row] = v.y;
+      }
+      for (int e = threadIdx.x; e < n1 * 128; e += kSepThreads) {
+        const int i1 = e / 128, col = e % 128;
+        const int64_t j1 = cb * 128 + col;
+        const double2 v = j1 < N1 ? E1g[(int64_t)i1 * N1 + j1] : make_double2(0.0, 0.0);
+        s.E1[(2 * i1) * 128 + col] = sp.ampMult * v.x;
+        s.E1[(2 * i1 + 1) * 128 + col] = -(sp.ampMult * v.y);
+      }
+    }
+    const double4* uv = UV + (rl * N3 + j3) * pairs;
+    for (int e = threadIdx.x; e < pairs; e += kSepThreads) {
+      const int i2 = e / n1, i1 = e % n1;
+      const double4 v = uv[e];
+      *reinterpret_cast<double2*>(s.W + (2 * i2) * 64 + 2 * i1) = make_double2(v.x, v.y);
+      *reinterpret_cast<double2*>(s.W + (2 * i2 + 1) * 64 + 2 * i1) = make_double2(-v.w, v.z);
+    }
+    __syncthreads();
+    {
+      double h[8][2];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) h[i][0] = h[i][1] = 0.0;
+      tile_fma<2>(s.E2T, s.W, 64, K2, warp, lane, h);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int col = lane + 32 * j;
+        if (col < K1) {
+          double* d = s.HT + col * kLdT + 8 * warp;
+#pragma unroll
+          for (int i = 0; i < 8; i += 2) *reinterpret_cast<double2*>(d + i) = make_double2(h[i][j], h[i + 1][j]);
+        }
+      }
+    }
+    __syncthreads();
+    double acc[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    tile_fma<4>(s.HT, s.E1, 128, K1, warp, lane, acc);
+    double* o = out + (int64_t)(sp.r0 + rl) * sp.n + j3 * (int64_t)N1 * N2;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int64_t j2 = rb * kRows + 8 * warp + i;
+      if (j2 >= N2) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int64_t j1 = cb * 128 + 32 * j + lane;
+        if (j1 >= N1) continue;
+        double v = acc[i][j];
+        if (sp.applyMarginal) {  // multiVariateTransformation, randomFieldND.f90:139-178
+          v = v * sp.margSd + sp.margAvg;
+          if (sp.lognormal) v = exp(v);
+        }
+        o[j2 * N1 + j1] = v;
+      }
+    }
+  }
+}
+
+size_t axis3_smem(const SepSpec& sp) { return (size_t)2 * sp.kn[2] * (kLdT + 128) * sizeof(double); }
+size_t axes21_smem(const SepSpec& sp) {
+  return ((size_t)2 * sp.kn[1] * (kLdT + 64) + (size_t)2 * sp.kn[0] * (kLdT + 128)) * sizeof(double);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double* xStep, const int64_t* xNStep,
+                     int corrMod, int margiFirst, const double* corrL, double fieldAvg, double fieldVar, int Nmc,
+                     int method, double* d_randField, const rf_options* opt, void* stream) {
+  g_err.clear();
+  if (!ctx || !xMin || !xStep || !xNStep || !corrL || !d_randField) return fail(RF_EINVAL_ARG, "null pointer argument");
+  if (nDim < 1 || nDim > 3) return fail(RF_EINVAL_NDIM, "nDim must be 1, 2 or 3 (got %d)", nDim);
+  int64_t n = 1;
+  for (int d = 0; d < nDim; ++d) {
+    if (xNStep[d] < 1 || xNStep[d] > (1 << 24))
+      return fail(RF_EINVAL_ARG, "xNStep(%d) = %lld outside 1..2^24", d + 1, (long long)xNStep[d]);
+    if (xNStep[d] > 1 && !(xStep[d] > 0.0) ) return fail(RF_EINVAL_ARG, "xStep(%d) must be > 0", d + 1);
+    n *= xNStep[d];
+  }
+  Request rq = make_request(nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
+  if (int rc = validate(rq)) return rc;
+  if (method != RF_SHINOZUKA)
+    return fail(RF_ENOTSUP, "the grid path sums the Shinozuka tensor-grid spectrum (method 2); methods 1 and 3 "
+                            "run through rf_generate_device");
+  if (rq.opt.literal) return fail(RF_ENOTSUP, "literal mode (per-slab amplitudes) runs through rf_generate_device");
+  // the extent the reference measures on the points: max - min of setGrid's coordinates
+  double ext[3] = {0, 0, 0};
+  for (int d = 0; d < nDim; ++d) ext[d] = (xMin[d] + xStep[d] * (double)(xNStep[d] - 1)) - xMin[d];
+  Plan P;
+  rq.opt.precision = RF_PREC_FP32;  // the plan's operand layout is not used here
+  if (int rc = build_plan(rq, ext, P)) return rc;
+  SepSpec sp;
+  memset(&sp, 0, sizeof(sp));
+  sp.nDim = nDim;
+  for (int d = 0; d < 3; ++d) {
+    sp.N[d] = d < nDim ? (int32_t)xNStep[d] : 1;
+    sp.kn[d] = d < nDim ? P.kNStep[d] : 1;
+    sp.kDelta[d] = d < nDim ? P.kDelta[d] : 0.0;
+    sp.xMin[d] = d < nDim ? xMin[d] : 0.0;
+    sp.xStep[d] = d < nDim ? xStep[d] : 0.0;
+    sp.corrL[d] = d < nDim ? corrL[d] : 1.0;
+    if (sp.kn[d] > kMaxSepN)
+      return fail(RF_ENOTSUP, "the grid path takes at most %d wavenumbers per axis (axis %d has %d); set "
+                              "k_nstep or use rf_generate_device", kMaxSepN, d + 1, sp.kn[d]);
+  }
+  sp.S2 = nDim >= 2 ? 2 : 1;
+  sp.S3 = nDim == 3 ? 2 : 1;
+  sp.corrMod = corrMod;
+  sp.ig1 = P.ig1;
+  sp.ig2 = P.ig2;
+  sp.K = P.K;
+  sp.n = n;
+  sp.ampMult = P.ampMult;
+  sp.margSd = P.margSd;
+  sp.margAvg = P.margAvg;
+  sp.lognormal = P.lognormal;
+  sp.applyMarginal = P.applyMarginal;
+
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
+  ctx->launches = 0;
+  ctx->evValid = false;
+  const int64_t eCount = (int64_t)sp.kn[0] * sp.N[0] + (int64_t)sp.kn[1] * sp.N[1] + (int64_t)sp.kn[2] * sp.N[2];
+  const int64_t pairs = (int64_t)sp.kn[0] * sp.kn[1];
+  const int64_t perR = (2 * pairs * sp.kn[2] + (int64_t)sp.N[2] * pairs) * (int64_t)sizeof(double4);
+  const int32_t rBlk = (int32_t)std::max<int64_t>(1, std::min<int64_t>(Nmc, (int64_t)kSepScratch / perR));
+  const size_t eBytes = (size_t)((eCount * (int64_t)sizeof(double2) + 255) / 256 * 256);
+  const size_t need = eBytes + (size_t)rBlk * (size_t)perR;
+  if (int rc = ensure(ctx->dGrid, ctx->capGrid, need, "grid path scratch")) return rc;
+  double2* E = reinterpret_cast<double2*>(ctx->dGrid);
+  double4* PQ = reinterpret_cast<double4*>(reinterpret_cast<unsigned char*>(ctx->dGrid) + eBytes);
+  double4* UV = PQ + (int64_t)rBlk * 2 * pairs * sp.kn[2];
+  const double2* E1 = E;
+  const double2* E2 = E1 + (int64_t)sp.kn[0] * sp.N[0];
+  const double2* E3 = E2 + (int64_t)sp.kn[1] * sp.N[1];
+
+  const size_t sm3 = axis3_smem(sp), sm21 = axes21_smem(sp);
+  RF_CUDA(cudaFuncSetAttribute(rf_sep_axis3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3), "smem attribute");
+  RF_CUDA(cudaFuncSetAttribute(rf_sep_axes21, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm21),
+          "smem attribute");
+  int occ3 = 0, occ21 = 0;
+  RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, rf_sep_axis3, kSepThreads, sm3), "occupancy");
+  RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ21, rf_sep_axes21, kSepThreads, sm21), "occupancy");
+  if (occ3 < 1 || occ21 < 1) return fail(RF_ENOTSUP, "grid path tiles do not fit shared memory");
+
+  if (ctx->timing) {
+    for (auto& e : ctx->ev)
+      if (!e) RF_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+    RF_CUDA(cudaEventRecord(ctx->ev[0], st), "cudaEventRecord");
+  }
+  rf_sep_phasors<<<(unsigned)((eCount + 255) / 256), 256, 0, st>>>(sp, E);
+  RF_CUDA(cudaGetLastError(), "grid phasor kernel");
+  ctx->launches = 1;
+  bool first = true;
+  for (int32_t r0 = 0; r0 < Nmc; r0 += rBlk) {
+    sp.r0 = r0;
+    sp.nr = std::min(rBlk, Nmc - r0);
+    const int64_t nCoef = (int64_t)sp.nr * 2 * sp.kn[1] * sp.kn[2];
+    rf_sep_coeffs<<<(unsigned)((nCoef + 255) / 256), 256, 0, st>>>(sp, jump_table(), PQ);
+    RF_CUDA(cudaGetLastError(), "grid coefficient kernel");
+    if (ctx->timing && first) RF_CUDA(cudaEventRecord(ctx->ev[1], st), "cudaEventRecord");
+    first = false;
+    const int64_t tiles3 = (int64_t)sp.nr * ((sp.N[2] + kRows - 1) / kRows) * ((pairs + 31) / 32);
+    const int g3 = (int)std::min<int64_t>(tiles3, (int64_t)occ3 * ctx->numSMs);
+    rf_sep_axis3<<<g3, kSepThreads, sm3, st>>>(sp, E3, PQ, UV);
+    RF_CUDA(cudaGetLastError(), "grid axis-3 kernel");
+    const int64_t items = ((sp.N[0] + 127) / 128) * ((sp.N[1] + kRows - 1) / kRows) * (int64_t)sp.nr * sp.N[2];
+    const int g21 = (int)std::min<int64_t>(items, (int64_t)occ21 * ctx->numSMs);
+    rf_sep_axes21<<<g21, kSepThreads, sm21, st>>>(sp, E1, E2, UV, d_randField);
+    RF_CUDA(cudaGetLastError(), "grid axes-2/1 kernel");
+    ctx->launches += 3;
+  }
+  if (ctx->timing) RF_CUDA(cudaEventRecord(ctx->ev[2], st), "cudaEventRecord");
+  if (P.normalize) {
+    if ((size_t)2 * Nmc * sizeof(double) > ctx->capWork)
+      if (int rc = ensure(ctx->dWork, ctx->capWork, (size_t)2 * Nmc * sizeof(double), "moments")) return rc;
+    RF_CUDA(launch_normalize_and_map(P, d_randField, Nmc, ctx->dWork, st), "normalisation kernels");
+    ctx->launches += 3;
+  }
+  if (ctx->timing) {
+    RF_CUDA(cudaEventRecord(ctx->ev[3], st), "cudaEventRecord");
+    ctx->evValid = true;
+  }
+  return RF_OK;
+}
+
+}  // extern "C"

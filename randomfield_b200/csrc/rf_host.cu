@@ -320,6 +320,7 @@ void context_free(rf_context* c) {
   cudaFree(c->dWork);
   cudaFree(c->dStats);
   cudaFree(c->dFft);
+  cudaFree(c->dGrid);
   if (c->hStats) cudaFreeHost(c->hStats);
   cudaFree(c->dErr);
   cudaFree(c->dX);

@@ -33,6 +33,8 @@ struct rf_context {
   double* hWork = nullptr;  // pinned mirror of dWork
   double* dFft = nullptr;   // FFT method: amplitudes, pass buffer, cosine matrices (rf_fft.cu)
   size_t capFft = 0;
+  void* dGrid = nullptr;    // grid path: phasor tables, coefficients, axis-3 partial sums (rf_grid.cu)
+  size_t capGrid = 0;
   double* dStats = nullptr; // field statistics scratch (rf_stats.cu)
   size_t capStats = 0;
   double* hStats = nullptr;

@@ -201,6 +201,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
   constexpr int kGridSteps = (LPAD > 0 ? LPAD / 2 : 4) / (kF8 ? 2 : 1);
   constexpr int kTabSteps = kTableSteps / (kF8 ? 2 : 1);
   constexpr int kGenWarps = Roles<GEN>::kGen, kParts = Roles<GEN>::kParts, kProdWarp = Roles<GEN>::kProd;
+  static_assert(!kHasGrid || kParts == 2, "GEN_GRID3 tiles: two column halves per lane quarter");
   extern __shared__ __align__(1024) unsigned char smem[];
   Bars* bars = reinterpret_cast<Bars*>(smem);
   unsigned char* sB = smem + kHeaderBytes;
@@ -378,7 +379,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
       Grid3Thread g3;
       Grid3Walk walk;
       if (kHasGrid && grid) {
-        grid3_thread_setup<LPAD>(g3, P, kParts == 4 ? (h & 1) : h, x);
+        grid3_thread_setup<LPAD>(g3, P, h, x);
         walk.init(P, x);
       }
 
@@ -398,14 +399,11 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
         if (lane == 0 && ch + 1 < nChunks) probe = mbar_test_wait(&bars->empty[s], ph ^ 1) ? 1u : 0u;
         const uint32_t aAddr = tbase + laneOff + (uint32_t)L.aCol0 + sc * (uint32_t)L.aStride;
         if (kHasGrid && grid) {
-          // Two groups per stage.  With two column parts per lane quarter a
-          // thread takes its half (h) of both groups; with four, half h & 1
-          // of group h >> 1 only, and walks past the other group's phasor.
+          // Two groups per stage; a thread takes its half (h) of both.
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
             const float2 Pq = walk.outer();
             walk.next(P, x);
-            if (kParts == 4 && u != (h >> 1)) continue;
             // one TMEM column per (cos, sin) pair, or per two pairs for e4m3
             constexpr int NW = kF8 ? (LPAD > 0 ? LPAD / 2 : 1) : (LPAD > 0 ? LPAD : 1);
             uint32_t words[NW];
@@ -425,7 +423,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
             grid3_pairs<LPAD>(g3, Pq, emit);
             // LPAD is a multiple of 8: 16-bit stores cover 8 columns at
             // 8-aligned offsets, e4m3 stores 4 columns at 4-aligned offsets.
-            const uint32_t col = aAddr + (uint32_t)(u * 2 * NW + (kParts == 4 ? (h & 1) : h) * NW);
+            const uint32_t col = aAddr + (uint32_t)(u * 2 * NW + h * NW);
             if (kF8) {
 #pragma unroll
               for (int pc = 0; pc < NW / 4; ++pc) tmem_st4(col + pc * 4, &words[pc * 4]);
