@@ -66,10 +66,10 @@ struct SepSpec {
 };
 
 // acc[i][j] += sum_{k < K} AT[k][8 warp + i] * B[k][32 j + lane]
-// (AT row stride kLdT, B row stride ldb, both in shared memory; K even).
+// (AT row stride lda, even; B row stride ldb; both in shared memory).
 template <int J>
-__device__ __forceinline__ void tile_fma(const double* __restrict__ AT, const double* __restrict__ B, int ldb,
-                                         int K, int warp, int lane, double (&acc)[8][J]) {
+__device__ __forceinline__ void tile_fma(const double* __restrict__ AT, int lda, const double* __restrict__ B,
+                                         int ldb, int K, int warp, int lane, double (&acc)[8][J]) {
   const double* a = AT + 8 * warp;
   const double* b = B + lane;
 #pragma unroll 2
@@ -77,7 +77,7 @@ __device__ __forceinline__ void tile_fma(const double* __restrict__ AT, const do
     double av[8], bv[J];
 #pragma unroll
     for (int i = 0; i < 8; i += 2) {
-      const double2 t = *reinterpret_cast<const double2*>(a + (int64_t)k * kLdT + i);
+      const double2 t = *reinterpret_cast<const double2*>(a + (int64_t)k * lda + i);
       av[i] = t.x;
       av[i + 1] = t.y;
     }
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(kSepThreads) rf_sep_axis3(const SepSpec sp, co
     for (int i = 0; i < 8; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-    tile_fma<4>(AT, B, 128, K, warp, lane, acc);
+    tile_fma<4>(AT, kLdT, B, 128, K, warp, lane, acc);
     const int64_t m = pb * 32 + lane;
     if (m < pairs) {
 #pragma unroll
@@ -235,112 +235,229 @@ __global__ void __launch_bounds__(kSepThreads) rf_sep_axis3(const SepSpec sp, co
   }
 }
 
-struct Axes21Smem {
-  double* E2T;  // [2 n2][kLdT]  rows j2 of the current row block: (c2, s2) per i2
-  double* W;    // [2 n2][64]    u, v of the current (rl, j3) as the axis-2 operand
-  double* HT;   // [2 n1][kLdT]  H transposed: (Hr, Hi) per i1
-  double* E1;   // [2 n1][128]   ampMult (c1, -s1) of the current column block
-};
+// 16-byte asynchronous copy global -> shared (sm_80 cp.async, L2 only), and
+// the group fences around it.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// acc[i][4] += sum_{k < K} AT[k][RW warp + i] * B[k][{2 lane, 2 lane + 1,
+// 64 + 2 lane, 65 + 2 lane}] (AT row stride lda, B row stride 128; RW even):
+// the column pairs of a lane are read, and later stored, as 16-byte words.
+template <int RW>
+__device__ __forceinline__ void tile_fma_pairs(const double* __restrict__ AT, int lda, const double* __restrict__ B,
+                                               int K, int warp, int lane, double (&acc)[RW][4]) {
+  const double* a = AT + RW * warp;
+  const double* b = B + 2 * lane;
+#pragma unroll 2
+  for (int k = 0; k < K; ++k) {
+    double av[RW];
+#pragma unroll
+    for (int i = 0; i < RW; i += 2) {
+      const double2 t = *reinterpret_cast<const double2*>(a + k * lda + i);
+      av[i] = t.x;
+      av[i + 1] = t.y;
+    }
+    const double2 b0 = *reinterpret_cast<const double2*>(b + k * 128);
+    const double2 b1 = *reinterpret_cast<const double2*>(b + k * 128 + 64);
+#pragma unroll
+    for (int i = 0; i < RW; ++i) {
+      acc[i][0] = fma(av[i], b0.x, acc[i][0]);
+      acc[i][1] = fma(av[i], b0.y, acc[i][1]);
+      acc[i][2] = fma(av[i], b1.x, acc[i][2]);
+      acc[i][3] = fma(av[i], b1.y, acc[i][3]);
+    }
+  }
+}
 
 // Axes 2 and 1, persistent over items (column block, row block, rl, j3),
 // the blocks outermost so that a CTA's consecutive items share E2T and E1.
-//   H (64 x 2 n1) = E2T^T (64 x 2 n2) * W (2 n2 x 2 n1),
-//     W[2 i2][2 i1 + {0,1}] = (ur, ui), W[2 i2 + 1][2 i1 + {0,1}] = (-vi, vr);
-//   f (64 x 128)  = H (64 x 2 n1) * E1 (2 n1 x 128).
+// An item covers ROWS rows j2 (64 or 128) and 128 columns j1.  The u, v slab
+// of item i + 1 streams into the other half of a double buffer (cp.async)
+// while item i computes.
+//   axis 2: H^T (2 n1 x ROWS) from the slab and E2T: warp w owns i1 in
+//           [RH w, RH w + RH), lane l the rows l + 32 j:
+//           Hr += ur c2 - vi s2, Hi += ui c2 + vr s2 over i2;
+//   axis 1: f (ROWS x 128) = H (ROWS x 2 n1) * E1 (2 n1 x 128), E1 rows
+//           ampMult (c1, -s1), warp w rows ROWS/8 w.. ; then the marginal
+//           map and the store.
+template <int RH, int ROWS>
 __global__ void __launch_bounds__(kSepThreads, 1) rf_sep_axes21(const SepSpec sp, const double2* __restrict__ E1g,
                                                                 const double2* __restrict__ E2g,
                                                                 const double4* __restrict__ UV,
                                                                 double* __restrict__ out) {
+  constexpr int RW = ROWS / 8, JB = ROWS / 32;
   extern __shared__ __align__(16) double sm[];
   const int32_t n1 = sp.kn[0], n2 = sp.kn[1], N1 = sp.N[0], N2 = sp.N[1], N3 = sp.N[2];
-  const int K2 = 2 * n2, K1 = 2 * n1;
-  Axes21Smem s;
-  s.E2T = sm;
-  s.W = s.E2T + K2 * kLdT;
-  s.HT = s.W + K2 * 64;
-  s.E1 = s.HT + K1 * kLdT;
+  const int K1 = 2 * n1;
+  const int32_t pairs = n1 * n2;
+  double* E2T = sm;                                                 // [2 n2][ROWS]: (c2, s2) rows of i2
+  double4* UVs = reinterpret_cast<double4*>(E2T + 2 * n2 * ROWS);  // [2][pairs]
+  double* HT = reinterpret_cast<double*>(UVs + 2 * pairs);          // [2 n1][ROWS]
+  double* E1 = HT + K1 * ROWS;                                      // [2 n1][128]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t pairs = (int64_t)n1 * n2;
-  const int64_t rowBlocks = (N2 + kRows - 1) / kRows, colBlocks = (N1 + 127) / 128;
+  const int64_t rowBlocks = (N2 + ROWS - 1) / ROWS, colBlocks = (N1 + 127) / 128;
   const int64_t inner = (int64_t)sp.nr * N3;
   const int64_t items = colBlocks * rowBlocks * inner;
-  for (int e = threadIdx.x; e < K2 * 64; e += kSepThreads) s.W[e] = 0.0;  // columns >= 2 n1 stay zero
+  const bool pairStore = (N1 % 2) == 0;  // 16-byte stores keep their alignment
+  auto prefetch = [&](int64_t it, int buf) {
+    if (it < items) {
+      const int64_t rl = (it % inner) / N3, j3 = it % N3;
+      const double2* src = reinterpret_cast<const double2*>(UV + (rl * N3 + j3) * pairs);
+      double2* dst = reinterpret_cast<double2*>(UVs + buf * pairs);
+      for (int e = threadIdx.x; e < 2 * pairs; e += kSepThreads) cp_async16(dst + e, src + e);
+    }
+    cp_async_commit();
+  };
   int64_t curBlock = -1;
-  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
+  int buf = 0;
+  prefetch(blockIdx.x, 0);
+  for (int64_t it = blockIdx.x; it < items; it += gridDim.x, buf ^= 1) {
     const int64_t blk = it / inner;
     const int64_t cb = blk / rowBlocks, rb = blk % rowBlocks;
     const int64_t rl = (it % inner) / N3, j3 = it % N3;
-    __syncthreads();  // the previous item is done with W, HT (and E2T, E1)
+    __syncthreads();  // the previous item is done with HT (and E2T, E1, its slab buffer)
+    prefetch(it + gridDim.x, buf ^ 1);
     if (blk != curBlock) {
       curBlock = blk;
-      for (int e = threadIdx.x; e < n2 * kRows; e += kSepThreads) {
-        const int i2 = e / kRows, row = e % kRows;
-        const int64_t j2 = rb * kRows + row;
+      for (int e = threadIdx.x; e < n2 * ROWS; e += kSepThreads) {
+        const int i2 = e / ROWS, row = e % ROWS;
+        const int64_t j2 = rb * ROWS + row;
         const double2 v = j2 < N2 ? E2g[(int64_t)i2 * N2 + j2] : make_double2(0.0, 0.0);
-        s.E2T[(2 * i2) * kLdT + row] = v.x;
-        s.E2T[(2 * i2 + 1) * kLdT + row] = v.y;
+        E2T[(2 * i2) * ROWS + row] = v.x;
+        E2T[(2 * i2 + 1) * ROWS + row] = v.y;
       }
       for (int e = threadIdx.x; e < n1 * 128; e += kSepThreads) {
         const int i1 = e / 128, col = e % 128;
         const int64_t j1 = cb * 128 + col;
         const double2 v = j1 < N1 ? E1g[(int64_t)i1 * N1 + j1] : make_double2(0.0, 0.0);
-        s.E1[(2 * i1) * 128 + col] = sp.ampMult * v.x;
-        s.E1[(2 * i1 + 1) * 128 + col] = -(sp.ampMult * v.y);
+        E1[(2 * i1) * 128 + col] = sp.ampMult * v.x;
+        E1[(2 * i1 + 1) * 128 + col] = -(sp.ampMult * v.y);
       }
     }
-    const double4* uv = UV + (rl * N3 + j3) * pairs;
-    for (int e = threadIdx.x; e < pairs; e += kSepThreads) {
-      const int i2 = e / n1, i1 = e % n1;
-      const double4 v = uv[e];
-      *reinterpret_cast<double2*>(s.W + (2 * i2) * 64 + 2 * i1) = make_double2(v.x, v.y);
-      *reinterpret_cast<double2*>(s.W + (2 * i2 + 1) * 64 + 2 * i1) = make_double2(-v.w, v.z);
-    }
+    cp_async_wait_prev();  // this item's slab (the group before the one just issued)
     __syncthreads();
     {
-      double h[8][2];
+      const double4* uv = UVs + buf * pairs;
+      double hr[RH][JB], hi[RH][JB];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) h[i][0] = h[i][1] = 0.0;
-      tile_fma<2>(s.E2T, s.W, 64, K2, warp, lane, h);
+      for (int t = 0; t < RH; ++t)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        const int col = lane + 32 * j;
-        if (col < K1) {
-          double* d = s.HT + col * kLdT + 8 * warp;
+        for (int j = 0; j < JB; ++j) hr[t][j] = hi[t][j] = 0.0;
+      const int i1b = RH * warp;
+      const double* e2 = E2T + lane;
+      for (int i2 = 0; i2 < n2; ++i2) {
+        double c[JB], sn[JB];
 #pragma unroll
-          for (int i = 0; i < 8; i += 2) *reinterpret_cast<double2*>(d + i) = make_double2(h[i][j], h[i + 1][j]);
+        for (int j = 0; j < JB; ++j) {
+          c[j] = e2[(2 * i2) * ROWS + 32 * j];
+          sn[j] = e2[(2 * i2 + 1) * ROWS + 32 * j];
+        }
+#pragma unroll
+        for (int t = 0; t < RH; ++t) {
+          const double4 u = (i1b + t < n1) ? uv[i2 * n1 + i1b + t] : make_double4(0.0, 0.0, 0.0, 0.0);
+#pragma unroll
+          for (int j = 0; j < JB; ++j) {
+            hr[t][j] = fma(u.x, c[j], hr[t][j]);
+            hr[t][j] = fma(-u.w, sn[j], hr[t][j]);
+            hi[t][j] = fma(u.y, c[j], hi[t][j]);
+            hi[t][j] = fma(u.z, sn[j], hi[t][j]);
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < RH; ++t) {
+        if (i1b + t >= n1) continue;
+#pragma unroll
+        for (int j = 0; j < JB; ++j) {
+          HT[(2 * (i1b + t)) * ROWS + lane + 32 * j] = hr[t][j];
+          HT[(2 * (i1b + t) + 1) * ROWS + lane + 32 * j] = hi[t][j];
         }
       }
     }
     __syncthreads();
-    double acc[8][4];
+    double acc[RW][4];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < RW; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-    tile_fma<4>(s.HT, s.E1, 128, K1, warp, lane, acc);
+    tile_fma_pairs<RW>(HT, ROWS, E1, K1, warp, lane, acc);
     double* o = out + (int64_t)(sp.r0 + rl) * sp.n + j3 * (int64_t)N1 * N2;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int64_t j2 = rb * kRows + 8 * warp + i;
+    for (int i = 0; i < RW; ++i) {
+      const int64_t j2 = rb * ROWS + RW * warp + i;
       if (j2 >= N2) continue;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int64_t j1 = cb * 128 + 32 * j + lane;
-        if (j1 >= N1) continue;
-        double v = acc[i][j];
+      for (int h = 0; h < 2; ++h) {
+        const int64_t j1 = cb * 128 + 64 * h + 2 * lane;
+        double v0 = acc[i][2 * h], v1 = acc[i][2 * h + 1];
         if (sp.applyMarginal) {  // multiVariateTransformation, randomFieldND.f90:139-178
-          v = v * sp.margSd + sp.margAvg;
-          if (sp.lognormal) v = exp(v);
+          v0 = v0 * sp.margSd + sp.margAvg;
+          v1 = v1 * sp.margSd + sp.margAvg;
+          if (sp.lognormal) {
+            v0 = exp(v0);
+            v1 = exp(v1);
+          }
         }
-        o[j2 * N1 + j1] = v;
+        double* d = o + j2 * N1 + j1;
+        if (pairStore && j1 + 1 < N1) {
+          *reinterpret_cast<double2*>(d) = make_double2(v0, v1);
+        } else {
+          if (j1 < N1) d[0] = v0;
+          if (j1 + 1 < N1) d[1] = v1;
+        }
       }
     }
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 size_t axis3_smem(const SepSpec& sp) { return (size_t)2 * sp.kn[2] * (kLdT + 128) * sizeof(double); }
-size_t axes21_smem(const SepSpec& sp) {
-  return ((size_t)2 * sp.kn[1] * (kLdT + 64) + (size_t)2 * sp.kn[0] * (kLdT + 128)) * sizeof(double);
+size_t axes21_smem(const SepSpec& sp, int rows) {
+  const size_t pairs = (size_t)sp.kn[0] * sp.kn[1];
+  return ((size_t)2 * sp.kn[1] * rows + 8 * pairs + (size_t)2 * sp.kn[0] * (rows + 128)) * sizeof(double);
+}
+
+template <int RH, int ROWS>
+cudaError_t launch_axes21(const SepSpec& sp, const double2* E1, const double2* E2, const double4* UV, double* out,
+                          int numSMs, cudaStream_t st) {
+  const size_t smem = axes21_smem(sp, ROWS);
+  cudaError_t e = cudaFuncSetAttribute(rf_sep_axes21<RH, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  int occ = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, rf_sep_axes21<RH, ROWS>, kSepThreads, smem);
+  if (e != cudaSuccess) return e;
+  if (occ < 1) return cudaErrorInvalidConfiguration;
+  const int64_t items = ((sp.N[0] + 127) / 128) * ((sp.N[1] + ROWS - 1) / ROWS) * (int64_t)sp.nr * sp.N[2];
+  const int grid = (int)std::min<int64_t>(items, (int64_t)occ * numSMs);
+  rf_sep_axes21<RH, ROWS><<<grid, kSepThreads, smem, st>>>(sp, E1, E2, UV, out);
+  return cudaGetLastError();
+}
+
+// Rows per item: 128 where the row axis is longer than 64 and the tiles fit
+// shared memory (half the slab loads and syncs per field value), else 64.
+// i1 per warp in the axis-2 stage: 8 warps cover n1 <= 8 RH.
+constexpr size_t kMaxSmem = (size_t)227 * 1024;
+template <int ROWS>
+cudaError_t launch_axes21_rows(const SepSpec& sp, const double2* E1, const double2* E2, const double4* UV,
+                               double* out, int numSMs, cudaStream_t st) {
+  switch ((sp.kn[0] + 7) / 8) {
+    case 1: return launch_axes21<1, ROWS>(sp, E1, E2, UV, out, numSMs, st);
+    case 2: return launch_axes21<2, ROWS>(sp, E1, E2, UV, out, numSMs, st);
+    case 3: return launch_axes21<3, ROWS>(sp, E1, E2, UV, out, numSMs, st);
+    default: return launch_axes21<4, ROWS>(sp, E1, E2, UV, out, numSMs, st);
+  }
+}
+cudaError_t launch_axes21_any(const SepSpec& sp, const double2* E1, const double2* E2, const double4* UV,
+                              double* out, int numSMs, cudaStream_t st) {
+  if (sp.N[1] > 64 && axes21_smem(sp, 128) <= kMaxSmem)
+    return launch_axes21_rows<128>(sp, E1, E2, UV, out, numSMs, st);
+  return launch_axes21_rows<64>(sp, E1, E2, UV, out, numSMs, st);
 }
 
 }  // namespace
@@ -418,14 +535,11 @@ int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double
   const double2* E2 = E1 + (int64_t)sp.kn[0] * sp.N[0];
   const double2* E3 = E2 + (int64_t)sp.kn[1] * sp.N[1];
 
-  const size_t sm3 = axis3_smem(sp), sm21 = axes21_smem(sp);
+  const size_t sm3 = axis3_smem(sp), sm21 = axes21_smem(sp, 64);
   RF_CUDA(cudaFuncSetAttribute(rf_sep_axis3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3), "smem attribute");
-  RF_CUDA(cudaFuncSetAttribute(rf_sep_axes21, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm21),
-          "smem attribute");
-  int occ3 = 0, occ21 = 0;
+  int occ3 = 0;
   RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, rf_sep_axis3, kSepThreads, sm3), "occupancy");
-  RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ21, rf_sep_axes21, kSepThreads, sm21), "occupancy");
-  if (occ3 < 1 || occ21 < 1) return fail(RF_ENOTSUP, "grid path tiles do not fit shared memory");
+  if (occ3 < 1 || sm21 > kMaxSmem) return fail(RF_ENOTSUP, "grid path tiles do not fit shared memory");
 
   if (ctx->timing) {
     for (auto& e : ctx->ev)
@@ -448,10 +562,7 @@ int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double
     const int g3 = (int)std::min<int64_t>(tiles3, (int64_t)occ3 * ctx->numSMs);
     rf_sep_axis3<<<g3, kSepThreads, sm3, st>>>(sp, E3, PQ, UV);
     RF_CUDA(cudaGetLastError(), "grid axis-3 kernel");
-    const int64_t items = ((sp.N[0] + 127) / 128) * ((sp.N[1] + kRows - 1) / kRows) * (int64_t)sp.nr * sp.N[2];
-    const int g21 = (int)std::min<int64_t>(items, (int64_t)occ21 * ctx->numSMs);
-    rf_sep_axes21<<<g21, kSepThreads, sm21, st>>>(sp, E1, E2, UV, d_randField);
-    RF_CUDA(cudaGetLastError(), "grid axes-2/1 kernel");
+    RF_CUDA(launch_axes21_any(sp, E1, E2, UV, d_randField, ctx->numSMs, st), "grid axes-2/1 kernel");
     ctx->launches += 3;
   }
   if (ctx->timing) RF_CUDA(cudaEventRecord(ctx->ev[2], st), "cudaEventRecord");
