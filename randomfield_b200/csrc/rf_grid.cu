@@ -21,16 +21,16 @@
 // whole computation stays in FP64: the field equals the reference's sum to
 // FP64 rounding, with no reduced-precision operand anywhere.
 //
-// Every stage is a small dense product whose tiles run through one register-
-// blocked FP64 routine (tile_fma): a 256-thread CTA computes a 64-row x 32J-
-// column tile, warp w rows 8w..8w+7, lane l columns l + 32j, operands in
-// shared memory (the row operand transposed, read as warp-wide broadcasts).
+// Every stage is a small dense product on the FP64 tensor path (mma.sync
+// m8n8k4 .f64, the only FP64 tensor-core instruction of sm_100a): operands
+// staged in shared memory with rows padded against bank conflicts, k padded
+// to a multiple of 4 with zero rows, FP64 accumulators in registers.
 //   rf_sep_phasors  E_d(i, j) for the three axes (FP64 sincos);
 //   rf_sep_coeffs   P, Q for every (r, s2, i2, i1, i3) from the rnglib stream;
 //   rf_sep_axis3    tiles (r, 64 rows j3, 32 pairs (i1,i2)) -> u, v;
-//   rf_sep_axes21   persistent: item (r, j3, 64 rows j2, 128 columns j1):
-//                   H into shared memory, then f, the marginal map and the
-//                   store of 64 x 128 field values.
+//   rf_sep_axes21   persistent: item (r, j3, 64 or 128 rows j2, 128 columns
+//                   j1): H into shared memory, then f, the marginal map and
+//                   the store of the item's field values.
 // Axes the request does not have are carried as length-1 axes with k = 0 and
 // one sign row, so 1-D and 2-D grids take the same kernels.
 #include <algorithm>
@@ -46,7 +46,6 @@ namespace {
 
 constexpr int kSepThreads = 256;
 constexpr int kRows = 64;     // rows of a tile
-constexpr int kLdT = 66;      // row stride of a transposed operand (doubles): 16-byte aligned, conflict-free writes
 constexpr int kMaxSepN = 32;  // wavenumbers per axis
 constexpr size_t kSepScratch = (size_t)512 << 20;  // P/Q and u/v of one realization block
 
@@ -65,30 +64,19 @@ struct SepSpec {
   double ampMult, margSd, margAvg;
 };
 
-// acc[i][j] += sum_{k < K} AT[k][8 warp + i] * B[k][32 j + lane]
-// (AT row stride lda, even; B row stride ldb; both in shared memory).
-template <int J>
-__device__ __forceinline__ void tile_fma(const double* __restrict__ AT, int lda, const double* __restrict__ B,
-                                         int ldb, int K, int warp, int lane, double (&acc)[8][J]) {
-  const double* a = AT + 8 * warp;
-  const double* b = B + lane;
-#pragma unroll 2
-  for (int k = 0; k < K; ++k) {
-    double av[8], bv[J];
-#pragma unroll
-    for (int i = 0; i < 8; i += 2) {
-      const double2 t = *reinterpret_cast<const double2*>(a + (int64_t)k * lda + i);
-      av[i] = t.x;
-      av[i + 1] = t.y;
-    }
-#pragma unroll
-    for (int j = 0; j < J; ++j) bv[j] = b[(int64_t)k * ldb + 32 * j];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < J; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
-  }
+// D += A B on the FP64 tensor path: one 8 x 8 x 4 product per warp
+// (mma.sync m8n8k4 .f64).  Lane l = 4 g + t holds A[g][t], B[t][g] and
+// D[g][2 t], D[g][2 t + 1].
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
 }
+
+// Row padding (doubles) of the 8 x 4 fragment operands: a stride of 4 mod 16
+// doubles puts the four k rows t of a half-warp's load (lanes 4 g + t, g < 4)
+// on four different 32-byte bank groups.
+constexpr int kPadLd = 4;
 
 // E_d(i, j) = (cos, sin)(k_d(i) x_d(j)), k_d(i) = 0 + kDelta_d i (setGrid from
 // 0, spectra_RF.f90:118), x_d(j) = (xMin_d + xStep_d j) / corrL_d
@@ -139,25 +127,28 @@ __global__ void rf_sep_coeffs(const SepSpec sp, const JumpTable jt, double4* __r
     return;
   }
   int64_t c1[2] = {0, 0}, c2[2] = {0, 0};
+  // S(k) = prod_d exp(-k_d^2 / (4 pi)) multiplied from axis 1 up, as
+  // spectra_RF.f90:202-208 does (corrL = 1); the sign of k_d does not enter
+  auto factor = [&](int d, int32_t i) {
+    const double k = 0.0 + sp.kDelta[d] * (double)i;
+    return exp(-((k * k) * 1.0) / (4.0 * kRefPi));
+  };
+  const double f2 = sp.nDim >= 2 ? factor(1, i2) : 1.0, f3 = sp.nDim >= 3 ? factor(2, i3) : 1.0;
   for (int s3 = 0; s3 < sp.S3; ++s3) {
     const int64_t k0 = (int64_t)(s2 * sp.S3 + s3) * kn + (int64_t)n1 * (i2 + (int64_t)n2 * i3);
     uni_state_at(jt, sp.ig1, sp.ig2, (uint64_t)(rg * sp.K + k0 + 1), c1[s3], c2[s3]);
   }
   for (int32_t i1 = 0; i1 < n1; ++i1) {
+    const double f1 = sp.corrMod == RF_CM_GAUSSIAN ? factor(0, i1) : 1.0;
     double cr[2] = {0.0, 0.0}, ci[2] = {0.0, 0.0};
     for (int s3 = 0; s3 < sp.S3; ++s3) {
       if (i1) uni_state_next(jt, c1[s3], c2[s3]);
       const int64_t kref = (int64_t)(s2 * sp.S3 + s3) * kn + i1 + (int64_t)n1 * (i2 + (int64_t)n2 * i3);
       double amp;
       if (sp.corrMod == RF_CM_GAUSSIAN) {
-        const int32_t idx[3] = {i1, i2, i3};
-        double S = 1.0;
-        for (int d = 0; d < sp.nDim; ++d) {
-          const double base = 0.0 + sp.kDelta[d] * (double)idx[d];
-          const bool neg = (d == 1 && s2) || (d == 2 && s3);
-          const double k = neg ? base * -1.0 : base * 1.0;
-          S = S * 1.0 * exp(-((k * k) * 1.0) / (4.0 * kRefPi));  // spectra_RF.f90:202-208, corrL = 1
-        }
+        double S = 1.0 * f1;
+        if (sp.nDim >= 2) S = S * 1.0 * f2;
+        if (sp.nDim >= 3) S = S * 1.0 * f3;
         amp = sqrt(S);
       } else {
         amp = (kref == 5) ? 1.0 : 0.0;  // cm_COS, spectra_RF.f90:210-220
@@ -172,23 +163,32 @@ __global__ void rf_sep_coeffs(const SepSpec sp, const JumpTable jt, double4* __r
   }
 }
 
-// Axis 3.  Tile (rl, row block of 64 j3, block of 32 pairs m = i2 n1 + i1):
-// columns 32 (2 s2 + reim) + lane of the product are G_{s2}(m) real/imag,
-// from the k-rows 2 i3 (cos) and 2 i3 + 1 (sin):
-//   Gr = sum Pr c3 - Qi s3,  Gi = sum Pi c3 + Qr s3.
-// The epilogue folds the two signs of axis 2 into u = G+ + G-, v = G+ - G-
-// and stores UV[rl][j3][m] = (ur, ui, vr, vi).
+// Axis 3.  Tile (rl, row block of 64 j3, block of 32 pairs m = i2 n1 + i1),
+// an m8n8k4 FP64 tensor product G (64 x 128) = E3 (64 x 2 n3) B (2 n3 x 128)
+// with k padded to a multiple of 4 by zero rows.  Column 8 q + c of B
+// (c < 8) belongs to pair 2 q + (c >> 2), component (c >> 1) & 1 (real,
+// imaginary) and sign row s2 = c & 1, from the k-rows 2 i3 (cos) and
+// 2 i3 + 1 (sin):
+//   Gr = sum Pr c3 - Qi s3,  Gi = sum Pi c3 + Qr s3,
+// so that the lane holding D[g][2 t], D[g][2 t + 1] has both sign rows of
+// one component and folds them into u = G+ + G-, v = G+ - G-.  The slab
+// UV[rl][j3][m] is stored as (ur, vr, ui, vi).  Warps: 2 x 4 tiles of
+// 32 rows x 32 columns.
 __global__ void __launch_bounds__(kSepThreads) rf_sep_axis3(const SepSpec sp, const double2* __restrict__ E3,
-                                                            const double4* __restrict__ PQ, double4* __restrict__ UV) {
+                                                            const double4* __restrict__ PQ, double* __restrict__ UV) {
+  constexpr int LDA = kRows + kPadLd, LDB = 128 + kPadLd;
   extern __shared__ __align__(16) double sm[];
   const int32_t n1 = sp.kn[0], n2 = sp.kn[1], n3 = sp.kn[2], N3 = sp.N[2];
-  const int K = 2 * n3;
-  double* AT = sm;              // [K][kLdT]
-  double* B = sm + K * kLdT;    // [K][128]
+  const int K = (2 * n3 + 3) & ~3;
+  double* AT = sm;           // [K][LDA]
+  double* B = sm + K * LDA;  // [K][LDB]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3, wr = warp & 1, wc = warp >> 1;
   const int64_t pairs = (int64_t)n1 * n2;
   const int64_t rowBlocks = (N3 + kRows - 1) / kRows, pairBlocks = (pairs + 31) / 32;
   const int64_t tiles = (int64_t)sp.nr * rowBlocks * pairBlocks;
+  for (int e = threadIdx.x; e < (K - 2 * n3) * LDA; e += kSepThreads) AT[2 * n3 * LDA + e] = 0.0;
+  for (int e = threadIdx.x; e < (K - 2 * n3) * LDB; e += kSepThreads) B[2 * n3 * LDB + e] = 0.0;
   for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const int64_t pb = tile % pairBlocks;
     const int64_t rb = (tile / pairBlocks) % rowBlocks;
@@ -198,8 +198,8 @@ __global__ void __launch_bounds__(kSepThreads) rf_sep_axis3(const SepSpec sp, co
       const int i3 = e / kRows, row = e % kRows;
       const int64_t j3 = rb * kRows + row;
       const double2 v = j3 < N3 ? E3[(int64_t)i3 * N3 + j3] : make_double2(0.0, 0.0);
-      AT[(2 * i3) * kLdT + row] = v.x;
-      AT[(2 * i3 + 1) * kLdT + row] = v.y;
+      AT[(2 * i3) * LDA + row] = v.x;
+      AT[(2 * i3 + 1) * LDA + row] = v.y;
     }
     for (int e = threadIdx.x; e < 2 * n3 * 32; e += kSepThreads) {
       const int ml = e % 32, i3 = (e / 32) % n3, s2 = e / (32 * n3);
@@ -209,27 +209,40 @@ __global__ void __launch_bounds__(kSepThreads) rf_sep_axis3(const SepSpec sp, co
         const int64_t i2 = m / n1, i1 = m % n1;
         pq = PQ[(((rl * 2 + s2) * n2 + i2) * n1 + i1) * n3 + i3];
       }
-      double* c = B + (2 * i3) * 128 + (2 * s2) * 32 + ml;
-      c[0] = pq.x;         // Pr   -> Gr
-      c[32] = pq.y;        // Pi   -> Gi
-      c[128] = -pq.w;      // -Qi  -> Gr
-      c[128 + 32] = pq.z;  // Qr   -> Gi
+      const int cr = 8 * (ml >> 1) + 4 * (ml & 1) + s2, ci = cr + 2;
+      B[(2 * i3) * LDB + cr] = pq.x;       // Pr   -> Gr
+      B[(2 * i3) * LDB + ci] = pq.y;       // Pi   -> Gi
+      B[(2 * i3 + 1) * LDB + cr] = -pq.w;  // -Qi  -> Gr
+      B[(2 * i3 + 1) * LDB + ci] = pq.z;   // Qr   -> Gi
     }
     __syncthreads();
-    double acc[8][4];
+    double acc[4][4][2];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int m = 0; m < 4; ++m)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-    tile_fma<4>(AT, kLdT, B, 128, K, warp, lane, acc);
-    const int64_t m = pb * 32 + lane;
-    if (m < pairs) {
+      for (int q = 0; q < 4; ++q) acc[m][q][0] = acc[m][q][1] = 0.0;
+#pragma unroll 2
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      double a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int64_t j3 = rb * kRows + 8 * warp + i;
+      for (int m = 0; m < 4; ++m) a[m] = AT[(k0 + t) * LDA + 32 * wr + 8 * m + g];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) b[q] = B[(k0 + t) * LDB + 32 * wc + 8 * q + g];
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dmma(acc[m][q], a[m], b[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int64_t mg = pb * 32 + 2 * (4 * wc + q) + (t >> 1);
+      if (mg >= pairs) continue;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int64_t j3 = rb * kRows + 32 * wr + 8 * m + g;
         if (j3 < N3)
-          UV[(rl * N3 + j3) * pairs + m] = make_double4(acc[i][0] + acc[i][2], acc[i][1] + acc[i][3],
-                                                        acc[i][0] - acc[i][2], acc[i][1] - acc[i][3]);
+          *reinterpret_cast<double2*>(UV + ((rl * N3 + j3) * pairs + mg) * 4 + 2 * (t & 1)) =
+              make_double2(acc[m][q][0] + acc[m][q][1], acc[m][q][0] - acc[m][q][1]);
       }
     }
   }
@@ -245,61 +258,46 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-// acc[i][4] += sum_{k < K} AT[k][RW warp + i] * B[k][{2 lane, 2 lane + 1,
-// 64 + 2 lane, 65 + 2 lane}] (AT row stride lda, B row stride 128; RW even):
-// the column pairs of a lane are read, and later stored, as 16-byte words.
-template <int RW>
-__device__ __forceinline__ void tile_fma_pairs(const double* __restrict__ AT, int lda, const double* __restrict__ B,
-                                               int K, int warp, int lane, double (&acc)[RW][4]) {
-  const double* a = AT + RW * warp;
-  const double* b = B + 2 * lane;
-#pragma unroll 2
-  for (int k = 0; k < K; ++k) {
-    double av[RW];
-#pragma unroll
-    for (int i = 0; i < RW; i += 2) {
-      const double2 t = *reinterpret_cast<const double2*>(a + k * lda + i);
-      av[i] = t.x;
-      av[i + 1] = t.y;
-    }
-    const double2 b0 = *reinterpret_cast<const double2*>(b + k * 128);
-    const double2 b1 = *reinterpret_cast<const double2*>(b + k * 128 + 64);
-#pragma unroll
-    for (int i = 0; i < RW; ++i) {
-      acc[i][0] = fma(av[i], b0.x, acc[i][0]);
-      acc[i][1] = fma(av[i], b0.y, acc[i][1]);
-      acc[i][2] = fma(av[i], b1.x, acc[i][2]);
-      acc[i][3] = fma(av[i], b1.y, acc[i][3]);
-    }
-  }
-}
+// Row stride (doubles) of a u, v slab in shared memory: 4 n1 rounded up to
+// 8 mod 16, so that the two i2 rows one W fragment load touches sit 64 bytes
+// apart in the banks.
+__host__ __device__ inline int32_t uv_row_stride(int32_t n1) { return 4 * n1 + ((8 - 4 * n1) % 16 + 16) % 16; }
 
 // Axes 2 and 1, persistent over items (column block, row block, rl, j3),
 // the blocks outermost so that a CTA's consecutive items share E2T and E1.
-// An item covers ROWS rows j2 (64 or 128) and 128 columns j1.  The u, v slab
-// of item i + 1 streams into the other half of a double buffer (cp.async)
-// while item i computes.
-//   axis 2: H^T (2 n1 x ROWS) from the slab and E2T: warp w owns i1 in
-//           [RH w, RH w + RH), lane l the rows l + 32 j:
-//           Hr += ur c2 - vi s2, Hi += ui c2 + vr s2 over i2;
-//   axis 1: f (ROWS x 128) = H (ROWS x 2 n1) * E1 (2 n1 x 128), E1 rows
-//           ampMult (c1, -s1), warp w rows ROWS/8 w.. ; then the marginal
-//           map and the store.
-template <int RH, int ROWS>
+// An item covers ROWS rows j2 (64 or 128) and 128 columns j1; both products
+// run as m8n8k4 FP64 tensor products with the k dimension padded to a
+// multiple of 4 by zero rows.  The u, v slab of item i + 1 streams into the
+// other half of a double buffer (cp.async) while item i computes.
+//   axis 2: H (ROWS x 2 n1) = E2 (ROWS x 2 n2) W (2 n2 x 2 n1), W read from
+//           the slab: W[2 i2][2 i1 + {0,1}] = (ur, ui), W[2 i2 + 1][...] =
+//           (-vi, vr); warp w takes ROWS/64 row tiles and every column tile;
+//   axis 1: f (ROWS x 128) = H (ROWS x 2 n1) E1 (2 n1 x 128), E1 rows
+//           ampMult (c1, -s1); warps in ROWS/32 x (256/ROWS) tiles of
+//           32 x (ROWS/2) ... then the marginal map and the store.
+template <int ROWS>
 __global__ void __launch_bounds__(kSepThreads, 1) rf_sep_axes21(const SepSpec sp, const double2* __restrict__ E1g,
                                                                 const double2* __restrict__ E2g,
                                                                 const double4* __restrict__ UV,
                                                                 double* __restrict__ out) {
-  constexpr int RW = ROWS / 8, JB = ROWS / 32;
+  constexpr int LD = ROWS + kPadLd;       // E2T, HT row stride
+  constexpr int LDE = 128 + kPadLd;       // E1 row stride
+  constexpr int WR = ROWS / 32;           // axis-1 warp rows (32 field rows each)
+  constexpr int WC = 8 / WR;              // axis-1 warp columns
+  constexpr int NTC = 128 / WC / 8;       // axis-1 column tiles per warp
+  constexpr int MB = ROWS / 64;           // axis-2 row tiles per warp
   extern __shared__ __align__(16) double sm[];
   const int32_t n1 = sp.kn[0], n2 = sp.kn[1], N1 = sp.N[0], N2 = sp.N[1], N3 = sp.N[2];
-  const int K1 = 2 * n1;
+  const int K1 = (2 * n1 + 3) & ~3, K2 = (2 * n2 + 3) & ~3;  // padded k extents
+  const int NTB = (2 * n1 + 7) / 8;                          // axis-2 column tiles
   const int32_t pairs = n1 * n2;
-  double* E2T = sm;                                                 // [2 n2][ROWS]: (c2, s2) rows of i2
-  double4* UVs = reinterpret_cast<double4*>(E2T + 2 * n2 * ROWS);  // [2][pairs]
-  double* HT = reinterpret_cast<double*>(UVs + 2 * pairs);          // [2 n1][ROWS]
-  double* E1 = HT + K1 * ROWS;                                      // [2 n1][128]
+  const int32_t uvLd = uv_row_stride(n1);                     // doubles per i2 row of a slab buffer
+  double* E2T = sm;                                          // [K2][LD]: (c2, s2) rows of i2
+  double* UVs = E2T + K2 * LD;                               // [2][n2][uvLd]: (ur, ui, vr, vi) per i1
+  double* HT = UVs + 2 * n2 * uvLd;                          // [K1][LD]
+  double* E1 = HT + K1 * LD;                                 // [K1][LDE]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
   const int64_t rowBlocks = (N2 + ROWS - 1) / ROWS, colBlocks = (N1 + 127) / 128;
   const int64_t inner = (int64_t)sp.nr * N3;
   const int64_t items = colBlocks * rowBlocks * inner;
@@ -308,11 +306,21 @@ __global__ void __launch_bounds__(kSepThreads, 1) rf_sep_axes21(const SepSpec sp
     if (it < items) {
       const int64_t rl = (it % inner) / N3, j3 = it % N3;
       const double2* src = reinterpret_cast<const double2*>(UV + (rl * N3 + j3) * pairs);
-      double2* dst = reinterpret_cast<double2*>(UVs + buf * pairs);
-      for (int e = threadIdx.x; e < 2 * pairs; e += kSepThreads) cp_async16(dst + e, src + e);
+      double* dst = UVs + buf * n2 * uvLd;
+      for (int e = threadIdx.x; e < 2 * pairs; e += kSepThreads) {
+        const int p = e >> 1, i2 = p / n1, i1 = p - i2 * n1;
+        cp_async16(dst + i2 * uvLd + 4 * i1 + 2 * (e & 1), src + e);
+      }
     }
     cp_async_commit();
   };
+  // the padding rows of H (k >= 2 n1) are never written by the axis-2 stage
+  for (int e = threadIdx.x; e < (K1 - 2 * n1) * LD; e += kSepThreads) HT[2 * n1 * LD + e] = 0.0;
+  // axis-2 operand from the slab: this lane's k row and column are fixed
+  // modulo the tile steps, so are the component and sign it reads
+  const int bc = t & 1, bre = g & 1;
+  const int bcomp = bc ? (bre ? 1 : 3) : (bre ? 2 : 0);  // slab layout (ur, vr, ui, vi)
+  const double bsign = (bc && !bre) ? -1.0 : 1.0;
   int64_t curBlock = -1;
   int buf = 0;
   prefetch(blockIdx.x, 0);
@@ -324,77 +332,87 @@ __global__ void __launch_bounds__(kSepThreads, 1) rf_sep_axes21(const SepSpec sp
     prefetch(it + gridDim.x, buf ^ 1);
     if (blk != curBlock) {
       curBlock = blk;
-      for (int e = threadIdx.x; e < n2 * ROWS; e += kSepThreads) {
+      for (int e = threadIdx.x; e < K2 / 2 * ROWS; e += kSepThreads) {
         const int i2 = e / ROWS, row = e % ROWS;
         const int64_t j2 = rb * ROWS + row;
-        const double2 v = j2 < N2 ? E2g[(int64_t)i2 * N2 + j2] : make_double2(0.0, 0.0);
-        E2T[(2 * i2) * ROWS + row] = v.x;
-        E2T[(2 * i2 + 1) * ROWS + row] = v.y;
+        const double2 v = (i2 < n2 && j2 < N2) ? E2g[(int64_t)i2 * N2 + j2] : make_double2(0.0, 0.0);
+        E2T[(2 * i2) * LD + row] = v.x;
+        E2T[(2 * i2 + 1) * LD + row] = v.y;
       }
-      for (int e = threadIdx.x; e < n1 * 128; e += kSepThreads) {
+      for (int e = threadIdx.x; e < K1 / 2 * 128; e += kSepThreads) {
         const int i1 = e / 128, col = e % 128;
         const int64_t j1 = cb * 128 + col;
-        const double2 v = j1 < N1 ? E1g[(int64_t)i1 * N1 + j1] : make_double2(0.0, 0.0);
-        E1[(2 * i1) * 128 + col] = sp.ampMult * v.x;
-        E1[(2 * i1 + 1) * 128 + col] = -(sp.ampMult * v.y);
+        const double2 v = (i1 < n1 && j1 < N1) ? E1g[(int64_t)i1 * N1 + j1] : make_double2(0.0, 0.0);
+        E1[(2 * i1) * LDE + col] = sp.ampMult * v.x;
+        E1[(2 * i1 + 1) * LDE + col] = -(sp.ampMult * v.y);
       }
     }
     cp_async_wait_prev();  // this item's slab (the group before the one just issued)
     __syncthreads();
     {
-      const double4* uv = UVs + buf * pairs;
-      double hr[RH][JB], hi[RH][JB];
+      const double* uvd = UVs + buf * n2 * uvLd;
+      double h[MB][8][2];
 #pragma unroll
-      for (int t = 0; t < RH; ++t)
+      for (int m = 0; m < MB; ++m)
 #pragma unroll
-        for (int j = 0; j < JB; ++j) hr[t][j] = hi[t][j] = 0.0;
-      const int i1b = RH * warp;
-      const double* e2 = E2T + lane;
-      for (int i2 = 0; i2 < n2; ++i2) {
-        double c[JB], sn[JB];
+        for (int nt = 0; nt < 8; ++nt) h[m][nt][0] = h[m][nt][1] = 0.0;
+      const int r0 = warp * (ROWS / 8);
+      for (int k0 = 0; k0 < K2; k0 += 4) {
+        double a[MB];
 #pragma unroll
-        for (int j = 0; j < JB; ++j) {
-          c[j] = e2[(2 * i2) * ROWS + 32 * j];
-          sn[j] = e2[(2 * i2 + 1) * ROWS + 32 * j];
-        }
+        for (int m = 0; m < MB; ++m) a[m] = E2T[(k0 + t) * LD + r0 + 8 * m + g];
+        const int i2 = (k0 >> 1) + (t >> 1);
 #pragma unroll
-        for (int t = 0; t < RH; ++t) {
-          const double4 u = (i1b + t < n1) ? uv[i2 * n1 + i1b + t] : make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int nt = 0; nt < 8; ++nt) {
+          if (nt >= NTB) break;
+          const int i1 = 4 * nt + (g >> 1);
+          const double b = (i2 < n2 && i1 < n1) ? bsign * uvd[i2 * uvLd + 4 * i1 + bcomp] : 0.0;
 #pragma unroll
-          for (int j = 0; j < JB; ++j) {
-            hr[t][j] = fma(u.x, c[j], hr[t][j]);
-            hr[t][j] = fma(-u.w, sn[j], hr[t][j]);
-            hi[t][j] = fma(u.y, c[j], hi[t][j]);
-            hi[t][j] = fma(u.z, sn[j], hi[t][j]);
-          }
+          for (int m = 0; m < MB; ++m) dmma(h[m][nt], a[m], b);
         }
       }
 #pragma unroll
-      for (int t = 0; t < RH; ++t) {
-        if (i1b + t >= n1) continue;
+      for (int nt = 0; nt < 8; ++nt) {
+        if (nt >= NTB) break;
 #pragma unroll
-        for (int j = 0; j < JB; ++j) {
-          HT[(2 * (i1b + t)) * ROWS + lane + 32 * j] = hr[t][j];
-          HT[(2 * (i1b + t) + 1) * ROWS + lane + 32 * j] = hi[t][j];
+        for (int i = 0; i < 2; ++i) {
+          const int col = 8 * nt + 2 * t + i;
+          if (col < 2 * n1) {
+#pragma unroll
+            for (int m = 0; m < MB; ++m) HT[col * LD + r0 + 8 * m + g] = h[m][nt][i];
+          }
         }
       }
     }
     __syncthreads();
-    double acc[RW][4];
+    const int wr = warp % WR, wc = warp / WR;
+    const int r0 = 32 * wr, c0 = wc * (128 / WC);
+    double acc[4][NTC][2];
 #pragma unroll
-    for (int i = 0; i < RW; ++i)
+    for (int m = 0; m < 4; ++m)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-    tile_fma_pairs<RW>(HT, ROWS, E1, K1, warp, lane, acc);
+      for (int nt = 0; nt < NTC; ++nt) acc[m][nt][0] = acc[m][nt][1] = 0.0;
+#pragma unroll 2
+    for (int k0 = 0; k0 < K1; k0 += 4) {
+      double a[4], b[NTC];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) a[m] = HT[(k0 + t) * LD + r0 + 8 * m + g];
+#pragma unroll
+      for (int nt = 0; nt < NTC; ++nt) b[nt] = E1[(k0 + t) * LDE + c0 + 8 * nt + g];
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int nt = 0; nt < NTC; ++nt) dmma(acc[m][nt], a[m], b[nt]);
+    }
     double* o = out + (int64_t)(sp.r0 + rl) * sp.n + j3 * (int64_t)N1 * N2;
 #pragma unroll
-    for (int i = 0; i < RW; ++i) {
-      const int64_t j2 = rb * ROWS + RW * warp + i;
+    for (int m = 0; m < 4; ++m) {
+      const int64_t j2 = rb * ROWS + r0 + 8 * m + g;
       if (j2 >= N2) continue;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int64_t j1 = cb * 128 + 64 * h + 2 * lane;
-        double v0 = acc[i][2 * h], v1 = acc[i][2 * h + 1];
+      for (int nt = 0; nt < NTC; ++nt) {
+        const int64_t j1 = cb * 128 + c0 + 8 * nt + 2 * t;
+        double v0 = acc[m][nt][0], v1 = acc[m][nt][1];
         if (sp.applyMarginal) {  // multiVariateTransformation, randomFieldND.f90:139-178
           v0 = v0 * sp.margSd + sp.margAvg;
           v1 = v1 * sp.margSd + sp.margAvg;
@@ -416,48 +434,38 @@ __global__ void __launch_bounds__(kSepThreads, 1) rf_sep_axes21(const SepSpec sp
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
-size_t axis3_smem(const SepSpec& sp) { return (size_t)2 * sp.kn[2] * (kLdT + 128) * sizeof(double); }
+size_t axis3_smem(const SepSpec& sp) {
+  return (size_t)((2 * sp.kn[2] + 3) & ~3) * (kRows + kPadLd + 128 + kPadLd) * sizeof(double);
+}
 size_t axes21_smem(const SepSpec& sp, int rows) {
-  const size_t pairs = (size_t)sp.kn[0] * sp.kn[1];
-  return ((size_t)2 * sp.kn[1] * rows + 8 * pairs + (size_t)2 * sp.kn[0] * (rows + 128)) * sizeof(double);
+  const size_t K1 = (size_t)(2 * sp.kn[0] + 3) & ~(size_t)3, K2 = (size_t)(2 * sp.kn[1] + 3) & ~(size_t)3;
+  const size_t slabs = (size_t)2 * sp.kn[1] * uv_row_stride(sp.kn[0]);
+  return (K2 * (rows + kPadLd) + slabs + K1 * (rows + kPadLd) + K1 * (128 + kPadLd)) * sizeof(double);
 }
 
-template <int RH, int ROWS>
+template <int ROWS>
 cudaError_t launch_axes21(const SepSpec& sp, const double2* E1, const double2* E2, const double4* UV, double* out,
                           int numSMs, cudaStream_t st) {
   const size_t smem = axes21_smem(sp, ROWS);
-  cudaError_t e = cudaFuncSetAttribute(rf_sep_axes21<RH, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(rf_sep_axes21<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int occ = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, rf_sep_axes21<RH, ROWS>, kSepThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, rf_sep_axes21<ROWS>, kSepThreads, smem);
   if (e != cudaSuccess) return e;
   if (occ < 1) return cudaErrorInvalidConfiguration;
   const int64_t items = ((sp.N[0] + 127) / 128) * ((sp.N[1] + ROWS - 1) / ROWS) * (int64_t)sp.nr * sp.N[2];
   const int grid = (int)std::min<int64_t>(items, (int64_t)occ * numSMs);
-  rf_sep_axes21<RH, ROWS><<<grid, kSepThreads, smem, st>>>(sp, E1, E2, UV, out);
+  rf_sep_axes21<ROWS><<<grid, kSepThreads, smem, st>>>(sp, E1, E2, UV, out);
   return cudaGetLastError();
 }
 
 // Rows per item: 128 where the row axis is longer than 64 and the tiles fit
 // shared memory (half the slab loads and syncs per field value), else 64.
-// i1 per warp in the axis-2 stage: 8 warps cover n1 <= 8 RH.
 constexpr size_t kMaxSmem = (size_t)227 * 1024;
-template <int ROWS>
-cudaError_t launch_axes21_rows(const SepSpec& sp, const double2* E1, const double2* E2, const double4* UV,
-                               double* out, int numSMs, cudaStream_t st) {
-  switch ((sp.kn[0] + 7) / 8) {
-    case 1: return launch_axes21<1, ROWS>(sp, E1, E2, UV, out, numSMs, st);
-    case 2: return launch_axes21<2, ROWS>(sp, E1, E2, UV, out, numSMs, st);
-    case 3: return launch_axes21<3, ROWS>(sp, E1, E2, UV, out, numSMs, st);
-    default: return launch_axes21<4, ROWS>(sp, E1, E2, UV, out, numSMs, st);
-  }
-}
 cudaError_t launch_axes21_any(const SepSpec& sp, const double2* E1, const double2* E2, const double4* UV,
                               double* out, int numSMs, cudaStream_t st) {
-  if (sp.N[1] > 64 && axes21_smem(sp, 128) <= kMaxSmem)
-    return launch_axes21_rows<128>(sp, E1, E2, UV, out, numSMs, st);
-  return launch_axes21_rows<64>(sp, E1, E2, UV, out, numSMs, st);
+  if (sp.N[1] > 64 && axes21_smem(sp, 128) <= kMaxSmem) return launch_axes21<128>(sp, E1, E2, UV, out, numSMs, st);
+  return launch_axes21<64>(sp, E1, E2, UV, out, numSMs, st);
 }
 
 }  // namespace
@@ -560,7 +568,7 @@ int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double
     first = false;
     const int64_t tiles3 = (int64_t)sp.nr * ((sp.N[2] + kRows - 1) / kRows) * ((pairs + 31) / 32);
     const int g3 = (int)std::min<int64_t>(tiles3, (int64_t)occ3 * ctx->numSMs);
-    rf_sep_axis3<<<g3, kSepThreads, sm3, st>>>(sp, E3, PQ, UV);
+    rf_sep_axis3<<<g3, kSepThreads, sm3, st>>>(sp, E3, PQ, reinterpret_cast<double*>(UV));
     RF_CUDA(cudaGetLastError(), "grid axis-3 kernel");
     RF_CUDA(launch_axes21_any(sp, E1, E2, UV, d_randField, ctx->numSMs, st), "grid axes-2/1 kernel");
     ctx->launches += 3;
