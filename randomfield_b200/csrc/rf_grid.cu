@@ -45,6 +45,7 @@ using namespace rfh;
 namespace {
 
 constexpr int kSepThreads = 256;
+constexpr int kAxesThreads = 512, kAxesWarps = kAxesThreads / 32;  // rf_sep_axes21
 constexpr int kRows = 64;     // rows of a tile
 constexpr int kMaxSepN = 32;  // wavenumbers per axis
 constexpr size_t kSepScratch = (size_t)512 << 20;  // P/Q and u/v of one realization block
@@ -276,16 +277,18 @@ __host__ __device__ inline int32_t uv_row_stride(int32_t n1) { return 4 * n1 + (
 //           ampMult (c1, -s1); warps in ROWS/32 x (256/ROWS) tiles of
 //           32 x (ROWS/2) ... then the marginal map and the store.
 template <int ROWS>
-__global__ void __launch_bounds__(kSepThreads, 1) rf_sep_axes21(const SepSpec sp, const double2* __restrict__ E1g,
+__global__ void __launch_bounds__(kAxesThreads, 1) rf_sep_axes21(const SepSpec sp, const double2* __restrict__ E1g,
                                                                 const double2* __restrict__ E2g,
                                                                 const double4* __restrict__ UV,
                                                                 double* __restrict__ out) {
   constexpr int LD = ROWS + kPadLd;       // E2T, HT row stride
   constexpr int LDE = 128 + kPadLd;       // E1 row stride
   constexpr int WR = ROWS / 32;           // axis-1 warp rows (32 field rows each)
-  constexpr int WC = 8 / WR;              // axis-1 warp columns
+  constexpr int WC = kAxesWarps / WR;     // axis-1 warp columns
   constexpr int NTC = 128 / WC / 8;       // axis-1 column tiles per warp
-  constexpr int MB = ROWS / 64;           // axis-2 row tiles per warp
+  constexpr int MT = ROWS / 8;            // axis-2 row tiles, one per warp ...
+  constexpr int WPM = kAxesWarps / MT;    // ... shared by WPM warps, which split the column tiles
+  constexpr int NJ = 8 / WPM;             // axis-2 column tiles per warp (at most 8 in all)
   extern __shared__ __align__(16) double sm[];
   const int32_t n1 = sp.kn[0], n2 = sp.kn[1], N1 = sp.N[0], N2 = sp.N[1], N3 = sp.N[2];
   const int K1 = (2 * n1 + 3) & ~3, K2 = (2 * n2 + 3) & ~3;  // padded k extents
@@ -307,7 +310,7 @@ __global__ void __launch_bounds__(kSepThreads, 1) rf_sep_axes21(const SepSpec sp
       const int64_t rl = (it % inner) / N3, j3 = it % N3;
       const double2* src = reinterpret_cast<const double2*>(UV + (rl * N3 + j3) * pairs);
       double* dst = UVs + buf * n2 * uvLd;
-      for (int e = threadIdx.x; e < 2 * pairs; e += kSepThreads) {
+      for (int e = threadIdx.x; e < 2 * pairs; e += kAxesThreads) {
         const int p = e >> 1, i2 = p / n1, i1 = p - i2 * n1;
         cp_async16(dst + i2 * uvLd + 4 * i1 + 2 * (e & 1), src + e);
       }
@@ -315,7 +318,7 @@ __global__ void __launch_bounds__(kSepThreads, 1) rf_sep_axes21(const SepSpec sp
     cp_async_commit();
   };
   // the padding rows of H (k >= 2 n1) are never written by the axis-2 stage
-  for (int e = threadIdx.x; e < (K1 - 2 * n1) * LD; e += kSepThreads) HT[2 * n1 * LD + e] = 0.0;
+  for (int e = threadIdx.x; e < (K1 - 2 * n1) * LD; e += kAxesThreads) HT[2 * n1 * LD + e] = 0.0;
   // axis-2 operand from the slab: this lane's k row and column are fixed
   // modulo the tile steps, so are the component and sign it reads
   const int bc = t & 1, bre = g & 1;
@@ -332,14 +335,14 @@ __global__ void __launch_bounds__(kSepThreads, 1) rf_sep_axes21(const SepSpec sp
     prefetch(it + gridDim.x, buf ^ 1);
     if (blk != curBlock) {
       curBlock = blk;
-      for (int e = threadIdx.x; e < K2 / 2 * ROWS; e += kSepThreads) {
+      for (int e = threadIdx.x; e < K2 / 2 * ROWS; e += kAxesThreads) {
         const int i2 = e / ROWS, row = e % ROWS;
         const int64_t j2 = rb * ROWS + row;
         const double2 v = (i2 < n2 && j2 < N2) ? E2g[(int64_t)i2 * N2 + j2] : make_double2(0.0, 0.0);
         E2T[(2 * i2) * LD + row] = v.x;
         E2T[(2 * i2 + 1) * LD + row] = v.y;
       }
-      for (int e = threadIdx.x; e < K1 / 2 * 128; e += kSepThreads) {
+      for (int e = threadIdx.x; e < K1 / 2 * 128; e += kAxesThreads) {
         const int i1 = e / 128, col = e % 128;
         const int64_t j1 = cb * 128 + col;
         const double2 v = (i1 < n1 && j1 < N1) ? E1g[(int64_t)i1 * N1 + j1] : make_double2(0.0, 0.0);
@@ -351,36 +354,30 @@ __global__ void __launch_bounds__(kSepThreads, 1) rf_sep_axes21(const SepSpec sp
     __syncthreads();
     {
       const double* uvd = UVs + buf * n2 * uvLd;
-      double h[MB][8][2];
+      double h[NJ][2];
 #pragma unroll
-      for (int m = 0; m < MB; ++m)
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) h[m][nt][0] = h[m][nt][1] = 0.0;
-      const int r0 = warp * (ROWS / 8);
+      for (int j = 0; j < NJ; ++j) h[j][0] = h[j][1] = 0.0;
+      const int r0 = 8 * (warp % MT), no = warp / MT;
       for (int k0 = 0; k0 < K2; k0 += 4) {
-        double a[MB];
-#pragma unroll
-        for (int m = 0; m < MB; ++m) a[m] = E2T[(k0 + t) * LD + r0 + 8 * m + g];
+        const double a = E2T[(k0 + t) * LD + r0 + g];
         const int i2 = (k0 >> 1) + (t >> 1);
 #pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
+        for (int j = 0; j < NJ; ++j) {
+          const int nt = no + WPM * j;
           if (nt >= NTB) break;
           const int i1 = 4 * nt + (g >> 1);
           const double b = (i2 < n2 && i1 < n1) ? bsign * uvd[i2 * uvLd + 4 * i1 + bcomp] : 0.0;
-#pragma unroll
-          for (int m = 0; m < MB; ++m) dmma(h[m][nt], a[m], b);
+          dmma(h[j], a, b);
         }
       }
 #pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
+      for (int j = 0; j < NJ; ++j) {
+        const int nt = no + WPM * j;
         if (nt >= NTB) break;
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
           const int col = 8 * nt + 2 * t + i;
-          if (col < 2 * n1) {
-#pragma unroll
-            for (int m = 0; m < MB; ++m) HT[col * LD + r0 + 8 * m + g] = h[m][nt][i];
-          }
+          if (col < 2 * n1) HT[col * LD + r0 + g] = h[j][i];
         }
       }
     }
@@ -450,12 +447,12 @@ cudaError_t launch_axes21(const SepSpec& sp, const double2* E1, const double2* E
   cudaError_t e = cudaFuncSetAttribute(rf_sep_axes21<ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int occ = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, rf_sep_axes21<ROWS>, kSepThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, rf_sep_axes21<ROWS>, kAxesThreads, smem);
   if (e != cudaSuccess) return e;
   if (occ < 1) return cudaErrorInvalidConfiguration;
   const int64_t items = ((sp.N[0] + 127) / 128) * ((sp.N[1] + ROWS - 1) / ROWS) * (int64_t)sp.nr * sp.N[2];
   const int grid = (int)std::min<int64_t>(items, (int64_t)occ * numSMs);
-  rf_sep_axes21<ROWS><<<grid, kSepThreads, smem, st>>>(sp, E1, E2, UV, out);
+  rf_sep_axes21<ROWS><<<grid, kAxesThreads, smem, st>>>(sp, E1, E2, UV, out);
   return cudaGetLastError();
 }
 
