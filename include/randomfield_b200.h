@@ -213,6 +213,17 @@ int rf_generate_fft_grid(rf_context* ctx, int nDim, const int64_t* xNStep, const
 int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double* xStep, const int64_t* xNStep,
                      int corrMod, int margiFirst, const double* corrL, double fieldAvg, double fieldVar, int Nmc,
                      int method, double* d_randField, const rf_options* opt, void* stream);
+/*
+ * Host-buffer form of rf_generate_grid, the structured counterpart of
+ * rf_create_standard_gaussian_field_unstruct for callers that would build
+ * xPoints with set_XPoints: randField is a host array of prod(xNStep) x Nmc
+ * doubles, column-major.  Runs on opt->device's default context and returns
+ * when randField is filled.
+ */
+int rf_create_standard_gaussian_field_grid(int nDim, const double* xMin, const double* xStep, const int64_t* xNStep,
+                                           int corrMod, int margiFirst, const double* corrL, double fieldAvg,
+                                           double fieldVar, int Nmc, int method, double* randField,
+                                           const rf_options* opt);
 
 /* Phase timers.  With timing enabled the context records CUDA events on the
  * launching stream around each phase of a generation; rf_context_last_times

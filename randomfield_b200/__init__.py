@@ -52,7 +52,7 @@ EXPORTS = [
     "rf_generate_batch", "rf_generate_batch_device", "rf_batch_last_stats",
     "rf_server_config_init", "rf_server_create", "rf_server_submit", "rf_server_wait", "rf_server_get_stats",
     "rf_server_destroy", "rf_server_submit_blended", "rf_context_selftest_timeout", "rf_measure_sfu_rate", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
-    "rf_field_statistics", "rf_generate_fft_grid", "rf_generate_grid",
+    "rf_field_statistics", "rf_generate_fft_grid", "rf_generate_grid", "rf_create_standard_gaussian_field_grid",
 ]
 
 
@@ -258,6 +258,8 @@ def lib() -> C.CDLL:
                                            P(Options)]
         L.rf_generate_grid.argtypes = [C.c_void_p, i32, P(d), P(d), P(i64), i32, i32, P(d), d, d, i32, i32,
                                        C.c_void_p, P(Options), C.c_void_p]
+        L.rf_create_standard_gaussian_field_grid.argtypes = [i32, P(d), P(d), P(i64), i32, i32, P(d), d, d, i32, i32,
+                                                             P(d), P(Options)]
         L.rf_field_statistics.argtypes = [C.c_void_p, C.c_void_p, i64, i32, i32, P(i64), P(d), P(d), P(d), P(d),
                                           P(d), P(FieldStats)]
         L.rf_blend_layout.argtypes = [P(BlendGrid), P(d), P(C.c_int32), P(C.c_int32)]
@@ -328,6 +330,34 @@ def create_standard_gaussian_field_unstruct(xPoints, corrMod, margiFirst, corrL,
     _check(lib().rf_create_standard_gaussian_field_unstruct(
         x.ctypes.data_as(P), nDim, n, cm, mf, cl.ctypes.data_as(P), float(fieldAvg), float(fieldVar), int(Nmc),
         int(method), randField.ctypes.data_as(P), C.byref(o)))
+    return randField
+
+
+def create_standard_gaussian_field_grid(xMin, xStep, xNStep, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc,
+                                        method=SHINOZUKA, randField=None, options=None, **kw):
+    """rf_create_standard_gaussian_field_grid: the Shinozuka field on the
+    structured grid xMin + j * xStep (xNStep points per axis, axis 1
+    fastest), evaluated axis by axis in FP64; returns randField
+    (prod(xNStep) x Nmc, Fortran-ordered), filled in place if given."""
+    nDim = len(xNStep)
+    a = np.ascontiguousarray(np.asarray(xMin, dtype=np.float64).reshape(-1))
+    h = np.ascontiguousarray(np.asarray(xStep, dtype=np.float64).reshape(-1))
+    g = np.ascontiguousarray(np.asarray(xNStep, dtype=np.int64).reshape(-1))
+    cl = np.ascontiguousarray(np.asarray(corrL, dtype=np.float64).reshape(-1))
+    if not (len(a) == len(h) == len(cl) == nDim):
+        raise RandomFieldError(-9, "xMin, xStep, xNStep and corrL need one entry per axis")
+    n = int(np.prod(g))
+    if randField is None:
+        randField = np.empty((n, int(Nmc)), dtype=np.float64, order="F")
+    elif (randField.dtype != np.float64 or not randField.flags.f_contiguous
+          or randField.shape != (n, int(Nmc))):
+        raise RandomFieldError(-9, "randField must be a Fortran-ordered float64 n x Nmc array")
+    o = _opts(options if options is not None else (kw or None))
+    P = C.POINTER(C.c_double)
+    _check(lib().rf_create_standard_gaussian_field_grid(
+        int(nDim), a.ctypes.data_as(P), h.ctypes.data_as(P), g.ctypes.data_as(C.POINTER(C.c_int64)),
+        _id(corrMod, _CORRMOD, "corrMod"), _id(margiFirst, _MARGI, "margiFirst"), cl.ctypes.data_as(P),
+        float(fieldAvg), float(fieldVar), int(Nmc), int(method), randField.ctypes.data_as(P), C.byref(o)))
     return randField
 
 

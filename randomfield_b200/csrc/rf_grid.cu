@@ -465,25 +465,23 @@ cudaError_t launch_axes21_any(const SepSpec& sp, const double2* E1, const double
   return launch_axes21<64>(sp, E1, E2, UV, out, numSMs, st);
 }
 
-}  // namespace
-
-extern "C" {
-
-int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double* xStep, const int64_t* xNStep,
-                     int corrMod, int margiFirst, const double* corrL, double fieldAvg, double fieldVar, int Nmc,
-                     int method, double* d_randField, const rf_options* opt, void* stream) {
-  g_err.clear();
-  if (!ctx || !xMin || !xStep || !xNStep || !corrL || !d_randField) return fail(RF_EINVAL_ARG, "null pointer argument");
+// Validation and the separable spec of a grid request (no device work).
+int grid_spec(int nDim, const double* xMin, const double* xStep, const int64_t* xNStep, int corrMod, int margiFirst,
+              const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method, const rf_options* opt,
+              SepSpec& sp, Plan& P, int& device) {
+  if (!xMin || !xStep || !xNStep || !corrL) return fail(RF_EINVAL_ARG, "null pointer argument");
   if (nDim < 1 || nDim > 3) return fail(RF_EINVAL_NDIM, "nDim must be 1, 2 or 3 (got %d)", nDim);
   int64_t n = 1;
   for (int d = 0; d < nDim; ++d) {
     if (xNStep[d] < 1 || xNStep[d] > (1 << 24))
       return fail(RF_EINVAL_ARG, "xNStep(%d) = %lld outside 1..2^24", d + 1, (long long)xNStep[d]);
-    if (xNStep[d] > 1 && !(xStep[d] > 0.0) ) return fail(RF_EINVAL_ARG, "xStep(%d) must be > 0", d + 1);
+    if (xNStep[d] > 1 && !(xStep[d] > 0.0)) return fail(RF_EINVAL_ARG, "xStep(%d) must be > 0", d + 1);
+    if (n > ((int64_t)1 << 40) / xNStep[d]) return fail(RF_EINVAL_ARG, "more than 2^40 grid points");
     n *= xNStep[d];
   }
   Request rq = make_request(nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
   if (int rc = validate(rq)) return rc;
+  device = rq.opt.device;
   if (method != RF_SHINOZUKA)
     return fail(RF_ENOTSUP, "the grid path sums the Shinozuka tensor-grid spectrum (method 2); methods 1 and 3 "
                             "run through rf_generate_device");
@@ -491,10 +489,8 @@ int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double
   // the extent the reference measures on the points: max - min of setGrid's coordinates
   double ext[3] = {0, 0, 0};
   for (int d = 0; d < nDim; ++d) ext[d] = (xMin[d] + xStep[d] * (double)(xNStep[d] - 1)) - xMin[d];
-  Plan P;
   rq.opt.precision = RF_PREC_FP32;  // the plan's operand layout is not used here
   if (int rc = build_plan(rq, ext, P)) return rc;
-  SepSpec sp;
   memset(&sp, 0, sizeof(sp));
   sp.nDim = nDim;
   for (int d = 0; d < 3; ++d) {
@@ -520,10 +516,12 @@ int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double
   sp.margAvg = P.margAvg;
   sp.lognormal = P.lognormal;
   sp.applyMarginal = P.applyMarginal;
+  return RF_OK;
+}
 
-  std::lock_guard<std::mutex> lk(ctx->mu);
-  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
-  cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
+// The kernels of a grid request on `st` (the caller holds the context's
+// lock and has made its device current).
+int grid_run(rf_context* ctx, SepSpec sp, const Plan& P, int Nmc, double* d_randField, cudaStream_t st) {
   ctx->launches = 0;
   ctx->evValid = false;
   const int64_t eCount = (int64_t)sp.kn[0] * sp.N[0] + (int64_t)sp.kn[1] * sp.N[1] + (int64_t)sp.kn[2] * sp.N[2];
@@ -582,6 +580,50 @@ int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double
     ctx->evValid = true;
   }
   return RF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double* xStep, const int64_t* xNStep,
+                     int corrMod, int margiFirst, const double* corrL, double fieldAvg, double fieldVar, int Nmc,
+                     int method, double* d_randField, const rf_options* opt, void* stream) {
+  g_err.clear();
+  if (!ctx || !d_randField) return fail(RF_EINVAL_ARG, "null pointer argument");
+  SepSpec sp;
+  Plan P;
+  int device = 0;
+  if (int rc = grid_spec(nDim, xMin, xStep, xNStep, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt,
+                         sp, P, device))
+    return rc;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  return grid_run(ctx, sp, P, Nmc, d_randField, stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream);
+}
+
+int rf_create_standard_gaussian_field_grid(int nDim, const double* xMin, const double* xStep, const int64_t* xNStep,
+                                           int corrMod, int margiFirst, const double* corrL, double fieldAvg,
+                                           double fieldVar, int Nmc, int method, double* randField,
+                                           const rf_options* opt) {
+  g_err.clear();
+  if (!randField) return fail(RF_EINVAL_ARG, "null pointer argument");
+  SepSpec sp;
+  Plan P;
+  int device = 0;
+  if (int rc = grid_spec(nDim, xMin, xStep, xNStep, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt,
+                         sp, P, device))
+    return rc;
+  rf_context* c = nullptr;
+  if (int rc = default_context(device, &c)) return rc;
+  std::lock_guard<std::mutex> lk(c->mu);
+  RF_CUDA(cudaSetDevice(c->device), "cudaSetDevice");
+  const size_t oBytes = sizeof(double) * (size_t)sp.n * (size_t)Nmc;
+  if (int rc = ensure(c->dOut, c->capOut, oBytes, "field")) return rc;
+  if (int rc = grid_run(c, sp, P, Nmc, c->dOut, c->stream)) return rc;
+  RF_CUDA(cudaMemcpyAsync(randField, c->dOut, oBytes, cudaMemcpyDeviceToHost, c->stream), "copy of randField");
+  RF_CUDA(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  return check_device_error(c);
 }
 
 }  // extern "C"

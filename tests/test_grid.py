@@ -183,3 +183,23 @@ def test_grid_refusals(ctx):
         with pytest.raises(rf.RandomFieldError) as e:
             call(**kw)
         assert e.value.code == code, kw
+
+
+@pytest.mark.gpu
+def test_grid_host_entry_point(ctx):
+    """rf_create_standard_gaussian_field_grid (host randField) equals the
+    device entry point, and refuses what the device entry point refuses."""
+    xMin, xStep, xNStep, corrL = (0.0, 0.5, -1.0), (0.1, 0.2, 0.05), (30, 20, 40), (1.0, 2.0, 0.5)
+    dev = _device(ctx, xMin, xStep, xNStep, corrL, 6, margiFirst=2, fieldAvg=1.0, fieldVar=0.25,
+                  k_nstep=(10, 9, 12), seed_start=3)
+    host = rf.create_standard_gaussian_field_grid(xMin, xStep, xNStep, 1, 2, corrL, 1.0, 0.25, 6,
+                                                  k_nstep=(10, 9, 12), seed_start=3)
+    assert host.shape == (30 * 20 * 40, 6) and host.flags.f_contiguous
+    np.testing.assert_array_equal(host.T, dev)
+    out = np.zeros((30 * 20 * 40, 6), order="F")
+    rf.create_standard_gaussian_field_grid(xMin, xStep, xNStep, 1, 2, corrL, 1.0, 0.25, 6, randField=out,
+                                           k_nstep=(10, 9, 12), seed_start=3)
+    np.testing.assert_array_equal(out, host)
+    with pytest.raises(rf.RandomFieldError) as e:
+        rf.create_standard_gaussian_field_grid(xMin, xStep, xNStep, 1, 1, corrL, 0.0, 1.0, 2, method=1)
+    assert e.value.code == -10
