@@ -44,7 +44,7 @@ module rf_gpu
     integer(c_int32_t) :: reserved(7)
   end type rf_options_t
 
-  public :: createStandardGaussianFieldUnstruct, rf_options_init
+  public :: createStandardGaussianFieldUnstruct, createStandardGaussianFieldGrid, rf_options_init
 
   interface
     subroutine rf_options_init(opt) bind(C, name="rf_options_init")
@@ -65,6 +65,21 @@ module rf_gpu
       real(c_double), intent(inout) :: randField(*)
       type(rf_options_t), intent(in) :: opt
     end function c_create
+
+    integer(c_int) function c_create_grid(nDim, xMin, xStep, xNStep, corrMod, margiFirst, corrL, fieldAvg, &
+                                          fieldVar, Nmc, method, randField, opt) &
+                                          bind(C, name="rf_create_standard_gaussian_field_grid")
+      import :: c_int, c_int64_t, c_double, rf_options_t
+      integer(c_int), value :: nDim
+      real(c_double), intent(in) :: xMin(*), xStep(*)
+      integer(c_int64_t), intent(in) :: xNStep(*)
+      integer(c_int), value :: corrMod, margiFirst
+      real(c_double), intent(in) :: corrL(*)
+      real(c_double), value :: fieldAvg, fieldVar
+      integer(c_int), value :: Nmc, method
+      real(c_double), intent(inout) :: randField(*)
+      type(rf_options_t), intent(in) :: opt
+    end function c_create_grid
 
     type(c_ptr) function c_last_error() bind(C, name="rf_last_error")
       import :: c_ptr
@@ -135,6 +150,82 @@ contains
       stop 1
     end if
   end subroutine createStandardGaussianFieldUnstruct
+
+  ! The same field on the structured grid xMin + j xStep (xNStep points per
+  ! axis, axis 1 fastest), i.e. on the points set_XPoints would build
+  ! (mesh_RF.f90:17-64), without building them: the sum runs axis by axis in
+  ! FP64 (rf_create_standard_gaussian_field_grid).  Method 2 only; randField
+  ! is (product(xNStep), Nmc).
+  subroutine createStandardGaussianFieldGrid(xMin, xStep, xNStep, corrMod, margiFirst, corrL, fieldAvg, fieldVar, &
+                                             Nmc, method, randField, seedStart, options, status)
+    double precision, intent(in) :: xMin(:), xStep(:)
+    integer, intent(in) :: xNStep(:)
+    character(len=*), intent(in) :: corrMod, margiFirst
+    double precision, intent(in) :: corrL(:)
+    double precision, intent(in) :: fieldAvg, fieldVar
+    integer, intent(in) :: Nmc, method
+    double precision, intent(inout) :: randField(:, :)
+    integer, intent(in), optional :: seedStart
+    type(rf_options_t), intent(in), optional :: options
+    integer, intent(out), optional :: status
+
+    type(rf_options_t) :: opt
+    integer(c_int) :: rc
+    integer(c_int64_t) :: nsteps(3)
+    integer :: d, nd
+
+    if (present(options)) then
+      opt = options
+    else
+      call rf_options_init(opt)
+    end if
+    if (present(seedStart)) opt%seed_start = int(seedStart, c_int64_t)
+    nd = size(xNStep)
+    nsteps = 1
+    do d = 1, min(nd, 3)
+      nsteps(d) = int(xNStep(d), c_int64_t)
+    end do
+
+    if (nd < 1 .or. nd > 3 .or. size(xMin) /= nd .or. size(xStep) /= nd .or. size(corrL) /= nd .or. &
+        size(randField, 1) /= product(nsteps) .or. size(randField, 2) /= Nmc) then
+      rc = -9  ! RF_EINVAL_ARG
+    else
+      rc = c_create_grid(int(nd, c_int), xMin, xStep, nsteps, corrmod_id(corrMod), margi_id(margiFirst), corrL, &
+                         real(fieldAvg, c_double), real(fieldVar, c_double), int(Nmc, c_int), int(method, c_int), &
+                         randField, opt)
+    end if
+
+    if (present(status)) then
+      status = int(rc)
+    else if (rc /= 0) then
+      write (*, *) "createStandardGaussianFieldGrid: error ", rc, " ", last_error()
+      stop 1
+    end if
+  end subroutine createStandardGaussianFieldGrid
+
+  integer(c_int) function corrmod_id(name)
+    character(len=*), intent(in) :: name
+    select case (trim(adjustl(name)))
+    case ("gaussian")
+      corrmod_id = RF_CM_GAUSSIAN
+    case ("cos")
+      corrmod_id = RF_CM_COS
+    case default
+      corrmod_id = -1
+    end select
+  end function corrmod_id
+
+  integer(c_int) function margi_id(name)
+    character(len=*), intent(in) :: name
+    select case (trim(adjustl(name)))
+    case ("gaussian")
+      margi_id = RF_FOM_GAUSSIAN
+    case ("lognormal")
+      margi_id = RF_FOM_LOGNORMAL
+    case default
+      margi_id = -1
+    end select
+  end function margi_id
 
   function last_error() result(msg)
     character(len=:), allocatable :: msg

@@ -32,6 +32,18 @@ def test_header_and_exports_agree():
         assert hasattr(L, s), s
 
 
+def test_fortran_module_binds_exported_symbols():
+    """Every bind(C) name of the Fortran module (except libc's strlen) is a
+    symbol the header declares and the library exports."""
+    f90 = os.path.join(os.path.dirname(HEADER), "..", "randomfield_b200", "fortran", "rf_gpu.f90")
+    names = set(re.findall(r'bind\(C,\s*name="([a-z_0-9]+)"\)', open(f90).read())) - {"strlen"}
+    assert "rf_create_standard_gaussian_field_grid" in names
+    assert names <= set(declared_symbols())
+    L = rf.lib()
+    for s in names:
+        assert hasattr(L, s), s
+
+
 def test_abi_version_and_option_defaults():
     assert rf.lib().rf_abi_version() == 1
     o = rf.Options()
@@ -144,6 +156,25 @@ def test_no_gpu_fails_loudly():
     x = grid(4, 0.5).T
     rc, msg = call(x)
     assert rc == -25 and "device" in msg
+    with pytest.raises(rf.RandomFieldError) as e:
+        rf.create_standard_gaussian_field_grid((0.0, 0.0, 0.0), (0.5, 0.5, 0.5), (4, 4, 4), 1, 1, (1.0, 1.0, 1.0),
+                                               0.0, 1.0, 2)
+    assert e.value.code == -25
+
+
+def test_grid_entry_validates_before_touching_a_device():
+    """The structured-grid entry point's argument checks are host-side."""
+    base = dict(xMin=(0.0, 0.0, 0.0), xStep=(0.1, 0.1, 0.1), xNStep=(8, 8, 8), corrMod=1, margiFirst=1,
+                corrL=(1.0, 1.0, 1.0), fieldAvg=0.0, fieldVar=1.0, Nmc=2)
+    for kw, code in ((dict(Nmc=0), -1), (dict(corrL=(1.0, -1.0, 1.0)), -3), (dict(method=5), -5),
+                     (dict(method=1), -10), (dict(xStep=(0.1, 0.0, 0.1)), -9), (dict(k_nstep=(33, 4, 4)), -10),
+                     (dict(margiFirst=2, fieldAvg=-1.0), -4)):
+        a = dict(base)
+        opts = {k: kw.pop(k) for k in list(kw) if k in ("k_nstep",)}
+        a.update(kw)
+        with pytest.raises(rf.RandomFieldError) as e:
+            rf.create_standard_gaussian_field_grid(**a, **opts)
+        assert e.value.code == code, kw
 
 
 def test_blend_layout_rounds_overlap_and_checks_the_split():
