@@ -459,6 +459,8 @@ def bench_serving(args, rf, torch, local, rate=SERVE_RATE, seconds=None):
     pending = []
     done_evt = threading.Event()
 
+    errors = []
+
     def waiter():
         while True:
             with lock:
@@ -469,7 +471,10 @@ def bench_serving(args, rf, torch, local, rate=SERVE_RATE, seconds=None):
                 time.sleep(0.0005)
                 continue
             t, k = item
-            srv.wait(t)
+            try:
+                srv.wait(t, timeout_s=120.0)
+            except rf.RandomFieldError as e:  # reported in the line; the client becomes idle again
+                errors.append(str(e))
             with lock:
                 busy[k] = False
 
@@ -486,7 +491,7 @@ def bench_serving(args, rf, torch, local, rate=SERVE_RATE, seconds=None):
         while time.perf_counter() - t0 < ta:
             time.sleep(0.0002)
         k = None
-        while k is None:
+        while k is None and time.perf_counter() - t0 < T + 120.0:
             with lock:
                 for j in range(len(pool)):
                     c = (nxt + j) % len(pool)
@@ -498,13 +503,15 @@ def bench_serving(args, rf, torch, local, rate=SERVE_RATE, seconds=None):
                 tb = time.perf_counter()
                 time.sleep(0.0005)
                 blocked_s += time.perf_counter() - tb
+        if k is None:  # no client came back within the deadline: stop offering
+            break
         nxt = k + 1
         t = pool[k]["submit"]()
         offered += pool[k]["values"]
         with lock:
             pending.append((t, k))
     done_evt.set()
-    th.join()
+    th.join(timeout=300.0)
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
@@ -518,6 +525,7 @@ def bench_serving(args, rf, torch, local, rate=SERVE_RATE, seconds=None):
             "offered_field_values_per_s": offered / T, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
             "max_ms": st["max_ms"], "batches": st["batches"] - base["batches"],
             "arrivals_delayed_s": blocked_s, "failed": st["failed"], "duration_s": wall,
+            "errors": errors[:3], "n_errors": len(errors),
             "latency": "submit -> field in the caller's page-locked buffer; statistics over the whole run "
                        "including the four warm-up requests"}
 
@@ -735,16 +743,25 @@ def main():
     del dx, dout, flush
     torch.cuda.empty_cache()
     batched = serving = configs = sgrid = None
+    def section(fn, *a, **kw):
+        """One optional part of the line; an error is reported in its place."""
+        try:
+            return fn(*a, **kw)
+        except Exception as e:  # noqa: BLE001 - the headline line must still be printed
+            return {"error": f"{type(e).__name__}: {e}"}
+
     if rank == 0 and world == 1 and not args.no_forms:
-        configs = bench_configs(args, rf, torch, local, sfu, peak)
+        configs = section(bench_configs, args, rf, torch, local, sfu, peak)
     if rank == 0 and world == 1 and not args.no_grid and GRID == (128, 128, 128):
-        sgrid = bench_grid(args, rf, torch, local)
+        sgrid = section(bench_grid, args, rf, torch, local)
     if rank == 0 and world == 1 and not args.no_batched and args.precision != "fp32":
-        batched = bench_batched(args, rf, torch, local)
+        batched = section(bench_batched, args, rf, torch, local)
     if rank == 0 and world == 1 and not args.no_serve and args.precision != "fp32":
-        serving = bench_serving(args, rf, torch, local)
+        serving = section(bench_serving, args, rf, torch, local)
         # the same loop at an arrival rate the device sustains, for the latency of an unsaturated loop
-        serving["at_sustainable_rate"] = bench_serving(args, rf, torch, local, rate=args.serve_low_rate, seconds=10.0)
+        if "error" not in serving:
+            serving["at_sustainable_rate"] = section(bench_serving, args, rf, torch, local,
+                                                     rate=args.serve_low_rate, seconds=10.0)
     if rank == 0:
         line = {
             "metric": "field values/s", "value": value, "unit": "field values/s", "n_gpus": world,
