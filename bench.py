@@ -530,6 +530,42 @@ def bench_serving(args, rf, torch, local, rate=SERVE_RATE, seconds=None):
                        "including the four warm-up requests"}
 
 
+def run_grid_case(args):
+    """The structured-grid path alone: Shinozuka on the --grid grid (spacing
+    0.05, corrL (2, 1, 0.5), 24^3 x 4 wavevectors, Nmc 64) through
+    rf_generate_grid; W untimed and K timed calls, device field."""
+    import torch
+
+    import randomfield_b200 as rf
+
+    torch.cuda.set_device(0)
+    n = int(np.prod(GRID))
+    ctx = rf.Context(0)
+    ctx.set_timing(True)
+    dout = torch.empty((NMC, n), dtype=torch.float64, device="cuda")
+
+    def call():
+        ctx.generate_grid(dout, (0.0, 0.0, 0.0), (SPACING,) * 3, GRID, 1, 1, CORRL, 0.0, 1.0, NMC,
+                          k_nstep=(KN, KN, KN))
+
+    for _ in range(args.warmup):
+        call()
+    ctx.synchronize()
+    kms = []
+    for _ in range(args.steps):
+        call()
+        t_tab, t_axes, _, _ = ctx.last_times()
+        kms.append(t_tab + t_axes)
+    ctx.synchronize()
+    if not torch.isfinite(dout).all().item():
+        raise RuntimeError("non-finite field values")
+    ms = float(np.mean(kms))
+    print(json.dumps({"case": "grid", "workload": f"shinozuka {GRID} grid, h {SPACING}, K {KN}^3 x 4, Nmc {NMC}",
+                      "ms_per_call": ms, "value": n * NMC / (ms / 1e3), "unit": "field values/s",
+                      "steps": args.steps, "warmup": args.warmup}))
+    ctx.close()
+
+
 def run_iso_case(args):
     """The isotropic request of config 2 alone (GEN_TABLE, BF16 unless
     --precision): n points U[0,10]^3, 64 x 64 wavevectors, lognormal avg 1
@@ -585,9 +621,10 @@ def main():
                     help="second serving run at this arrival rate (requests/s), below the device's capacity")
     ap.add_argument("--serve-seconds", type=float, default=20.0,
                     help="duration of the Poisson arrival stream (the serving config names 60 s)")
-    ap.add_argument("--case", default="headline", choices=["headline", "iso"],
-                    help="iso: only the isotropic request of config 2 (GEN_TABLE), on --points points, for "
-                         "profiler captures of that kernel; prints one JSON line of its own")
+    ap.add_argument("--case", default="headline", choices=["headline", "iso", "grid"],
+                    help="iso: only the isotropic request of config 2 (GEN_TABLE), on --points points; grid: only "
+                         "the structured-grid path (rf_generate_grid) on --grid; both for profiler captures of "
+                         "those kernels, each printing one JSON line of its own")
     ap.add_argument("--points", type=int, default=200000, help="points of the --case iso request")
     ap.add_argument("--grid", default="128,128,128",
                     help="grid points per axis; a smaller grid (e.g. 32,32,18 = one wave of 144 tiles) "
@@ -604,6 +641,9 @@ def main():
         return
     if args.case == "iso":
         run_iso_case(args)
+        return
+    if args.case == "grid":
+        run_grid_case(args)
         return
 
     import torch
