@@ -238,6 +238,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
     if (lane == 0) {
       uint32_t s = 0, ph = 0;
       uint32_t ktabSlots = 0;  // slots whose last copy carried a wavevector chunk
+      uint32_t kph = 0;        // per slot: parity of the kfull phase its next wavevector copy completes
       int64_t issued = 0;
       TileView v;
       for (int64_t i = 0; i < count && !*abort_flag; ++i) {
@@ -259,6 +260,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
             mbar_arrive_expect_tx(&bars->kfull[s], (uint32_t)kKtabStageBytes);
             bulk_g2s(sK + s * kKtabStageDoubles, v.ktab + ch * kKtabStageDoubles, kKtabStageBytes, &bars->kfull[s]);
             ktabSlots |= 1u << s;
+            kph ^= 1u << s;
           } else {
             ktabSlots &= ~(1u << s);
           }
@@ -276,7 +278,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
         for (int k = 0; k < S && issued > 0; ++k, --issued) {
           if (s == 0) { s = S; ph ^= 1; }
           --s;
-          if (ktabSlots & (1u << s)) mbar_wait(&bars->kfull[s], ph, &never);
+          if (ktabSlots & (1u << s)) mbar_wait(&bars->kfull[s], ((kph >> s) & 1u) ^ 1u, &never);
         }
         const uint64_t t0 = globaltimer_ns();
         while (globaltimer_ns() - t0 < 1000000ull) {
@@ -358,6 +360,10 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
     const int row = q * 32 + lane;
     const uint32_t laneOff = (uint32_t)(q * 32) << 16;
     uint32_t s = 0, ph = 0, accPh = 0;
+    // Per slot, the parity of the kfull phase the next wavevector chunk
+    // completes.  Only table stages arrive on kfull, so in a grouped launch
+    // whose tiles mix both generators this parity and the ring's differ.
+    uint32_t kph = 0;
     bool ok = true;
     TileView v;
     for (int64_t i = 0; i < count && ok; ++i) {
@@ -392,7 +398,10 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
         const uint32_t sc = s, phc = ph;
         if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
         bool wt = freeSeen || mbar_wait_warp(&bars->empty[sc], phc ^ 1, abort_flag);
-        if (kHasTable && !grid) wt = wt && mbar_wait_warp(&bars->kfull[sc], phc, abort_flag, true);
+        if (kHasTable && !grid) {
+          wt = wt && mbar_wait_warp(&bars->kfull[sc], (kph >> sc) & 1u, abort_flag, true);
+          kph ^= 1u << sc;
+        }
         if (!wt) { ok = false; break; }
         tc_fence_after();
         uint32_t probe = 0;
