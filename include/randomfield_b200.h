@@ -225,6 +225,29 @@ int rf_create_standard_gaussian_field_grid(int nDim, const double* xMin, const d
                                            double fieldVar, int Nmc, int method, double* randField,
                                            const rf_options* opt);
 
+/*
+ * Result files (writeResultFile_RF.f90: write_MONO_proc_result :737-829,
+ * write_XMF_Elements :835-938, write_HDF5_attributes :1758-1849).  Writes
+ * <folder>/h5/<fileName>.h5 with the dataset "samples": one realization
+ * (host array, axis 1 fastest) on the structured grid of
+ * nint((xMax - xMin)/xStep) + 1 points per axis, stored with the slowest axis
+ * first as the reference's files are; with `attr` non-NULL the run's
+ * parameters become attributes of the file's root group (integer scalars,
+ * and vectors of nDim entries).  For nDim 2 and 3 it also writes
+ * <folder>/xmf/<fileName>.xmf, the XDMF 2.0 description the reference writes
+ * (CoRectMesh, origin, step, node-centred scalar RF1 read from
+ * ../h5/<fileName>.h5:/samples).  The h5 and xmf folders are created when
+ * missing.  The HDF5 file is written without an HDF5 library, in the
+ * format's oldest layout (superblock version 0).  Host only: needs no GPU.
+ */
+typedef struct rf_result_attributes {
+  int32_t nb_procs, nDim, Nmc, method, seedStart, corrMod, margiFirst, localizationLevel;
+  int32_t kNStep[3], nFields[3];
+  double xMinGlob[3], xMaxGlob[3], xStep[3], corrL[3], overlap[3], procExtent[3], kMax_out[3];
+} rf_result_attributes;
+int rf_write_result_grid(const char* folder, const char* fileName, int nDim, const double* xMin, const double* xMax,
+                         const double* xStep, const double* field, const rf_result_attributes* attr);
+
 /* Phase timers.  With timing enabled the context records CUDA events on the
  * launching stream around each phase of a generation; rf_context_last_times
  * waits for the last one and returns the device milliseconds of the table

@@ -53,6 +53,7 @@ EXPORTS = [
     "rf_server_config_init", "rf_server_create", "rf_server_submit", "rf_server_wait", "rf_server_get_stats",
     "rf_server_destroy", "rf_server_submit_blended", "rf_context_selftest_timeout", "rf_measure_sfu_rate", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
     "rf_field_statistics", "rf_generate_fft_grid", "rf_generate_grid", "rf_create_standard_gaussian_field_grid",
+    "rf_write_result_grid",
 ]
 
 
@@ -258,6 +259,8 @@ def lib() -> C.CDLL:
                                            P(Options)]
         L.rf_generate_grid.argtypes = [C.c_void_p, i32, P(d), P(d), P(i64), i32, i32, P(d), d, d, i32, i32,
                                        C.c_void_p, P(Options), C.c_void_p]
+        L.rf_write_result_grid.argtypes = [C.c_char_p, C.c_char_p, i32, P(d), P(d), P(d), P(d),
+                                           C.POINTER(ResultAttributes)]
         L.rf_create_standard_gaussian_field_grid.argtypes = [i32, P(d), P(d), P(i64), i32, i32, P(d), d, d, i32, i32,
                                                              P(d), P(Options)]
         L.rf_field_statistics.argtypes = [C.c_void_p, C.c_void_p, i64, i32, i32, P(i64), P(d), P(d), P(d), P(d),
@@ -331,6 +334,53 @@ def create_standard_gaussian_field_unstruct(xPoints, corrMod, margiFirst, corrL,
         x.ctypes.data_as(P), nDim, n, cm, mf, cl.ctypes.data_as(P), float(fieldAvg), float(fieldVar), int(Nmc),
         int(method), randField.ctypes.data_as(P), C.byref(o)))
     return randField
+
+
+class ResultAttributes(C.Structure):
+    """rf_result_attributes: the run parameters written on a result file
+    (write_HDF5_attributes, writeResultFile_RF.f90:1758-1849)."""
+
+    _fields_ = [(nm, C.c_int32) for nm in ("nb_procs", "nDim", "Nmc", "method", "seedStart", "corrMod",
+                                           "margiFirst", "localizationLevel")] + [
+        ("kNStep", C.c_int32 * 3), ("nFields", C.c_int32 * 3)] + [
+        (nm, C.c_double * 3) for nm in ("xMinGlob", "xMaxGlob", "xStep", "corrL", "overlap", "procExtent",
+                                        "kMax_out")]
+
+    @classmethod
+    def make(cls, **kw) -> "ResultAttributes":
+        a = cls()
+        for k, v in kw.items():
+            f = getattr(a, k)
+            if isinstance(f, (int, float)):
+                setattr(a, k, v)
+            else:
+                for i, x in enumerate(v):
+                    f[i] = x
+        return a
+
+
+def write_result_grid(folder, fileName, xMin, xMax, xStep, field, attributes=None) -> None:
+    """rf_write_result_grid: <folder>/h5/<fileName>.h5 (dataset "samples",
+    one realization on the structured grid, attributes from a dict or a
+    ResultAttributes) and, in 2-D and 3-D, <folder>/xmf/<fileName>.xmf."""
+    nDim = len(xMin)
+    P = C.POINTER(C.c_double)
+    a = np.ascontiguousarray(np.asarray(xMin, dtype=np.float64).reshape(-1))
+    b = np.ascontiguousarray(np.asarray(xMax, dtype=np.float64).reshape(-1))
+    h = np.ascontiguousarray(np.asarray(xStep, dtype=np.float64).reshape(-1))
+    f = np.ascontiguousarray(np.asarray(field, dtype=np.float64).reshape(-1))
+    if np.all(h > 0):  # otherwise the library reports the bad step
+        n = 1
+        for d in range(nDim):
+            n *= int(round((b[d] - a[d]) / h[d])) + 1
+        if f.size != n:
+            raise RandomFieldError(-9, f"field has {f.size} values, the grid {n}")
+    at = attributes
+    if isinstance(at, dict):
+        at = ResultAttributes.make(**at)
+    _check(lib().rf_write_result_grid(str(folder).encode(), str(fileName).encode(), int(nDim), a.ctypes.data_as(P),
+                                      b.ctypes.data_as(P), h.ctypes.data_as(P), f.ctypes.data_as(P),
+                                      C.byref(at) if at is not None else None))
 
 
 def create_standard_gaussian_field_grid(xMin, xStep, xNStep, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc,
