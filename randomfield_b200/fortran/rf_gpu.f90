@@ -44,7 +44,17 @@ module rf_gpu
     integer(c_int32_t) :: reserved(7)
   end type rf_options_t
 
+  ! rf_result_attributes (include/randomfield_b200.h): write_HDF5_attributes' parameters
+  type, bind(C), public :: rf_result_attributes_t
+    integer(c_int32_t) :: nb_procs = 1, nDim = 0, Nmc = 0, method = 0, seedStart = 0, corrMod = 0, &
+                          margiFirst = 0, localizationLevel = 0
+    integer(c_int32_t) :: kNStep(3) = 0, nFields(3) = 1
+    real(c_double) :: xMinGlob(3) = 0d0, xMaxGlob(3) = 0d0, xStep(3) = 0d0, corrL(3) = 0d0, overlap(3) = 0d0, &
+                      procExtent(3) = 0d0, kMax_out(3) = 0d0
+  end type rf_result_attributes_t
+
   public :: createStandardGaussianFieldUnstruct, createStandardGaussianFieldGrid, rf_options_init
+  public :: writeResultGrid
 
   interface
     subroutine rf_options_init(opt) bind(C, name="rf_options_init")
@@ -80,6 +90,15 @@ module rf_gpu
       real(c_double), intent(inout) :: randField(*)
       type(rf_options_t), intent(in) :: opt
     end function c_create_grid
+
+    integer(c_int) function c_write_result_grid(folder, fileName, nDim, xMin, xMax, xStep, field, attr) &
+                                                bind(C, name="rf_write_result_grid")
+      import :: c_int, c_double, c_char, rf_result_attributes_t
+      character(kind=c_char), intent(in) :: folder(*), fileName(*)
+      integer(c_int), value :: nDim
+      real(c_double), intent(in) :: xMin(*), xMax(*), xStep(*), field(*)
+      type(rf_result_attributes_t), intent(in) :: attr
+    end function c_write_result_grid
 
     type(c_ptr) function c_last_error() bind(C, name="rf_last_error")
       import :: c_ptr
@@ -202,6 +221,25 @@ contains
       stop 1
     end if
   end subroutine createStandardGaussianFieldGrid
+
+  ! The result files of one realization, as write_MONO_proc_result writes
+  ! them (writeResultFile_RF.f90:737-829): <folder>/h5/<fileName>.h5 with
+  ! the dataset "samples" and the attributes, <folder>/xmf/<fileName>.xmf.
+  subroutine writeResultGrid(folder, fileName, xMin, xMax, xStep, field, attributes, status)
+    character(len=*), intent(in) :: folder, fileName
+    double precision, intent(in) :: xMin(:), xMax(:), xStep(:), field(:)
+    type(rf_result_attributes_t), intent(in) :: attributes
+    integer, intent(out), optional :: status
+    integer(c_int) :: rc
+    rc = c_write_result_grid(trim(folder)//c_null_char, trim(fileName)//c_null_char, int(size(xMin), c_int), &
+                             xMin, xMax, xStep, field, attributes)
+    if (present(status)) then
+      status = int(rc)
+    else if (rc /= 0) then
+      write (*, *) "writeResultGrid: error ", rc, " ", last_error()
+      stop 1
+    end if
+  end subroutine writeResultGrid
 
   integer(c_int) function corrmod_id(name)
     character(len=*), intent(in) :: name
