@@ -15,8 +15,8 @@
 // where the two signs of an axis share one cosine and one sine:
 // P = C(s3=+) + C(s3=-), Q = C(s3=+) - C(s3=-), u = G(s2=+) + G(s2=-),
 // v = G(s2=+) - G(s2=-).  Per realization that is
-//   4 n1 n2 n3 N3 + 4 n1 n2 N2 N3 + 2 n1 N1 N2 N3
-// FP64 multiply-adds instead of the reference's N1 N2 N3 x 4 n1 n2 n3 cosines
+//   8 n1 n2 n3 N3 + 4 n1 n2 N2 N3 + 2 n1 N1 N2 N3
+// FP64 multiply-adds (axis 3 for both sign rows of axis 2) instead of the reference's N1 N2 N3 x 4 n1 n2 n3 cosines
 // (128^3 points, 24^3 x 4 wavevectors: 1.5e8 instead of 1.2e11), so the
 // whole computation stays in FP64: the field equals the reference's sum to
 // FP64 rounding, with no reduced-precision operand anywhere.
