@@ -1,0 +1,108 @@
+"""The trig-tile generators' arithmetic (rf_gen.cuh), restated in numpy and
+checked against exact phases on the CPU:
+
+- the fixed-point phase of the table generator (table_pairs_fxp, tables
+  written by rf_tables.cu::table_element).  Per component x = A/4 + b with
+  integer A and |b| <= 1/8, k/2pi = C 2^-30 + e with integer C; the coarse
+  phase is the wrapped 32-bit integer dot product sum A_d C_d (units of
+  2^-32 turn) truncated to 2^-23 turn, the fine phase sum b_d k_d is FP32
+  (fused multiply-adds) with half a unit added so that the truncation
+  rounds.  For points with |x|_1 <= 128 correlation lengths the angle is
+  within 1e-6 rad of k.x modulo 2 pi and within [-1.51 pi, 1.51 pi] for the
+  isotropic wavevectors (|k| <= kMax = 7.355);
+- the FP64 reduction of the table generator's FAST form (table_pairs<true>);
+- the outer-phasor walk of GEN_GRID3 (Grid3Walk).
+float32 fused multiply-adds are emulated in float64 (exact products) with
+one final rounding.
+"""
+import numpy as np
+
+UNIT = np.float32(6.283185307179586) * np.float32(2.0 ** -23)  # radians per 2^-23 turn
+
+
+def fmaf(a, b, c):
+    return (a.astype(np.float64) * b.astype(np.float64) + c.astype(np.float64)).astype(np.float32)
+
+
+def fxp_angle(x, k):
+    """x: (n, 3) FP64 points; k: (m, 3) FP64 wavevectors -> (n, m) angles."""
+    t = k / 6.283185307179586  # turns, as the table builder writes them
+    C = np.rint(t * 2.0 ** 30).astype(np.int64).astype(np.uint32)
+    kf = k.astype(np.float32)
+    A = np.rint(x * 4.0)
+    b = (x - 0.25 * A).astype(np.float32)
+    A = A.astype(np.int64).astype(np.uint32)
+    P = np.zeros((x.shape[0], k.shape[0]), dtype=np.uint32)
+    s = np.full(P.shape, np.float32(0.5) * UNIT, dtype=np.float32)
+    for d in range(3):
+        P = P + A[:, d:d + 1] * C[None, :, d]  # uint32 arithmetic wraps
+        s = fmaf(b[:, d:d + 1], kf[None, :, d], s)
+    q = P.view(np.int32) >> 9
+    qf = q.astype(np.float32)  # |q| < 2^22: exact
+    return fmaf(qf, np.broadcast_to(UNIT, qf.shape), s)
+
+
+def test_fixed_point_phase_error_bound():
+    rs = np.random.RandomState(5)
+    n, m = 4000, 256
+    # points spread over |x|_1 <= 128, wavevectors |k| <= kMax (isotropic) and grid-like ones
+    x = rs.uniform(-1, 1, size=(n, 3))
+    x *= (128.0 * rs.uniform(0, 1, size=(n, 1)) ** 0.5) / np.abs(x).sum(axis=1, keepdims=True)
+    kdir = rs.normal(size=(m, 3))
+    k = kdir / np.linalg.norm(kdir, axis=1, keepdims=True) * rs.uniform(0, 7.355, size=(m, 1))
+    r = fxp_angle(x, k).astype(np.float64)
+    exact = (x.astype(np.longdouble) @ k.astype(np.longdouble).T)
+    two_pi = 2 * np.pi
+    d = np.asarray((r - exact) % two_pi, dtype=np.float64)
+    d = np.where(d > np.pi, d - two_pi, d)
+    assert np.abs(d).max() <= 1e-6
+    assert np.sqrt(np.mean(d ** 2)) <= 3e-7
+    assert np.abs(r).max() <= 1.51 * np.pi
+
+
+def test_fixed_point_phase_wraps_exactly_far_from_the_origin():
+    """The coarse term is exact modulo one turn at any magnitude: shifting a
+    point by a whole number of periods of every wavevector's grid leaves the
+    integer part's contribution unchanged modulo 2^32."""
+    k = np.array([[0.5, -1.25, 2.0], [7.0, 0.0, -3.5]])
+    x = np.array([[0.1, 0.2, -0.3], [60.0, -40.0, 27.75]])
+    r = fxp_angle(x, k).astype(np.float64)
+    exact = (x @ k.T) % (2 * np.pi)
+    d = (r - exact) % (2 * np.pi)
+    d = np.where(d > np.pi, d - 2 * np.pi, d)
+    assert np.abs(d).max() <= 1e-6
+
+
+def test_fast_fp64_reduction_of_the_table_phase():
+    """table_pairs<FAST>: the phase in turns plus 1.5 * 2^20 (+ half a unit of
+    2^-23) puts it on the FP64 grid of 2^-32 turn, so the sum's low word is
+    the phase modulo one turn in 32-bit fixed point; an arithmetic shift keeps
+    2^-23 turn.  The angle stays within 2^-24 turn of the FP64 phase (plus the
+    FP32 product's rounding) and inside [-pi, pi], for |x.k| < 2^18 turns."""
+    rs = np.random.RandomState(9)
+    th = np.concatenate([rs.uniform(-1, 1, 20000) * 2.0 ** e for e in (0, 4, 10, 17)])  # turns
+    shift = 1572864.0 + 2.0 ** -24
+    low = (np.asarray(th + shift, dtype=np.float64).view(np.uint64) & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+    q = low.view(np.int32) >> 9
+    r = q.astype(np.float32) * UNIT  # the float through 0x4B400000 + q equals q exactly
+    exact = 2 * np.pi * (th - np.rint(th))
+    d = r.astype(np.float64) - exact
+    d = (d + np.pi) % (2 * np.pi) - np.pi
+    assert np.abs(d).max() <= 2 * np.pi * 2.0 ** -24 + 4e-7
+    assert np.abs(r).max() <= np.pi * (1 + 2.0 ** -20)
+
+
+def test_grid3_outer_phasor_walk():
+    """GEN_GRID3's E1(i1) = E1(i1 - 1) E1(1) in FP32 complex products from
+    E1(0) = 1, restarted at every wrap (at most 31 products): relative error
+    below 4e-6 of the exact exp(i i1 k1 x1)."""
+    rs = np.random.RandomState(11)
+    theta = rs.uniform(-np.pi, np.pi, 5000)  # k1(1) x1 reduced, as axis_phasor returns it
+    c, s = np.cos(theta).astype(np.float32), np.sin(theta).astype(np.float32)
+    er, ei = np.ones_like(c), np.zeros_like(c)
+    worst = 0.0
+    for i in range(1, 32):
+        er, ei = er * c - ei * s, er * s + ei * c  # float32 arithmetic
+        ex = np.exp(1j * i * theta)
+        worst = max(worst, float(np.abs((er.astype(np.float64) + 1j * ei.astype(np.float64)) - ex).max()))
+    assert worst <= 4e-6
