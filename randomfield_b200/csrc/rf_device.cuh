@@ -66,14 +66,19 @@ __device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
 // Bounded wait for the phase of the given parity.  Returns false once the
 // wall-clock limit passes, or at once when *abort is already set.  A cheap
 // non-blocking probe first: most waits on the hot path find the phase done.
+// The limit counts as passed only when the SM's own cycle counter agrees
+// (at least limitNs / 2 cycles, i.e. the limit at an SM clock of 0.5 GHz or
+// more), so a step of the global timer alone cannot end a wait early.
 __device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, volatile int* abort, uint64_t limitNs) {
   if (mbar_test_wait(bar, parity)) return true;
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
+  const long long c0 = clock64();
+  const long long minCycles = (long long)(limitNs / 2);
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*abort) return false;
-    if (globaltimer_ns() - t0 > limitNs) return false;
+    if (globaltimer_ns() - t0 > limitNs && clock64() - c0 > minCycles) return false;
   }
 }
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
