@@ -17,6 +17,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librfo.so")
+# RFO_LIB names another build of the same library (the sanitizer build of
+# `make -C oracle sanitize`); it is loaded as it is, never rebuilt here.
+_LIB_OVERRIDE = os.environ.get("RFO_LIB")
 
 ISOTROPIC, SHINOZUKA, RANDOMIZATION = 1, 2, 3
 CM_GAUSSIAN, CM_COS = 1, 2
@@ -76,11 +79,14 @@ def build() -> None:
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(
-            os.path.join(HERE, "rf_oracle.c")
-        ):
-            build()
-        L = C.CDLL(LIB_PATH)
+        if _LIB_OVERRIDE:
+            L = C.CDLL(_LIB_OVERRIDE)
+        else:
+            if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(
+                os.path.join(HERE, "rf_oracle.c")
+            ):
+                build()
+            L = C.CDLL(LIB_PATH)
         P = C.POINTER
         d = C.c_double
         L.rfo_multmod.argtypes = [C.c_int32] * 3
