@@ -537,6 +537,7 @@ int rf_blend_layout(const rf_blend_grid* grid, const double* corrL, int32_t* sub
 int rf_generate_blended_device(rf_context* ctx, const rf_blend_grid* grid, int corrMod, int margiFirst,
                                const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method,
                                double* d_randField, const rf_options* opt, void* stream) {
+  rfh::NvtxRange nvtx_("rf_generate_blended_device");
   g_err.clear();
   if (!ctx || !grid || !corrL || !d_randField) return fail(RF_EINVAL_ARG, "null pointer argument");
   Request rq = make_request(grid->nDim, 1, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
@@ -551,6 +552,7 @@ int rf_generate_blended_device(rf_context* ctx, const rf_blend_grid* grid, int c
 int rf_generate_blended(rf_context* ctx, const rf_blend_grid* grid, int corrMod, int margiFirst, const double* corrL,
                         double fieldAvg, double fieldVar, int Nmc, int method, double* randField,
                         const rf_options* opt) {
+  rfh::NvtxRange nvtx_("rf_generate_blended");
   g_err.clear();
   if (!ctx || !grid || !corrL || !randField) return fail(RF_EINVAL_ARG, "null pointer argument");
   Request rq = make_request(grid->nDim, 1, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
@@ -570,6 +572,7 @@ int rf_generate_blended(rf_context* ctx, const rf_blend_grid* grid, int corrMod,
 }
 
 int rf_generate_batch(rf_context* ctx, const rf_request* reqs, int32_t count) {
+  rfh::NvtxRange nvtx_("rf_generate_batch");
   g_err.clear();
   if (!ctx) return fail(RF_EINVAL_ARG, "null context");
   std::vector<Request> rq;
@@ -634,6 +637,7 @@ int rf_generate_batch(rf_context* ctx, const rf_request* reqs, int32_t count) {
 }
 
 int rf_generate_batch_device(rf_context* ctx, const rf_request* reqs, int32_t count, void* stream) {
+  rfh::NvtxRange nvtx_("rf_generate_batch_device");
   g_err.clear();
   if (!ctx) return fail(RF_EINVAL_ARG, "null context");
   std::vector<Request> rq;

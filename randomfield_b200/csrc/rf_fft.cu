@@ -107,6 +107,7 @@ extern "C" {
 int rf_generate_fft_grid(rf_context* ctx, int nDim, const int64_t* xNStep, const double* xStep, int corrMod,
                          int margiFirst, const double* corrL, double fieldAvg, double fieldVar, int Nmc,
                          double* d_randField, const rf_options* opt) {
+  rfh::NvtxRange nvtx_("rf_generate_fft_grid");
   g_err.clear();
   if (!ctx || !xNStep || !xStep || !corrL || !d_randField) return fail(RF_EINVAL_ARG, "null pointer argument");
   if (nDim != 2 && nDim != 3)

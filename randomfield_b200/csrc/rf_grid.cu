@@ -589,6 +589,7 @@ extern "C" {
 int rf_generate_grid(rf_context* ctx, int nDim, const double* xMin, const double* xStep, const int64_t* xNStep,
                      int corrMod, int margiFirst, const double* corrL, double fieldAvg, double fieldVar, int Nmc,
                      int method, double* d_randField, const rf_options* opt, void* stream) {
+  rfh::NvtxRange nvtx_("rf_generate_grid");
   g_err.clear();
   if (!ctx || !d_randField) return fail(RF_EINVAL_ARG, "null pointer argument");
   SepSpec sp;
@@ -606,6 +607,7 @@ int rf_create_standard_gaussian_field_grid(int nDim, const double* xMin, const d
                                            int corrMod, int margiFirst, const double* corrL, double fieldAvg,
                                            double fieldVar, int Nmc, int method, double* randField,
                                            const rf_options* opt) {
+  rfh::NvtxRange nvtx_("rf_create_standard_gaussian_field_grid");
   g_err.clear();
   if (!randField) return fail(RF_EINVAL_ARG, "null pointer argument");
   SepSpec sp;

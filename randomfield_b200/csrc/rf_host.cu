@@ -753,6 +753,7 @@ int rf_context_last_times(rf_context* ctx, double* tables_ms, double* contract_m
 int rf_generate_device(rf_context* ctx, const double* d_xPoints, int nDim, int64_t n, int corrMod, int margiFirst,
                        const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method,
                        double* d_randField, const rf_options* opt, void* stream) {
+  rfh::NvtxRange nvtx_("rf_generate_device");
   g_err.clear();
   if (!ctx || !d_xPoints || !corrL || !d_randField) return fail(RF_EINVAL_ARG, "null pointer argument");
   Request rq = make_request(nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
@@ -776,6 +777,7 @@ int rf_create_standard_gaussian_field_unstruct(const double* xPoints, int nDim, 
                                                int margiFirst, const double* corrL, double fieldAvg,
                                                double fieldVar, int Nmc, int method, double* randField,
                                                const rf_options* opt) {
+  rfh::NvtxRange nvtx_("rf_create_standard_gaussian_field_unstruct");
   g_err.clear();
   if (!xPoints || !corrL || !randField) return fail(RF_EINVAL_ARG, "null pointer argument");
   Request rq = make_request(nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);

@@ -2,6 +2,7 @@
 // (rf_host.cu: single requests; rf_batch.cu: batches and the serving loop).
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <map>
 #include <mutex>
@@ -84,6 +85,15 @@ namespace rfh {
 extern thread_local std::string g_err;
 int fail(int code, const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* where);
+
+// NVTX range over a host entry point or phase, visible in Nsight Systems
+// timelines; without a tool attached the calls return at once.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 #define RF_CUDA(call, where)                                     \
   do {                                                           \

@@ -102,6 +102,7 @@ bool pinned(const void* p) {
 }
 
 int launch_slot(rf_server* s, Slot& sl) {
+  rfh::NvtxRange nvtx_("serving batch launch");
   rf_context* c = sl.ctx;
   cudaStream_t st = c->stream;
   RF_CUDA(cudaSetDevice(c->device), "cudaSetDevice");

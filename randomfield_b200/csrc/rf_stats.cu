@@ -146,6 +146,7 @@ extern "C" {
 int rf_field_statistics(rf_context* ctx, const double* d_randField, int64_t n, int Nmc, int nDim,
                         const int64_t* xNStep, const double* xStep, double* evnt_avg, double* evnt_std, double* sk,
                         double* corrL_out, rf_field_stats* out) {
+  rfh::NvtxRange nvtx_("rf_field_statistics");
   g_err.clear();
   if (!ctx || !d_randField) return fail(RF_EINVAL_ARG, "null pointer argument");
   if (n < 1) return fail(RF_EINVAL_ARG, "n must be >= 1 (got %lld)", (long long)n);
