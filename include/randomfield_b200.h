@@ -126,7 +126,9 @@ int rf_generate_device(rf_context* ctx, const double* d_xPoints, int nDim, int64
  * come before any stream capture on that device.  All calls share the array:
  * calls whose work overlaps on the GPU race, so serialise them.  Runs on
  * opt->device on `stream` (0 = legacy default) and returns when the field is
- * complete; allocates nothing (no cudaMalloc, cudaFree or context).
+ * complete: it synchronises `stream` before returning (and once more after
+ * the extent pass when the point extent is needed).  Allocates nothing (no
+ * cudaMalloc, cudaFree or context).
  */
 int rf_generate_device_noalloc(const double* d_xPoints, int nDim, int64_t n, int corrMod, int margiFirst,
                                const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method,
@@ -145,6 +147,21 @@ int rf_context_selftest_timeout(rf_context* ctx, double limit_ms);
 /* Measured MUFU (sin, cos) pair rate of the device: the SFU bound of the
  * GEN_TABLE generator (one pair per point and wavevector). */
 int rf_measure_sfu_rate(int device, double* pairs_per_second);
+
+/*
+ * Debug export of the device table builder's rnglib draws (the random_number
+ * calls of randomFieldND.f90:278 and :460-468, drawn from rnglib generator 1,
+ * RANDLIB/rnglib.f90:548-659), for a bit-exact comparison with a sequential
+ * rnglib run.  The request is described without points: opt->k_nstep (or
+ * opt->iso_n_radial) or opt->x_range must fix the wavevector count.  Writes
+ * *K_out = K; with draws non-NULL also draws[(r * K + k) * D + j], the i4_uni
+ * values the builder consumed for realization r and wavevector k in
+ * reference order (D = 1: the phase; isotropic D = 2: gamma, psi), and for
+ * the isotropic method k_draws[2 k + j] (theta, then phi in 3-D; 0 in 2-D).
+ * Uses the same realization blocks as a generation with opt->precision.
+ */
+int rf_debug_table_draws(int nDim, int method, int Nmc, const rf_options* opt, int64_t* K_out, int32_t* draws,
+                         int64_t draws_capacity, int32_t* k_draws, int64_t k_capacity);
 
 /*
  * Field statistics on the device (statistics_RF.f90), for a field already in

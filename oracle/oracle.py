@@ -99,6 +99,8 @@ def lib() -> C.CDLL:
         L.rfo_rng_cgn_set.argtypes = [P(RNG), C.c_int32]
         L.rfo_rng_i4_uni.argtypes = [P(RNG)]
         L.rfo_rng_i4_uni.restype = C.c_int32
+        L.rfo_rng_i4_stream.argtypes = [P(RNG), C.c_int64, P(C.c_int32)]
+        L.rfo_rng_i4_stream.restype = None
         L.rfo_rng_r8_uni_01.argtypes = [P(RNG)]
         L.rfo_rng_r8_uni_01.restype = d
         L.rfo_geometry_of.argtypes = [P(Request), P(Geometry)]
@@ -212,6 +214,15 @@ def rng(seedStart=None) -> RNG:
         if lib().rfo_rng_seed(C.byref(r), seedStart):
             raise ValueError(seedStart)
     return r
+
+
+def i4_stream(seedStart, count):
+    """The first `count` i4_uni values of generator 1 seeded from seedStart,
+    drawn one call after another (rnglib.f90:548-659)."""
+    r = rng(seedStart)
+    out = np.zeros(int(count), dtype=np.int32)
+    lib().rfo_rng_i4_stream(C.byref(r), int(count), out.ctypes.data_as(C.POINTER(C.c_int32)))
+    return out
 
 
 def grid(xMin, xStep, xNStep):
@@ -333,3 +344,42 @@ def fft_method_field(xNStep, xStep, corrL, seedStart, corrMod=CM_GAUSSIAN):
     Y = sfft.dctn(X.reshape(tuple(reversed(n))), type=3, norm=None)
     scale = (2.0 if nd == 3 else 1.0) * np.sqrt(np.prod(h))
     return Y.reshape(-1) * scale
+
+
+def separable_field(xMin, xStep, xNStep, corrL, Nmc, kNStep=(0, 0, 0), seedStart=0, corrMod=CM_GAUSSIAN):
+    """The Shinozuka field on the structured grid xMin + j xStep (axis 1
+    fastest) from the oracle's own wavevectors and phases, evaluated axis by
+    axis with complex matrix products (FP64): the whole field of a large grid
+    in seconds, for full-field comparisons.  Returns [r, i] before the
+    marginal map.  Pinned against the oracle's point-by-point sum in
+    tests/test_full_field.py.  Test infrastructure: the checker of the
+    whole-field comparisons, never the thing measured."""
+    nd = len(xNStep)
+    xr = tuple((xNStep[d] - 1) * xStep[d] for d in range(nd))
+    req = OracleRequest(np.asarray(xMin, dtype=np.float64).reshape(1, nd), corrL=corrL, Nmc=Nmc, kNStep=kNStep,
+                        seedStart=seedStart, corrMod=corrMod, xRange=xr)
+    g = req.geometry()
+    Bc, Bs = req.phase_matrix()  # [r, k]: a cos(phi), -a sin(phi)
+    R = Nmc
+    kn = [g.kNStep[d] if d < nd else 1 for d in range(3)]
+    S2 = 2 if nd >= 2 else 1
+    S3 = 2 if nd == 3 else 1
+    N = [xNStep[d] if d < nd else 1 for d in range(3)]
+    C = (Bc - 1j * Bs).reshape(R, S2, S3, kn[2], kn[1] * kn[0])  # k = q kn + i1 + n1 (i2 + n2 i3), q = s2 S3 + s3
+    E = []
+    for d in range(3):
+        if d < nd:
+            xd = (xMin[d] + xStep[d] * np.arange(N[d])) / corrL[d]
+            E.append(np.exp(1j * np.outer(g.kDelta[d] * np.arange(kn[d]), xd)))  # [i, j]
+        else:
+            E.append(np.ones((1, 1), dtype=complex))
+    G = np.matmul(E[2].T, C[:, :, 0])  # (R, S2, N3, k2 k1)
+    if S3 == 2:
+        G = G + np.matmul(np.conj(E[2]).T, C[:, :, 1])
+    G = G.reshape(R, S2, N[2], kn[1], kn[0]).transpose(0, 1, 2, 4, 3)  # (R, S2, N3, k1, k2)
+    H = np.matmul(G[:, 0], E[1])  # (R, N3, k1, N2)
+    if S2 == 2:
+        H = H + np.matmul(G[:, 1], np.conj(E[1]))
+    H = H.transpose(0, 1, 3, 2)  # (R, N3, N2, k1)
+    f = np.matmul(H.real, E[0].real) - np.matmul(H.imag, E[0].imag)  # (R, N3, N2, N1)
+    return g.ampMult * f.reshape(R, -1)

@@ -145,6 +145,10 @@ int32_t rfo_rng_i4_uni(rfo_rnglib* r) {
   return z;
 }
 
+void rfo_rng_i4_stream(rfo_rnglib* r, int64_t count, int32_t* out) {
+  for (int64_t i = 0; i < count; ++i) out[i] = rfo_rng_i4_uni(r);
+}
+
 /* rnglib.f90:1459-1520 */
 double rfo_rng_r8_uni_01(rfo_rnglib* r) {
   int32_t i = rfo_rng_i4_uni(r);

@@ -58,6 +58,8 @@ void    rfo_rng_advance_state(rfo_rnglib* r, int32_t k);         /* rnglib.f90:3
 void    rfo_rng_cgn_set(rfo_rnglib* r, int32_t g);               /* rnglib.f90:457-489   */
 int32_t rfo_rng_i4_uni(rfo_rnglib* r);                           /* rnglib.f90:548-659   */
 double  rfo_rng_r8_uni_01(rfo_rnglib* r);                        /* rnglib.f90:1459-1520 */
+/* `count` successive i4_uni calls into out[0..count) (the sequential stream). */
+void    rfo_rng_i4_stream(rfo_rnglib* r, int64_t count, int32_t* out);
 /* Seed words from seedStart, after math_RF.f90:561 (72 + 18*seedStart + 37*(i-1)). */
 void    rfo_seed_words(int64_t seedStart, int32_t* ig1, int32_t* ig2);
 /* initialize + set_initial_seed(seed words); generator 1 current. */

@@ -53,7 +53,7 @@ EXPORTS = [
     "rf_server_config_init", "rf_server_create", "rf_server_submit", "rf_server_wait", "rf_server_get_stats",
     "rf_server_destroy", "rf_server_submit_blended", "rf_context_selftest_timeout", "rf_measure_sfu_rate", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
     "rf_field_statistics", "rf_generate_fft_grid", "rf_generate_grid", "rf_create_standard_gaussian_field_grid",
-    "rf_write_result_grid",
+    "rf_write_result_grid", "rf_debug_table_draws",
 ]
 
 
@@ -255,6 +255,7 @@ def lib() -> C.CDLL:
         L.rf_server_destroy.argtypes = [C.c_void_p]
         L.rf_context_selftest_timeout.argtypes = [C.c_void_p, d]
         L.rf_measure_sfu_rate.argtypes = [i32, P(d)]
+        L.rf_debug_table_draws.argtypes = [i32, i32, i32, P(Options), P(i64), P(i32), i64, P(i32), i64]
         L.rf_generate_fft_grid.argtypes = [C.c_void_p, i32, P(i64), P(d), i32, i32, P(d), d, d, i32, C.c_void_p,
                                            P(Options)]
         L.rf_generate_grid.argtypes = [C.c_void_p, i32, P(d), P(d), P(i64), i32, i32, P(d), d, d, i32, i32,
@@ -448,6 +449,28 @@ def measure_sfu_rate(device: int = 0) -> float:
     v = C.c_double()
     _check(lib().rf_measure_sfu_rate(int(device), C.byref(v)))
     return v.value
+
+
+def debug_table_draws(nDim, method, Nmc, options=None, **kw):
+    """rf_debug_table_draws: the i4_uni draws the device table builder
+    consumes, in reference order.  Returns (draws, k_draws): draws is
+    [Nmc, K] (the phase draw) or [Nmc, K, 2] for the isotropic method (gamma,
+    psi); k_draws is [K, 2] (theta, phi) for the isotropic method, else None.
+    The options must fix the wavevector count (k_nstep / iso_n_radial, or
+    x_range)."""
+    o = _opts(options if options is not None else (kw or None))
+    K = C.c_int64()
+    _check(lib().rf_debug_table_draws(int(nDim), int(method), int(Nmc), C.byref(o), C.byref(K), None, 0, None, 0))
+    D = 2 if int(method) == ISOTROPIC else 1
+    draws = np.zeros(int(Nmc) * K.value * D, dtype=np.int32)
+    kd = np.zeros(2 * K.value, dtype=np.int32) if int(method) == ISOTROPIC else None
+    P32 = C.POINTER(C.c_int32)
+    _check(lib().rf_debug_table_draws(int(nDim), int(method), int(Nmc), C.byref(o), C.byref(K),
+                                      draws.ctypes.data_as(P32), draws.size,
+                                      kd.ctypes.data_as(P32) if kd is not None else None,
+                                      kd.size if kd is not None else 0))
+    shape = (int(Nmc), K.value, 2) if D == 2 else (int(Nmc), K.value)
+    return draws.reshape(shape), (kd.reshape(K.value, 2) if kd is not None else None)
 
 
 def make_request(xPoints, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, randField,

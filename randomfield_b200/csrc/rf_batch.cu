@@ -130,7 +130,7 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
       g.x = B.dx[i];
       g.out = B.dout[i];
       subs.push_back(g);
-      elems.push_back(P.nChunks * P.chunkK * P.nmcPad);
+      elems.push_back(table_threads(P));
       tiles.push_back((P.n + kTileM - 1) / kTileM);
       tileCost.push_back((double)P.nChunks * stage_cost(P));
       maxBRows = std::max(maxBRows, P.bRows);

@@ -422,6 +422,76 @@ void lo_layout(Plan& P) {
   P.loSkip = 1;
 }
 
+// GEN_OUTER (rf_outer.cu) for single 3-D Shinozuka requests on the 16-bit
+// tensor-core forms: the same sum as GEN_GRID3 with the outer phasors as the
+// generated operand.  Its BF16 form splits both operands into hi and lo
+// terms where they matter: a 16-bit rounding of either operand leaves a
+// relative error of about 1.3e-3 in the field, in proportion to the share of
+// the field's variance the rounded terms carry.  The K-steps (8 outer groups
+// each) are ranked by that share (sum of S1(k1) S2(k2) over the K-step's
+// groups; the axis-3 factor is common), and the top ones keep a lo term:
+// A's on those carrying all but kOuterALoLeft of the variance, B's on those
+// carrying all but kOuterBLoLeft.  An A lo term costs one more MMA per tile
+// and K-step and no operand bytes; a B lo term one more MMA per tile and a
+// second B block.
+constexpr double kOuterALoLeft = 0.10;
+constexpr double kOuterBLoLeft = 0.20;
+
+void outer_layout(Plan& P) {
+  if (P.gen != GEN_GRID3 || P.blend || P.literal) return;
+  if (P.prec != PREC_BF16 && P.prec != PREC_FP16 && P.prec != PREC_BF16_FAST) return;
+  if (P.kNStep[0] > kOuterMaxN1P || P.lPad > 32) return;
+  const int32_t n1 = P.kNStep[0], n2 = P.kNStep[1];
+  const int32_t n1p = (int32_t)round_up(n1, 8);
+  const int32_t nK = (n1p / 8) * n2 * 2;
+  if (nK > kOuterMaxKsteps) return;
+  P.gen = GEN_OUTER;
+  P.n1p = n1p;
+  P.oNK = nK;
+  P.oRc = std::min<int32_t>(P.nmcBlk, 256 / (2 * P.lPad));
+  P.oNR = (P.nmcBlk + P.oRc - 1) / P.oRc;
+  P.oKstepBytes = (int64_t)16 * (2 * P.lPad * P.oRc) * 2;
+  memset(P.loMask, 0, sizeof(P.loMask));
+  memset(P.aLoMask, 0, sizeof(P.aLoMask));
+  P.loSkip = 1;  // B lo blocks only where loMask says
+  if (P.prec == PREC_BF16) {
+    std::vector<std::pair<double, int32_t>> E((size_t)nK);
+    double total = 0.0;
+    for (int32_t j = 0; j < nK; ++j) {
+      const int32_t jj = j % (n1p / 8), i2 = (j / (n1p / 8)) % n2;
+      double w = 0.0;
+      for (int32_t i1 = 8 * jj; i1 < std::min(n1, 8 * jj + 8); ++i1) {
+        if (P.corrMod != RF_CM_GAUSSIAN) {
+          w += 1.0;  // cm_COS: no ranking, every K-step keeps both lo terms
+          continue;
+        }
+        const double k1 = P.kDelta[0] * i1, k2 = P.kDelta[1] * i2;
+        w += std::exp(-(k1 * k1) / (4.0 * kRefPi)) * std::exp(-(k2 * k2) / (4.0 * kRefPi));
+      }
+      E[(size_t)j] = {w, j};
+      total += w;
+    }
+    std::sort(E.begin(), E.end(), [](const std::pair<double, int32_t>& a, const std::pair<double, int32_t>& b) {
+      return a.first > b.first || (a.first == b.first && a.second < b.second);
+    });
+    const bool all = P.corrMod != RF_CM_GAUSSIAN;
+    double covered = 0.0;
+    for (const auto& e : E) {
+      const int32_t j = e.second;
+      if (all || covered < (1.0 - kOuterALoLeft) * total) P.aLoMask[j >> 5] |= 1u << (j & 31);
+      if (all || covered < (1.0 - kOuterBLoLeft) * total) P.loMask[j >> 5] |= 1u << (j & 31);
+      covered += e.first;
+    }
+  }
+  P.oChunkBytes = (int64_t)(nK + mask_rank(P.loMask, nK)) * P.oKstepBytes;
+  // FP16: B holds sums of two amplitudes (|W| <= 2), scaled so that the
+  // largest sits near 2^15
+  if (P.prec == PREC_FP16) {
+    P.bScaleLog2 = 14;
+    P.outScale = P.ampMult * std::ldexp(1.0, -P.bScaleLog2);
+  }
+}
+
 // Realizations per launch: one MMA holds at most 256 accumulator columns,
 // and the hi/lo form uses two per realization.
 int32_t realization_block(const Plan& P) {
@@ -446,6 +516,7 @@ int run_plan(rf_context* c, const Plan& P0, const double* dX, double* dOut, cuda
     P.nmcBlk = std::min(blk, P0.Nmc - r0);
     if (int rc = layout(P)) return rc;
     lo_layout(P);
+    outer_layout(P);
     if (int rc = run_block(c, P, dX, dOut, st)) return rc;
   }
   if (c->timing) RF_CUDA(cudaEventRecord(c->ev[2], st), "cudaEventRecord");
@@ -463,7 +534,7 @@ int run_plan(rf_context* c, const Plan& P0, const double* dX, double* dOut, cuda
 }
 
 int run_block(rf_context* c, const Plan& P, const double* dX, double* dOut, cudaStream_t st) {
-  const size_t bBytes = (size_t)P.nChunks * P.stageBytes;
+  const size_t bBytes = (size_t)operand_bytes(P);
   if (int rc = ensure(c->dB, c->capB, bBytes, "contraction operand")) return rc;
   double* ktab = nullptr;
   if (P.gen == GEN_TABLE) {
@@ -517,6 +588,7 @@ int run_plan_slabs(rf_context* c, const Plan& P0, double* dX, double* dOut, doub
   P.nmcBlk = P0.Nmc;
   if (int rc = layout(P)) return rc;
   lo_layout(P);
+  outer_layout(P);
   if (tc_smem_bytes(P, nullptr) == 0)
     return fail(RF_ENOTSUP, "stage too large for shared memory (Nmc or wavenumbers per axis too large)");
   if (!c->copyStream) RF_CUDA(cudaStreamCreateWithFlags(&c->copyStream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -525,7 +597,7 @@ int run_plan_slabs(rf_context* c, const Plan& P0, double* dX, double* dOut, doub
     if (!e) RF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
   for (auto& e : c->h2dEv)
     if (!e) RF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
-  if (int rc = ensure(c->dB, c->capB, (size_t)P.nChunks * P.stageBytes, "contraction operand")) return rc;
+  if (int rc = ensure(c->dB, c->capB, (size_t)operand_bytes(P), "contraction operand")) return rc;
   double* ktab = nullptr;
   if (P.gen == GEN_TABLE) {
     if (int rc = ensure(c->dKtab, c->capK, (size_t)P.nChunks * kKtabStageBytes, "wavevector table")) return rc;
@@ -634,7 +706,7 @@ int host_validate(int nDim, int64_t n, int corrMod, int margiFirst, const double
   Request rq = make_request(nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
   if (int rc = validate(rq)) return rc;
   bool need = false;
-  for (int d = 0; d < nDim; ++d) need = need || !(rq.opt.x_range[d] > 0.0);
+  for (int d = 0; d < nDim; ++d) need = need || (!(rq.opt.x_range[d] > 0.0) && extent_needed(rq, d));
   if (needExtent) *needExtent = need;
   return RF_OK;
 }
@@ -645,10 +717,14 @@ int host_build_plan(int nDim, int64_t n, int corrMod, int margiFirst, const doub
   return build_plan(rq, ext, *P);
 }
 
+// The same block layout as run_plan: stage layout, then the hi-only stages.
 int host_block_layout(Plan* P, int32_t rOff, int32_t nmcBlk) {
   P->rOff = rOff;
   P->nmcBlk = nmcBlk;
-  return layout(*P);
+  if (int rc = layout(*P)) return rc;
+  lo_layout(*P);
+  outer_layout(*P);
+  return RF_OK;
 }
 
 int32_t host_realization_block(const Plan& P) { return realization_block(P); }

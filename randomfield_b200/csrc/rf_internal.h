@@ -119,7 +119,10 @@ int layout(rfb::Plan& P);
 int build_plan(const Request& rq, const double* ext, rfb::Plan& P);
 int seeds(int64_t seedStart, rfb::Plan& P);
 // BF16 GEN_GRID3 plans: the stages that keep only the hi term (rf_host.cu)
-void lo_layout(rfb::Plan& P);  // rnglib seed words of seed_start (< 0: from the clock)
+void lo_layout(rfb::Plan& P);
+// Single-request 3-D Shinozuka plans on the 16-bit tensor-core forms: the
+// outer-group contraction (rf_outer.cu) and its lo masks (rf_host.cu)
+void outer_layout(rfb::Plan& P);
 int32_t realization_block(const rfb::Plan& P);
 int device_extent(rf_context* c, const double* dX, int nDim, int64_t n, cudaStream_t st, double* ext);
 int run_plan(rf_context* c, const rfb::Plan& P0, const double* dX, double* dOut, cudaStream_t st);

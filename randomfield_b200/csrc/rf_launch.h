@@ -15,9 +15,22 @@ struct JumpTable;
 cudaError_t launch_tables(const Plan& P, const JumpTable& jt, void* dB, double* dKtab, int64_t literalSlab,
                           int64_t nSlab, cudaStream_t st);
 
+// The i4_uni draws the table builder consumes for this plan's realization
+// block, in reference order: dRk[(r * K + k) * D + j] (D = 2 isotropic:
+// gamma, psi; else 1: the phase), dK[2 k + j] the isotropic direction draws
+// (theta, phi); dK may be null.
+cudaError_t launch_table_draws(const Plan& P, const JumpTable& jt, int32_t* dRk, int32_t* dK, cudaStream_t st);
+
 // tcgen05 contraction + fused epilogue over points [row0, row0 + rows).
 cudaError_t launch_tc(const Plan& P, const double* dX, const void* dB, const double* dKtab, double* dOut,
                       int64_t row0, int64_t rows, uint32_t* dErr, int numSMs, cudaStream_t st);
+
+// Outer-group contraction of GEN_OUTER plans (rf_outer.cu) over points
+// [row0, row0 + rows); outer_smem_bytes is its shared-memory size (0: the
+// slot does not fit), *stages its slot count.
+cudaError_t launch_outer(const Plan& P, const double* dX, const void* dB, double* dOut, int64_t row0, int64_t rows,
+                         uint32_t* dErr, int numSMs, cudaStream_t st);
+size_t outer_smem_bytes(const Plan& P, int* stages);
 
 // Plain FP32 contraction (FFMA) + the same epilogue.
 cudaError_t launch_fp32(const Plan& P, const double* dX, const void* dB, const double* dKtab, double* dOut,

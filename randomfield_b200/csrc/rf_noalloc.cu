@@ -19,7 +19,10 @@
 //   - all calls share the one array per device: calls whose work overlaps on
 //     the GPU (different streams or threads) race and corrupt each other's
 //     tables; serialise them;
-//   - requests whose tables exceed the array are rejected with RF_ESCRATCH.
+//   - requests whose tables exceed the array are rejected with RF_ESCRATCH;
+//   - the call returns only after its work on `stream` has finished: it
+//     synchronises the stream (after the extent pass when one is needed,
+//     and at the end to read the device error word).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -199,7 +202,7 @@ extern "C" int rf_generate_device_noalloc(const double* d_xPoints, int nDim, int
   for (int32_t r0 = 0; r0 < P0.Nmc; r0 += blk) {
     Plan P = P0;
     if (int rc = host_block_layout(&P, r0, std::min(blk, P0.Nmc - r0))) return rc;
-    const size_t opBytes = (size_t)P.nChunks * P.stageBytes;
+    const size_t opBytes = (size_t)operand_bytes(P);
     const size_t tabBytes = P.gen == GEN_TABLE ? (size_t)P.nChunks * kKtabStageBytes : 0;
     if (opBytes > kOperandBytes || tabBytes > kTableBytes) {
       char buf[256];

@@ -1,0 +1,421 @@
+// rf_outer.cu -- the Shinozuka sum over 3-D tensor-grid wavevectors as an
+// outer-group contraction on tcgen05 tensor cores.
+//
+// Replaces the hot loop of gen_Std_Gauss_Shinozuka (randomFieldND.f90:276-330)
+// for 3-D requests whose wavevectors form the set_kPoints tensor grid
+// (spectra_RF.f90:87-133): k = (k1(i1), s2 k2(i2), s3 k3(i3)).  With the
+// outer phasor P_g(x) = exp(i (k1 x1 + s2 k2 x2)) of the group g = (i1, i2,
+// s2) and E3 = exp(i k3 x3) = c3 + i s3, the field is
+//
+//   f(x, r) = ampMult sum_{i3} [ c3(i3) Yc(x, i3, r) + s3(i3) Ys(x, i3, r) ],
+//   Y (points x (r, i3, cos|sin)) = A (points x 2G) B (2G x N),
+//
+// with A = (Re P_g, Im P_g) generated on chip and B built from the phases
+// (rf_tables.cu, outer_element).  Against the plain contraction
+// [cos Kx | sin Kx] x [a cos phi; -a sin phi] this is the same number of
+// multiply-adds and the same operand bytes, but the generated operand shrinks
+// from 2K = 8 n1 n2 n3 to 2G = 4 n1 n2 values per point and chunk, the MMAs
+// run at N = 2 lPad x (realizations per chunk), up to 256, and the last
+// contraction over i3 (2 lPad multiply-adds per output) runs in the epilogue
+// in FP32 with FP64-reduced per-point phasors.
+//
+// One persistent CTA per SM; a work item is a pair of 128-point tiles that
+// share every B stage (M = 256 per operand byte streamed from L2).  The
+// realization block is cut into N chunks of oRc realizations (TMEM: one
+// 256-column accumulator per tile); for each chunk the K-steps (16 K = 8
+// outer groups of consecutive i1) stream through a ring of shared-memory
+// slots, each holding both tiles' A K-step (hi, and lo where the plan keeps
+// it) and B's K-step block (hi, and lo).
+//
+// Warp roles (576 threads):
+//   warp 0      MMA issuer: the warp runs the slot loop, one elected lane
+//               issues tcgen05.mma (A and B by shared-memory descriptor, D in
+//               TMEM) and tcgen05.commit;
+//   warp 1      producer (one thread): 1-D bulk copies (TMA, no multicast) of
+//               B's K-step blocks from HBM/L2 into the slots;
+//   warps 2-9   generators: one point each (256 = two tiles); per K-step the
+//               8 outer phasors E1(i1) E2(i2)^{s2} of the point, rounded to
+//               16 bits (and the lo residual), stored in the K-major core-
+//               matrix layout; E1 from FP64-reduced phases per work item, E2
+//               walked by angle addition per chunk;
+//   warps 10-17 epilogue: tcgen05.ld of a tile's accumulator (warp % 4 picks
+//               the TMEM lane quarter), the i3 sum with the point's own
+//               E3 phasors, ampMult, the marginal map, FP64 stores.
+// Every wait is bounded (globaltimer); on expiry the kernel raises the error
+// word, drains its own async work, frees TMEM and returns.
+#include "rf_device.cuh"
+#include "rf_gen.cuh"
+#include "rf_launch.h"
+
+namespace rfb {
+
+namespace {
+
+constexpr int kIssuerWarp = 0, kProducerWarp = 1, kGenWarp0 = 2, kGenWarps = 8;
+constexpr int kEpiWarp0 = kGenWarp0 + kGenWarps, kEpiWarps = 8;
+constexpr int kOuterThreads = (kEpiWarp0 + kEpiWarps) * 32;
+constexpr int kPairRows = 2 * kTileM;
+constexpr int kOuterMaxSlots = 8;
+constexpr int kATileBytes = kTileM * 16 * 2;  // one tile's K-step of A: 128 rows x 16 K x 16 bits
+constexpr uint32_t kOuterTmemCols = 512;
+constexpr int kAccCols = 256;  // accumulator columns per tile
+
+struct OuterBars {
+  uint64_t full[kOuterMaxSlots];   // 8 generator warps + producer (bytes)
+  uint64_t empty[kOuterMaxSlots];  // MMA commit
+  uint64_t acc_full;               // MMA commit after a chunk's last K-step
+  uint64_t acc_empty[2];           // the 4 epilogue warps of a tile
+  uint64_t done;
+  uint32_t tmem_base;
+  int abort_flag;
+};
+constexpr int kOuterHeader = 256;
+static_assert(sizeof(OuterBars) <= kOuterHeader, "header");
+
+struct OuterArgs {
+  Plan P;
+  const double* x;
+  const unsigned char* B;
+  double* out;
+  uint32_t* err;
+  int64_t row0, rows;
+  int32_t S;          // slots
+  int32_t slotBytes;  // A area + B area, 128-byte multiple
+  int32_t aBytes;     // A area: two tiles x 4 KB, twice with a lo term
+};
+
+__device__ __forceinline__ void outer_abort(OuterBars* bars, uint32_t* err) {
+  *reinterpret_cast<volatile int*>(&bars->abort_flag) = 1;
+  atomicOr(err, kErrTimeout);
+}
+
+__device__ __forceinline__ double outer_finish(const Plan& P, float acc) {
+  double v = (double)acc * P.outScale;
+  if (P.applyMarginal) {
+    v = v * P.margSd + P.margAvg;
+    if (P.lognormal) v = exp(v);
+  }
+  return v;
+}
+
+template <int PREC>
+__device__ __forceinline__ uint32_t pack16(float lo, float hi) {
+  return PREC == PREC_FP16 ? pack_f16x2(lo, hi) : pack_bf16x2(lo, hi);
+}
+// The 16-bit values of a packed pair back in FP32.
+template <int PREC>
+__device__ __forceinline__ float2 unpack16(uint32_t w) {
+  if (PREC == PREC_FP16) {
+    const __half2 h = *reinterpret_cast<const __half2*>(&w);
+    return __half22float2(h);
+  }
+  return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+}
+
+// LPAD: axis-3 length padded to 8, 16, 24 or 32 (the epilogue's phasor table).
+template <int PREC, int LPAD>
+__global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid_constant__ OuterArgs a) {
+  const Plan& P = a.P;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  OuterBars* bars = reinterpret_cast<OuterBars*>(smem);
+  unsigned char* slots = smem + kOuterHeader;
+  volatile int* abort_flag = &bars->abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int S = a.S;
+  const int64_t tiles = (a.rows + kTileM - 1) / kTileM;
+  const int64_t pairs = (tiles + 1) / 2;
+  const int64_t count = (int64_t)blockIdx.x < pairs ? (pairs - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int32_t nK = P.oNK, nR = P.oNR;
+  const int32_t nRows = 2 * P.lPad * P.oRc;  // B rows (N) of a full chunk
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&bars->full[s], kGenWarps + 1);
+      mbar_init(&bars->empty[s], 1);
+    }
+    mbar_init(&bars->acc_full, 1);
+    mbar_init(&bars->acc_empty[0], 4);
+    mbar_init(&bars->acc_empty[1], 4);
+    mbar_init(&bars->done, 1);
+    bars->abort_flag = 0;
+    mbar_fence_init();
+  }
+  if (warp == kIssuerWarp) {
+    tmem_alloc(&bars->tmem_base, kOuterTmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = bars->tmem_base;
+
+  if (warp == kProducerWarp) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      uint32_t s = 0, ph = 0;
+      bool ok = true;
+      for (int64_t i = 0; i < count && ok; ++i) {
+        for (int32_t c = 0; c < nR && ok; ++c) {
+          const unsigned char* src = a.B + (int64_t)c * P.oChunkBytes;
+          for (int32_t j = 0; j < nK; ++j) {
+            if (!mbar_wait(&bars->empty[s], ph ^ 1, abort_flag)) {
+              ok = false;
+              break;
+            }
+            const uint32_t bytes = (uint32_t)(outer_b_lo(P, j) ? 2 * P.oKstepBytes : P.oKstepBytes);
+            mbar_arrive_expect_tx(&bars->full[s], bytes);
+            bulk_g2s(slots + (size_t)s * a.slotBytes + a.aBytes, src, bytes, &bars->full[s]);
+            src += bytes;
+            if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+          }
+        }
+      }
+      if (!ok) outer_abort(bars, a.err);
+      if (*abort_flag) {
+        // copies still in flight complete_tx on full barriers whose generator
+        // arrivals may never come: wait for them by time before the CTA exits
+        const uint64_t t0 = globaltimer_ns();
+        while (globaltimer_ns() - t0 < 1000000ull) {
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == kIssuerWarp) {
+    // ---------------------------------------------------------- MMA issuer
+    const bool leader = elect_one();
+    uint32_t s = 0, ph = 0, accPh = 0;
+    bool ok = true;
+    const uint32_t ab = PREC == PREC_FP16 ? 0u : 1u;
+    const uint32_t aDescLo = (uint32_t)(2 * kATileBytes) >> 4;  // descriptor step to the lo A tiles
+    const uint32_t bDescLo = (uint32_t)(P.oKstepBytes >> 4);
+    for (int64_t i = 0; i < count && ok; ++i) {
+      for (int32_t c = 0; c < nR && ok; ++c) {
+        const int32_t rc = min(P.oRc, P.nmcBlk - c * P.oRc);
+        const uint32_t idesc = make_idesc(ab, 128u, (uint32_t)(2 * P.lPad * rc));
+        for (int32_t j = 0; j < nK; ++j) {
+          if (!mbar_wait_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t base = smem_u32(slots + (size_t)s * a.slotBytes);
+          const uint64_t aDesc = make_sdesc(base, 2048u, 128u);
+          const uint64_t bDesc = make_sdesc(base + (uint32_t)a.aBytes, (uint32_t)nRows * 16u, 128u);
+          const bool bLo = outer_b_lo(P, j), aLo = outer_a_lo(P, j);
+#pragma unroll
+          for (int t = 0; t < 2; ++t) {
+            if (j == 0) {  // the tile's accumulator is free once its epilogue has read the last chunk
+              if (!mbar_wait_warp(&bars->acc_empty[t], accPh ^ 1, abort_flag)) { ok = false; break; }
+              tc_fence_after();
+            }
+            if (leader) {
+              const uint32_t d = tbase + (uint32_t)(t * kAccCols);
+              const uint64_t at = aDesc + (uint64_t)((t * kATileBytes) >> 4);
+              mma_ss(d, at, bDesc, idesc, j > 0 ? 1u : 0u);
+              if (bLo) mma_ss(d, at, bDesc + bDescLo, idesc, 1u);
+              if (aLo) mma_ss(d, at + aDescLo, bDesc, idesc, 1u);
+            }
+          }
+          if (!ok) break;
+          if (leader) mma_commit(&bars->empty[s]);
+          __syncwarp();
+          if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+        }
+        if (!ok) break;
+        if (leader) mma_commit(&bars->acc_full);
+        __syncwarp();
+        accPh ^= 1;
+      }
+    }
+    if (!ok && lane == 0) outer_abort(bars, a.err);
+    if (leader) mma_commit(&bars->done);
+    __syncwarp();
+    volatile int never = 0;
+    mbar_wait(&bars->done, 0, &never);
+    __syncwarp();
+  } else if (warp < kEpiWarp0) {
+    // ---------------------------------------------------------- generators
+    const int gi = threadIdx.x - kGenWarp0 * 32;  // 0 .. 255
+    const int t = gi >> 7, row = gi & 127;
+    const uint32_t rowOff = (uint32_t)((row >> 3) * 128 + (row & 7) * 16);
+    const int32_t n1 = P.kNStep[0], n2 = P.kNStep[1], nJJ = P.n1p >> 3;
+    uint32_t s = 0, ph = 0;
+    bool ok = true;
+    for (int64_t i = 0; i < count && ok; ++i) {
+      const int64_t pair = blockIdx.x + i * gridDim.x;
+      const int64_t p = a.row0 + pair * kPairRows + t * kTileM + row;
+      const bool valid = p < a.row0 + a.rows;
+      double x0 = 0.0, x1 = 0.0;
+      if (valid) {
+        x0 = a.x[p * 3 + 0] / P.corrL[0];
+        x1 = a.x[p * 3 + 1] / P.corrL[1];
+      }
+      float2 e1[kOuterMaxN1P];
+#pragma unroll
+      for (int u = 0; u < kOuterMaxN1P; ++u)
+        e1[u] = (u < n1) ? axis_phasor(P.kDelta[0], u, x0) : make_float2(0.f, 0.f);
+      const float2 e2step = axis_phasor(P.kDelta[1], 1, x1);
+      for (int32_t c = 0; c < nR && ok; ++c) {
+        for (int32_t s2 = 0; s2 < 2 && ok; ++s2) {
+          float2 e2 = make_float2(1.f, 0.f);  // E2(i2), walked by angle addition
+          for (int32_t i2 = 0; i2 < n2 && ok; ++i2) {
+            const float2 E = make_float2(e2.x, s2 ? -e2.y : e2.y);
+#pragma unroll
+            for (int jj = 0; jj < kOuterMaxN1P / 8; ++jj) {
+              if (jj < nJJ) {
+                const int32_t j = jj + nJJ * (i2 + n2 * s2);
+                if (!mbar_wait_warp(&bars->empty[s], ph ^ 1, abort_flag)) {
+                  ok = false;
+                  break;
+                }
+                float2 pv[8];
+                uint32_t hi[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                  const float2 q = e1[8 * jj + u];
+                  pv[u] = make_float2(q.x * E.x - q.y * E.y, q.x * E.y + q.y * E.x);
+                  hi[u] = pack16<PREC>(pv[u].x, pv[u].y);
+                }
+                unsigned char* A = slots + (size_t)s * a.slotBytes + t * kATileBytes + rowOff;
+                *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+                *reinterpret_cast<uint4*>(A + 2048) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+                if (outer_a_lo(P, j)) {  // the residual of the 16-bit rounding, rounded again
+                  uint32_t lo[8];
+#pragma unroll
+                  for (int u = 0; u < 8; ++u) {
+                    const float2 h = unpack16<PREC>(hi[u]);
+                    lo[u] = pack16<PREC>(pv[u].x - h.x, pv[u].y - h.y);
+                  }
+                  *reinterpret_cast<uint4*>(A + 2 * kATileBytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+                  *reinterpret_cast<uint4*>(A + 2 * kATileBytes + 2048) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+                }
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bars->full[s]);
+                if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+              }
+            }
+            e2 = make_float2(e2.x * e2step.x - e2.y * e2step.y, e2.x * e2step.y + e2.y * e2step.x);
+          }
+        }
+      }
+    }
+    if (!ok) outer_abort(bars, a.err);
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3, t = (warp - kEpiWarp0) >> 2;
+    const int row = q * 32 + lane;
+    const uint32_t taddr0 = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(t * kAccCols);
+    constexpr int LH = LPAD / 8;  // 16-column pieces per realization
+    uint32_t accPh = 0;
+    bool ok = true;
+    for (int64_t i = 0; i < count && ok; ++i) {
+      const int64_t pair = blockIdx.x + i * gridDim.x;
+      const int64_t p = a.row0 + pair * kPairRows + t * kTileM + row;
+      const bool valid = p < a.row0 + a.rows;
+      const double x2 = valid ? a.x[p * 3 + 2] / P.corrL[2] : 0.0;
+      float2 e3[LPAD];
+#pragma unroll
+      for (int u = 0; u < LPAD; ++u)
+        e3[u] = (u < P.kNStep[2]) ? axis_phasor(P.kDelta[2], u, x2) : make_float2(0.f, 0.f);
+      for (int32_t c = 0; c < nR; ++c) {
+        if (!mbar_wait_warp(&bars->acc_full, accPh, abort_flag)) { ok = false; break; }
+        tc_fence_after();
+        const int32_t rc = min(P.oRc, P.nmcBlk - c * P.oRc);
+        for (int32_t rl = 0; rl < rc; ++rl) {
+          float acc = 0.f;
+#pragma unroll
+          for (int h = 0; h < LH; ++h) {
+            uint32_t y[16];
+            tmem_ld16(taddr0 + (uint32_t)(rl * 2 * LPAD + 16 * h), y);
+            tmem_ld_wait();
+#pragma unroll
+            for (int v = 0; v < 8; ++v) {
+              acc = fmaf(e3[8 * h + v].x, __uint_as_float(y[2 * v]), acc);
+              acc = fmaf(e3[8 * h + v].y, __uint_as_float(y[2 * v + 1]), acc);
+            }
+          }
+          if (valid) a.out[(int64_t)(P.rOff + c * P.oRc + rl) * P.n + p] = outer_finish(P, acc);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bars->acc_empty[t]);
+        accPh ^= 1;
+      }
+    }
+    if (!ok) outer_abort(bars, a.err);
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == kIssuerWarp) tmem_dealloc(tbase, kOuterTmemCols);
+}
+
+// Slot layout of a plan: A area (two tiles, twice with a lo term somewhere)
+// and B area (one K-step block, twice with a lo block somewhere).
+void outer_slot(const Plan& P, int32_t* aBytes, int32_t* slotBytes) {
+  bool aLo = false, bLo = false;
+  for (int32_t j = 0; j < P.oNK; ++j) {
+    aLo = aLo || outer_a_lo(P, j);
+    bLo = bLo || outer_b_lo(P, j);
+  }
+  *aBytes = 2 * kATileBytes * (aLo ? 2 : 1);
+  const int64_t b = P.oKstepBytes * (bLo ? 2 : 1);
+  *slotBytes = (int32_t)((*aBytes + b + 127) / 128 * 128);
+}
+
+template <int PREC, int LPAD>
+cudaError_t launch_outer_t(const OuterArgs& a, size_t smem, int grid, cudaStream_t st) {
+  auto fn = rf_outer_kernel<PREC, LPAD>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fn<<<grid, kOuterThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int PREC>
+cudaError_t launch_outer_p(const OuterArgs& a, size_t smem, int grid, cudaStream_t st) {
+  switch (a.P.lPad) {
+    case 8: return launch_outer_t<PREC, 8>(a, smem, grid, st);
+    case 16: return launch_outer_t<PREC, 16>(a, smem, grid, st);
+    case 24: return launch_outer_t<PREC, 24>(a, smem, grid, st);
+    case 32: return launch_outer_t<PREC, 32>(a, smem, grid, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+size_t outer_smem_bytes(const Plan& P, int* stages) {
+  int32_t aBytes = 0, slotBytes = 0;
+  outer_slot(P, &aBytes, &slotBytes);
+  const size_t limit = 227 * 1024, floor = 120 * 1024;  // > half the SM: one CTA (and its 512 TMEM columns) per SM
+  int S = (int)((limit - kOuterHeader) / (size_t)slotBytes);
+  if (S > kOuterMaxSlots) S = kOuterMaxSlots;
+  if (stages) *stages = S;
+  if (S < 2) return 0;
+  const size_t total = (size_t)kOuterHeader + (size_t)S * slotBytes;
+  return total < floor ? floor : total;
+}
+
+cudaError_t launch_outer(const Plan& P, const double* dX, const void* dB, double* dOut, int64_t row0, int64_t rows,
+                         uint32_t* dErr, int numSMs, cudaStream_t st) {
+  OuterArgs a;
+  a.P = P;
+  a.x = dX;
+  a.B = reinterpret_cast<const unsigned char*>(dB);
+  a.out = dOut;
+  a.err = dErr;
+  a.row0 = row0;
+  a.rows = rows;
+  outer_slot(P, &a.aBytes, &a.slotBytes);
+  int S = 0;
+  const size_t smem = outer_smem_bytes(P, &S);
+  if (smem == 0) return cudaErrorInvalidValue;
+  a.S = S;
+  const int64_t tiles = (rows + kTileM - 1) / kTileM;
+  const int64_t pairs = (tiles + 1) / 2;
+  const int grid = (int)(pairs < numSMs ? pairs : numSMs);
+  if (P.prec == PREC_FP16) return launch_outer_p<PREC_FP16>(a, smem, grid, st);
+  return launch_outer_p<PREC_BF16>(a, smem, grid, st);
+}
+
+}  // namespace rfb

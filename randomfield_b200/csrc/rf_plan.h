@@ -20,6 +20,8 @@ enum Generator : int32_t {
   GEN_TABLE = 0,  // explicit wavevector table, one FP64 phase + SFU sincos per (point, k)
   GEN_GRID3 = 1,  // 3-D tensor-grid wavevectors: per-axis tables and angle addition
   GEN_MIXED = 2,  // kernel variant only: the generator is chosen per tile (grouped launch)
+  GEN_OUTER = 3,  // 3-D tensor grid, outer-group contraction (rf_outer.cu): A = outer phasors
+                  // E1 E2^{s2}, N = (realization, i3, cos|sin), the i3 sum in the epilogue
 };
 
 enum Precision : int32_t { PREC_BF16 = 0, PREC_FP16 = 1, PREC_FP32 = 2, PREC_BF16_FAST = 3, PREC_FP8 = 4 };
@@ -84,6 +86,20 @@ struct Plan {
   int32_t gDims[3];           // group grid points per axis
   int32_t bRamp[3];           // overlapNPoints per axis (< 1: no ramp)
   int64_t gTotal;             // group grid points
+  // GEN_OUTER layout (rf_outer.cu; single 3-D Shinozuka requests on the
+  // tensor-core forms).  K = 2 x outer groups g = (i1, i2, s2) (re, im of
+  // E1 E2^{s2}), in K-steps of 16 = 8 groups of consecutive i1; N chunk c
+  // = realizations [c oRc, (c+1) oRc) of the block, each 2 lPad columns
+  // (i3, cos|sin).  B of chunk c is oNK K-step blocks of oKstepBytes (hi),
+  // each followed by its lo block where bit j of loMask is set; A carries its
+  // lo term on the K-steps of aLoMask.
+  int32_t n1p;                // axis-1 wavenumbers padded to a multiple of 8 (8, 16, 24)
+  int32_t oRc;                // realizations per N chunk
+  int32_t oNR;                // N chunks of the realization block
+  int32_t oNK;                // K-steps per chunk
+  int64_t oKstepBytes;        // bytes of one K-step block of B: 16 x (2 lPad oRc) x 2
+  int64_t oChunkBytes;        // bytes of one chunk of B, lo blocks included
+  uint32_t aLoMask[8];        // K-steps whose A tile carries the lo term (up to 256)
 };
 
 __host__ __device__ inline int popcount32(uint32_t x) {
@@ -105,6 +121,45 @@ __host__ __device__ inline int64_t stage_offset(const Plan& P, int64_t s) {
   if (s & 31) lo += popcount32(P.loMask[s >> 5] & ((1u << (s & 31)) - 1u));
   return (s + lo) * (P.stageBytes / 2);
 }
+
+constexpr int kOuterMaxN1P = 24;  // GEN_OUTER: axis-1 wavenumbers (register table of the generators)
+constexpr int kOuterMaxKsteps = 256;
+
+__host__ __device__ inline bool mask_bit(const uint32_t* m, int64_t j) { return (m[j >> 5] >> (j & 31)) & 1u; }
+// Set bits of m below bit j.
+__host__ __device__ inline int64_t mask_rank(const uint32_t* m, int64_t j) {
+  int64_t c = 0;
+  for (int64_t w = 0; w < (j >> 5); ++w) c += popcount32(m[w]);
+  if (j & 31) c += popcount32(m[j >> 5] & ((1u << (j & 31)) - 1u));
+  return c;
+}
+// GEN_OUTER: byte offset of K-step j's hi block inside a chunk of B.
+__host__ __device__ inline int64_t outer_kstep_offset(const Plan& P, int64_t j) {
+  return (j + (P.loSkip ? mask_rank(P.loMask, j) : 0)) * P.oKstepBytes;
+}
+__host__ __device__ inline bool outer_b_lo(const Plan& P, int64_t j) { return P.loSkip && mask_bit(P.loMask, j); }
+__host__ __device__ inline bool outer_a_lo(const Plan& P, int64_t j) { return mask_bit(P.aLoMask, j); }
+
+// Bytes of the contraction operand of a plan (one realization block).
+__host__ __device__ inline int64_t operand_bytes(const Plan& P) {
+  if (P.gen == GEN_OUTER) return (int64_t)P.oNR * P.oChunkBytes;
+  return stage_offset(P, P.nChunks);
+}
+
+// Table builder threads (rf_tables.cu): one per (run, realization column).
+// A run is n1 wavevectors of one GEN_GRID3 column (consecutive i1) or kRun
+// consecutive wavevectors of the other generators.
+constexpr int kRun = 32;
+__host__ __device__ inline int64_t table_runs(const Plan& P) {
+  if (P.gen == GEN_OUTER) return (int64_t)P.lPad * P.kNStep[1] * 2;  // (i3, i2, s2), a run over i1
+  if (P.gen == GEN_GRID3) return (int64_t)(2 * P.lPad) * (P.nChunks * P.gps / P.kNStep[0]);
+  return (P.nChunks * P.chunkK + kRun - 1) / kRun;
+}
+// Realization columns of the builder: GEN_OUTER lays out whole N chunks.
+__host__ __device__ inline int32_t table_cols(const Plan& P) {
+  return P.gen == GEN_OUTER ? P.oNR * P.oRc : P.nmcPad;
+}
+__host__ __device__ inline int64_t table_threads(const Plan& P) { return table_runs(P) * table_cols(P); }
 
 // Shared-memory and TMEM slot layout of one tcgen05 launch: B slot s at
 // byte slotBytes*s of the slot area, its wavevector chunk (GEN_TABLE) at

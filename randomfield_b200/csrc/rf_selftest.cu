@@ -10,7 +10,10 @@
 // passes and return.  The context stays usable afterwards.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "rf_internal.h"
+#include "rf_launch.h"
 
 using namespace rfb;
 using namespace rfh;
@@ -92,4 +95,57 @@ extern "C" int rf_context_selftest_timeout(rf_context* ctx, double limit_ms) {
   RF_CUDA(cudaGetLastError(), "self-test kernel");
   RF_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
   return check_device_error(ctx);
+}
+
+// The draws of the table builder, exported for a bit-exact check against a
+// sequential rnglib run: the same runs, cursors and draw positions as the
+// operand build (rf_tables.cu), realization block by realization block.
+extern "C" int rf_debug_table_draws(int nDim, int method, int Nmc, const rf_options* opt, int64_t* K_out,
+                                    int32_t* draws, int64_t draws_capacity, int32_t* k_draws,
+                                    int64_t k_capacity) {
+  g_err.clear();
+  if (!K_out) return fail(RF_EINVAL_ARG, "null K_out");
+  const double corrL[3] = {1.0, 1.0, 1.0};
+  const Request rq = make_request(nDim, 1, RF_CM_GAUSSIAN, RF_FOM_GAUSSIAN, corrL, 0.0, 1.0, Nmc, method, opt);
+  if (int rc = validate(rq)) return rc;
+  const double ext[3] = {0.0, 0.0, 0.0};  // extents come from opt->x_range (or are unused with k_nstep)
+  Plan P0;
+  if (int rc = build_plan(rq, ext, P0)) return rc;
+  *K_out = P0.K;
+  if (!draws) return RF_OK;  // query of K only
+  const int64_t D = method == RF_ISOTROPIC ? 2 : 1;
+  const int64_t need = (int64_t)Nmc * P0.K * D;
+  if (draws_capacity < need) return fail(RF_EINVAL_ARG, "draws needs Nmc * K * %d entries", (int)D);
+  const bool wantK = k_draws && method == RF_ISOTROPIC;
+  if (wantK && k_capacity < 2 * P0.K) return fail(RF_EINVAL_ARG, "k_draws needs 2 * K entries");
+  RF_CUDA(cudaSetDevice(rq.opt.device), "cudaSetDevice");
+  int32_t *dRk = nullptr, *dK = nullptr;
+  RF_CUDA(cudaMalloc(&dRk, (size_t)need * sizeof(int32_t)), "cudaMalloc");
+  if (wantK && cudaMalloc(&dK, (size_t)2 * P0.K * sizeof(int32_t)) != cudaSuccess) {
+    cudaFree(dRk);
+    return fail(RF_ENOMEM, "cudaMalloc of the direction draws failed");
+  }
+  cudaError_t e = cudaSuccess;
+  const int32_t blk = realization_block(P0);
+  for (int32_t r0 = 0; r0 < P0.Nmc && e == cudaSuccess; r0 += blk) {
+    Plan P = P0;
+    P.rOff = r0;
+    P.nmcBlk = std::min(blk, P0.Nmc - r0);
+    if (int rc = layout(P)) {
+      cudaFree(dRk);
+      cudaFree(dK);
+      return rc;
+    }
+    lo_layout(P);
+    outer_layout(P);  // the same plan as a generation of this request
+    e = launch_table_draws(P, jump_table(), dRk, dK, 0);
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(draws, dRk, (size_t)need * sizeof(int32_t), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && wantK)
+    e = cudaMemcpy(k_draws, dK, (size_t)2 * P0.K * sizeof(int32_t), cudaMemcpyDeviceToHost);
+  cudaFree(dRk);
+  cudaFree(dK);
+  if (e != cudaSuccess) return cuda_fail(e, "table draws");
+  return RF_OK;
 }

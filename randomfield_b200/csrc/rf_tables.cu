@@ -4,13 +4,17 @@
 // (randomFieldND.f90:276-330) is evaluated as the contraction
 //   f = ampMult * [cos(Kx) | sin(Kx)] (points x 2K)  *  B (2K x Nmc),
 //   B[2k, r] = a_k cos(phi_{k,r}),  B[2k+1, r] = -a_k sin(phi_{k,r}).
-// One thread per (wavevector in kernel order, realization).  The phases come
-// from the rnglib stream (rnglib.f90:548-659) by jump-ahead: the p-th draw of
-// generator 1 is (a1^p s1 mod m1) - (a2^p s2 mod m2) folded, so every
-// element is computed independently and the table matches a sequential run
-// draw for draw.  Draw order follows the reference: Shinozuka K phases per
-// realization in k order (:278-279); isotropic direction blocks then, per
-// realization, a gamma block and a psi block (:460-468 restated).
+// One thread per (run, realization): a run is a set of wavevectors whose
+// reference indices are consecutive (GEN_GRID3: the n1 values of i1 at fixed
+// (i2, s2, column); the other generators: kRun consecutive wavevectors), so
+// the draws a thread needs are consecutive calls of the generator.  The
+// phases come from the rnglib stream (rnglib.f90:548-659): the p-th draw of
+// generator 1 is (a1^p s1 mod m1) - (a2^p s2 mod m2) folded; a thread jumps
+// ahead once per stream (square-and-multiply) and then steps one call at a
+// time (DrawCursor), and the table matches a sequential run draw for draw.
+// Draw order follows the reference: Shinozuka K phases per realization in k
+// order (:278-279); isotropic direction blocks then, per realization, a gamma
+// block and a psi block (:460-468 restated).
 #include <cuda_fp8.h>
 
 #include "rf_device.cuh"
@@ -37,7 +41,41 @@ __device__ __forceinline__ double gauss_spectrum(const double* k, int nDim) {
   return s;
 }
 
-__device__ KVal kvalue(const Plan& P, const JumpTable& jt, int64_t kk) {
+// Position in one rnglib stream: the state after `pos` calls (pos = 0: not
+// set).  A draw at pos + 1 costs one step (two modular products); any other
+// position a jump-ahead.
+struct DrawCursor {
+  int64_t c1, c2;
+  uint64_t pos;
+  int32_t last;  // i4_uni value of call `pos`
+};
+
+// r8_uni_01 of the p-th call (p >= 1), through the cursor.
+__device__ __forceinline__ double draw_r8(const JumpTable& jt, int64_t s1, int64_t s2, DrawCursor& cur, uint64_t p) {
+  if (cur.pos != 0 && p == cur.pos + 1) uni_state_next(jt, cur.c1, cur.c2);
+  else if (p != cur.pos) uni_state_at(jt, s1, s2, p, cur.c1, cur.c2);
+  cur.pos = p;
+  cur.last = uni_value(cur.c1, cur.c2);
+  return (double)cur.last * kR8Scale;
+}
+
+// Where the draw export (rf_debug_table_draws) writes the i4_uni values the
+// builder consumed, in reference order: per (realization, wavevector) the
+// phase draw (isotropic: gamma, then psi), and per wavevector the isotropic
+// direction draws (theta, then phi in 3-D).  Null in the operand builds.
+struct DrawSink {
+  int32_t* rk;
+  int32_t* k;
+};
+
+// The streams a run draws from: wavevector draws (randomization bases,
+// isotropic directions phi and theta) and per-realization draws (phase, or
+// isotropic gamma and psi).
+struct RunCursors {
+  DrawCursor kA, kB, rA, rB;
+};
+
+__device__ KVal kvalue(const Plan& P, const JumpTable& jt, int64_t kk, RunCursors& cu) {
   KVal v;
   v.ref = -1;
   v.k[0] = v.k[1] = v.k[2] = 0.0;
@@ -67,7 +105,7 @@ __device__ KVal kvalue(const Plan& P, const JumpTable& jt, int64_t kk) {
       // randomization: kPoints_base = random_number * kMax, axis fastest,
       // the first nDim*kn draws of the stream (spectra_RF.f90:119-124)
       const double base =
-          (P.method == 3) ? r8_uni_at(jt, P.ig1, P.ig2, (uint64_t)(b * P.nDim + d + 1)) * P.kMax
+          (P.method == 3) ? draw_r8(jt, P.ig1, P.ig2, cu.kA, (uint64_t)(b * P.nDim + d + 1)) * P.kMax
                           : 0.0 + P.kDelta[d] * (double)i;
       // B2 in literal mode: the first quadrant is never written.
       v.k[d] = (P.literal && q == 0) ? 0.0 : base * (d == 0 ? 1.0 : quad_sign(q, d, P.nDim));
@@ -80,14 +118,14 @@ __device__ KVal kvalue(const Plan& P, const JumpTable& jt, int64_t kk) {
     const int j = (int)(kk / nd);
     const double r = (double)j * P.kDelta[0];
     const double s1 = P.ig1, s2 = P.ig2;
-    const double uth = r8_uni_at(jt, (int64_t)s1, (int64_t)s2, (uint64_t)((P.nDim == 3 ? K : 0) + kk + 1));
+    const double uth = draw_r8(jt, (int64_t)s1, (int64_t)s2, cu.kA, (uint64_t)((P.nDim == 3 ? K : 0) + kk + 1));
     const double th = 2.0 * kRefPi * uth;
     double S;
     if (P.corrMod == 1) S = exp(-((r * r) * 1.0) / (4.0 * kRefPi));
     else S = (j == 5) ? 1.0 : 0.0;
     double shell;
     if (P.nDim == 3) {
-      const double uphi = r8_uni_at(jt, (int64_t)s1, (int64_t)s2, (uint64_t)(kk + 1));
+      const double uphi = draw_r8(jt, (int64_t)s1, (int64_t)s2, cu.kB, (uint64_t)(kk + 1));
       const double cph = 1.0 - 2.0 * uphi;
       const double sph = sqrt(fmax(0.0, 1.0 - cph * cph));
       v.k[0] = r * (sph * cos(th));
@@ -129,20 +167,18 @@ __device__ __forceinline__ double from_e4m3(unsigned char b) {
   return (double)__half2float(__half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)b, __NV_E4M3)));
 }
 
-// Element tid = kk * nmcPad + r of the operand: B rows of wavevector kk (in
-// kernel order) for realization column r, and the wavevector itself (r = 0).
+// Element (kk, r) of the operand: B rows of wavevector kk (in kernel order)
+// for realization column r, and the wavevector itself (r = 0).
+// SINK: write the consumed draws to `sink` instead of the operand.
+template <bool SINK>
 __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt, void* __restrict__ B,
                                               double* __restrict__ ktab, int64_t literalSlab, int64_t nSlab,
-                                              int64_t tid) {
-  const int64_t total = P.nChunks * P.chunkK;
-  const int r = (int)(tid % P.nmcPad);
-  const int64_t kk = tid / P.nmcPad;
-  if (kk >= total) return;
-  const KVal v = kvalue(P, jt, kk);
+                                              int64_t kk, int r, RunCursors& cu, const DrawSink& sink) {
+  const KVal v = kvalue(P, jt, kk, cu);
   const int64_t stage = kk / P.chunkK;
   const int32_t c = (int32_t)(kk % P.chunkK);
 
-  if (ktab && r == 0) {
+  if (!SINK && ktab && r == 0) {
     // k / 2 pi in FP64 and as fixed point with 30 fraction bits (range
     // |k / 2 pi| < 2; every table has |k_d| <= kMax <= 7.36 < 4 pi), and k in
     // FP32 (radians).  GEN_TABLE plans have chunkK == kTableChunk.
@@ -165,7 +201,7 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
     if (P.method != 1) {
       // randomization: the phases follow the nDim*kn wavevector draws
       const int64_t skip = (P.method == 3) ? (P.K >> (P.nDim - 1)) * P.nDim : 0;
-      phi = 2.0 * kRefPi * r8_uni_at(jt, s1, s2, (uint64_t)(skip + rg * P.K + v.ref + 1));
+      phi = 2.0 * kRefPi * draw_r8(jt, s1, s2, cu.rA, (uint64_t)(skip + rg * P.K + v.ref + 1));
       if (P.literal && literalSlab >= 0) {
         // B1: slab m of realization n uses S^(1/2^t), t = (n-1)*nSlab + m
         // (randomFieldND.f90:312 inside the loops :276 and :284).
@@ -177,14 +213,31 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
       }
     } else {
       const int64_t base = (P.nDim == 3 ? 2 : 1) * P.K + rg * 2 * P.K;
-      const double ug = r8_uni_at(jt, s1, s2, (uint64_t)(base + v.ref + 1));
-      const double up = r8_uni_at(jt, s1, s2, (uint64_t)(base + P.K + v.ref + 1));
+      const double ug = draw_r8(jt, s1, s2, cu.rA, (uint64_t)(base + v.ref + 1));
+      const double up = draw_r8(jt, s1, s2, cu.rB, (uint64_t)(base + P.K + v.ref + 1));
       gam = (double)sqrtf(12.0f) * (ug - 0.5);  // randomFieldND.f90:468 (single-precision sqrt(12.0))
       phi = 2.0 * kRefPi * up;
     }
     const double a = amp * gam;
     bc = a * cos(phi);
     bs = -a * sin(phi);
+  }
+  if (SINK) {
+    if (v.ref < 0) return;
+    if (P.method == 1 && r == 0 && sink.k) {
+      sink.k[v.ref * 2] = cu.kA.last;
+      sink.k[v.ref * 2 + 1] = P.nDim == 3 ? cu.kB.last : 0;
+    }
+    if (r < P.nmcBlk) {
+      const int64_t rg = (int64_t)P.rOff + r;
+      if (P.method == 1) {
+        sink.rk[(rg * P.K + v.ref) * 2] = cu.rA.last;
+        sink.rk[(rg * P.K + v.ref) * 2 + 1] = cu.rB.last;
+      } else {
+        sink.rk[rg * P.K + v.ref] = cu.rA.last;
+      }
+    }
+    return;
   }
 
   if (P.prec == PREC_FP32) {
@@ -223,13 +276,133 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
   }
 }
 
-__global__ void rf_tables_kernel(const Plan P, const JumpTable jt, void* __restrict__ B, double* __restrict__ ktab,
-                                 int64_t literalSlab, int64_t nSlab) {
-  table_element(P, jt, B, ktab, literalSlab, nSlab, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+// Run j's element i (i < table_run_length) in kernel order.  GEN_GRID3: run
+// j = cc + gw (i2 + n2 s2) holds column cc of the groups g = i + n1 (i2 +
+// n2 s2), whose reference indices are consecutive in i = i1
+// (grid3_ref_index); the other generators keep the reference order.
+__device__ __forceinline__ int64_t table_run_kk(const Plan& P, int64_t j, int32_t i) {
+  if (P.gen == GEN_GRID3) {
+    const int32_t gw = 2 * P.lPad;
+    const int64_t cc = j % gw, g = (int64_t)i + (int64_t)P.kNStep[0] * (j / gw);
+    return (g / P.gps) * P.chunkK + (g % P.gps) * gw + cc;
+  }
+  return j * kRun + i;
+}
+__device__ __forceinline__ int32_t table_run_length(const Plan& P, int64_t j) {
+  if (P.gen == GEN_GRID3) return P.kNStep[0];
+  const int64_t left = P.nChunks * P.chunkK - j * kRun;
+  return (int32_t)(left < kRun ? left : kRun);
 }
 
-// Grouped builder: a grid-stride loop over the concatenated elements of all
-// units (a fixed grid, so that the launch can sit in a captured graph).
+// GEN_OUTER operand.  For the outer group g = (i1, i2, s2), axis-3 index i3
+// and realization r, the two wavevectors s3 = +/- give C+- = a+- e^{i phi+-};
+// with P = C+ + C-, Q = C+ - C- the field's term is
+//   Re[E1 E2^{s2} (P cos(k3 x3) + i Q sin(k3 x3))]
+//     = pr c3 Re P - pi c3 Im P - pr s3 Im Q - pi s3 Re Q
+// (pr, pi: the outer phasor, the A operand; c3, s3: the epilogue's factors),
+// so B row (g, re) holds (Re P, -Im Q) and row (g, im) holds (-Im P, -Re Q)
+// in the (i3, cos) and (i3, sin) columns of realization r.  In terms of the
+// plain operand's pair (a cos phi, -a sin phi) = (bc, bs):
+//   W(re, cos) = bc+ + bc-,  W(im, cos) = bs+ + bs-,
+//   W(re, sin) = bs+ - bs-,  W(im, sin) = bc- - bc+.
+template <bool SINK>
+__device__ __forceinline__ void outer_element(const Plan& P, const JumpTable& jt, unsigned char* __restrict__ B,
+                                              int32_t i1, int32_t i2, int32_t s2, int32_t i3, int32_t rc,
+                                              RunCursors& cu, const DrawSink& sink) {
+  const int32_t n1 = P.kNStep[0], n2 = P.kNStep[1], n3 = P.kNStep[2];
+  double W[4] = {0.0, 0.0, 0.0, 0.0};  // (re, cos), (im, cos), (re, sin), (im, sin)
+  if (i1 < n1 && i3 < n3 && rc < P.nmcBlk) {
+    const int64_t n123 = (int64_t)n1 * n2 * n3;
+    const int64_t refP = (int64_t)(2 * s2) * n123 + i1 + (int64_t)n1 * (i2 + (int64_t)n2 * i3);
+    const int64_t refM = refP + n123;
+    const int64_t rg = (int64_t)P.rOff + rc;
+    double k[3];
+    k[0] = 0.0 + P.kDelta[0] * (double)i1;
+    k[1] = (0.0 + P.kDelta[1] * (double)i2) * (s2 ? -1.0 : 1.0);
+    k[2] = 0.0 + P.kDelta[2] * (double)i3;
+    double aP, aM;
+    if (P.corrMod == 1) {
+      aP = aM = sqrt(gauss_spectrum(k, 3));  // S(k) is even in k3
+    } else {
+      aP = (refP == 5) ? 1.0 : 0.0;  // cm_COS, spectra_RF.f90:210-220
+      aM = (refM == 5) ? 1.0 : 0.0;
+    }
+    const double phP = 2.0 * kRefPi * draw_r8(jt, P.ig1, P.ig2, cu.rA, (uint64_t)(rg * P.K + refP + 1));
+    const double phM = 2.0 * kRefPi * draw_r8(jt, P.ig1, P.ig2, cu.rB, (uint64_t)(rg * P.K + refM + 1));
+    if (SINK) {
+      sink.rk[rg * P.K + refP] = cu.rA.last;
+      sink.rk[rg * P.K + refM] = cu.rB.last;
+      return;
+    }
+    const double bcP = aP * cos(phP), bsP = -aP * sin(phP);
+    const double bcM = aM * cos(phM), bsM = -aM * sin(phM);
+    W[0] = bcP + bcM;
+    W[1] = bsP + bsM;
+    W[2] = bsP - bsM;
+    W[3] = bcM - bcP;
+  }
+  if (SINK) return;
+  // K-step j of the chunk, element k = 2 (i1 % 8) + e; column n = rl 2 lPad + 2 i3 + cs
+  const int32_t c = rc / P.oRc, rl = rc % P.oRc;
+  const int64_t j = (int64_t)(i1 >> 3) + (int64_t)(P.n1p >> 3) * (i2 + (int64_t)n2 * s2);
+  unsigned char* blk = B + (int64_t)c * P.oChunkBytes + outer_kstep_offset(P, j);
+  const int32_t nRows = 2 * P.lPad * P.oRc;
+  const bool lo = outer_b_lo(P, j);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int32_t e = q & 1, cs = q >> 1;
+    const int32_t kel = 2 * (i1 & 7) + e, row = rl * 2 * P.lPad + 2 * i3 + cs;
+    const int64_t off = tc_b_offset(nRows, row, kel);
+    if (P.prec == PREC_FP16) {
+      *reinterpret_cast<__half*>(blk + off) = __double2half(W[q] * ldexp(1.0, P.bScaleLog2));
+    } else {
+      const __nv_bfloat16 h = __double2bfloat16(W[q]);
+      *reinterpret_cast<__nv_bfloat16*>(blk + off) = h;
+      if (lo) *reinterpret_cast<__nv_bfloat16*>(blk + P.oKstepBytes + off) = __double2bfloat16(W[q] - (double)__bfloat162float(h));
+    }
+  }
+}
+
+// Thread t = j * cols + r: run j for realization column r.
+template <bool SINK = false>
+__device__ __forceinline__ void table_run(const Plan& P, const JumpTable& jt, void* __restrict__ B,
+                                         double* __restrict__ ktab, int64_t literalSlab, int64_t nSlab, int64_t t,
+                                         const DrawSink& sink = DrawSink{nullptr, nullptr}) {
+  const int32_t cols = table_cols(P);
+  const int64_t j = t / cols;
+  const int r = (int)(t % cols);
+  if (j >= table_runs(P)) return;
+  RunCursors cu;
+  cu.kA.pos = cu.kB.pos = cu.rA.pos = cu.rB.pos = 0;
+  cu.kA.last = cu.kB.last = cu.rA.last = cu.rB.last = 0;
+  if (P.gen == GEN_OUTER) {
+    // run j = i3 + lPad (i2 + n2 s2): i1 = 0 .. n1p-1, consecutive draws per sign s3
+    const int32_t i3 = (int32_t)(j % P.lPad);
+    const int64_t t2 = j / P.lPad;
+    const int32_t i2 = (int32_t)(t2 % P.kNStep[1]), s2 = (int32_t)(t2 / P.kNStep[1]);
+    for (int32_t i1 = 0; i1 < P.n1p; ++i1)
+      outer_element<SINK>(P, jt, reinterpret_cast<unsigned char*>(B), i1, i2, s2, i3, r, cu, sink);
+    return;
+  }
+  const int32_t len = table_run_length(P, j);
+  for (int32_t i = 0; i < len; ++i)
+    table_element<SINK>(P, jt, B, ktab, literalSlab, nSlab, table_run_kk(P, j, i), r, cu, sink);
+}
+
+__global__ void rf_tables_kernel(const Plan P, const JumpTable jt, void* __restrict__ B, double* __restrict__ ktab,
+                                 int64_t literalSlab, int64_t nSlab) {
+  table_run(P, jt, B, ktab, literalSlab, nSlab, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The same runs, cursors and draw positions as rf_tables_kernel, writing the
+// draws it consumes to `sink` (the bit-exact check of the device rnglib).
+__global__ void rf_table_draws_kernel(const Plan P, const JumpTable jt, DrawSink sink) {
+  table_run<true>(P, jt, nullptr, nullptr, -1, 1, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, sink);
+}
+
+// Grouped builder: a grid-stride loop over the concatenated run threads
+// (table_threads) of all units (a fixed grid, so that the launch can sit in
+// a captured graph).
 __global__ void rf_group_tables_kernel(const GroupSub* __restrict__ subs, const int64_t* __restrict__ prefix,
                                        const int32_t* __restrict__ nsubsPtr, const JumpTable jt) {
   const int32_t nsubs = *nsubsPtr;
@@ -242,7 +415,7 @@ __global__ void rf_group_tables_kernel(const GroupSub* __restrict__ subs, const 
       else hi = mid - 1;
     }
     const GroupSub& u = subs[lo];
-    table_element(u.P, jt, u.B, u.ktab, -1, 1, t - prefix[lo]);
+    table_run(u.P, jt, u.B, u.ktab, -1, 1, t - prefix[lo]);
   }
 }
 
@@ -252,10 +425,18 @@ cudaError_t launch_group_tables(const GroupSub* subs, const int64_t* prefix, con
   return cudaGetLastError();
 }
 
+cudaError_t launch_table_draws(const Plan& P, const JumpTable& jt, int32_t* dRk, int32_t* dK, cudaStream_t st) {
+  const int64_t total = table_threads(P);
+  const int threads = 128;
+  const int64_t blocks = (total + threads - 1) / threads;
+  rf_table_draws_kernel<<<(unsigned)blocks, threads, 0, st>>>(P, jt, DrawSink{dRk, dK});
+  return cudaGetLastError();
+}
+
 cudaError_t launch_tables(const Plan& P, const JumpTable& jt, void* dB, double* dKtab, int64_t literalSlab,
                           int64_t nSlab, cudaStream_t st) {
-  const int64_t total = P.nChunks * P.chunkK * P.nmcPad;
-  const int threads = 256;
+  const int64_t total = table_threads(P);
+  const int threads = 128;
   const int64_t blocks = (total + threads - 1) / threads;
   rf_tables_kernel<<<(unsigned)blocks, threads, 0, st>>>(P, jt, dB, dKtab, literalSlab, nSlab);
   return cudaGetLastError();

@@ -580,6 +580,7 @@ size_t fit_layout(SlotLayout& L, bool table, int maxS = kMaxStages) {
 }  // namespace
 
 size_t tc_smem_bytes(const Plan& P, int* stages) {
+  if (P.gen == GEN_OUTER) return outer_smem_bytes(P, stages);
   SlotLayout L;
   L.aCol0 = P.bRows;
   L.aStride = a_cols(P);
@@ -591,6 +592,7 @@ size_t tc_smem_bytes(const Plan& P, int* stages) {
 
 cudaError_t launch_tc(const Plan& P, const double* dX, const void* dB, const double* dKtab, double* dOut,
                       int64_t row0, int64_t rows, uint32_t* dErr, int numSMs, cudaStream_t st) {
+  if (P.gen == GEN_OUTER) return launch_outer(P, dX, dB, dOut, row0, rows, dErr, numSMs, st);
   TcArgs args;
   args.P = P;
   args.x = dX;

@@ -11,11 +11,15 @@ checked against exact phases on the CPU:
   within 1e-6 rad of k.x modulo 2 pi and within [-1.51 pi, 1.51 pi] for the
   isotropic wavevectors (|k| <= kMax = 7.355);
 - the FP64 reduction of the table generator's FAST form (table_pairs<true>);
-- the outer-phasor walk of GEN_GRID3 (Grid3Walk).
+- the outer-phasor walk of GEN_GRID3 (Grid3Walk);
+- the outer-group factorisation of GEN_OUTER (rf_outer.cu, and the operand
+  rf_tables.cu outer_element writes), against the oracle's field.
 float32 fused multiply-adds are emulated in float64 (exact products) with
 one final rounding.
 """
 import numpy as np
+
+from oracle import oracle as O
 
 UNIT = np.float32(6.283185307179586) * np.float32(2.0 ** -23)  # radians per 2^-23 turn
 
@@ -106,3 +110,34 @@ def test_grid3_outer_phasor_walk():
         ex = np.exp(1j * i * theta)
         worst = max(worst, float(np.abs((er.astype(np.float64) + 1j * ei.astype(np.float64)) - ex).max()))
     assert worst <= 4e-6
+
+
+def test_outer_group_factorisation_equals_oracle():
+    """The outer-group contraction of rf_outer.cu restated in numpy: A = the
+    outer phasors (Re, Im of E1(i1) E2(i2)^{s2}), B = the four coefficients
+    built from the s3 = +/- pair of each (outer group, i3) exactly as
+    rf_tables.cu outer_element writes them, and the epilogue's sum over i3
+    with cos and sin of k3 x3.  Equals the oracle's point-by-point sum."""
+    x = O.grid([0.0, 0.0, 0.0], [0.13, 0.11, 0.17], [7, 6, 5])
+    kn, Nmc = (5, 4, 3), 3
+    req = O.OracleRequest(x, Nmc=Nmc, kNStep=kn)
+    ref = req.generate()
+    g = req.geometry()
+    Bc, Bs = req.phase_matrix()  # [r, k]: a cos(phi), -a sin(phi)
+    n1, n2, n3 = kn
+    n123 = n1 * n2 * n3
+    f = np.zeros_like(ref)
+    for s2 in range(2):
+        for i2 in range(n2):
+            for i1 in range(n1):
+                k2 = g.kDelta[1] * i2 * (-1.0 if s2 else 1.0)
+                P = np.exp(1j * (g.kDelta[0] * i1 * x[:, 0] + k2 * x[:, 1]))
+                for i3 in range(n3):
+                    kp = 2 * s2 * n123 + i1 + n1 * (i2 + n2 * i3)
+                    km = kp + n123
+                    W = (Bc[:, kp] + Bc[:, km], Bs[:, kp] + Bs[:, km], Bs[:, kp] - Bs[:, km], Bc[:, km] - Bc[:, kp])
+                    c3, s3 = np.cos(g.kDelta[2] * i3 * x[:, 2]), np.sin(g.kDelta[2] * i3 * x[:, 2])
+                    f += (np.outer(W[0], P.real * c3) + np.outer(W[1], P.imag * c3) + np.outer(W[2], P.real * s3)
+                          + np.outer(W[3], P.imag * s3))
+    f *= g.ampMult
+    assert np.abs(f - ref).max() <= 1e-12 * np.abs(ref).max()
