@@ -308,6 +308,10 @@ typedef struct rf_batch_stats {
   int32_t stages;             /* pipeline depth of the grouped kernel */
   int32_t graph_replayed;     /* 1: the launch replayed a captured CUDA graph */
   int32_t tuned;              /* 1: this call ran the tuner */
+  int32_t outer_stages;       /* pipeline depth of the outer-group kernel (0: not launched) */
+  int32_t tune_candidates;    /* configurations the tuner timed for this batch class */
+  double tune_default_ms;     /* the default configuration's time in the tuner's search */
+  double tune_best_ms;        /* the chosen configuration's time in the tuner's search */
 } rf_batch_stats;
 
 /* Host buffers; returns when every field has been copied back. */

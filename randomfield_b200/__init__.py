@@ -145,6 +145,10 @@ class BatchStats(C.Structure):
         ("stages", C.c_int32),
         ("graph_replayed", C.c_int32),
         ("tuned", C.c_int32),
+        ("outer_stages", C.c_int32),
+        ("tune_candidates", C.c_int32),
+        ("tune_default_ms", C.c_double),
+        ("tune_best_ms", C.c_double),
     ]
 
     def as_dict(self) -> dict:

@@ -40,8 +40,18 @@ double stage_cost(const Plan& P) {
   return P.gen == GEN_GRID3 ? 1130.0 * std::max(0.6, n) : 600.0 * std::max(0.6, n);
 }
 
+// Relative device cost of one pair of tiles of a GEN_OUTER unit: MMAs of
+// N columns per K-step and tile, lo terms included.
+double outer_pair_cost(const Plan& P) {
+  const double mmas = (double)P.oNK + (double)mask_rank(P.loMask, P.oNK) + (double)mask_rank(P.aLoMask, P.oNK);
+  return (double)P.oNR * mmas * (double)(2 * P.lPad * P.oRc);
+}
+
+// Descriptor buffer: unit count, units, table prefix, then for each of the
+// two grouped kernels (tcgen05 contraction; outer-group contraction) its CTA
+// slices and work items.
 struct DescLayout {
-  size_t subs, prefix, cta, items, total;
+  size_t subs, prefix, cta, items, octa, oitems, total;
   size_t capUnits, capItems;
 };
 
@@ -53,8 +63,44 @@ DescLayout desc_layout(size_t capUnits, size_t capItems, int numSMs) {
   d.prefix = d.subs + align_up(capUnits * sizeof(GroupSub));
   d.cta = d.prefix + align_up((capUnits + 1) * sizeof(int64_t));
   d.items = d.cta + align_up((size_t)(numSMs + 1) * sizeof(int32_t));
-  d.total = d.items + align_up(capItems * sizeof(GroupItem));
+  d.octa = d.items + align_up(capItems * sizeof(GroupItem));
+  d.oitems = d.octa + align_up((size_t)(numSMs + 1) * sizeof(int32_t));
+  d.total = d.oitems + align_up(capItems * sizeof(GroupItem));
   return d;
+}
+
+// Longest-processing-time-first assignment of the work items of `units`
+// (`count[u]` items of cost `cost[u]` each) to nCta CTAs.
+std::vector<std::vector<GroupItem>> lpt_schedule(const std::vector<size_t>& units, const std::vector<int64_t>& count,
+                                                 const std::vector<double>& cost, int nCta) {
+  std::vector<size_t> order = units;
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+  using Load = std::pair<double, int>;
+  std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+  for (int b = 0; b < nCta; ++b) heap.push({0.0, b});
+  std::vector<std::vector<GroupItem>> perCta(nCta);
+  for (size_t u : order) {
+    for (int64_t t = 0; t < count[u]; ++t) {
+      Load l = heap.top();
+      heap.pop();
+      perCta[l.second].push_back(GroupItem{(int32_t)u, (int32_t)t});
+      l.first += cost[u];
+      heap.push(l);
+    }
+  }
+  return perCta;
+}
+
+// Writes CTA slices and items of one kernel into the staging buffer; returns the item count.
+int64_t put_schedule(const std::vector<std::vector<GroupItem>>& perCta, int32_t* cta, GroupItem* it) {
+  int32_t pos = 0;
+  for (size_t b = 0; b < perCta.size(); ++b) {
+    cta[b] = pos;
+    memcpy(it + pos, perCta[b].data(), perCta[b].size() * sizeof(GroupItem));
+    pos += (int32_t)perCta[b].size();
+  }
+  cta[perCta.size()] = pos;
+  return pos;
 }
 
 struct BatchState {
@@ -82,6 +128,8 @@ struct GroupRun {
   int rblk = 0;
   SlotLayout L{};
   size_t smem = 0;
+  OuterGroupArgs og{};  // slot layout of the outer-group kernel
+  size_t osmem = 0;
   int64_t units = 0, items = 0;
   bool replayed = false;
 };
@@ -103,7 +151,8 @@ int destroy_graphs(rf_context* c) {
 // Builds the units, operands, schedule and descriptors of one grouped run
 // with realization block `rblk`, and launches it (graph replay when one is
 // cached for the layout).  Timing events bev[0..2] bracket the two kernels.
-int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream_t st, GroupRun& run) {
+int group_run(rf_context* c, const BatchState& B, int prec, int rblk, int sTc, int sOuter, cudaStream_t st,
+              GroupRun& run) {
   run.prec = prec;
   run.rblk = rblk;
   // ---- units
@@ -124,6 +173,7 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
       if (int rc = layout(P)) return rc;
       if (!B.blend.empty() && B.blend[i].gTotal > 0) apply_blend(P, B.blend[i]);
       lo_layout(P);
+      if (P.gen == GEN_GRID3 && P.lPad == kGroupLPad) outer_layout(P);  // the outer-group kernel
       GroupSub g;
       memset(&g, 0, sizeof(g));
       g.P = P;
@@ -131,58 +181,68 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
       g.out = B.dout[i];
       subs.push_back(g);
       elems.push_back(table_threads(P));
-      tiles.push_back((P.n + kTileM - 1) / kTileM);
-      tileCost.push_back((double)P.nChunks * stage_cost(P));
-      maxBRows = std::max(maxBRows, P.bRows);
-      maxStage = std::max(maxStage, P.stageBytes);
-      arena += align_up((size_t)(P.nChunks * P.stageBytes));
+      const int64_t nt = (P.n + kTileM - 1) / kTileM;
+      if (P.gen == GEN_OUTER) {
+        tiles.push_back((nt + 1) / 2);  // pairs of tiles
+        tileCost.push_back(outer_pair_cost(P));
+      } else {
+        tiles.push_back(nt);
+        tileCost.push_back((double)P.nChunks * stage_cost(P));
+        maxBRows = std::max(maxBRows, P.bRows);
+        maxStage = std::max(maxStage, P.stageBytes);
+      }
+      arena += align_up((size_t)operand_bytes(P));
       if (P.gen == GEN_TABLE) arena += align_up((size_t)P.nChunks * kKtabStageBytes);
     }
   }
   const size_t nU = subs.size();
   run.units = (int64_t)nU;
-  run.smem = group_layout(maxBRows, maxStage, 0, &run.L);
-  if (run.smem == 0) return fail(RF_ENOTSUP, "grouped launch: stages of %lld bytes do not fit", (long long)maxStage);
+  std::vector<size_t> tcUnits, outerUnits;
+  std::vector<const Plan*> outerPlans;
+  for (size_t u = 0; u < nU; ++u) {
+    if (subs[u].P.gen == GEN_OUTER) {
+      outerUnits.push_back(u);
+      outerPlans.push_back(&subs[u].P);
+    } else {
+      tcUnits.push_back(u);
+    }
+  }
+  if (!tcUnits.empty()) {
+    run.smem = group_layout(maxBRows, maxStage, sTc, &run.L);
+    if (run.smem == 0) return fail(RF_ENOTSUP, "grouped launch: stages of %lld bytes do not fit", (long long)maxStage);
+  }
+  if (!outerUnits.empty()) {
+    run.osmem = outer_group_layout(outerPlans.data(), outerPlans.size(), sOuter, &run.og);
+    if (run.osmem == 0) return fail(RF_ENOTSUP, "grouped launch: outer-group slots do not fit");
+  }
 
   // ---- operands in the arena
   if (int rc = ensure(c->dArena, c->capArena, std::max<size_t>(arena, kAlign), "batch operands")) return rc;
   size_t off = 0;
   for (auto& g : subs) {
     g.B = c->dArena + off;
-    off += align_up((size_t)(g.P.nChunks * g.P.stageBytes));
+    off += align_up((size_t)operand_bytes(g.P));
     if (g.P.gen == GEN_TABLE) {
       g.ktab = reinterpret_cast<double*>(c->dArena + off);
       off += align_up((size_t)g.P.nChunks * kKtabStageBytes);
     }
   }
 
-  // ---- schedule: LPT over the tiles, longest units first
+  // ---- schedules: LPT over each kernel's items (tiles; pairs of tiles for
+  // the outer-group kernel), longest units first
   const int nCta = c->numSMs;
-  std::vector<size_t> order(nU);
-  for (size_t u = 0; u < nU; ++u) order[u] = u;
-  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return tileCost[a] > tileCost[b]; });
-  using Load = std::pair<double, int>;
-  std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
-  for (int b = 0; b < nCta; ++b) heap.push({0.0, b});
-  std::vector<std::vector<GroupItem>> perCta(nCta);
-  int64_t nItems = 0;
-  for (size_t u : order) {
-    for (int64_t t = 0; t < tiles[u]; ++t) {
-      Load l = heap.top();
-      heap.pop();
-      perCta[l.second].push_back(GroupItem{(int32_t)u, (int32_t)t});
-      l.first += tileCost[u];
-      heap.push(l);
-    }
-    nItems += tiles[u];
-  }
-  run.items = nItems;
+  const auto perCta = lpt_schedule(tcUnits, tiles, tileCost, nCta);
+  const auto perCtaO = lpt_schedule(outerUnits, tiles, tileCost, nCta);
+  int64_t nItems = 0, nItemsO = 0;
+  for (size_t u : tcUnits) nItems += tiles[u];
+  for (size_t u : outerUnits) nItemsO += tiles[u];
+  run.items = nItems + nItemsO;
 
   // ---- descriptors (pinned staging -> device).  Their capacities only
   // grow, so the offsets inside the buffer stay those of the cached graphs.
   size_t capU = std::max<size_t>(c->descCapU, 1024), capI = std::max<size_t>(c->descCapI, (size_t)1 << 16);
   while (capU < nU) capU *= 2;
-  while (capI < (size_t)nItems) capI *= 2;
+  while (capI < (size_t)std::max(nItems, nItemsO)) capI *= 2;
   const DescLayout D = desc_layout(capU, capI, nCta);
   if (capU != c->descCapU || capI != c->descCapI || !c->dDesc) {
     RF_CUDA(cudaStreamSynchronize(st), "batch sync");
@@ -202,16 +262,9 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
   int64_t* pre = reinterpret_cast<int64_t*>(h + D.prefix);
   pre[0] = 0;
   for (size_t u = 0; u < nU; ++u) pre[u + 1] = pre[u] + elems[u];
-  int32_t* cta = reinterpret_cast<int32_t*>(h + D.cta);
-  GroupItem* it = reinterpret_cast<GroupItem*>(h + D.items);
-  int32_t pos = 0;
-  for (int b = 0; b < nCta; ++b) {
-    cta[b] = pos;
-    memcpy(it + pos, perCta[b].data(), perCta[b].size() * sizeof(GroupItem));
-    pos += (int32_t)perCta[b].size();
-  }
-  cta[nCta] = pos;
-  RF_CUDA(cudaMemcpyAsync(c->dDesc, h, D.items + (size_t)nItems * sizeof(GroupItem), cudaMemcpyHostToDevice, st),
+  put_schedule(perCta, reinterpret_cast<int32_t*>(h + D.cta), reinterpret_cast<GroupItem*>(h + D.items));
+  put_schedule(perCtaO, reinterpret_cast<int32_t*>(h + D.octa), reinterpret_cast<GroupItem*>(h + D.oitems));
+  RF_CUDA(cudaMemcpyAsync(c->dDesc, h, D.oitems + (size_t)nItemsO * sizeof(GroupItem), cudaMemcpyHostToDevice, st),
           "batch descriptor copy");
 
   // ---- launch: tables, contraction (graph per layout)
@@ -221,13 +274,22 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
   g.ctaStart = reinterpret_cast<const int32_t*>(c->dDesc + D.cta);
   g.err = c->dErr;
   g.L = run.L;
+  OuterGroupArgs og = run.og;
+  og.subs = g.subs;
+  og.items = reinterpret_cast<const GroupItem*>(c->dDesc + D.oitems);
+  og.ctaStart = reinterpret_cast<const int32_t*>(c->dDesc + D.octa);
+  og.err = c->dErr;
+  const bool hasTc = !tcUnits.empty(), hasOuter = !outerUnits.empty();
   const GroupSub* dSubs = g.subs;
   const int64_t* dPrefix = reinterpret_cast<const int64_t*>(c->dDesc + D.prefix);
   const int32_t* dCount = reinterpret_cast<const int32_t*>(c->dDesc);
   for (auto& e : c->bev)
     if (!e) RF_CUDA(cudaEventCreate(&e), "cudaEventCreate");
-  RF_CUDA(group_set_smem(prec, run.smem), "grouped kernel attributes");
-  rf_context::GraphKey key{prec, run.L.S, run.L.aCol0, run.L.slotBytes, c->dDesc};
+  if (hasTc) RF_CUDA(group_set_smem(prec, run.smem), "grouped kernel attributes");
+  if (hasOuter) RF_CUDA(outer_group_set_smem(prec, run.osmem), "outer-group kernel attributes");
+  rf_context::GraphKey key{prec,          hasTc ? run.L.S : 0, hasTc ? run.L.aCol0 : 0, hasTc ? run.L.slotBytes : 0,
+                           hasOuter ? og.S : 0, hasOuter ? og.slotBytes : 0, hasOuter ? og.aBytes : 0,
+                           hasTc ? 1 : 0, c->dDesc};
   auto found = c->graphs.find(key);
   cudaGraphExec_t exec = nullptr;
   if (found != c->graphs.end()) {
@@ -239,10 +301,11 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
     cudaError_t e1 = cudaEventRecordWithFlags(c->bev[0], st, cudaEventRecordExternal);
     cudaError_t e2 = launch_group_tables(dSubs, dPrefix, dCount, jump_table(), nCta * 8, st);
     cudaError_t e3 = cudaEventRecordWithFlags(c->bev[1], st, cudaEventRecordExternal);
-    cudaError_t e4 = launch_group(prec, g, run.smem, nCta, st);
+    cudaError_t e4 = hasTc ? launch_group(prec, g, run.smem, nCta, st) : cudaSuccess;
+    cudaError_t e4o = hasOuter ? launch_outer_group(prec, og, run.osmem, nCta, st) : cudaSuccess;
     cudaError_t e5 = cudaEventRecordWithFlags(c->bev[2], st, cudaEventRecordExternal);
     cudaError_t ee = cudaStreamEndCapture(st, &graph);
-    for (cudaError_t e : {e1, e2, e3, e4, e5, ee})
+    for (cudaError_t e : {e1, e2, e3, e4, e4o, e5, ee})
       if (e != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
@@ -254,8 +317,20 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, cudaStream
     c->graphs[key] = exec;
   }
   RF_CUDA(cudaGraphLaunch(exec, st), "cudaGraphLaunch");
-  c->launches += 2;
+  c->launches += 1 + (hasTc ? 1 : 0) + (hasOuter ? 1 : 0);
   return RF_OK;
+}
+
+// The batch class of the tuner's key: whether the batch holds units of the
+// grouped tcgen05 kernel (bit 0) and of the outer-group kernel (bit 1).
+int batch_class(const BatchState& B) {
+  int cls = 0;
+  for (const Plan& P : B.plans) {
+    const bool outer = P.gen == GEN_GRID3 && P.lPad == kGroupLPad && P.kNStep[0] <= kOuterMaxN1P &&
+                       (P.prec == PREC_BF16 || P.prec == PREC_FP16 || P.prec == PREC_BF16_FAST);
+    cls |= outer ? 2 : 1;
+  }
+  return cls;
 }
 
 int batch_times(rf_context* c, double* tables, double* contract) {
@@ -279,29 +354,88 @@ int run_batch(rf_context* c, const rf_request* reqs, int32_t count, const std::v
   (void)reqs;
   GroupRun run;
   rf_batch_stats stats{};
-  if (c->tunedBlock[prec] == 0 && !B.accumulate) {
-    double best = 1e300;
-    int bestBlk = 0;
-    for (int blk : block_candidates(prec)) {
+  const int key = prec * 4 + batch_class(B);
+  auto tuned = c->tuned.find(key);
+  if (tuned == c->tuned.end() && !B.accumulate) {
+    // Coordinate search from the default (first realization block, deepest
+    // pipelines): the realization block, then one slot fewer in the grouped
+    // tcgen05 kernel, then a shallower outer-group pipeline; a candidate is
+    // kept when the whole batch (tables + contractions) runs faster.  Every
+    // candidate computes the same field.
+    rf_context::TuneChoice best;
+    best.blk = block_candidates(prec)[0];
+    auto time_of = [&](const rf_context::TuneChoice& t, double* ms, GroupRun* r) -> int {
+      if (int rc = group_run(c, B, prec, t.blk, t.sTc, t.sOuter, st, *r)) return rc;
+      double a = 0, b = 0;
+      if (int rc = batch_times(c, &a, &b)) return rc;
+      *ms = a + b;
+      return RF_OK;
+    };
+    GroupRun r0;
+    if (int rc = time_of(best, &best.bestMs, &r0)) return rc;
+    best.defaultMs = best.bestMs;
+    best.candidates = 1;
+    std::vector<rf_context::TuneChoice> tries;
+    for (int blk : block_candidates(prec))
+      if (blk != best.blk) {
+        rf_context::TuneChoice t = best;
+        t.blk = blk;
+        tries.push_back(t);
+      }
+    for (const rf_context::TuneChoice& t0 : tries) {
+      double ms = 0;
       GroupRun r;
-      if (int rc = group_run(c, B, prec, blk, st, r)) return rc;
-      double t = 0, k = 0;
-      if (int rc = batch_times(c, &t, &k)) return rc;
-      if (t + k < best) {
-        best = t + k;
-        bestBlk = blk;
+      if (int rc = time_of(t0, &ms, &r)) return rc;
+      ++best.candidates;
+      if (ms < best.bestMs) {
+        const int n = best.candidates;
+        const double d = best.defaultMs;
+        best = t0;
+        best.bestMs = ms;
+        best.defaultMs = d;
+        best.candidates = n;
       }
     }
-    c->tunedBlock[prec] = bestBlk;
+    // pipeline depths, one coordinate at a time (only the kernels the batch launches)
+    if (r0.L.S > 2) {
+      rf_context::TuneChoice t = best;
+      t.sTc = r0.L.S - 1;
+      double ms = 0;
+      GroupRun r;
+      if (int rc = time_of(t, &ms, &r)) return rc;
+      ++best.candidates;
+      if (ms < best.bestMs) {
+        best.sTc = t.sTc;
+        best.bestMs = ms;
+      }
+    }
+    if (r0.og.S > 4) {
+      rf_context::TuneChoice t = best;
+      t.sOuter = 4;
+      double ms = 0;
+      GroupRun r;
+      if (int rc = time_of(t, &ms, &r)) return rc;
+      ++best.candidates;
+      if (ms < best.bestMs) {
+        best.sOuter = t.sOuter;
+        best.bestMs = ms;
+      }
+    }
+    tuned = c->tuned.emplace(key, best).first;
     stats.tuned = 1;
   }
-  const int blk = c->tunedBlock[prec] ? c->tunedBlock[prec] : block_candidates(prec)[0];
-  if (int rc = group_run(c, B, prec, blk, st, run)) return rc;
+  const rf_context::TuneChoice choice =
+      tuned != c->tuned.end() ? tuned->second : rf_context::TuneChoice{block_candidates(prec)[0], 0, 0, 0, 0.0, 0.0};
+  if (int rc = group_run(c, B, prec, choice.blk, choice.sTc, choice.sOuter, st, run)) return rc;
   stats.units = run.units;
   stats.work_items = run.items;
   stats.realization_block = run.rblk;
   stats.stages = run.L.S;
+  stats.outer_stages = run.og.S;
   stats.graph_replayed = run.replayed ? 1 : 0;
+  stats.tune_candidates = choice.candidates;
+  stats.tune_default_ms = choice.defaultMs;
+  stats.tune_best_ms = choice.bestMs;
   // normalisation passes (per request, after the contraction)
   for (int32_t i = 0; i < count; ++i) {
     const Plan& P = B.plans[i];
@@ -342,7 +476,9 @@ int request_footprint(const Request& rq, const double* ext, int rblk, size_t* by
     P.rOff = r0;
     P.nmcBlk = std::min(rblk, P0.Nmc - r0);
     if (int rc = layout(P)) return rc;
-    b += align_up((size_t)(P.nChunks * P.stageBytes));
+    lo_layout(P);
+    if (P.gen == GEN_GRID3 && P.lPad == kGroupLPad) outer_layout(P);  // as group_run plans it
+    b += align_up((size_t)operand_bytes(P));
     if (P.gen == GEN_TABLE) b += align_up((size_t)P.nChunks * kKtabStageBytes);
   }
   *bytes = b;
@@ -502,8 +638,11 @@ int blend_finish(rf_context* c, const Plan& Gp, double* dOut, cudaStream_t st) {
 
 namespace {
 
-// The blended field of `grid` into the device array dOut (group points x Nmc).
+// The blended field of `grid` into the device array dOut (group points x Nmc):
+// through the structured-grid path where it applies (its subdomains are
+// grids), else as grouped-launch units whose epilogue adds the weighted field.
 int run_blended(rf_context* c, const rf_blend_grid* grid, const Request& base, double* dOut, cudaStream_t st) {
+  if (grid_blend_ok(grid, base)) return grid_blend_run(c, grid, base, dOut, st);
   size_t pb = 0;
   if (int rc = blend_points_bytes(grid, base.corrL, &pb)) return rc;
   if (int rc = ensure(c->dX, c->capX, pb, "subdomain points")) return rc;

@@ -281,6 +281,43 @@ __device__ __forceinline__ void table_pairs_fxp(const double* kt, int h, const F
   }
 }
 
+// GEN_TABLE for the tensor-core forms near the origin: the phase k.x in FP32
+// (three fused multiply-adds of the FP32 wavevector and point) and
+// __sincosf on it.  Rounding k and x to FP32 and the three operations leave
+// at most about |k|_2 |x|_1 2^-22 rad of error, and __sincosf's argument
+// reduction of an angle of n turns keeps 24 - log2(n) bits of its fraction;
+// for |x|_1 kMax <= 256 (table_f32_phase) both stay below 1e-4 rad, about
+// 1/20 of the 16-bit rounding of the trig tile that follows.  Five
+// instructions per pair besides the two MUFU operations, against about
+// twelve for the fixed-point phase.
+template <int T, typename Emit>
+__device__ __forceinline__ void table_pairs_f32(const double* kt, int h, const float* xf, Emit&& emit) {
+  static_assert(T % 4 == 0 && T <= kTableChunk, "pairs of wavevectors per thread");
+  const float* kf = reinterpret_cast<const float*>(reinterpret_cast<const int32_t*>(kt + 3 * kTableChunk) +
+                                                   3 * kTableChunk);
+  float r[T];
+#pragma unroll
+  for (int t = 0; t < T; t += 4) {
+    const int j = h * T + t;
+    const float4 f0 = *reinterpret_cast<const float4*>(kf + j);
+    const float4 f1 = *reinterpret_cast<const float4*>(kf + kTableChunk + j);
+    const float4 f2 = *reinterpret_cast<const float4*>(kf + 2 * kTableChunk + j);
+    r[t + 0] = fmaf(xf[2], f2.x, fmaf(xf[1], f1.x, xf[0] * f0.x));
+    r[t + 1] = fmaf(xf[2], f2.y, fmaf(xf[1], f1.y, xf[0] * f0.y));
+    r[t + 2] = fmaf(xf[2], f2.z, fmaf(xf[1], f1.z, xf[0] * f0.z));
+    r[t + 3] = fmaf(xf[2], f2.w, fmaf(xf[1], f1.w, xf[0] * f0.w));
+  }
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    float s, c;
+    __sincosf(r[t], &s, &c);
+    emit(t, c, s);
+  }
+}
+__device__ __forceinline__ bool table_f32_phase(const double* x, double kMax) {
+  return (fabs(x[0]) + fabs(x[1]) + fabs(x[2])) * kMax <= 256.0;
+}
+
 // Whether a point may take the FAST reduction of table_pairs: |x.k| / 2 pi is
 // below 2^18 turns for every |k_d| <= kMax (every table's bound).
 __device__ __forceinline__ bool table_fast_phase(const double* x, double kMax) {

@@ -37,6 +37,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <chrono>
+
 #include "rf_internal.h"
 
 using namespace rfb;
@@ -582,7 +584,101 @@ int grid_run(rf_context* ctx, SepSpec sp, const Plan& P, int Nmc, double* d_rand
   return RF_OK;
 }
 
+// The separable spec of subdomain f of a blend (seed seedStart + f + 1, the
+// reference's fieldNumber = f + 1, sample_RF.f90:311), its placement in the
+// group grid in `bp`; the subdomain field leaves the marginal map to the group.
+int blend_sub_spec(const rf_blend_grid* grid, const Request& base, const int32_t* L, const int32_t* O, int f,
+                   int64_t seed0, SepSpec& sp, Plan& P, Plan& bp) {
+  const int nd = grid->nDim;
+  int32_t F[3] = {1, 1, 1}, G[3] = {1, 1, 1};
+  for (int d = 0; d < nd; ++d) {
+    F[d] = grid->nFields[d];
+    G[d] = grid->xNStep[d];
+  }
+  const int32_t fi[3] = {f % F[0], (f / F[0]) % F[1], f / (F[0] * F[1])};
+  double x0[3] = {0, 0, 0}, h[3] = {0, 0, 0};
+  int64_t N[3] = {1, 1, 1};
+  memset(&bp, 0, sizeof(bp));
+  bp.nDim = nd;
+  for (int d = 0; d < 3; ++d) {
+    bp.bDims[d] = L[d];
+    bp.bOrigin[d] = d < nd ? fi[d] * (L[d] - std::max(O[d], 0)) : 0;
+    bp.gDims[d] = G[d];
+    bp.bRamp[d] = d < nd ? O[d] : 0;
+    if (d < nd) {
+      h[d] = grid->xStep[d];
+      x0[d] = grid->xMin[d] + (double)bp.bOrigin[d] * h[d];
+      N[d] = L[d];
+    }
+  }
+  bp.gTotal = (int64_t)G[0] * G[1] * G[2];
+  rf_options o = base.opt;
+  o.seed_start = seed0 + f + 1;
+  o.normalize = 0;
+  int device = 0;
+  if (int rc = grid_spec(nd, x0, h, N, base.corrMod, base.margiFirst, base.corrL, base.fieldAvg, base.fieldVar,
+                         base.Nmc, base.method, &o, sp, P, device))
+    return rc;
+  sp.applyMarginal = 0;
+  return RF_OK;
+}
+
 }  // namespace
+
+namespace rfh {
+
+bool grid_blend_ok(const rf_blend_grid* grid, const Request& base) {
+  if (base.method != RF_SHINOZUKA || base.opt.literal) return false;
+  int32_t L[3], O[3];
+  if (rf_blend_layout(grid, base.corrL, L, O) != RF_OK) return false;
+  SepSpec sp;
+  Plan P, bp;
+  const int ok = blend_sub_spec(grid, base, L, O, 0, std::max<int64_t>(base.opt.seed_start, 0), sp, P, bp);
+  g_err.clear();
+  return ok == RF_OK;
+}
+
+int grid_blend_run(rf_context* c, const rf_blend_grid* grid, const Request& base, double* dOut, cudaStream_t st) {
+  int32_t L[3], O[3];
+  if (int rc = rf_blend_layout(grid, base.corrL, L, O)) return rc;
+  int nSub = 1;
+  int64_t gTotal = 1;
+  for (int d = 0; d < grid->nDim; ++d) {
+    nSub *= grid->nFields[d];
+    gTotal *= grid->xNStep[d];
+  }
+  const int64_t sub = (int64_t)L[0] * L[1] * L[2];
+  int64_t seed0 = base.opt.seed_start;
+  if (seed0 < 0) {  // one stochastic seed, then + fieldNumber (sample_RF.f90:316-317)
+    const auto t = std::chrono::steady_clock::now().time_since_epoch().count();
+    seed0 = (int64_t)((uint64_t)t % 100000000ull);
+  }
+  if (int rc = ensure(c->dBlendSub, c->capBlendSub, sizeof(double) * (size_t)sub * base.Nmc, "blend subdomain field"))
+    return rc;
+  RF_CUDA(cudaMemsetAsync(dOut, 0, sizeof(double) * (size_t)gTotal * base.Nmc, st), "clear of randField");
+  Plan Gp;
+  for (int f = 0; f < nSub; ++f) {
+    SepSpec sp;
+    Plan P, bp;
+    if (int rc = blend_sub_spec(grid, base, L, O, f, seed0, sp, P, bp)) return rc;
+    if (int rc = grid_run(c, sp, P, base.Nmc, c->dBlendSub, st)) return rc;
+    RF_CUDA(launch_blend_add(bp, c->dBlendSub, dOut, sub, base.Nmc, st), "blend add kernel");
+    if (f == nSub - 1) Gp = P;  // marginal parameters of the request
+  }
+  // the group plan of the border correction and the marginal map
+  Gp.nDim = grid->nDim;
+  Gp.Nmc = base.Nmc;
+  Gp.n = gTotal;
+  Gp.gTotal = gTotal;
+  for (int d = 0; d < 3; ++d) {
+    Gp.gDims[d] = d < grid->nDim ? grid->xNStep[d] : 1;
+    Gp.bRamp[d] = d < grid->nDim ? O[d] : 0;
+  }
+  Gp.normalize = base.opt.normalize ? 1 : 0;
+  return blend_finish(c, Gp, dOut, st);
+}
+
+}  // namespace rfh
 
 extern "C" {
 

@@ -321,6 +321,7 @@ void context_free(rf_context* c) {
   cudaFree(c->dStats);
   cudaFree(c->dFft);
   cudaFree(c->dGrid);
+  cudaFree(c->dBlendSub);
   if (c->hStats) cudaFreeHost(c->hStats);
   cudaFree(c->dErr);
   cudaFree(c->dX);
@@ -438,7 +439,7 @@ constexpr double kOuterALoLeft = 0.10;
 constexpr double kOuterBLoLeft = 0.20;
 
 void outer_layout(Plan& P) {
-  if (P.gen != GEN_GRID3 || P.blend || P.literal) return;
+  if (P.gen != GEN_GRID3 || P.literal) return;
   if (P.prec != PREC_BF16 && P.prec != PREC_FP16 && P.prec != PREC_BF16_FAST) return;
   if (P.kNStep[0] > kOuterMaxN1P || P.lPad > 32) return;
   const int32_t n1 = P.kNStep[0], n2 = P.kNStep[1];

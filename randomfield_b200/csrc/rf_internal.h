@@ -36,6 +36,8 @@ struct rf_context {
   size_t capFft = 0;
   void* dGrid = nullptr;    // grid path: phasor tables, coefficients, axis-3 partial sums (rf_grid.cu)
   size_t capGrid = 0;
+  double* dBlendSub = nullptr;  // grid path blend: one subdomain's field
+  size_t capBlendSub = 0;
   double* dStats = nullptr; // field statistics scratch (rf_stats.cu)
   size_t capStats = 0;
   double* hStats = nullptr;
@@ -66,17 +68,31 @@ struct rf_context {
   struct GraphKey {
     int prec, S, aCol0;
     int64_t slotBytes;
+    int oS, oSlotBytes, oABytes;  // the outer-group kernel's slot layout (oS = 0: not launched)
+    int hasTc;                    // the grouped tcgen05 kernel is launched
     const void* desc;
     bool operator<(const GraphKey& o) const {
       if (prec != o.prec) return prec < o.prec;
       if (S != o.S) return S < o.S;
       if (aCol0 != o.aCol0) return aCol0 < o.aCol0;
       if (slotBytes != o.slotBytes) return slotBytes < o.slotBytes;
+      if (oS != o.oS) return oS < o.oS;
+      if (oSlotBytes != o.oSlotBytes) return oSlotBytes < o.oSlotBytes;
+      if (oABytes != o.oABytes) return oABytes < o.oABytes;
+      if (hasTc != o.hasTc) return hasTc < o.hasTc;
       return desc < o.desc;
     }
   };
   std::map<GraphKey, cudaGraphExec_t> graphs;
-  int tunedBlock[4] = {0, 0, 0, 0};  // realization block chosen by the tuner, per precision form
+  // The grouped launch's tuner: per (precision form, batch class) the chosen
+  // realization block and pipeline depths of both grouped kernels, with the
+  // report of the search that chose them.
+  struct TuneChoice {
+    int blk = 0, sTc = 0, sOuter = 0;  // 0: the deepest pipeline that fits
+    int candidates = 0;
+    double defaultMs = 0.0, bestMs = 0.0;
+  };
+  std::map<int, TuneChoice> tuned;
   rf_batch_stats last{};
 };
 
@@ -115,6 +131,8 @@ constexpr int kExtentBlocks = 128;
 const rfb::JumpTable& jump_table();
 int64_t round_up(int64_t v, int64_t m);
 int validate(const Request& r);
+// Whether axis d's extent enters the geometry (no explicit wavenumber count).
+bool extent_needed(const Request& r, int d);
 int layout(rfb::Plan& P);
 int build_plan(const Request& rq, const double* ext, rfb::Plan& P);
 int seeds(int64_t seedStart, rfb::Plan& P);
@@ -153,6 +171,13 @@ int blend_expand(const rf_blend_grid* grid, const Request& base, double* dOut, d
                  std::vector<Request>& rq, std::vector<const double*>& dx, std::vector<double*>& dout,
                  std::vector<BlendSpec>& spec, rfb::Plan* groupPlan);
 int blend_finish(rf_context* c, const rfb::Plan& Gp, double* dOut, cudaStream_t st);
+// Whether the structured-grid path takes the blend of `grid` (Shinozuka, at
+// most the grid path's wavenumbers per axis, not literal); no device work.
+bool grid_blend_ok(const rf_blend_grid* grid, const Request& base);
+// The blend through the structured-grid path (rf_grid.cu): each subdomain
+// summed axis by axis in FP64, weighted and added into dOut, then the border
+// correction and the marginal map.  Call only where grid_blend_ok holds.
+int grid_blend_run(rf_context* c, const rf_blend_grid* grid, const Request& base, double* dOut, cudaStream_t st);
 // Device bytes a request holds in a batch with realization block rblk:
 // points, field, operands.
 int request_footprint(const Request& rq, const double* ext, int rblk, size_t* bytes);

@@ -45,6 +45,12 @@ cudaError_t launch_normalize_and_map(const Plan& P, double* dOut, int32_t ncols,
 cudaError_t launch_grid_points(double* dX, int32_t nDim, const int32_t* L, const double* x0, const double* h,
                                cudaStream_t st);
 
+// One subdomain's field (subPoints x Nmc) times its partition-of-unity
+// weights added into the group field; P carries nDim, bDims, bOrigin, gDims,
+// bRamp and gTotal.
+cudaError_t launch_blend_add(const Plan& P, const double* dSub, double* dGroup, int64_t subPoints, int32_t Nmc,
+                             cudaStream_t st);
+
 // Border correction of a blended group field, then (applyMarginal) the
 // marginal map; G carries nDim, Nmc, gDims, gTotal, bRamp and the marginal.
 cudaError_t launch_blend_finish(const Plan& G, double* dOut, int32_t applyMarginal, cudaStream_t st);
@@ -72,6 +78,25 @@ size_t group_layout(int32_t maxBRows, int64_t maxStageBytes, int32_t maxStages, 
 // then launch_group queues it.
 cudaError_t group_set_smem(int prec, size_t smem);
 cudaError_t launch_group(int prec, const GroupArgs& g, size_t smem, int grid, cudaStream_t st);
+
+// Grouped outer-group contraction (rf_outer.cu): every CTA b runs the items
+// items[ctaStart[b] .. ctaStart[b+1]) of the GEN_OUTER units `subs` (an
+// item's `tile` is a pair of 128-point tiles; lPad == kGroupLPad), with one
+// slot layout for all: S slots of slotBytes, the A area aBytes.
+struct OuterGroupArgs {
+  const GroupSub* subs;
+  const GroupItem* items;
+  const int32_t* ctaStart;
+  uint32_t* err;
+  int32_t S, slotBytes, aBytes;
+};
+// Slot layout covering every plan (its largest A and B areas), at most
+// maxStages slots (0: as many as fit); returns the shared-memory bytes (0:
+// none fits) and fills S, slotBytes, aBytes.
+size_t outer_group_layout(const Plan* const* plans, size_t count, int maxStages, OuterGroupArgs* g);
+// Sets the kernel's shared-memory size (outside any stream capture).
+cudaError_t outer_group_set_smem(int prec, size_t smem);
+cudaError_t launch_outer_group(int prec, const OuterGroupArgs& g, size_t smem, int grid, cudaStream_t st);
 
 // Grouped table builder: B (and the wavevector chunks) of every unit; the
 // element range of unit u is [prefix[u], prefix[u+1]) of prefix[*nsubs]

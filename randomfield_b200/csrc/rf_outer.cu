@@ -43,6 +43,7 @@
 //               E3 phasors, ampMult, the marginal map, FP64 stores.
 // Every wait is bounded (globaltimer); on expiry the kernel raises the error
 // word, drains its own async work, frees TMEM and returns.
+#include "rf_blend.cuh"
 #include "rf_device.cuh"
 #include "rf_gen.cuh"
 #include "rf_launch.h"
@@ -84,6 +85,53 @@ struct OuterArgs {
   int32_t aBytes;     // A area: two tiles x 4 KB, twice with a lo term
 };
 
+// One work item (a pair of 128-point tiles of one request) as every role sees it.
+struct OuterView {
+  const Plan* P;
+  const double* x;
+  double* out;
+  const unsigned char* B;
+  int64_t row0, rows;  // point range of the request covered by the launch
+  int64_t pair;        // pair of tiles inside that range
+};
+
+// The pairs blockIdx.x, blockIdx.x + gridDim.x, ... of one request.
+struct SingleOuterWork {
+  const OuterArgs* a;
+  int64_t pairs;
+  __device__ __forceinline__ int64_t count() const {
+    return (int64_t)blockIdx.x < pairs ? (pairs - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  }
+  __device__ __forceinline__ void get(int64_t i, OuterView& v) const {
+    v.P = &a->P;
+    v.x = a->x;
+    v.out = a->out;
+    v.B = a->B;
+    v.row0 = a->row0;
+    v.rows = a->rows;
+    v.pair = blockIdx.x + i * gridDim.x;
+  }
+};
+
+// This CTA's slice [ctaStart[b], ctaStart[b+1]) of a grouped work list; an
+// item's `tile` field holds its pair index.
+struct GroupOuterWork {
+  const OuterGroupArgs* g;
+  int64_t begin, end;
+  __device__ __forceinline__ int64_t count() const { return end - begin; }
+  __device__ __forceinline__ void get(int64_t i, OuterView& v) const {
+    const GroupItem it = g->items[begin + i];
+    const GroupSub& s = g->subs[it.sub];
+    v.P = &s.P;
+    v.x = s.x;
+    v.out = s.out;
+    v.B = s.B;
+    v.row0 = 0;
+    v.rows = s.P.n;
+    v.pair = it.tile;
+  }
+};
+
 __device__ __forceinline__ void outer_abort(OuterBars* bars, uint32_t* err) {
   *reinterpret_cast<volatile int*>(&bars->abort_flag) = 1;
   atomicOr(err, kErrTimeout);
@@ -112,21 +160,16 @@ __device__ __forceinline__ float2 unpack16(uint32_t w) {
   return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
 }
 
-// LPAD: axis-3 length padded to 8, 16, 24 or 32 (the epilogue's phasor table).
-template <int PREC, int LPAD>
-__global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid_constant__ OuterArgs a) {
-  const Plan& P = a.P;
+// The pipeline of one CTA over the work items of `w`.  LPAD: axis-3 length
+// padded to 8, 16, 24 or 32 (every item of a launch has this lPad).
+template <int PREC, int LPAD, class Work>
+__device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotBytes, int32_t aBytes, uint32_t* err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   OuterBars* bars = reinterpret_cast<OuterBars*>(smem);
   unsigned char* slots = smem + kOuterHeader;
   volatile int* abort_flag = &bars->abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int S = a.S;
-  const int64_t tiles = (a.rows + kTileM - 1) / kTileM;
-  const int64_t pairs = (tiles + 1) / 2;
-  const int64_t count = (int64_t)blockIdx.x < pairs ? (pairs - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  const int32_t nK = P.oNK, nR = P.oNR;
-  const int32_t nRows = 2 * P.lPad * P.oRc;  // B rows (N) of a full chunk
+  const int64_t count = w.count();
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -148,6 +191,7 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = bars->tmem_base;
+  OuterView v;
 
   if (warp == kProducerWarp) {
     // ------------------------------------------------------------ producer
@@ -155,22 +199,24 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid
       uint32_t s = 0, ph = 0;
       bool ok = true;
       for (int64_t i = 0; i < count && ok; ++i) {
-        for (int32_t c = 0; c < nR && ok; ++c) {
-          const unsigned char* src = a.B + (int64_t)c * P.oChunkBytes;
-          for (int32_t j = 0; j < nK; ++j) {
+        w.get(i, v);
+        const Plan& P = *v.P;
+        for (int32_t c = 0; c < P.oNR && ok; ++c) {
+          const unsigned char* src = v.B + (int64_t)c * P.oChunkBytes;
+          for (int32_t j = 0; j < P.oNK; ++j) {
             if (!mbar_wait(&bars->empty[s], ph ^ 1, abort_flag)) {
               ok = false;
               break;
             }
             const uint32_t bytes = (uint32_t)(outer_b_lo(P, j) ? 2 * P.oKstepBytes : P.oKstepBytes);
             mbar_arrive_expect_tx(&bars->full[s], bytes);
-            bulk_g2s(slots + (size_t)s * a.slotBytes + a.aBytes, src, bytes, &bars->full[s]);
+            bulk_g2s(slots + (size_t)s * slotBytes + aBytes, src, bytes, &bars->full[s]);
             src += bytes;
             if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
           }
         }
       }
-      if (!ok) outer_abort(bars, a.err);
+      if (!ok) outer_abort(bars, err);
       if (*abort_flag) {
         // copies still in flight complete_tx on full barriers whose generator
         // arrivals may never come: wait for them by time before the CTA exits
@@ -187,17 +233,20 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid
     bool ok = true;
     const uint32_t ab = PREC == PREC_FP16 ? 0u : 1u;
     const uint32_t aDescLo = (uint32_t)(2 * kATileBytes) >> 4;  // descriptor step to the lo A tiles
-    const uint32_t bDescLo = (uint32_t)(P.oKstepBytes >> 4);
     for (int64_t i = 0; i < count && ok; ++i) {
-      for (int32_t c = 0; c < nR && ok; ++c) {
+      w.get(i, v);
+      const Plan& P = *v.P;
+      const uint32_t bDescLo = (uint32_t)(P.oKstepBytes >> 4);
+      const uint32_t nRows = (uint32_t)(2 * P.lPad * P.oRc);  // B rows (N) of a full chunk
+      for (int32_t c = 0; c < P.oNR && ok; ++c) {
         const int32_t rc = min(P.oRc, P.nmcBlk - c * P.oRc);
         const uint32_t idesc = make_idesc(ab, 128u, (uint32_t)(2 * P.lPad * rc));
-        for (int32_t j = 0; j < nK; ++j) {
+        for (int32_t j = 0; j < P.oNK; ++j) {
           if (!mbar_wait_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
           tc_fence_after();
-          const uint32_t base = smem_u32(slots + (size_t)s * a.slotBytes);
+          const uint32_t base = smem_u32(slots + (size_t)s * slotBytes);
           const uint64_t aDesc = make_sdesc(base, 2048u, 128u);
-          const uint64_t bDesc = make_sdesc(base + (uint32_t)a.aBytes, (uint32_t)nRows * 16u, 128u);
+          const uint64_t bDesc = make_sdesc(base + (uint32_t)aBytes, nRows * 16u, 128u);
           const bool bLo = outer_b_lo(P, j), aLo = outer_a_lo(P, j);
 #pragma unroll
           for (int t = 0; t < 2; ++t) {
@@ -224,7 +273,7 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid
         accPh ^= 1;
       }
     }
-    if (!ok && lane == 0) outer_abort(bars, a.err);
+    if (!ok && lane == 0) outer_abort(bars, err);
     if (leader) mma_commit(&bars->done);
     __syncwarp();
     volatile int never = 0;
@@ -235,24 +284,25 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid
     const int gi = threadIdx.x - kGenWarp0 * 32;  // 0 .. 255
     const int t = gi >> 7, row = gi & 127;
     const uint32_t rowOff = (uint32_t)((row >> 3) * 128 + (row & 7) * 16);
-    const int32_t n1 = P.kNStep[0], n2 = P.kNStep[1], nJJ = P.n1p >> 3;
     uint32_t s = 0, ph = 0;
     bool ok = true;
     for (int64_t i = 0; i < count && ok; ++i) {
-      const int64_t pair = blockIdx.x + i * gridDim.x;
-      const int64_t p = a.row0 + pair * kPairRows + t * kTileM + row;
-      const bool valid = p < a.row0 + a.rows;
+      w.get(i, v);
+      const Plan& P = *v.P;
+      const int32_t n1 = P.kNStep[0], n2 = P.kNStep[1], nJJ = P.n1p >> 3;
+      const int64_t p = v.row0 + v.pair * kPairRows + t * kTileM + row;
+      const bool valid = p < v.row0 + v.rows;
       double x0 = 0.0, x1 = 0.0;
       if (valid) {
-        x0 = a.x[p * 3 + 0] / P.corrL[0];
-        x1 = a.x[p * 3 + 1] / P.corrL[1];
+        x0 = v.x[p * 3 + 0] / P.corrL[0];
+        x1 = v.x[p * 3 + 1] / P.corrL[1];
       }
       float2 e1[kOuterMaxN1P];
 #pragma unroll
       for (int u = 0; u < kOuterMaxN1P; ++u)
         e1[u] = (u < n1) ? axis_phasor(P.kDelta[0], u, x0) : make_float2(0.f, 0.f);
       const float2 e2step = axis_phasor(P.kDelta[1], 1, x1);
-      for (int32_t c = 0; c < nR && ok; ++c) {
+      for (int32_t c = 0; c < P.oNR && ok; ++c) {
         for (int32_t s2 = 0; s2 < 2 && ok; ++s2) {
           float2 e2 = make_float2(1.f, 0.f);  // E2(i2), walked by angle addition
           for (int32_t i2 = 0; i2 < n2 && ok; ++i2) {
@@ -273,7 +323,7 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid
                   pv[u] = make_float2(q.x * E.x - q.y * E.y, q.x * E.y + q.y * E.x);
                   hi[u] = pack16<PREC>(pv[u].x, pv[u].y);
                 }
-                unsigned char* A = slots + (size_t)s * a.slotBytes + t * kATileBytes + rowOff;
+                unsigned char* A = slots + (size_t)s * slotBytes + t * kATileBytes + rowOff;
                 *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
                 *reinterpret_cast<uint4*>(A + 2048) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
                 if (outer_a_lo(P, j)) {  // the residual of the 16-bit rounding, rounded again
@@ -297,7 +347,7 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid
         }
       }
     }
-    if (!ok) outer_abort(bars, a.err);
+    if (!ok) outer_abort(bars, err);
   } else {
     // ------------------------------------------------------------ epilogue
     const int q = warp & 3, t = (warp - kEpiWarp0) >> 2;
@@ -307,15 +357,19 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid
     uint32_t accPh = 0;
     bool ok = true;
     for (int64_t i = 0; i < count && ok; ++i) {
-      const int64_t pair = blockIdx.x + i * gridDim.x;
-      const int64_t p = a.row0 + pair * kPairRows + t * kTileM + row;
-      const bool valid = p < a.row0 + a.rows;
-      const double x2 = valid ? a.x[p * 3 + 2] / P.corrL[2] : 0.0;
+      w.get(i, v);
+      const Plan& P = *v.P;
+      const int64_t p = v.row0 + v.pair * kPairRows + t * kTileM + row;
+      const bool valid = p < v.row0 + v.rows;
+      const double x2 = valid ? v.x[p * 3 + 2] / P.corrL[2] : 0.0;
+      double bw = 0.0;  // localization blend: weight and group index of this point
+      int64_t bg = 0;
+      if (P.blend && valid) bw = blend_weight(P, p, &bg);
       float2 e3[LPAD];
 #pragma unroll
       for (int u = 0; u < LPAD; ++u)
         e3[u] = (u < P.kNStep[2]) ? axis_phasor(P.kDelta[2], u, x2) : make_float2(0.f, 0.f);
-      for (int32_t c = 0; c < nR; ++c) {
+      for (int32_t c = 0; c < P.oNR; ++c) {
         if (!mbar_wait_warp(&bars->acc_full, accPh, abort_flag)) { ok = false; break; }
         tc_fence_after();
         const int32_t rc = min(P.oRc, P.nmcBlk - c * P.oRc);
@@ -327,12 +381,16 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid
             tmem_ld16(taddr0 + (uint32_t)(rl * 2 * LPAD + 16 * h), y);
             tmem_ld_wait();
 #pragma unroll
-            for (int v = 0; v < 8; ++v) {
-              acc = fmaf(e3[8 * h + v].x, __uint_as_float(y[2 * v]), acc);
-              acc = fmaf(e3[8 * h + v].y, __uint_as_float(y[2 * v + 1]), acc);
+            for (int u = 0; u < 8; ++u) {
+              acc = fmaf(e3[8 * h + u].x, __uint_as_float(y[2 * u]), acc);
+              acc = fmaf(e3[8 * h + u].y, __uint_as_float(y[2 * u + 1]), acc);
             }
           }
-          if (valid) a.out[(int64_t)(P.rOff + c * P.oRc + rl) * P.n + p] = outer_finish(P, acc);
+          if (valid) {
+            const int64_t r = (int64_t)P.rOff + c * P.oRc + rl;
+            if (P.blend) atomicAdd(&v.out[r * P.gTotal + bg], bw * ((double)acc * P.outScale));
+            else v.out[r * P.n + p] = outer_finish(P, acc);
+          }
         }
         tc_fence_before();
         __syncwarp();
@@ -340,13 +398,26 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid
         accPh ^= 1;
       }
     }
-    if (!ok) outer_abort(bars, a.err);
+    if (!ok) outer_abort(bars, err);
   }
 
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   if (warp == kIssuerWarp) tmem_dealloc(tbase, kOuterTmemCols);
+}
+
+template <int PREC, int LPAD>
+__global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid_constant__ OuterArgs a) {
+  const int64_t tiles = (a.rows + kTileM - 1) / kTileM;
+  const SingleOuterWork w{&a, (tiles + 1) / 2};
+  outer_body<PREC, LPAD>(w, a.S, a.slotBytes, a.aBytes, a.err);
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_group_kernel(const __grid_constant__ OuterGroupArgs g) {
+  const GroupOuterWork w{&g, g.ctaStart[blockIdx.x], g.ctaStart[blockIdx.x + 1]};
+  outer_body<PREC, kGroupLPad>(w, g.S, g.slotBytes, g.aBytes, g.err);
 }
 
 // Slot layout of a plan: A area (two tiles, twice with a lo term somewhere)
@@ -382,18 +453,54 @@ cudaError_t launch_outer_p(const OuterArgs& a, size_t smem, int grid, cudaStream
   }
 }
 
+// Slots of slotBytes that fit the shared memory, and the bytes to request
+// (0 when fewer than two fit).  More than half of the SM's shared memory is
+// requested so that one CTA (and its 512 TMEM columns) sits on an SM.
+size_t outer_fit(int32_t slotBytes, int* stages, int maxStages = 0) {
+  const size_t limit = 227 * 1024, floor = 120 * 1024;
+  int S = (int)((limit - kOuterHeader) / (size_t)slotBytes);
+  if (S > kOuterMaxSlots) S = kOuterMaxSlots;
+  if (maxStages > 0 && S > maxStages) S = maxStages;
+  if (stages) *stages = S;
+  if (S < 2) return 0;
+  const size_t total = (size_t)kOuterHeader + (size_t)S * slotBytes;
+  return total < floor ? floor : total;
+}
+
 }  // namespace
 
 size_t outer_smem_bytes(const Plan& P, int* stages) {
   int32_t aBytes = 0, slotBytes = 0;
   outer_slot(P, &aBytes, &slotBytes);
-  const size_t limit = 227 * 1024, floor = 120 * 1024;  // > half the SM: one CTA (and its 512 TMEM columns) per SM
-  int S = (int)((limit - kOuterHeader) / (size_t)slotBytes);
-  if (S > kOuterMaxSlots) S = kOuterMaxSlots;
-  if (stages) *stages = S;
-  if (S < 2) return 0;
-  const size_t total = (size_t)kOuterHeader + (size_t)S * slotBytes;
-  return total < floor ? floor : total;
+  return outer_fit(slotBytes, stages);
+}
+
+size_t outer_group_layout(const Plan* const* plans, size_t count, int maxStages, OuterGroupArgs* g) {
+  int32_t aMax = 2 * kATileBytes, bMax = 0;
+  for (size_t i = 0; i < count; ++i) {
+    int32_t a = 0, sb = 0;
+    outer_slot(*plans[i], &a, &sb);
+    aMax = a > aMax ? a : aMax;
+    bMax = (sb - a) > bMax ? (sb - a) : bMax;
+  }
+  g->aBytes = aMax;
+  g->slotBytes = (aMax + bMax + 127) / 128 * 128;
+  int S = 0;
+  const size_t smem = outer_fit(g->slotBytes, &S, maxStages);
+  g->S = S;
+  return smem;
+}
+
+cudaError_t outer_group_set_smem(int prec, size_t smem) {
+  const int b = (int)smem;
+  if (prec == PREC_FP16) return cudaFuncSetAttribute(rf_outer_group_kernel<PREC_FP16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  return cudaFuncSetAttribute(rf_outer_group_kernel<PREC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+}
+
+cudaError_t launch_outer_group(int prec, const OuterGroupArgs& g, size_t smem, int grid, cudaStream_t st) {
+  if (prec == PREC_FP16) rf_outer_group_kernel<PREC_FP16><<<grid, kOuterThreads, smem, st>>>(g);
+  else rf_outer_group_kernel<PREC_BF16><<<grid, kOuterThreads, smem, st>>>(g);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_outer(const Plan& P, const double* dX, const void* dB, double* dOut, int64_t row0, int64_t rows,

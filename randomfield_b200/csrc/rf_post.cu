@@ -4,6 +4,8 @@
 // for normalisation; otherwise the map is fused into the contraction
 // epilogue.  Sums are FP64: column mean, then the mean square of the
 // centred column, exactly the two reductions of the reference.
+#include <algorithm>
+
 #include "rf_blend.cuh"
 #include "rf_device.cuh"
 #include "rf_launch.h"
@@ -56,6 +58,22 @@ __global__ void rf_apply_kernel(double* __restrict__ f, int64_t n, int32_t ncols
     v = v * P.margSd + P.margAvg;
     if (P.lognormal) v = exp(v);
     c[i] = v;
+  }
+}
+
+// One subdomain's field (bDims points, axis 1 fastest, x Nmc, column-major)
+// times its partition-of-unity weights, added into the group field
+// (add_RF_to_Group, localization_RF.f90:199-263).  The subdomains of a group
+// are added one launch after another on one stream, so plain read-modify-
+// writes suffice and the sum is deterministic.
+__global__ void rf_blend_add_kernel(const double* __restrict__ sub, double* __restrict__ group, const Plan P,
+                                    int64_t subPoints, int32_t Nmc) {
+  const int64_t total = subPoints * Nmc;
+  for (int64_t t = (int64_t)blockIdx.x * kThreads + threadIdx.x; t < total; t += (int64_t)gridDim.x * kThreads) {
+    const int64_t r = t / subPoints, p = t % subPoints;
+    int64_t g = 0;
+    const double w = blend_weight(P, p, &g);
+    group[r * P.gTotal + g] += w * sub[t];
   }
 }
 
@@ -113,6 +131,14 @@ cudaError_t launch_blend_finish(const Plan& G, double* dOut, int32_t applyMargin
   const int64_t want = (G.gTotal + kThreads - 1) / kThreads;
   const unsigned bx = (unsigned)(want < 296 ? want : 296);
   rf_blend_finish_kernel<<<dim3(bx, G.Nmc), kThreads, 0, st>>>(dOut, G, applyMarginal);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_blend_add(const Plan& P, const double* dSub, double* dGroup, int64_t subPoints, int32_t Nmc,
+                             cudaStream_t st) {
+  const int64_t total = subPoints * Nmc;
+  const int blocks = (int)std::min<int64_t>((total + kThreads - 1) / kThreads, 4096);
+  rf_blend_add_kernel<<<blocks, kThreads, 0, st>>>(dSub, dGroup, P, subPoints, Nmc);
   return cudaGetLastError();
 }
 

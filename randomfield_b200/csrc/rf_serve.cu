@@ -128,7 +128,8 @@ int launch_slot(rf_server* s, Slot& sl) {
   std::vector<double*> dout, fieldOut(n);
   std::vector<double> ext;
   std::vector<BlendSpec> spec;
-  std::vector<std::pair<size_t, Plan>> groups;  // blended requests: index, group plan
+  std::vector<std::pair<size_t, Plan>> groups;  // blended requests in the grouped launch: index, group plan
+  std::vector<size_t> gridBlends;               // blended requests through the structured-grid path
   sl.outOff.assign(n, 0);
   unsigned char* dbase = reinterpret_cast<unsigned char*>(c->dX);
   size_t off = 0, soff = 0;
@@ -145,6 +146,10 @@ int launch_slot(rf_server* s, Slot& sl) {
     } else {
       sl.outOff[i] = soff;
       soff += align_up(ob);
+    }
+    if (p.blended && grid_blend_ok(&p.grid, p.rq)) {
+      gridBlends.push_back(i);
+      continue;
     }
     if (p.blended) {
       Plan Gp;
@@ -169,9 +174,12 @@ int launch_slot(rf_server* s, Slot& sl) {
     memset(&none, 0, sizeof(none));
     spec.push_back(none);
   }
-  if (int rc = batch_run_device(c, rq, dx, dout, ext, st, groups.empty() ? nullptr : &spec)) return rc;
+  if (!rq.empty())
+    if (int rc = batch_run_device(c, rq, dx, dout, ext, st, groups.empty() ? nullptr : &spec)) return rc;
   for (auto& g : groups)
     if (int rc = blend_finish(c, g.second, fieldOut[g.first], st)) return rc;
+  for (size_t i : gridBlends)
+    if (int rc = grid_blend_run(c, &sl.batch[i].grid, sl.batch[i].rq, fieldOut[i], st)) return rc;
   for (size_t i = 0; i < n; ++i) {
     const Pending& p = sl.batch[i];
     const size_t ob = sizeof(double) * (size_t)p.fieldPoints() * p.rq.Nmc;
@@ -366,6 +374,7 @@ int rf_server_create(const rf_server_config* cfg, rf_server** out) {
 }
 
 int rf_server_submit(rf_server* s, const rf_request* req, int64_t* ticket) {
+  const double tEnter = now_s();  // latency counts the caller's whole wait, validation included
   g_err.clear();
   if (!s || !req || !ticket) return fail(RF_EINVAL_ARG, "null pointer argument");
   if (!req->xPoints || !req->randField) return fail(RF_EINVAL_ARG, "null request buffer");
@@ -379,7 +388,7 @@ int rf_server_submit(rf_server* s, const rf_request* req, int64_t* ticket) {
   if (p.rq.opt.literal) return fail(RF_ENOTSUP, "literal mode is not available in the serving loop");
   for (int d = 0; d < 3; ++d) p.ext[d] = 0.0;
   for (int d = 0; d < p.rq.nDim; ++d) {
-    if (p.rq.opt.x_range[d] > 0.0) continue;
+    if (p.rq.opt.x_range[d] > 0.0 || !extent_needed(p.rq, d)) continue;  // no pass over the points
     double lo = req->xPoints[d], hi = req->xPoints[d];
     for (int64_t k = 1; k < req->n; ++k) {
       lo = std::min(lo, req->xPoints[k * req->nDim + d]);
@@ -388,7 +397,7 @@ int rf_server_submit(rf_server* s, const rf_request* req, int64_t* ticket) {
     p.ext[d] = hi - lo;
   }
   if (int rc = request_footprint(p.rq, p.ext, s->block, &p.bytes)) return rc;
-  p.tSubmit = now_s();
+  p.tSubmit = tEnter;
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return fail(RF_EINVAL_ARG, "the server is stopping");
@@ -405,6 +414,7 @@ int rf_server_submit(rf_server* s, const rf_request* req, int64_t* ticket) {
 int rf_server_submit_blended(rf_server* s, const rf_blend_grid* grid, int corrMod, int margiFirst,
                              const double* corrL, double fieldAvg, double fieldVar, int Nmc, int method,
                              double* randField, const rf_options* opt, int64_t* ticket) {
+  const double tEnter = now_s();
   g_err.clear();
   if (!s || !grid || !corrL || !randField || !ticket) return fail(RF_EINVAL_ARG, "null pointer argument");
   Pending p;
@@ -434,7 +444,7 @@ int rf_server_submit_blended(rf_server* s, const rf_blend_grid* grid, int corrMo
   const size_t subIO = sizeof(double) * (size_t)sub.n * (sub.nDim + sub.Nmc);
   p.bytes = p.pointBytes + sizeof(double) * (size_t)p.gPoints * Nmc + (size_t)nSub * (subBytes > subIO ? subBytes - subIO : 0);
   for (int d = 0; d < 3; ++d) p.ext[d] = 0.0;
-  p.tSubmit = now_s();
+  p.tSubmit = tEnter;
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return fail(RF_EINVAL_ARG, "the server is stopping");

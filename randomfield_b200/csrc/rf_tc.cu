@@ -381,6 +381,8 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
       }
 
       const bool fastPhase = table_fast_phase(x, P.kMax);
+      const bool f32Phase = table_f32_phase(x, P.kMax);
+      const float xf[3] = {(float)x[0], (float)x[1], (float)x[2]};
       const FxpPoint fxp = fxp_point(x, P.kMax);
       Grid3Thread g3;
       Grid3Walk walk;
@@ -459,7 +461,8 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
             }
           };
           const double* kt = sK + sc * kKtabStageDoubles;
-          if (fxp.ok) table_pairs_fxp<T>(kt, h, fxp, emit);
+          if (f32Phase) table_pairs_f32<T>(kt, h, xf, emit);
+          else if (fxp.ok) table_pairs_fxp<T>(kt, h, fxp, emit);
           else if (fastPhase) table_pairs<true, T>(kt, h, x, emit);
           else table_pairs<false, T>(kt, h, x, emit);
           const uint32_t col = aAddr + (uint32_t)(h * NW);
