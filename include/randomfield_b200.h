@@ -77,7 +77,22 @@ typedef struct rf_options {
   int32_t normalize;     /* 1: empirical per-realization normalisation (randomFieldND.f90:820-926) */
   double x_range[3];     /* physical extent per axis; 0 = extent of xPoints             */
   int32_t device;        /* CUDA device ordinal                                         */
-  int32_t reserved[7];
+  int32_t reserved0;
+  /* Optional caller-supplied uniform draws in [0, 1) that replace the rnglib
+   * stream: draw p (1-based) of the request is draws[p - 1].  The order is the
+   * reference's sequence of random_number calls for the method:
+   *   Shinozuka: per realization, K phases in k order (randomFieldND.f90:278)
+   *   randomization: nDim * kn base-wavevector draws, axis fastest
+   *     (spectra_RF.f90:119-124), then the Shinozuka phases
+   *   isotropic: the phi block (3-D only) and the theta block of K draws, then
+   *     per realization a gamma block and a psi block of K (:460-468).
+   * n_draws must cover every draw the request makes (RF_EINVAL_ARG if not).
+   * Host memory.  rf_create_standard_gaussian_field_unstruct and
+   * rf_generate_device take it; the batch, serving, blend, grid and
+   * no-allocation entry points return RF_ENOTSUP.  NULL: rnglib. */
+  const double* draws;
+  int64_t n_draws;
+  int32_t reserved[2];
 } rf_options;
 
 /* Fills defaults: BF16 form, seed_start 0, reference rules, device 0. */

@@ -80,12 +80,18 @@ class Options(C.Structure):
         ("normalize", C.c_int32),
         ("x_range", C.c_double * 3),
         ("device", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("reserved0", C.c_int32),
+        ("draws", C.c_void_p),
+        ("n_draws", C.c_int64),
+        ("reserved", C.c_int32 * 2),
     ]
 
     @classmethod
     def make(cls, precision="bf16", seed_start=0, k_nstep=(0, 0, 0), iso_n_radial=0, iso_n_dir=0,
-             literal=False, normalize=False, x_range=(0.0, 0.0, 0.0), device=0) -> "Options":
+             literal=False, normalize=False, x_range=(0.0, 0.0, 0.0), device=0, draws=None) -> "Options":
+        """``draws``: optional float64 uniform draws in [0, 1) replacing the
+        rnglib stream, in the reference's order of random_number calls (see
+        rf_options.draws); the array must stay alive while the call runs."""
         o = cls()
         lib().rf_options_init(C.byref(o))
         o.precision = _PREC[precision] if isinstance(precision, str) else int(precision)
@@ -98,6 +104,11 @@ class Options(C.Structure):
         o.literal = int(bool(literal))
         o.normalize = int(bool(normalize))
         o.device = int(device)
+        if draws is not None:
+            d = np.ascontiguousarray(np.asarray(draws, dtype=np.float64).reshape(-1))
+            o._draws_keep = d  # the struct points into it
+            o.draws = d.ctypes.data
+            o.n_draws = int(d.size)
         return o
 
 

@@ -68,6 +68,9 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
 // type_inputRF.f90:1159-1206, randomFieldND.f90:162-166, constants_RF.f90:12-21
 int validate(const Request& r) {
+  if (r.opt.draws || r.opt.n_draws)
+    return fail(RF_ENOTSUP, "caller-supplied draws are taken by rf_create_standard_gaussian_field_unstruct and "
+                            "rf_generate_device only");
   if (r.n < 1) return fail(RF_EINVAL_ARG, "n must be >= 1 (got %lld)", (long long)r.n);
   if (r.nDim < 1 || r.nDim > 3) return fail(RF_EINVAL_NDIM, "nDim must be 1, 2 or 3 (got %d)", r.nDim);
   if (r.Nmc < 1) return fail(RF_EINVAL_NMC, "Nmc must be >= 1 (got %d)", r.Nmc);
@@ -322,6 +325,7 @@ void context_free(rf_context* c) {
   cudaFree(c->dFft);
   cudaFree(c->dGrid);
   cudaFree(c->dBlendSub);
+  cudaFree(c->dDraws);
   if (c->hStats) cudaFreeHost(c->hStats);
   cudaFree(c->dErr);
   cudaFree(c->dX);
@@ -372,7 +376,35 @@ int device_extent(rf_context* c, const double* dX, int nDim, int64_t n, cudaStre
 int build_plan(const Request& rq, const double* ext, Plan& P) {
   if (int rc = geometry(rq, ext, P)) return rc;
   if (int rc = seeds(rq.opt.seed_start, P)) return rc;
+  if (rq.opt.draws && rq.opt.n_draws < draws_needed(P))
+    return fail(RF_EINVAL_ARG, "the request makes %lld draws; draws holds %lld", (long long)draws_needed(P),
+                (long long)rq.opt.n_draws);
   return layout(P);
+}
+
+// The caller's uniform draws (rf_options.draws) to the device, on `st`.
+int upload_draws(rf_context* c, const Request& rq, Plan& P, cudaStream_t st) {
+  P.dDraws = nullptr;
+  P.nDraws = 0;
+  if (!rq.opt.draws) return RF_OK;
+  const int64_t need = draws_needed(P);
+  if (int rc = ensure(c->dDraws, c->capDraws, sizeof(double) * (size_t)need, "caller draws")) return rc;
+  RF_CUDA(cudaMemcpyAsync(c->dDraws, rq.opt.draws, sizeof(double) * (size_t)need, cudaMemcpyHostToDevice, st),
+          "copy of the caller's draws");
+  P.dDraws = c->dDraws;
+  P.nDraws = need;
+  return RF_OK;
+}
+
+// validate() for the entry points that take caller-supplied draws.
+int validate_with_draws(const Request& rq) {
+  Request r = rq;
+  r.opt.draws = nullptr;
+  r.opt.n_draws = 0;
+  if (int rc = validate(r)) return rc;
+  if (rq.opt.n_draws < 0 || (rq.opt.n_draws > 0 && !rq.opt.draws))
+    return fail(RF_EINVAL_ARG, "draws must be non-null with n_draws > 0, or null");
+  return RF_OK;
 }
 
 // The BF16 form splits each amplitude into hi and lo BF16 terms because one
@@ -834,7 +866,7 @@ int rf_generate_device(rf_context* ctx, const double* d_xPoints, int nDim, int64
   g_err.clear();
   if (!ctx || !d_xPoints || !corrL || !d_randField) return fail(RF_EINVAL_ARG, "null pointer argument");
   Request rq = make_request(nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
-  if (int rc = validate(rq)) return rc;
+  if (int rc = validate_with_draws(rq)) return rc;
   std::lock_guard<std::mutex> lk(ctx->mu);
   RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
   cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->stream;
@@ -847,6 +879,7 @@ int rf_generate_device(rf_context* ctx, const double* d_xPoints, int nDim, int64
     if (int rc = device_extent(ctx, d_xPoints, nDim, n, st, ext)) return rc;
   Plan P;
   if (int rc = build_plan(rq, ext, P)) return rc;
+  if (int rc = upload_draws(ctx, rq, P, st)) return rc;
   return run_plan(ctx, P, d_xPoints, d_randField, st);
 }
 
@@ -858,7 +891,7 @@ int rf_create_standard_gaussian_field_unstruct(const double* xPoints, int nDim, 
   g_err.clear();
   if (!xPoints || !corrL || !randField) return fail(RF_EINVAL_ARG, "null pointer argument");
   Request rq = make_request(nDim, n, corrMod, margiFirst, corrL, fieldAvg, fieldVar, Nmc, method, opt);
-  if (int rc = validate(rq)) return rc;
+  if (int rc = validate_with_draws(rq)) return rc;
   rf_context* c = nullptr;
   if (int rc = default_context(rq.opt.device, &c)) return rc;
   std::lock_guard<std::mutex> lk(c->mu);
@@ -881,6 +914,7 @@ int rf_create_standard_gaussian_field_unstruct(const double* xPoints, int nDim, 
   }
   Plan P;
   if (int rc = build_plan(rq, ext, P)) return rc;
+  if (int rc = upload_draws(c, rq, P, st)) return rc;
   // page-locked destination: copy slabs out while the next ones compute (and,
   // when the points are still on the host, copy them up slab by slab)
   cudaPointerAttributes pa;

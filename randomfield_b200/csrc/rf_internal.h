@@ -38,6 +38,8 @@ struct rf_context {
   size_t capGrid = 0;
   double* dBlendSub = nullptr;  // grid path blend: one subdomain's field
   size_t capBlendSub = 0;
+  double* dDraws = nullptr;     // the caller's uniform draws (rf_options.draws)
+  size_t capDraws = 0;
   double* dStats = nullptr; // field statistics scratch (rf_stats.cu)
   size_t capStats = 0;
   double* hStats = nullptr;

@@ -100,7 +100,21 @@ struct Plan {
   int64_t oKstepBytes;        // bytes of one K-step block of B: 16 x (2 lPad oRc) x 2
   int64_t oChunkBytes;        // bytes of one chunk of B, lo blocks included
   uint32_t aLoMask[8];        // K-steps whose A tile carries the lo term (up to 256)
+  // caller-supplied uniform draws (device copy of rf_options.draws): draw p
+  // (1-based) of the request is dDraws[p - 1]; null: the rnglib stream
+  const double* dDraws;
+  int64_t nDraws;
 };
+
+// Draws a request consumes, in the reference's order of random_number calls:
+// Shinozuka Nmc K phases; randomization nDim kn base-wavevector draws first;
+// isotropic the direction blocks (two in 3-D, one in 2-D), then per
+// realization a gamma and a psi block.
+__host__ __device__ inline int64_t draws_needed(const Plan& P) {
+  if (P.method == 1) return (int64_t)(P.nDim == 3 ? 2 : 1) * P.K + (int64_t)P.Nmc * 2 * P.K;
+  const int64_t skip = (P.method == 3) ? (P.K >> (P.nDim - 1)) * P.nDim : 0;
+  return skip + (int64_t)P.Nmc * P.K;
+}
 
 __host__ __device__ inline int popcount32(uint32_t x) {
 #ifdef __CUDA_ARCH__

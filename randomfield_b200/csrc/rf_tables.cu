@@ -50,8 +50,15 @@ struct DrawCursor {
   int32_t last;  // i4_uni value of call `pos`
 };
 
-// r8_uni_01 of the p-th call (p >= 1), through the cursor.
-__device__ __forceinline__ double draw_r8(const JumpTable& jt, int64_t s1, int64_t s2, DrawCursor& cur, uint64_t p) {
+// r8_uni_01 of the p-th call (p >= 1), through the cursor; the caller's
+// draw p - 1 where the request supplies its own stream.
+__device__ __forceinline__ double draw_r8(const Plan& P, const JumpTable& jt, int64_t s1, int64_t s2, DrawCursor& cur,
+                                          uint64_t p) {
+  if (P.dDraws) {
+    cur.pos = p;
+    cur.last = 0;
+    return P.dDraws[p - 1];
+  }
   if (cur.pos != 0 && p == cur.pos + 1) uni_state_next(jt, cur.c1, cur.c2);
   else if (p != cur.pos) uni_state_at(jt, s1, s2, p, cur.c1, cur.c2);
   cur.pos = p;
@@ -105,7 +112,7 @@ __device__ KVal kvalue(const Plan& P, const JumpTable& jt, int64_t kk, RunCursor
       // randomization: kPoints_base = random_number * kMax, axis fastest,
       // the first nDim*kn draws of the stream (spectra_RF.f90:119-124)
       const double base =
-          (P.method == 3) ? draw_r8(jt, P.ig1, P.ig2, cu.kA, (uint64_t)(b * P.nDim + d + 1)) * P.kMax
+          (P.method == 3) ? draw_r8(P, jt, P.ig1, P.ig2, cu.kA, (uint64_t)(b * P.nDim + d + 1)) * P.kMax
                           : 0.0 + P.kDelta[d] * (double)i;
       // B2 in literal mode: the first quadrant is never written.
       v.k[d] = (P.literal && q == 0) ? 0.0 : base * (d == 0 ? 1.0 : quad_sign(q, d, P.nDim));
@@ -118,14 +125,14 @@ __device__ KVal kvalue(const Plan& P, const JumpTable& jt, int64_t kk, RunCursor
     const int j = (int)(kk / nd);
     const double r = (double)j * P.kDelta[0];
     const double s1 = P.ig1, s2 = P.ig2;
-    const double uth = draw_r8(jt, (int64_t)s1, (int64_t)s2, cu.kA, (uint64_t)((P.nDim == 3 ? K : 0) + kk + 1));
+    const double uth = draw_r8(P, jt, (int64_t)s1, (int64_t)s2, cu.kA, (uint64_t)((P.nDim == 3 ? K : 0) + kk + 1));
     const double th = 2.0 * kRefPi * uth;
     double S;
     if (P.corrMod == 1) S = exp(-((r * r) * 1.0) / (4.0 * kRefPi));
     else S = (j == 5) ? 1.0 : 0.0;
     double shell;
     if (P.nDim == 3) {
-      const double uphi = draw_r8(jt, (int64_t)s1, (int64_t)s2, cu.kB, (uint64_t)(kk + 1));
+      const double uphi = draw_r8(P, jt, (int64_t)s1, (int64_t)s2, cu.kB, (uint64_t)(kk + 1));
       const double cph = 1.0 - 2.0 * uphi;
       const double sph = sqrt(fmax(0.0, 1.0 - cph * cph));
       v.k[0] = r * (sph * cos(th));
@@ -201,7 +208,7 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
     if (P.method != 1) {
       // randomization: the phases follow the nDim*kn wavevector draws
       const int64_t skip = (P.method == 3) ? (P.K >> (P.nDim - 1)) * P.nDim : 0;
-      phi = 2.0 * kRefPi * draw_r8(jt, s1, s2, cu.rA, (uint64_t)(skip + rg * P.K + v.ref + 1));
+      phi = 2.0 * kRefPi * draw_r8(P, jt, s1, s2, cu.rA, (uint64_t)(skip + rg * P.K + v.ref + 1));
       if (P.literal && literalSlab >= 0) {
         // B1: slab m of realization n uses S^(1/2^t), t = (n-1)*nSlab + m
         // (randomFieldND.f90:312 inside the loops :276 and :284).
@@ -213,8 +220,8 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
       }
     } else {
       const int64_t base = (P.nDim == 3 ? 2 : 1) * P.K + rg * 2 * P.K;
-      const double ug = draw_r8(jt, s1, s2, cu.rA, (uint64_t)(base + v.ref + 1));
-      const double up = draw_r8(jt, s1, s2, cu.rB, (uint64_t)(base + P.K + v.ref + 1));
+      const double ug = draw_r8(P, jt, s1, s2, cu.rA, (uint64_t)(base + v.ref + 1));
+      const double up = draw_r8(P, jt, s1, s2, cu.rB, (uint64_t)(base + P.K + v.ref + 1));
       gam = (double)sqrtf(12.0f) * (ug - 0.5);  // randomFieldND.f90:468 (single-precision sqrt(12.0))
       phi = 2.0 * kRefPi * up;
     }
@@ -327,8 +334,8 @@ __device__ __forceinline__ void outer_element(const Plan& P, const JumpTable& jt
       aP = (refP == 5) ? 1.0 : 0.0;  // cm_COS, spectra_RF.f90:210-220
       aM = (refM == 5) ? 1.0 : 0.0;
     }
-    const double phP = 2.0 * kRefPi * draw_r8(jt, P.ig1, P.ig2, cu.rA, (uint64_t)(rg * P.K + refP + 1));
-    const double phM = 2.0 * kRefPi * draw_r8(jt, P.ig1, P.ig2, cu.rB, (uint64_t)(rg * P.K + refM + 1));
+    const double phP = 2.0 * kRefPi * draw_r8(P, jt, P.ig1, P.ig2, cu.rA, (uint64_t)(rg * P.K + refP + 1));
+    const double phM = 2.0 * kRefPi * draw_r8(P, jt, P.ig1, P.ig2, cu.rB, (uint64_t)(rg * P.K + refM + 1));
     if (SINK) {
       sink.rk[rg * P.K + refP] = cu.rA.last;
       sink.rk[rg * P.K + refM] = cu.rB.last;

@@ -41,7 +41,10 @@ module rf_gpu
     integer(c_int32_t) :: normalize
     real(c_double) :: x_range(3)
     integer(c_int32_t) :: device
-    integer(c_int32_t) :: reserved(7)
+    integer(c_int32_t) :: reserved0
+    type(c_ptr) :: draws            ! c_loc of real(c_double) draws(n_draws), or c_null_ptr
+    integer(c_int64_t) :: n_draws
+    integer(c_int32_t) :: reserved(2)
   end type rf_options_t
 
   ! rf_result_attributes (include/randomfield_b200.h): write_HDF5_attributes' parameters
