@@ -59,6 +59,7 @@ extern "C" {
 #define RF_ENOMEM_ADMISSION -23 /* request larger than the context's HBM budget              */
 #define RF_ESCRATCH -24         /* request larger than rf_generate_device_noalloc's scratch */
 #define RF_ENODEV -25           /* no CUDA device                                           */
+#define RF_EBOUNDS -26          /* a device index check failed (RF_DEBUG_BOUNDS build only)  */
 
 /*
  * Options.  Zero-initialise (or call rf_options_init) and set what differs;
@@ -158,6 +159,16 @@ int rf_context_synchronize(rf_context* ctx);
  * word and returns, and the call reports RF_ETIMEDOUT, as a generation whose
  * wait expired would.  No fault, trap or hang; the context stays usable. */
 int rf_context_selftest_timeout(rf_context* ctx, double limit_ms);
+
+/* Self test of the index checks of the RF_DEBUG_BOUNDS build (the library
+ * compiled with -DRF_DEBUG_BOUNDS, librf_b200_bounds.so): a kernel computes an
+ * index one past a buffer, its check records the failure in the context's
+ * error word and skips the access, and the call reports RF_EBOUNDS; the
+ * context stays usable.  The normal build returns RF_ENOTSUP and launches
+ * nothing. */
+int rf_context_selftest_bounds(rf_context* ctx);
+/* 1 in the RF_DEBUG_BOUNDS build, 0 otherwise. */
+int rf_debug_bounds_build(void);
 
 /* Measured MUFU (sin, cos) pair rate of the device: the SFU bound of the
  * GEN_TABLE generator (one pair per point and wavevector). */

@@ -37,7 +37,7 @@ STATUS = {
     0: "RF_OK", -1: "RF_EINVAL_NMC", -2: "RF_EINVAL_NDIM", -3: "RF_EINVAL_CORRL", -4: "RF_EINVAL_LOGNORMAL",
     -5: "RF_EINVAL_METHOD", -6: "RF_EINVAL_CORRMOD", -7: "RF_EINVAL_MARGINAL", -8: "RF_EINVAL_RANGE",
     -9: "RF_EINVAL_ARG", -10: "RF_ENOTSUP", -20: "RF_ECUDA", -21: "RF_ENOMEM", -22: "RF_ETIMEDOUT",
-    -23: "RF_ENOMEM_ADMISSION", -24: "RF_ESCRATCH", -25: "RF_ENODEV",
+    -23: "RF_ENOMEM_ADMISSION", -24: "RF_ESCRATCH", -25: "RF_ENODEV", -26: "RF_EBOUNDS",
 }
 
 _CORRMOD = {"gaussian": CM_GAUSSIAN, "cos": CM_COS, "cm_gaussian": CM_GAUSSIAN, "cm_cos": CM_COS}
@@ -53,7 +53,7 @@ EXPORTS = [
     "rf_server_config_init", "rf_server_create", "rf_server_submit", "rf_server_wait", "rf_server_get_stats",
     "rf_server_destroy", "rf_server_submit_blended", "rf_context_selftest_timeout", "rf_measure_sfu_rate", "rf_blend_layout", "rf_generate_blended", "rf_generate_blended_device",
     "rf_field_statistics", "rf_generate_fft_grid", "rf_generate_grid", "rf_create_standard_gaussian_field_grid",
-    "rf_write_result_grid", "rf_debug_table_draws",
+    "rf_write_result_grid", "rf_debug_table_draws", "rf_context_selftest_bounds", "rf_debug_bounds_build",
 ]
 
 
@@ -234,12 +234,15 @@ _lib = None
 
 
 def lib() -> C.CDLL:
-    """The loaded librf_b200.so (raises if it was not built)."""
+    """The loaded librf_b200.so (raises if it was not built).  RF_LIB names
+    another build of the same library to load instead (the index-checked
+    librf_b200_bounds.so of `python -m randomfield_b200.build --debug-bounds`)."""
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise RandomFieldError(-25, f"{LIB_PATH} is missing: run `python -m randomfield_b200.build`")
-        L = C.CDLL(LIB_PATH)
+        path = os.environ.get("RF_LIB") or LIB_PATH
+        if not os.path.exists(path):
+            raise RandomFieldError(-25, f"{path} is missing: run `python -m randomfield_b200.build`")
+        L = C.CDLL(path)
         P, d, i32, i64 = C.POINTER, C.c_double, C.c_int, C.c_int64
         L.rf_options_init.argtypes = [P(Options)]
         L.rf_options_init.restype = None
@@ -271,6 +274,8 @@ def lib() -> C.CDLL:
         L.rf_context_selftest_timeout.argtypes = [C.c_void_p, d]
         L.rf_measure_sfu_rate.argtypes = [i32, P(d)]
         L.rf_debug_table_draws.argtypes = [i32, i32, i32, P(Options), P(i64), P(i32), i64, P(i32), i64]
+        L.rf_context_selftest_bounds.argtypes = [C.c_void_p]
+        L.rf_debug_bounds_build.argtypes = []
         L.rf_generate_fft_grid.argtypes = [C.c_void_p, i32, P(i64), P(d), i32, i32, P(d), d, d, i32, C.c_void_p,
                                            P(Options)]
         L.rf_generate_grid.argtypes = [C.c_void_p, i32, P(d), P(d), P(i64), i32, i32, P(d), d, d, i32, i32,
@@ -630,6 +635,12 @@ class Context:
                                         cl.ctypes.data_as(C.POINTER(C.c_double)), float(fieldAvg), float(fieldVar),
                                         int(Nmc), int(method), C.c_void_p(self._ptr(d_out)), C.byref(o),
                                         C.c_void_p(s)))
+
+    def selftest_bounds(self) -> None:
+        """rf_context_selftest_bounds: raises RandomFieldError(RF_EBOUNDS) in
+        the RF_DEBUG_BOUNDS build (its index check caught the planted index),
+        RF_ENOTSUP in the normal build."""
+        _check(lib().rf_context_selftest_bounds(self._h))
 
     def selftest_timeout(self, limit_ms: float = 50.0) -> None:
         """rf_context_selftest_timeout: raises RandomFieldError(RF_ETIMEDOUT)

@@ -176,6 +176,7 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, int sTc, i
       if (P.gen == GEN_GRID3 && P.lPad == kGroupLPad) outer_layout(P);  // the outer-group kernel
       GroupSub g;
       memset(&g, 0, sizeof(g));
+      P.dbgErr = c->dErr;
       g.P = P;
       g.x = B.dx[i];
       g.out = B.dout[i];

@@ -11,8 +11,25 @@
 
 namespace rfb {
 
-// Device error word written by kernels whose bounded waits expire.
+// Device error word written by kernels whose bounded waits expire, and (in
+// the RF_DEBUG_BOUNDS build) by a failed index check.
 constexpr uint32_t kErrTimeout = 1u;
+constexpr uint32_t kErrBounds = 2u;
+
+// Index checks of the RF_DEBUG_BOUNDS build (the stand-in for a memory
+// checker): RF_IN_BOUNDS(i, n, err) is true when 0 <= i < n; otherwise it
+// records kErrBounds in *err and is false, and the caller skips the access.
+// In the normal build it is `true` and compiles away.
+#ifdef RF_DEBUG_BOUNDS
+__device__ __forceinline__ bool bounds_ok(int64_t i, int64_t n, uint32_t* err) {
+  if (i >= 0 && i < n) return true;
+  if (err) atomicOr(err, kErrBounds);
+  return false;
+}
+#define RF_IN_BOUNDS(i, n, err) ::rfb::bounds_ok((int64_t)(i), (int64_t)(n), (err))
+#else
+#define RF_IN_BOUNDS(i, n, err) true
+#endif
 // Wall-clock limit of one device wait (globaltimer nanoseconds).
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
 

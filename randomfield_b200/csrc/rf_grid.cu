@@ -662,6 +662,7 @@ int grid_blend_run(rf_context* c, const rf_blend_grid* grid, const Request& base
     Plan P, bp;
     if (int rc = blend_sub_spec(grid, base, L, O, f, seed0, sp, P, bp)) return rc;
     if (int rc = grid_run(c, sp, P, base.Nmc, c->dBlendSub, st)) return rc;
+    bp.dbgErr = c->dErr;
     RF_CUDA(launch_blend_add(bp, c->dBlendSub, dOut, sub, base.Nmc, st), "blend add kernel");
     if (f == nSub - 1) Gp = P;  // marginal parameters of the request
   }

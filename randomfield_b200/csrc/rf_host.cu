@@ -550,6 +550,7 @@ int run_plan(rf_context* c, const Plan& P0, const double* dX, double* dOut, cuda
     if (int rc = layout(P)) return rc;
     lo_layout(P);
     outer_layout(P);
+    P.dbgErr = c->dErr;
     if (int rc = run_block(c, P, dX, dOut, st)) return rc;
   }
   if (c->timing) RF_CUDA(cudaEventRecord(c->ev[2], st), "cudaEventRecord");
@@ -622,6 +623,7 @@ int run_plan_slabs(rf_context* c, const Plan& P0, double* dX, double* dOut, doub
   if (int rc = layout(P)) return rc;
   lo_layout(P);
   outer_layout(P);
+  P.dbgErr = c->dErr;
   if (tc_smem_bytes(P, nullptr) == 0)
     return fail(RF_ENOTSUP, "stage too large for shared memory (Nmc or wavenumbers per axis too large)");
   if (!c->copyStream) RF_CUDA(cudaStreamCreateWithFlags(&c->copyStream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -674,6 +676,8 @@ int check_device_error(rf_context* c) {
   RF_CUDA(cudaMemcpy(&err, c->dErr, sizeof(err), cudaMemcpyDeviceToHost), "error word");
   if (err) {
     cudaMemset(c->dErr, 0, sizeof(uint32_t));
+    if (err & kErrBounds)
+      return fail(RF_EBOUNDS, "a device index check failed (error word 0x%x); results are invalid", err);
     return fail(RF_ETIMEDOUT, "a bounded device wait expired (error word 0x%x); results are invalid", err);
   }
   return RF_OK;

@@ -202,6 +202,7 @@ extern "C" int rf_generate_device_noalloc(const double* d_xPoints, int nDim, int
   for (int32_t r0 = 0; r0 < P0.Nmc; r0 += blk) {
     Plan P = P0;
     if (int rc = host_block_layout(&P, r0, std::min(blk, P0.Nmc - r0))) return rc;
+    P.dbgErr = dErr;
     const size_t opBytes = (size_t)operand_bytes(P);
     const size_t tabBytes = P.gen == GEN_TABLE ? (size_t)P.nChunks * kKtabStageBytes : 0;
     if (opBytes > kOperandBytes || tabBytes > kTableBytes) {

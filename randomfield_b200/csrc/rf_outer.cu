@@ -209,6 +209,10 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
               break;
             }
             const uint32_t bytes = (uint32_t)(outer_b_lo(P, j) ? 2 * P.oKstepBytes : P.oKstepBytes);
+            if (!RF_IN_BOUNDS((src - v.B) + bytes - 1, operand_bytes(P), err)) {
+              ok = false;  // no copy: the slot stays empty, and the waits on it end the kernel
+              break;
+            }
             mbar_arrive_expect_tx(&bars->full[s], bytes);
             bulk_g2s(slots + (size_t)s * slotBytes + aBytes, src, bytes, &bars->full[s]);
             src += bytes;
@@ -293,7 +297,7 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
       const int64_t p = v.row0 + v.pair * kPairRows + t * kTileM + row;
       const bool valid = p < v.row0 + v.rows;
       double x0 = 0.0, x1 = 0.0;
-      if (valid) {
+      if (valid && RF_IN_BOUNDS(p * 3 + 2, P.n * 3, err)) {
         x0 = v.x[p * 3 + 0] / P.corrL[0];
         x1 = v.x[p * 3 + 1] / P.corrL[1];
       }
@@ -388,8 +392,12 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
           }
           if (valid) {
             const int64_t r = (int64_t)P.rOff + c * P.oRc + rl;
-            if (P.blend) atomicAdd(&v.out[r * P.gTotal + bg], bw * ((double)acc * P.outScale));
-            else v.out[r * P.n + p] = outer_finish(P, acc);
+            if (P.blend) {
+              if (RF_IN_BOUNDS(r * P.gTotal + bg, (int64_t)P.Nmc * P.gTotal, err))
+                atomicAdd(&v.out[r * P.gTotal + bg], bw * ((double)acc * P.outScale));
+            } else if (RF_IN_BOUNDS(r * P.n + p, (int64_t)P.Nmc * P.n, err)) {
+              v.out[r * P.n + p] = outer_finish(P, acc);
+            }
           }
         }
         tc_fence_before();

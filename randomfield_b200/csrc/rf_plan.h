@@ -104,6 +104,9 @@ struct Plan {
   // (1-based) of the request is dDraws[p - 1]; null: the rnglib stream
   const double* dDraws;
   int64_t nDraws;
+  // error word of the launch's context: the RF_DEBUG_BOUNDS build records
+  // failed index checks in it (the normal build never reads it)
+  uint32_t* dbgErr;
 };
 
 // Draws a request consumes, in the reference's order of random_number calls:

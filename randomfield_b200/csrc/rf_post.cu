@@ -73,7 +73,7 @@ __global__ void rf_blend_add_kernel(const double* __restrict__ sub, double* __re
     const int64_t r = t / subPoints, p = t % subPoints;
     int64_t g = 0;
     const double w = blend_weight(P, p, &g);
-    group[r * P.gTotal + g] += w * sub[t];
+    if (RF_IN_BOUNDS(g, P.gTotal, P.dbgErr)) group[r * P.gTotal + g] += w * sub[t];
   }
 }
 

@@ -56,7 +56,42 @@ __global__ void rf_sfu_rate_kernel(float* sink, int iters) {
   if (acc == 12345.678f) sink[threadIdx.x] = acc;
 }
 
+#ifdef RF_DEBUG_BOUNDS
+// One thread stores at index n of an n-element buffer through the checked
+// form: the check records kErrBounds and skips the store.  Built only into
+// the RF_DEBUG_BOUNDS library, where the check exists.
+__global__ void rf_bounds_selftest_kernel(uint32_t* buf, int64_t n, uint32_t* err) {
+  const int64_t i = n;
+  if (RF_IN_BOUNDS(i, n, err)) buf[i] = 1u;
+}
+#endif
+
 }  // namespace
+
+extern "C" int rf_debug_bounds_build(void) {
+#ifdef RF_DEBUG_BOUNDS
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+extern "C" int rf_context_selftest_bounds(rf_context* ctx) {
+  g_err.clear();
+  if (!ctx) return fail(RF_EINVAL_ARG, "null context");
+#ifdef RF_DEBUG_BOUNDS
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  RF_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+  // the context's 4-byte error word doubles as the one-element buffer: the
+  // kernel's index (1) is one past it
+  rf_bounds_selftest_kernel<<<1, 1, 0, ctx->stream>>>(ctx->dErr, 1, ctx->dErr);
+  RF_CUDA(cudaGetLastError(), "bounds self-test kernel");
+  RF_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  return check_device_error(ctx);
+#else
+  return fail(RF_ENOTSUP, "index checks exist only in the RF_DEBUG_BOUNDS build (librf_b200_bounds.so)");
+#endif
+}
 
 extern "C" int rf_measure_sfu_rate(int device, double* pairs_per_second) {
   g_err.clear();

@@ -192,6 +192,7 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
     double* kt = ktab + stage * kKtabStageDoubles;
     int32_t* kc = reinterpret_cast<int32_t*>(kt + 3 * kTableChunk);
     float* kf = reinterpret_cast<float*>(kc + 3 * kTableChunk);
+    if (!RF_IN_BOUNDS(stage, P.nChunks, P.dbgErr)) return;
     for (int d = 0; d < 3; ++d) {
       const double t = v.k[d] / 6.283185307179586;
       kt[d * kTableChunk + c] = t;
@@ -247,6 +248,8 @@ __device__ __forceinline__ void table_element(const Plan& P, const JumpTable& jt
     return;
   }
 
+  // every operand write of this element lies in stage `stage` of B
+  if (!RF_IN_BOUNDS(stage_offset(P, stage), operand_bytes(P), P.dbgErr)) return;
   if (P.prec == PREC_FP32) {
     float* b = reinterpret_cast<float*>(B) + stage * (int64_t)(2 * P.chunkK) * P.nmcPad;
     b[(int64_t)(2 * c) * P.nmcPad + r] = (float)bc;
@@ -355,6 +358,9 @@ __device__ __forceinline__ void outer_element(const Plan& P, const JumpTable& jt
   unsigned char* blk = B + (int64_t)c * P.oChunkBytes + outer_kstep_offset(P, j);
   const int32_t nRows = 2 * P.lPad * P.oRc;
   const bool lo = outer_b_lo(P, j);
+  if (!RF_IN_BOUNDS((int64_t)c * P.oChunkBytes + outer_kstep_offset(P, j) + (lo ? 2 : 1) * P.oKstepBytes - 1,
+                    operand_bytes(P), P.dbgErr))
+    return;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const int32_t e = q & 1, cs = q >> 1;

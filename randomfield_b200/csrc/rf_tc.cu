@@ -253,6 +253,10 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
             break;
           }
           const uint32_t bytes = (uint32_t)(stage_has_lo(P, ch) ? P.stageBytes : P.stageBytes / 2);
+          if (!RF_IN_BOUNDS(off + bytes - 1, operand_bytes(P), err)) {
+            raise_abort(bars, err);  // no copy: the waits on the slot end the kernel
+            break;
+          }
           mbar_arrive_expect_tx(&bars->full[s], bytes);
           bulk_g2s(sB + (size_t)s * L.slotBytes, v.B + off, bytes, &bars->full[s]);
           off += bytes;
@@ -374,7 +378,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
       const int64_t p = v.row0 + v.tile * kTileM + row;
       const bool valid = (p < v.row0 + v.rows);
       double x[3] = {0.0, 0.0, 0.0};
-      if (valid) {
+      if (valid && RF_IN_BOUNDS(p * P.nDim + P.nDim - 1, P.n * P.nDim, err)) {
 #pragma unroll
         for (int d = 0; d < 3; ++d)
           if (d < P.nDim) x[d] = v.x[p * P.nDim + d] / P.corrL[d];
@@ -495,10 +499,12 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
             float acc = __uint_as_float(va[j]);
             if (kHiLo) acc += __uint_as_float(lo[j]);
             if (r >= P.nmcBlk) continue;
-            if (P.blend)
-              atomicAdd(&v.out[(int64_t)(P.rOff + r) * P.gTotal + bg], bw * ((double)acc * P.outScale));
-            else
+            if (P.blend) {
+              if (RF_IN_BOUNDS((int64_t)(P.rOff + r) * P.gTotal + bg, (int64_t)P.Nmc * P.gTotal, err))
+                atomicAdd(&v.out[(int64_t)(P.rOff + r) * P.gTotal + bg], bw * ((double)acc * P.outScale));
+            } else if (RF_IN_BOUNDS((int64_t)(P.rOff + r) * P.n + p, (int64_t)P.Nmc * P.n, err)) {
               v.out[(int64_t)(P.rOff + r) * P.n + p] = finish_value(P, acc);
+            }
           }
         }
       }
