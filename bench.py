@@ -865,12 +865,17 @@ def main():
     hbm_bytes = 8.0 * n * NMC + 24.0 * n + 2.0 * (2 * K) * (2 * NMC)
     bounds = {"tensor_ms": flops / (peak * 1e12) * 1e3, "sfu_ms": pairs / sfu * 1e3,
               "hbm_ms": hbm_bytes / (pk.get("hbm_gbs", 6650.0) * 1e9) * 1e3}
+    # the 16-bit forms of this 3-D grid workload run the outer-group contraction, FP8 the trig-tile one
+    kname = ("rf_outer_kernel (outer-group tcgen05 contraction + fused i3 epilogue)"
+             if args.precision in ("bf16", "fp16", "bf16_fast") else
+             "rf_tc_kernel (tcgen05 contraction + fused epilogue)")
     roof = {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s", "frac": tflops / peak,
-            "traffic": traffic, "kernel": "rf_tc_kernel (tcgen05 contraction + fused epilogue)",
+            "traffic": traffic, "kernel": kname,
             "kernel_ms": kern_ms, "peak_source": f"bf16_tflops_sustained, {src}",
             "algorithmic_flops_per_launch": flops, "bounds": bounds,
             "sfu_pairs_per_s": sfu, "sfu_pairs_per_launch": pairs,
-            "note": "the slowest of the three bounds is the tensor MMA; GEN_GRID3 needs sincos only for the "
+            "note": "the slowest of the three bounds is the tensor MMA (algorithmic FLOPs 2 n 2K Nmc; the hi/lo "
+                    "terms' extra MMAs are not credited); the tensor-grid generators need sincos only for the "
                     "per-axis phasors (n1 + n2 + n3 per point), GEN_TABLE one pair per (point, wavevector)"}
 
     cpu = None

@@ -466,9 +466,13 @@ void lo_layout(Plan& P) {
 // A's on those carrying all but kOuterALoLeft of the variance, B's on those
 // carrying all but kOuterBLoLeft.  An A lo term costs one more MMA per tile
 // and K-step and no operand bytes; a B lo term one more MMA per tile and a
-// second B block.
-constexpr double kOuterALoLeft = 0.10;
-constexpr double kOuterBLoLeft = 0.20;
+// second B block.  A numpy emulation of this rounding on the 128^3 workload
+// (24^3 x 4 wavevectors, Nmc 64, 24,576 points) gives, per (A, B) share
+// left without a lo term: (1, 1) relative L2 2.1e-3 (no lo term at all);
+// (0.3, 0.3) 1.16e-3, worst realization 1.27e-3, 1.46x the MMAs of the hi
+// terms alone; (0.1, 0.2) 8.5e-4 at 1.71x; (0, 0) 3e-6 at 3x.
+constexpr double kOuterALoLeft = 0.30;
+constexpr double kOuterBLoLeft = 0.30;
 
 void outer_layout(Plan& P) {
   if (P.gen != GEN_GRID3 || P.literal) return;

@@ -8,8 +8,10 @@ matrix products, which turns the 1.2e11 cosines of the point-by-point sum
 into seconds of BLAS.  It is pinned here on the CPU against the oracle's
 point-by-point sum (rfo_generate) on rows of the same 128^3 workload and on
 small grids in 1-D to 3-D; the GPU tests then compare all 134 M values of the
-BF16 and FP16 forms (relative-L2 <= 2e-3 overall, <= 2.5e-3 per
-realization) and of the structured-grid path (<= 1e-11).
+BF16 and FP16 forms (relative-L2 <= 2e-3 overall and for every
+realization; the BF16 form, the outer-group contraction with its hi/lo terms,
+also within 1.5e-3 for every realization, its margin under the bound) and of
+the structured-grid path (<= 1e-11).
 """
 import numpy as np
 import pytest
@@ -56,7 +58,9 @@ def test_whole_field_tensor_core_forms(head_ref, prec):
     d = got - head_ref
     assert np.linalg.norm(d) <= 2e-3 * np.linalg.norm(head_ref)
     per = np.linalg.norm(d, axis=1) / np.linalg.norm(head_ref, axis=1)
-    assert per.max() <= 2.5e-3, per.max()
+    assert per.max() <= 2e-3, per.max()
+    if prec == "bf16":
+        assert per.max() <= 1.5e-3, per.max()
 
 
 @pytest.mark.gpu
