@@ -455,6 +455,26 @@ void lo_layout(Plan& P) {
   P.loSkip = 1;
 }
 
+// The table generator's trig tile in BF16 leaves a relative error of about
+// 1.3e-3 in the field whatever the amplitude side does.  On a domain of a few
+// correlation lengths the norm of one realization fluctuates a lot, and with
+// it that realization's relative error (a 1-D field over 5 correlation
+// lengths and 40 wavevectors: 2.4e-3 in one of 8).  Single BF16 requests of
+// at most kTableALoPairs (point, wavevector) pairs therefore carry the trig
+// tile's lo term too (its rounding residual: one more MMA per K-step), which
+// removes that error; larger requests, whose cost it would double on the
+// tensor side and whose realizations span many correlation lengths (the
+// 200k-point isotropic config: 1.5e-3 worst realization without it), keep
+// the hi term alone.
+constexpr double kTableALoPairs = 67108864.0;  // 2^26
+
+void table_alo_layout(Plan& P) {
+  P.tableALo = 0;
+  if (P.gen != GEN_TABLE || P.prec != PREC_BF16) return;
+  if ((double)P.n * (double)P.K > kTableALoPairs) return;
+  P.tableALo = 1;
+}
+
 // GEN_OUTER (rf_outer.cu) for single 3-D Shinozuka requests on the 16-bit
 // tensor-core forms: the same sum as GEN_GRID3 with the outer phasors as the
 // generated operand.  Its BF16 form splits both operands into hi and lo
@@ -554,6 +574,7 @@ int run_plan(rf_context* c, const Plan& P0, const double* dX, double* dOut, cuda
     if (int rc = layout(P)) return rc;
     lo_layout(P);
     outer_layout(P);
+    table_alo_layout(P);
     P.dbgErr = c->dErr;
     if (int rc = run_block(c, P, dX, dOut, st)) return rc;
   }
@@ -627,6 +648,7 @@ int run_plan_slabs(rf_context* c, const Plan& P0, double* dX, double* dOut, doub
   if (int rc = layout(P)) return rc;
   lo_layout(P);
   outer_layout(P);
+  table_alo_layout(P);
   P.dbgErr = c->dErr;
   if (tc_smem_bytes(P, nullptr) == 0)
     return fail(RF_ENOTSUP, "stage too large for shared memory (Nmc or wavenumbers per axis too large)");
@@ -765,6 +787,7 @@ int host_block_layout(Plan* P, int32_t rOff, int32_t nmcBlk) {
   if (int rc = layout(*P)) return rc;
   lo_layout(*P);
   outer_layout(*P);
+  table_alo_layout(*P);
   return RF_OK;
 }
 

@@ -143,6 +143,8 @@ void lo_layout(rfb::Plan& P);
 // Single-request 3-D Shinozuka plans on the 16-bit tensor-core forms: the
 // outer-group contraction (rf_outer.cu) and its lo masks (rf_host.cu)
 void outer_layout(rfb::Plan& P);
+// Small single BF16 table-generator requests: the trig tile's lo term (rf_host.cu)
+void table_alo_layout(rfb::Plan& P);
 int32_t realization_block(const rfb::Plan& P);
 int device_extent(rf_context* c, const double* dX, int nDim, int64_t n, cudaStream_t st, double* ext);
 int run_plan(rf_context* c, const rfb::Plan& P0, const double* dX, double* dOut, cudaStream_t st);

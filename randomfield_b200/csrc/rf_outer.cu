@@ -69,8 +69,10 @@ struct OuterBars {
   uint64_t done;
   uint32_t tmem_base;
   int abort_flag;
+  // the issuer's table of the current item's K-steps: bit 0 B lo, bit 1 A lo
+  uint8_t kflags[kOuterMaxKsteps];
 };
-constexpr int kOuterHeader = 256;
+constexpr int kOuterHeader = 512;
 static_assert(sizeof(OuterBars) <= kOuterHeader, "header");
 
 struct OuterArgs {
@@ -232,44 +234,62 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
     __syncwarp();
   } else if (warp == kIssuerWarp) {
     // ---------------------------------------------------------- MMA issuer
+    // The whole warp runs the loop (warp-uniform state); one elected lane
+    // issues.  The MMAs of a K-step go out back to back: the lo terms through
+    // a guard predicate from the item's flag table (no branch between MMAs;
+    // a branch per MMA costs the issuing thread a resolution it cannot hide),
+    // and the next slot's barrier is probed before the last MMA so that the
+    // wait proper runs only when the probe failed.
     const bool leader = elect_one();
     uint32_t s = 0, ph = 0, accPh = 0;
-    bool ok = true;
+    bool ok = true, ready = false;  // ready: full[s] of the next K-step already observed
     const uint32_t ab = PREC == PREC_FP16 ? 0u : 1u;
-    const uint32_t aDescLo = (uint32_t)(2 * kATileBytes) >> 4;  // descriptor step to the lo A tiles
+    const uint64_t aStepLo = (uint64_t)((2 * kATileBytes) >> 4);  // descriptor step to the lo A tiles
+    const uint64_t aStepT = (uint64_t)(kATileBytes >> 4);         // descriptor step to tile 1's A
     for (int64_t i = 0; i < count && ok; ++i) {
       w.get(i, v);
       const Plan& P = *v.P;
-      const uint32_t bDescLo = (uint32_t)(P.oKstepBytes >> 4);
+      for (int32_t j = lane; j < P.oNK; j += 32)
+        bars->kflags[j] = (uint8_t)((outer_b_lo(P, j) ? 1u : 0u) | (outer_a_lo(P, j) ? 2u : 0u));
+      __syncwarp();
+      const uint64_t bStepLo = (uint64_t)(P.oKstepBytes >> 4);
       const uint32_t nRows = (uint32_t)(2 * P.lPad * P.oRc);  // B rows (N) of a full chunk
       for (int32_t c = 0; c < P.oNR && ok; ++c) {
         const int32_t rc = min(P.oRc, P.nmcBlk - c * P.oRc);
         const uint32_t idesc = make_idesc(ab, 128u, (uint32_t)(2 * P.lPad * rc));
+        // both accumulators are free once the epilogue has read the last chunk
+        if (!mbar_wait_warp(&bars->acc_empty[0], accPh ^ 1, abort_flag) ||
+            !mbar_wait_warp(&bars->acc_empty[1], accPh ^ 1, abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
         for (int32_t j = 0; j < P.oNK; ++j) {
-          if (!mbar_wait_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
+          if (!ready && !mbar_wait_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
           tc_fence_after();
           const uint32_t base = smem_u32(slots + (size_t)s * slotBytes);
           const uint64_t aDesc = make_sdesc(base, 2048u, 128u);
           const uint64_t bDesc = make_sdesc(base + (uint32_t)aBytes, nRows * 16u, 128u);
-          const bool bLo = outer_b_lo(P, j), aLo = outer_a_lo(P, j);
-#pragma unroll
-          for (int t = 0; t < 2; ++t) {
-            if (j == 0) {  // the tile's accumulator is free once its epilogue has read the last chunk
-              if (!mbar_wait_warp(&bars->acc_empty[t], accPh ^ 1, abort_flag)) { ok = false; break; }
-              tc_fence_after();
-            }
-            if (leader) {
-              const uint32_t d = tbase + (uint32_t)(t * kAccCols);
-              const uint64_t at = aDesc + (uint64_t)((t * kATileBytes) >> 4);
-              mma_ss(d, at, bDesc, idesc, j > 0 ? 1u : 0u);
-              if (bLo) mma_ss(d, at, bDesc + bDescLo, idesc, 1u);
-              if (aLo) mma_ss(d, at + aDescLo, bDesc, idesc, 1u);
-            }
+          const uint32_t f = bars->kflags[j];
+          const uint32_t bLo = f & 1u, aLo = f & 2u, acc = j > 0 ? 1u : 0u;
+          const uint32_t sn = (s + 1 == (uint32_t)S) ? 0u : s + 1;
+          const uint32_t phn = (s + 1 == (uint32_t)S) ? ph ^ 1 : ph;
+          const bool more = (j + 1 < P.oNK) || (c + 1 < P.oNR) || (i + 1 < count);
+          if (leader) {
+            mma_ss(tbase, aDesc, bDesc, idesc, acc);
+            mma_ss_if(tbase, aDesc, bDesc + bStepLo, idesc, 1u, bLo);
+            mma_ss_if(tbase, aDesc + aStepLo, bDesc, idesc, 1u, aLo);
+            mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc, idesc, acc);
+            mma_ss_if(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc + bStepLo, idesc, 1u, bLo);
           }
-          if (!ok) break;
-          if (leader) mma_commit(&bars->empty[s]);
+          ready = __all_sync(0xffffffffu, more && mbar_test_wait(&bars->full[sn], phn));
+          if (leader) {
+            mma_ss_if(tbase + (uint32_t)kAccCols, aDesc + aStepT + aStepLo, bDesc, idesc, 1u, aLo);
+            mma_commit(&bars->empty[s]);
+          }
           __syncwarp();
-          if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+          s = sn;
+          ph = phn;
         }
         if (!ok) break;
         if (leader) mma_commit(&bars->acc_full);
@@ -378,16 +398,22 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
         tc_fence_after();
         const int32_t rc = min(P.oRc, P.nmcBlk - c * P.oRc);
         for (int32_t rl = 0; rl < rc; ++rl) {
+          // the realization's 2 LPAD columns in 32-column round trips (a load
+          // then a wait for it; the last piece of an odd LH is 16 columns)
           float acc = 0.f;
 #pragma unroll
-          for (int h = 0; h < LH; ++h) {
-            uint32_t y[16];
-            tmem_ld16(taddr0 + (uint32_t)(rl * 2 * LPAD + 16 * h), y);
+          for (int h = 0; h < LH; h += 2) {
+            uint32_t y[32];
+            const uint32_t col = taddr0 + (uint32_t)(rl * 2 * LPAD + 16 * h);
+            if (h + 1 < LH) tmem_ld32(col, y);
+            else tmem_ld16(col, y);
             tmem_ld_wait();
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-              acc = fmaf(e3[8 * h + u].x, __uint_as_float(y[2 * u]), acc);
-              acc = fmaf(e3[8 * h + u].y, __uint_as_float(y[2 * u + 1]), acc);
+            for (int u = 0; u < 16; ++u) {
+              if (h + (u >> 3) < LH) {
+                acc = fmaf(e3[8 * h + u].x, __uint_as_float(y[2 * u]), acc);
+                acc = fmaf(e3[8 * h + u].y, __uint_as_float(y[2 * u + 1]), acc);
+              }
             }
           }
           if (valid) {

@@ -100,6 +100,9 @@ struct Plan {
   int64_t oKstepBytes;        // bytes of one K-step block of B: 16 x (2 lPad oRc) x 2
   int64_t oChunkBytes;        // bytes of one chunk of B, lo blocks included
   uint32_t aLoMask[8];        // K-steps whose A tile carries the lo term (up to 256)
+  // GEN_TABLE, BF16 single requests: the trig tile also carries its lo term
+  // (the stage's A columns twice, one more MMA per K-step)
+  int32_t tableALo;
   // caller-supplied uniform draws (device copy of rf_options.draws): draw p
   // (1-based) of the request is dDraws[p - 1]; null: the rnglib stream
   const double* dDraws;
@@ -208,6 +211,6 @@ struct GroupItem {
 
 // TMEM columns of one stage's A tile: one 32-bit column holds a (cos, sin)
 // pair of 16-bit values, or two pairs of 8-bit values.
-inline int32_t a_cols(const Plan& P) { return P.prec == PREC_FP8 ? P.chunkK / 2 : P.chunkK; }
+inline int32_t a_cols(const Plan& P) { return (P.prec == PREC_FP8 ? P.chunkK / 2 : P.chunkK) * (P.tableALo ? 2 : 1); }
 
 }  // namespace rfb

@@ -173,6 +173,7 @@ extern "C" int rf_debug_table_draws(int nDim, int method, int Nmc, const rf_opti
     }
     lo_layout(P);
     outer_layout(P);  // the same plan as a generation of this request
+    table_alo_layout(P);
     e = launch_table_draws(P, jump_table(), dRk, dK, 0);
   }
   if (e == cudaSuccess) e = cudaDeviceSynchronize();

@@ -168,15 +168,21 @@ __device__ __forceinline__ void mma_one(uint32_t tbase, uint32_t a, uint64_t b, 
   else mma_ts(tbase, a, b, idesc, acc);
 }
 
+// aLo > 0: the stage's A tile also holds its lo term aLo columns after the
+// hi term, multiplied by the same B rows (one more MMA per K-step).
 template <int STEPS, bool F8>
 __device__ __forceinline__ bool issue_stage(bool leader, uint32_t tbase, uint32_t aBase, uint64_t d0, uint64_t jStep,
                                             uint32_t idesc, uint32_t acc0, bool more, uint64_t* fullNext,
-                                            uint32_t phn, uint64_t* emptyBar) {
+                                            uint32_t phn, uint64_t* emptyBar, uint32_t aLo = 0) {
   static_assert(STEPS >= 2, "a stage holds at least two MMAs");
   if (leader) {
     mma_one<F8>(tbase, aBase, d0, idesc, acc0);  // the tile's first MMA overwrites D
 #pragma unroll
     for (int j = 1; j < STEPS - 1; ++j) mma_one<F8>(tbase, aBase + 8u * j, d0 + jStep * j, idesc, 1u);
+    if (aLo) {
+#pragma unroll
+      for (int j = 0; j < STEPS; ++j) mma_one<F8>(tbase, aBase + aLo + 8u * j, d0 + jStep * j, idesc, 1u);
+    }
   }
   const bool ready = __all_sync(0xffffffffu, more && mbar_test_wait(fullNext, phn));
   if (leader) {
@@ -340,7 +346,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
                                                phn, &bars->empty[s]);
         else
           ready = issue_stage<kTabSteps, kF8>(leader, tbase, aBase, d0, jStep, idesc, acc0, more, &bars->full[sn],
-                                              phn, &bars->empty[s]);
+                                              phn, &bars->empty[s], P.tableALo ? (uint32_t)P.chunkK : 0u);
         s = sn;
         ph = phn;
       }
@@ -451,6 +457,8 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
           constexpr int T = kTableChunk / kParts;  // pairs of this thread
           constexpr int NW = kF8 ? T / 2 : T;
           uint32_t words[NW];
+          uint32_t lows[PREC == PREC_BF16 ? NW : 1];  // the BF16 residuals (tableALo)
+          const bool aLo = PREC == PREC_BF16 && P.tableALo;
           float pc0 = 0.f, ps0 = 0.f;
           auto emit = [&](int idx, float c, float sn) {
             if (kF8) {
@@ -462,6 +470,10 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
               }
             } else {
               words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
+              if (PREC == PREC_BF16 && aLo) {
+                const uint32_t w = words[idx];
+                lows[idx] = pack_bf16x2(c - __uint_as_float(w << 16), sn - __uint_as_float(w & 0xffff0000u));
+              }
             }
           };
           const double* kt = sK + sc * kKtabStageDoubles;
@@ -472,6 +484,10 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
           const uint32_t col = aAddr + (uint32_t)(h * NW);
 #pragma unroll
           for (int pc = 0; pc < NW / 8; ++pc) tmem_st8(col + pc * 8, &words[pc * 8]);
+          if (PREC == PREC_BF16 && aLo) {
+#pragma unroll
+            for (int pc = 0; pc < NW / 8; ++pc) tmem_st8(col + (uint32_t)P.chunkK + pc * 8, &lows[pc * 8]);
+          }
         }
         freeSeen = __shfl_sync(0xffffffffu, probe, 0) != 0;
         tmem_st_wait();
