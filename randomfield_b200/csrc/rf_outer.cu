@@ -60,6 +60,10 @@ constexpr int kOuterMaxSlots = 8;
 constexpr int kATileBytes = kTileM * 16 * 2;  // one tile's K-step of A: 128 rows x 16 K x 16 bits
 constexpr uint32_t kOuterTmemCols = 512;
 constexpr int kAccCols = 256;  // accumulator columns per tile
+#ifndef RF_OUTER_GEN_PER_FENCE
+#define RF_OUTER_GEN_PER_FENCE 1
+#endif
+constexpr int kGenPerFence = RF_OUTER_GEN_PER_FENCE;  // K-steps a generator warp writes per proxy fence
 
 struct OuterBars {
   uint64_t full[kOuterMaxSlots];   // 8 generator warps + producer (bytes)
@@ -331,6 +335,13 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
           float2 e2 = make_float2(1.f, 0.f);  // E2(i2), walked by angle addition
           for (int32_t i2 = 0; i2 < n2 && ok; ++i2) {
             const float2 E = make_float2(e2.x, s2 ? -e2.y : e2.y);
+            // The block's K-steps go to consecutive slots, each written as
+            // soon as its slot is free; the proxy fence and the arrivals are
+            // paid once per kGenPerFence K-steps (the fence waits for the
+            // warp's stores, so one per K-step would put its latency on every
+            // K-step of the pipeline).
+            uint32_t s0 = s;  // first slot not yet arrived on
+            int pending = 0;
 #pragma unroll
             for (int jj = 0; jj < kOuterMaxN1P / 8; ++jj) {
               if (jj < nJJ) {
@@ -360,10 +371,17 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
                   *reinterpret_cast<uint4*>(A + 2 * kATileBytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
                   *reinterpret_cast<uint4*>(A + 2 * kATileBytes + 2048) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
                 }
-                fence_proxy_async_smem();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&bars->full[s]);
                 if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+                ++pending;
+                if (pending == kGenPerFence || jj + 1 == nJJ) {
+                  fence_proxy_async_smem();
+                  __syncwarp();
+                  for (int k = 0; k < pending; ++k) {
+                    if (lane == 0) mbar_arrive(&bars->full[s0]);
+                    if (++s0 == (uint32_t)S) s0 = 0;
+                  }
+                  pending = 0;
+                }
               }
             }
             e2 = make_float2(e2.x * e2step.x - e2.y * e2step.y, e2.x * e2step.y + e2.y * e2step.x);

@@ -469,10 +469,11 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
                 words[idx >> 1] = pack_e4m3x4(pc0, ps0, c, sn);
               }
             } else {
-              words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
+              // BF16 packed on the integer pipes: the SFU pipe is this loop's bound
+              words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2_int(c, sn);
               if (PREC == PREC_BF16 && aLo) {
                 const uint32_t w = words[idx];
-                lows[idx] = pack_bf16x2(c - __uint_as_float(w << 16), sn - __uint_as_float(w & 0xffff0000u));
+                lows[idx] = pack_bf16x2_int(c - __uint_as_float(w << 16), sn - __uint_as_float(w & 0xffff0000u));
               }
             }
           };
