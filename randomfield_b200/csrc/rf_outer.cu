@@ -24,15 +24,15 @@
 // realization block is cut into N chunks of oRc realizations (TMEM: one
 // 256-column accumulator per tile); for each chunk the K-steps (16 K = 8
 // outer groups of consecutive i1) stream through a ring of shared-memory
-// slots, each holding both tiles' A K-step (hi, and lo where the plan keeps
-// it) and B's K-step block (hi, and lo).
+// stages of two K-steps, each K-step with both tiles' A (hi, and lo where the
+// plan keeps it) and B's K-step block (hi, and lo).
 //
 // Warp roles (576 threads):
-//   warp 0      MMA issuer: the warp runs the slot loop, one elected lane
+//   warp 0      MMA issuer: the warp runs the stage loop, one elected lane
 //               issues tcgen05.mma (A and B by shared-memory descriptor, D in
 //               TMEM) and tcgen05.commit;
 //   warp 1      producer (one thread): 1-D bulk copies (TMA, no multicast) of
-//               B's K-step blocks from HBM/L2 into the slots;
+//               a stage's B blocks from HBM/L2 into the ring;
 //   warps 2-9   generators: one point each (256 = two tiles); per K-step the
 //               8 outer phasors E1(i1) E2(i2)^{s2} of the point, rounded to
 //               16 bits (and the lo residual), stored in the K-major core-
@@ -60,14 +60,17 @@ constexpr int kOuterMaxSlots = 8;
 constexpr int kATileBytes = kTileM * 16 * 2;  // one tile's K-step of A: 128 rows x 16 K x 16 bits
 constexpr uint32_t kOuterTmemCols = 512;
 constexpr int kAccCols = 256;  // accumulator columns per tile
-#ifndef RF_OUTER_GEN_PER_FENCE
-#define RF_OUTER_GEN_PER_FENCE 1
-#endif
-constexpr int kGenPerFence = RF_OUTER_GEN_PER_FENCE;  // K-steps a generator warp writes per proxy fence
+// K-steps per ring stage: one full/empty barrier pair, one bulk copy, one
+// generator fence and one commit serve kStageK K-steps.  A K-step's MMAs keep
+// the tensor pipe busy for about as long as the issuing thread takes to issue
+// them, so the per-stage bookkeeping (barrier probe, commit, loop control)
+// shows up directly in the kernel's time; two K-steps per stage halve it.
+// A chunk's K-step count 2 n2 nJJ is always even.
+constexpr int kStageK = 2;
 
 struct OuterBars {
-  uint64_t full[kOuterMaxSlots];   // 8 generator warps + producer (bytes)
-  uint64_t empty[kOuterMaxSlots];  // MMA commit
+  uint64_t full[kOuterMaxSlots];   // per stage: 8 generator warps + producer (bytes)
+  uint64_t empty[kOuterMaxSlots];  // per stage: MMA commit
   uint64_t acc_full;               // MMA commit after a chunk's last K-step
   uint64_t acc_empty[2];           // the 4 epilogue warps of a tile
   uint64_t done;
@@ -86,9 +89,9 @@ struct OuterArgs {
   double* out;
   uint32_t* err;
   int64_t row0, rows;
-  int32_t S;          // slots
-  int32_t slotBytes;  // A area + B area, 128-byte multiple
-  int32_t aBytes;     // A area: two tiles x 4 KB, twice with a lo term
+  int32_t S;          // ring stages
+  int32_t slotBytes;  // one stage: kStageK A areas, then kStageK B blocks; 128-byte multiple
+  int32_t aBytes;     // one K-step's A area: two tiles x 4 KB, twice with a lo term
 };
 
 // One work item (a pair of 128-point tiles of one request) as every role sees it.
@@ -209,18 +212,21 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
         const Plan& P = *v.P;
         for (int32_t c = 0; c < P.oNR && ok; ++c) {
           const unsigned char* src = v.B + (int64_t)c * P.oChunkBytes;
-          for (int32_t j = 0; j < P.oNK; ++j) {
+          for (int32_t j = 0; j < P.oNK; j += kStageK) {
             if (!mbar_wait(&bars->empty[s], ph ^ 1, abort_flag)) {
               ok = false;
               break;
             }
-            const uint32_t bytes = (uint32_t)(outer_b_lo(P, j) ? 2 * P.oKstepBytes : P.oKstepBytes);
+            // the stage's B blocks lie back to back in the operand
+            uint32_t bytes = 0;
+            for (int g = 0; g < kStageK; ++g)
+              bytes += (uint32_t)(outer_b_lo(P, j + g) ? 2 * P.oKstepBytes : P.oKstepBytes);
             if (!RF_IN_BOUNDS((src - v.B) + bytes - 1, operand_bytes(P), err)) {
-              ok = false;  // no copy: the slot stays empty, and the waits on it end the kernel
+              ok = false;  // no copy: the stage stays empty, and the waits on it end the kernel
               break;
             }
             mbar_arrive_expect_tx(&bars->full[s], bytes);
-            bulk_g2s(slots + (size_t)s * slotBytes + aBytes, src, bytes, &bars->full[s]);
+            bulk_g2s(slots + (size_t)s * slotBytes + kStageK * aBytes, src, bytes, &bars->full[s]);
             src += bytes;
             if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
           }
@@ -239,17 +245,23 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
   } else if (warp == kIssuerWarp) {
     // ---------------------------------------------------------- MMA issuer
     // The whole warp runs the loop (warp-uniform state); one elected lane
-    // issues.  The MMAs of a K-step go out back to back: the lo terms through
-    // a guard predicate from the item's flag table (no branch between MMAs;
-    // a branch per MMA costs the issuing thread a resolution it cannot hide),
-    // and the next slot's barrier is probed before the last MMA so that the
-    // wait proper runs only when the probe failed.
+    // issues.  A stage's MMAs go out back to back, and the next stage's
+    // barrier is probed before the last MMA so that the wait proper runs only
+    // when the probe failed.  K-step 1 of a stage accumulates in any order
+    // (acc = 1), so its tile-1 hi MMA goes last, after the probe, in every
+    // case.  The lo K-steps are the top of a variance ranking and come in
+    // runs: stages whose K-steps both have or both lack every lo term take a
+    // straight path; the others issue the lo terms through a guard predicate
+    // from the item's flag table (no branch between MMAs; a branch per MMA
+    // costs the issuing thread a resolution it cannot hide).
+    static_assert(kStageK == 2, "the issuer writes out two K-steps per stage");
     const bool leader = elect_one();
     uint32_t s = 0, ph = 0, accPh = 0;
-    bool ok = true, ready = false;  // ready: full[s] of the next K-step already observed
+    bool ok = true, ready = false;  // ready: full[s] of the next stage already observed
     const uint32_t ab = PREC == PREC_FP16 ? 0u : 1u;
     const uint64_t aStepLo = (uint64_t)((2 * kATileBytes) >> 4);  // descriptor step to the lo A tiles
     const uint64_t aStepT = (uint64_t)(kATileBytes >> 4);         // descriptor step to tile 1's A
+    const uint64_t aStepK = (uint64_t)((uint32_t)aBytes >> 4);    // descriptor step to the next K-step's A
     for (int64_t i = 0; i < count && ok; ++i) {
       w.get(i, v);
       const Plan& P = *v.P;
@@ -268,27 +280,55 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
           break;
         }
         tc_fence_after();
-        for (int32_t j = 0; j < P.oNK; ++j) {
+        for (int32_t j = 0; j < P.oNK; j += kStageK) {
           if (!ready && !mbar_wait_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
           tc_fence_after();
           const uint32_t base = smem_u32(slots + (size_t)s * slotBytes);
           const uint64_t aDesc = make_sdesc(base, 2048u, 128u);
-          const uint64_t bDesc = make_sdesc(base + (uint32_t)aBytes, nRows * 16u, 128u);
-          const uint32_t f = bars->kflags[j];
-          const uint32_t bLo = f & 1u, aLo = f & 2u, acc = j > 0 ? 1u : 0u;
+          const uint64_t bDesc = make_sdesc(base + (uint32_t)(kStageK * aBytes), nRows * 16u, 128u);
+          // both K-steps' flags in one load (j is even)
+          const uint32_t f = *reinterpret_cast<const uint16_t*>(&bars->kflags[j]);
+          const uint32_t bLo0 = f & 1u, aLo0 = f & 2u, bLo1 = f & 0x100u, aLo1 = f & 0x200u;
+          const uint32_t acc = j > 0 ? 1u : 0u;
+          const uint64_t aDesc1 = aDesc + aStepK;
+          const uint64_t bDesc1 = bDesc + (bLo0 ? 2 * bStepLo : bStepLo);
           const uint32_t sn = (s + 1 == (uint32_t)S) ? 0u : s + 1;
           const uint32_t phn = (s + 1 == (uint32_t)S) ? ph ^ 1 : ph;
-          const bool more = (j + 1 < P.oNK) || (c + 1 < P.oNR) || (i + 1 < count);
+          const bool more = (j + kStageK < P.oNK) || (c + 1 < P.oNR) || (i + 1 < count);
           if (leader) {
-            mma_ss(tbase, aDesc, bDesc, idesc, acc);
-            mma_ss_if(tbase, aDesc, bDesc + bStepLo, idesc, 1u, bLo);
-            mma_ss_if(tbase, aDesc + aStepLo, bDesc, idesc, 1u, aLo);
-            mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc, idesc, acc);
-            mma_ss_if(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc + bStepLo, idesc, 1u, bLo);
+            if (f == 0u) {
+              mma_ss(tbase, aDesc, bDesc, idesc, acc);
+              mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc, idesc, acc);
+              mma_ss(tbase, aDesc1, bDesc1, idesc, 1u);
+            } else if (f == 0x0303u) {
+              mma_ss(tbase, aDesc, bDesc, idesc, acc);
+              mma_ss(tbase, aDesc, bDesc + bStepLo, idesc, 1u);
+              mma_ss(tbase, aDesc + aStepLo, bDesc, idesc, 1u);
+              mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc, idesc, acc);
+              mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc + bStepLo, idesc, 1u);
+              mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT + aStepLo, bDesc, idesc, 1u);
+              mma_ss(tbase, aDesc1, bDesc1, idesc, 1u);
+              mma_ss(tbase, aDesc1, bDesc1 + bStepLo, idesc, 1u);
+              mma_ss(tbase, aDesc1 + aStepLo, bDesc1, idesc, 1u);
+              mma_ss(tbase + (uint32_t)kAccCols, aDesc1 + aStepT, bDesc1 + bStepLo, idesc, 1u);
+              mma_ss(tbase + (uint32_t)kAccCols, aDesc1 + aStepT + aStepLo, bDesc1, idesc, 1u);
+            } else {
+              mma_ss(tbase, aDesc, bDesc, idesc, acc);
+              mma_ss_if(tbase, aDesc, bDesc + bStepLo, idesc, 1u, bLo0);
+              mma_ss_if(tbase, aDesc + aStepLo, bDesc, idesc, 1u, aLo0);
+              mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc, idesc, acc);
+              mma_ss_if(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc + bStepLo, idesc, 1u, bLo0);
+              mma_ss_if(tbase + (uint32_t)kAccCols, aDesc + aStepT + aStepLo, bDesc, idesc, 1u, aLo0);
+              mma_ss(tbase, aDesc1, bDesc1, idesc, 1u);
+              mma_ss_if(tbase, aDesc1, bDesc1 + bStepLo, idesc, 1u, bLo1);
+              mma_ss_if(tbase, aDesc1 + aStepLo, bDesc1, idesc, 1u, aLo1);
+              mma_ss_if(tbase + (uint32_t)kAccCols, aDesc1 + aStepT, bDesc1 + bStepLo, idesc, 1u, bLo1);
+              mma_ss_if(tbase + (uint32_t)kAccCols, aDesc1 + aStepT + aStepLo, bDesc1, idesc, 1u, aLo1);
+            }
           }
           ready = __all_sync(0xffffffffu, more && mbar_test_wait(&bars->full[sn], phn));
           if (leader) {
-            mma_ss_if(tbase + (uint32_t)kAccCols, aDesc + aStepT + aStepLo, bDesc, idesc, 1u, aLo);
+            mma_ss(tbase + (uint32_t)kAccCols, aDesc1 + aStepT, bDesc1, idesc, 1u);
             mma_commit(&bars->empty[s]);
           }
           __syncwarp();
@@ -313,6 +353,7 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
     const int t = gi >> 7, row = gi & 127;
     const uint32_t rowOff = (uint32_t)((row >> 3) * 128 + (row & 7) * 16);
     uint32_t s = 0, ph = 0;
+    int g = 0;  // the next K-step's place in its stage
     bool ok = true;
     for (int64_t i = 0; i < count && ok; ++i) {
       w.get(i, v);
@@ -335,18 +376,14 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
           float2 e2 = make_float2(1.f, 0.f);  // E2(i2), walked by angle addition
           for (int32_t i2 = 0; i2 < n2 && ok; ++i2) {
             const float2 E = make_float2(e2.x, s2 ? -e2.y : e2.y);
-            // The block's K-steps go to consecutive slots, each written as
-            // soon as its slot is free; the proxy fence and the arrivals are
-            // paid once per kGenPerFence K-steps (the fence waits for the
-            // warp's stores, so one per K-step would put its latency on every
-            // K-step of the pipeline).
-            uint32_t s0 = s;  // first slot not yet arrived on
-            int pending = 0;
+            // A stage is written once its barrier says the MMAs have
+            // released it; the proxy fence and the arrival are paid once per
+            // stage, after its last K-step (stages run across the blocks).
 #pragma unroll
             for (int jj = 0; jj < kOuterMaxN1P / 8; ++jj) {
               if (jj < nJJ) {
                 const int32_t j = jj + nJJ * (i2 + n2 * s2);
-                if (!mbar_wait_warp(&bars->empty[s], ph ^ 1, abort_flag)) {
+                if (g == 0 && !mbar_wait_warp(&bars->empty[s], ph ^ 1, abort_flag)) {
                   ok = false;
                   break;
                 }
@@ -358,7 +395,7 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
                   pv[u] = make_float2(q.x * E.x - q.y * E.y, q.x * E.y + q.y * E.x);
                   hi[u] = pack16<PREC>(pv[u].x, pv[u].y);
                 }
-                unsigned char* A = slots + (size_t)s * slotBytes + t * kATileBytes + rowOff;
+                unsigned char* A = slots + (size_t)s * slotBytes + g * aBytes + t * kATileBytes + rowOff;
                 *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
                 *reinterpret_cast<uint4*>(A + 2048) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
                 if (outer_a_lo(P, j)) {  // the residual of the 16-bit rounding, rounded again
@@ -371,16 +408,12 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
                   *reinterpret_cast<uint4*>(A + 2 * kATileBytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
                   *reinterpret_cast<uint4*>(A + 2 * kATileBytes + 2048) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
                 }
-                if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
-                ++pending;
-                if (pending == kGenPerFence || jj + 1 == nJJ) {
+                if (++g == kStageK) {
+                  g = 0;
                   fence_proxy_async_smem();
                   __syncwarp();
-                  for (int k = 0; k < pending; ++k) {
-                    if (lane == 0) mbar_arrive(&bars->full[s0]);
-                    if (++s0 == (uint32_t)S) s0 = 0;
-                  }
-                  pending = 0;
+                  if (lane == 0) mbar_arrive(&bars->full[s]);
+                  if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
                 }
               }
             }
@@ -472,17 +505,21 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_group_kernel(const 
   outer_body<PREC, kGroupLPad>(w, g.S, g.slotBytes, g.aBytes, g.err);
 }
 
-// Slot layout of a plan: A area (two tiles, twice with a lo term somewhere)
-// and B area (one K-step block, twice with a lo block somewhere).
-void outer_slot(const Plan& P, int32_t* aBytes, int32_t* slotBytes) {
+// Stage layout of a plan: per K-step an A area (two tiles, twice with a lo
+// term somewhere) and a B block (twice with a lo block somewhere); a stage
+// holds kStageK A areas and then kStageK B blocks.
+void outer_slot(const Plan& P, int32_t* aBytes, int32_t* bBytes) {
   bool aLo = false, bLo = false;
   for (int32_t j = 0; j < P.oNK; ++j) {
     aLo = aLo || outer_a_lo(P, j);
     bLo = bLo || outer_b_lo(P, j);
   }
   *aBytes = 2 * kATileBytes * (aLo ? 2 : 1);
-  const int64_t b = P.oKstepBytes * (bLo ? 2 : 1);
-  *slotBytes = (int32_t)((*aBytes + b + 127) / 128 * 128);
+  *bBytes = (int32_t)(P.oKstepBytes * (bLo ? 2 : 1));
+}
+
+int32_t outer_stage_bytes(int32_t aBytes, int32_t bBytes) {
+  return (kStageK * (aBytes + bBytes) + 127) / 128 * 128;
 }
 
 template <int PREC, int LPAD>
@@ -505,7 +542,7 @@ cudaError_t launch_outer_p(const OuterArgs& a, size_t smem, int grid, cudaStream
   }
 }
 
-// Slots of slotBytes that fit the shared memory, and the bytes to request
+// Stages of slotBytes that fit the shared memory, and the bytes to request
 // (0 when fewer than two fit).  More than half of the SM's shared memory is
 // requested so that one CTA (and its 512 TMEM columns) sits on an SM.
 size_t outer_fit(int32_t slotBytes, int* stages, int maxStages = 0) {
@@ -522,21 +559,21 @@ size_t outer_fit(int32_t slotBytes, int* stages, int maxStages = 0) {
 }  // namespace
 
 size_t outer_smem_bytes(const Plan& P, int* stages) {
-  int32_t aBytes = 0, slotBytes = 0;
-  outer_slot(P, &aBytes, &slotBytes);
-  return outer_fit(slotBytes, stages);
+  int32_t aBytes = 0, bBytes = 0;
+  outer_slot(P, &aBytes, &bBytes);
+  return outer_fit(outer_stage_bytes(aBytes, bBytes), stages);
 }
 
 size_t outer_group_layout(const Plan* const* plans, size_t count, int maxStages, OuterGroupArgs* g) {
   int32_t aMax = 2 * kATileBytes, bMax = 0;
   for (size_t i = 0; i < count; ++i) {
-    int32_t a = 0, sb = 0;
-    outer_slot(*plans[i], &a, &sb);
+    int32_t a = 0, b = 0;
+    outer_slot(*plans[i], &a, &b);
     aMax = a > aMax ? a : aMax;
-    bMax = (sb - a) > bMax ? (sb - a) : bMax;
+    bMax = b > bMax ? b : bMax;
   }
   g->aBytes = aMax;
-  g->slotBytes = (aMax + bMax + 127) / 128 * 128;
+  g->slotBytes = outer_stage_bytes(aMax, bMax);
   int S = 0;
   const size_t smem = outer_fit(g->slotBytes, &S, maxStages);
   g->S = S;
@@ -565,7 +602,9 @@ cudaError_t launch_outer(const Plan& P, const double* dX, const void* dB, double
   a.err = dErr;
   a.row0 = row0;
   a.rows = rows;
-  outer_slot(P, &a.aBytes, &a.slotBytes);
+  int32_t bBytes = 0;
+  outer_slot(P, &a.aBytes, &bBytes);
+  a.slotBytes = outer_stage_bytes(a.aBytes, bBytes);
   int S = 0;
   const size_t smem = outer_smem_bytes(P, &S);
   if (smem == 0) return cudaErrorInvalidValue;
