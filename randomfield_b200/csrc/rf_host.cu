@@ -515,7 +515,8 @@ void outer_layout(Plan& P) {
     std::vector<std::pair<double, int32_t>> E((size_t)nK);
     double total = 0.0;
     for (int32_t j = 0; j < nK; ++j) {
-      const int32_t jj = j % (n1p / 8), i2 = (j / (n1p / 8)) % n2;
+      int32_t jj = 0, i2 = 0, s2 = 0;
+      outer_kstep_groups(P, j, &jj, &i2, &s2);
       double w = 0.0;
       for (int32_t i1 = 8 * jj; i1 < std::min(n1, 8 * jj + 8); ++i1) {
         if (P.corrMod != RF_CM_GAUSSIAN) {
@@ -541,6 +542,18 @@ void outer_layout(Plan& P) {
     }
   }
   P.oChunkBytes = (int64_t)(nK + mask_rank(P.loMask, nK)) * P.oKstepBytes;
+  memset(P.oStageEnd, 0, sizeof(P.oStageEnd));
+  int32_t ua = 0, ub = 0;
+  for (int32_t j = 0; j < nK; ++j) {
+    const int32_t a = outer_a_lo(P, j) ? 2 : 1, b = outer_b_lo(P, j) ? 2 : 1;
+    if (ua + a > kOuterStageUnits || ub + b > kOuterStageUnits) {
+      P.oStageEnd[(j - 1) >> 5] |= 1u << ((j - 1) & 31);
+      ua = ub = 0;
+    }
+    ua += a;
+    ub += b;
+  }
+  P.oStageEnd[(nK - 1) >> 5] |= 1u << ((nK - 1) & 31);
   // FP16: B holds sums of two amplitudes (|W| <= 2), scaled so that the
   // largest sits near 2^15
   if (P.prec == PREC_FP16) {

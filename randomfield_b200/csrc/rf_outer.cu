@@ -24,8 +24,8 @@
 // realization block is cut into N chunks of oRc realizations (TMEM: one
 // 256-column accumulator per tile); for each chunk the K-steps (16 K = 8
 // outer groups of consecutive i1) stream through a ring of shared-memory
-// stages of two K-steps, each K-step with both tiles' A (hi, and lo where the
-// plan keeps it) and B's K-step block (hi, and lo).
+// stages, each holding two to four consecutive K-steps: both tiles' A (hi,
+// and lo where the plan keeps it) and B's K-step blocks (hi, and lo).
 //
 // Warp roles (576 threads):
 //   warp 0      MMA issuer: the warp runs the stage loop, one elected lane
@@ -36,8 +36,9 @@
 //   warps 2-9   generators: one point each (256 = two tiles); per K-step the
 //               8 outer phasors E1(i1) E2(i2)^{s2} of the point, rounded to
 //               16 bits (and the lo residual), stored in the K-major core-
-//               matrix layout; E1 from FP64-reduced phases per work item, E2
-//               walked by angle addition per chunk;
+//               matrix layout; the K-steps run axis-1 block by block (E1 of
+//               the block's 8 i1 from FP64-reduced phases), E2 walked by
+//               angle addition over i2;
 //   warps 10-17 epilogue: tcgen05.ld of a tile's accumulator (warp % 4 picks
 //               the TMEM lane quarter), the i3 sum with the point's own
 //               E3 phasors, ampMult, the marginal map, FP64 stores.
@@ -60,13 +61,15 @@ constexpr int kOuterMaxSlots = 8;
 constexpr int kATileBytes = kTileM * 16 * 2;  // one tile's K-step of A: 128 rows x 16 K x 16 bits
 constexpr uint32_t kOuterTmemCols = 512;
 constexpr int kAccCols = 256;  // accumulator columns per tile
-// K-steps per ring stage: one full/empty barrier pair, one bulk copy, one
-// generator fence and one commit serve kStageK K-steps.  A K-step's MMAs keep
-// the tensor pipe busy for about as long as the issuing thread takes to issue
-// them, so the per-stage bookkeeping (barrier probe, commit, loop control)
-// shows up directly in the kernel's time; two K-steps per stage halve it.
-// A chunk's K-step count 2 n2 nJJ is always even.
-constexpr int kStageK = 2;
+// Ring stages of kOuterStageUnits units (rf_plan.h): one full/empty barrier
+// pair, one bulk copy, one generator fence and one commit serve a stage of
+// two to four K-steps.  The issuing thread keeps the tensor pipe fed only
+// when it issues about eight or more MMAs per loop pass (measured on this
+// kernel's MMA shape: 4 MMAs per pass ran at 1.4x the pipe's time per MMA,
+// 8 at 1.03x, 12 at 1.0x, whatever the pass did besides), and a stage of
+// four K-steps without lo terms carries 8, one of two K-steps with both 12.
+constexpr int kAUnitBytes = 2 * kATileBytes;                    // both tiles' hi A of one K-step
+constexpr int kStageABytes = kOuterStageUnits * kAUnitBytes;    // A area of a stage
 
 struct OuterBars {
   uint64_t full[kOuterMaxSlots];   // per stage: 8 generator warps + producer (bytes)
@@ -76,10 +79,12 @@ struct OuterBars {
   uint64_t done;
   uint32_t tmem_base;
   int abort_flag;
-  // the issuer's table of the current item's K-steps: bit 0 B lo, bit 1 A lo
-  uint8_t kflags[kOuterMaxKsteps];
+  int32_t nStages;                 // stages per chunk of the current item
+  // the issuer's table of the current item's stages: first K-step (bits
+  // 0-8), K-steps (bits 9-11), per K-step k bits 12+2k (B lo) and 13+2k (A lo)
+  uint32_t stab[kOuterMaxKsteps];
 };
-constexpr int kOuterHeader = 512;
+constexpr int kOuterHeader = 2048;
 static_assert(sizeof(OuterBars) <= kOuterHeader, "header");
 
 struct OuterArgs {
@@ -90,8 +95,8 @@ struct OuterArgs {
   uint32_t* err;
   int64_t row0, rows;
   int32_t S;          // ring stages
-  int32_t slotBytes;  // one stage: kStageK A areas, then kStageK B blocks; 128-byte multiple
-  int32_t aBytes;     // one K-step's A area: two tiles x 4 KB, twice with a lo term
+  int32_t slotBytes;  // one stage: A area (kStageABytes), then kOuterStageUnits B units; 128-byte multiple
+  int32_t aBytes;     // A area of a stage (kStageABytes)
 };
 
 // One work item (a pair of 128-point tiles of one request) as every role sees it.
@@ -144,15 +149,6 @@ struct GroupOuterWork {
 __device__ __forceinline__ void outer_abort(OuterBars* bars, uint32_t* err) {
   *reinterpret_cast<volatile int*>(&bars->abort_flag) = 1;
   atomicOr(err, kErrTimeout);
-}
-
-__device__ __forceinline__ double outer_finish(const Plan& P, float acc) {
-  double v = (double)acc * P.outScale;
-  if (P.applyMarginal) {
-    v = v * P.margSd + P.margAvg;
-    if (P.lognormal) v = exp(v);
-  }
-  return v;
 }
 
 template <int PREC>
@@ -210,23 +206,28 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
       for (int64_t i = 0; i < count && ok; ++i) {
         w.get(i, v);
         const Plan& P = *v.P;
-        for (int32_t c = 0; c < P.oNR && ok; ++c) {
-          const unsigned char* src = v.B + (int64_t)c * P.oChunkBytes;
-          for (int32_t j = 0; j < P.oNK; j += kStageK) {
+        const int32_t oNK = P.oNK, oNR = P.oNR;
+        const int64_t chunkBytes = P.oChunkBytes, opBytes = operand_bytes(P);
+        for (int32_t c = 0; c < oNR && ok; ++c) {
+          const unsigned char* src = v.B + (int64_t)c * chunkBytes;
+          for (int32_t j = 0; j < oNK;) {
             if (!mbar_wait(&bars->empty[s], ph ^ 1, abort_flag)) {
               ok = false;
               break;
             }
             // the stage's B blocks lie back to back in the operand
             uint32_t bytes = 0;
-            for (int g = 0; g < kStageK; ++g)
-              bytes += (uint32_t)(outer_b_lo(P, j + g) ? 2 * P.oKstepBytes : P.oKstepBytes);
-            if (!RF_IN_BOUNDS((src - v.B) + bytes - 1, operand_bytes(P), err)) {
+            bool end = false;
+            for (; j < oNK && !end; ++j) {
+              bytes += (uint32_t)(outer_b_lo(P, j) ? 2 * P.oKstepBytes : P.oKstepBytes);
+              end = outer_stage_end(P, j);
+            }
+            if (!RF_IN_BOUNDS((src - v.B) + bytes - 1, opBytes, err)) {
               ok = false;  // no copy: the stage stays empty, and the waits on it end the kernel
               break;
             }
             mbar_arrive_expect_tx(&bars->full[s], bytes);
-            bulk_g2s(slots + (size_t)s * slotBytes + kStageK * aBytes, src, bytes, &bars->full[s]);
+            bulk_g2s(slots + (size_t)s * slotBytes + kStageABytes, src, bytes, &bars->full[s]);
             src += bytes;
             if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
           }
@@ -247,32 +248,47 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
     // The whole warp runs the loop (warp-uniform state); one elected lane
     // issues.  A stage's MMAs go out back to back, and the next stage's
     // barrier is probed before the last MMA so that the wait proper runs only
-    // when the probe failed.  K-step 1 of a stage accumulates in any order
-    // (acc = 1), so its tile-1 hi MMA goes last, after the probe, in every
-    // case.  The lo K-steps are the top of a variance ranking and come in
-    // runs: stages whose K-steps both have or both lack every lo term take a
-    // straight path; the others issue the lo terms through a guard predicate
-    // from the item's flag table (no branch between MMAs; a branch per MMA
-    // costs the issuing thread a resolution it cannot hide).
-    static_assert(kStageK == 2, "the issuer writes out two K-steps per stage");
+    // when the probe failed.  Stages of four K-steps without lo terms and of
+    // two K-steps with both (nearly all of them: the lo K-steps are the top
+    // of a variance ranking and come in runs) take straight paths, whose last
+    // MMA is a tile-1 hi MMA that may accumulate in any order (acc = 1) and
+    // so goes after the probe; other stages loop over their K-steps with the
+    // lo terms under a guard predicate.
     const bool leader = elect_one();
     uint32_t s = 0, ph = 0, accPh = 0;
     bool ok = true, ready = false;  // ready: full[s] of the next stage already observed
     const uint32_t ab = PREC == PREC_FP16 ? 0u : 1u;
-    const uint64_t aStepLo = (uint64_t)((2 * kATileBytes) >> 4);  // descriptor step to the lo A tiles
-    const uint64_t aStepT = (uint64_t)(kATileBytes >> 4);         // descriptor step to tile 1's A
-    const uint64_t aStepK = (uint64_t)((uint32_t)aBytes >> 4);    // descriptor step to the next K-step's A
+    const uint64_t aT = (uint64_t)(kATileBytes >> 4);  // descriptor step to tile 1's A
+    const uint64_t aU = (uint64_t)(kAUnitBytes >> 4);  // descriptor step of one A unit
     for (int64_t i = 0; i < count && ok; ++i) {
       w.get(i, v);
       const Plan& P = *v.P;
-      for (int32_t j = lane; j < P.oNK; j += 32)
-        bars->kflags[j] = (uint8_t)((outer_b_lo(P, j) ? 1u : 0u) | (outer_a_lo(P, j) ? 2u : 0u));
+      // the item's loop bounds in registers: every tcgen05 and mbarrier
+      // statement clobbers memory, and a plan field read inside the loop
+      // would be loaded again after each of them
+      const int32_t oNK = P.oNK, oNR = P.oNR, oRc = P.oRc, nmcBlk = P.nmcBlk, lPad = P.lPad;
+      const uint64_t bU = (uint64_t)(P.oKstepBytes >> 4);  // descriptor step of one B unit
+      if (lane == 0) {
+        int32_t ns = 0, j0 = 0, n = 0;
+        uint32_t fl = 0;
+        for (int32_t j = 0; j < oNK; ++j) {
+          fl |= ((outer_b_lo(P, j) ? 1u : 0u) | (outer_a_lo(P, j) ? 2u : 0u)) << (2 * n);
+          ++n;
+          if (outer_stage_end(P, j) || j + 1 == oNK) {
+            bars->stab[ns++] = (uint32_t)j0 | ((uint32_t)n << 9) | (fl << 12);
+            j0 = j + 1;
+            n = 0;
+            fl = 0;
+          }
+        }
+        bars->nStages = ns;
+      }
       __syncwarp();
-      const uint64_t bStepLo = (uint64_t)(P.oKstepBytes >> 4);
-      const uint32_t nRows = (uint32_t)(2 * P.lPad * P.oRc);  // B rows (N) of a full chunk
-      for (int32_t c = 0; c < P.oNR && ok; ++c) {
-        const int32_t rc = min(P.oRc, P.nmcBlk - c * P.oRc);
-        const uint32_t idesc = make_idesc(ab, 128u, (uint32_t)(2 * P.lPad * rc));
+      const int32_t nSt = *reinterpret_cast<volatile int32_t*>(&bars->nStages);
+      const uint32_t nRows = (uint32_t)(2 * lPad * oRc);  // B rows (N) of a full chunk
+      for (int32_t c = 0; c < oNR && ok; ++c) {
+        const int32_t rc = min(oRc, nmcBlk - c * oRc);
+        const uint32_t idesc = make_idesc(ab, 128u, (uint32_t)(2 * lPad * rc));
         // both accumulators are free once the epilogue has read the last chunk
         if (!mbar_wait_warp(&bars->acc_empty[0], accPh ^ 1, abort_flag) ||
             !mbar_wait_warp(&bars->acc_empty[1], accPh ^ 1, abort_flag)) {
@@ -280,55 +296,63 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
           break;
         }
         tc_fence_after();
-        for (int32_t j = 0; j < P.oNK; j += kStageK) {
+        uint32_t eNext = bars->stab[0];
+        for (int32_t st = 0; st < nSt; ++st) {
           if (!ready && !mbar_wait_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
           tc_fence_after();
+          const uint32_t e = eNext;  // read one stage ahead
+          if (st + 1 < nSt) eNext = bars->stab[st + 1];
+          const uint32_t n = (e >> 9) & 7u, fl = e >> 12;
+          const uint32_t acc = (e & 0x1ffu) ? 1u : 0u;  // the chunk's first K-step starts the accumulators
           const uint32_t base = smem_u32(slots + (size_t)s * slotBytes);
-          const uint64_t aDesc = make_sdesc(base, 2048u, 128u);
-          const uint64_t bDesc = make_sdesc(base + (uint32_t)(kStageK * aBytes), nRows * 16u, 128u);
-          // both K-steps' flags in one load (j is even)
-          const uint32_t f = *reinterpret_cast<const uint16_t*>(&bars->kflags[j]);
-          const uint32_t bLo0 = f & 1u, aLo0 = f & 2u, bLo1 = f & 0x100u, aLo1 = f & 0x200u;
-          const uint32_t acc = j > 0 ? 1u : 0u;
-          const uint64_t aDesc1 = aDesc + aStepK;
-          const uint64_t bDesc1 = bDesc + (bLo0 ? 2 * bStepLo : bStepLo);
+          const uint64_t aD = make_sdesc(base, 2048u, 128u);
+          const uint64_t bD = make_sdesc(base + (uint32_t)kStageABytes, nRows * 16u, 128u);
           const uint32_t sn = (s + 1 == (uint32_t)S) ? 0u : s + 1;
           const uint32_t phn = (s + 1 == (uint32_t)S) ? ph ^ 1 : ph;
-          const bool more = (j + kStageK < P.oNK) || (c + 1 < P.oNR) || (i + 1 < count);
+          const bool more = (st + 1 < nSt) || (c + 1 < oNR) || (i + 1 < count);
+          const bool quad = fl == 0u && n == 4u, pair = fl == 0xFu && n == 2u;
           if (leader) {
-            if (f == 0u) {
-              mma_ss(tbase, aDesc, bDesc, idesc, acc);
-              mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc, idesc, acc);
-              mma_ss(tbase, aDesc1, bDesc1, idesc, 1u);
-            } else if (f == 0x0303u) {
-              mma_ss(tbase, aDesc, bDesc, idesc, acc);
-              mma_ss(tbase, aDesc, bDesc + bStepLo, idesc, 1u);
-              mma_ss(tbase, aDesc + aStepLo, bDesc, idesc, 1u);
-              mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc, idesc, acc);
-              mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc + bStepLo, idesc, 1u);
-              mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT + aStepLo, bDesc, idesc, 1u);
-              mma_ss(tbase, aDesc1, bDesc1, idesc, 1u);
-              mma_ss(tbase, aDesc1, bDesc1 + bStepLo, idesc, 1u);
-              mma_ss(tbase, aDesc1 + aStepLo, bDesc1, idesc, 1u);
-              mma_ss(tbase + (uint32_t)kAccCols, aDesc1 + aStepT, bDesc1 + bStepLo, idesc, 1u);
-              mma_ss(tbase + (uint32_t)kAccCols, aDesc1 + aStepT + aStepLo, bDesc1, idesc, 1u);
+            if (quad) {
+              mma_ss(tbase, aD, bD, idesc, acc);
+              mma_ss(tbase + (uint32_t)kAccCols, aD + aT, bD, idesc, acc);
+              mma_ss(tbase, aD + aU, bD + bU, idesc, 1u);
+              mma_ss(tbase + (uint32_t)kAccCols, aD + aU + aT, bD + bU, idesc, 1u);
+              mma_ss(tbase, aD + 2 * aU, bD + 2 * bU, idesc, 1u);
+              mma_ss(tbase + (uint32_t)kAccCols, aD + 2 * aU + aT, bD + 2 * bU, idesc, 1u);
+              mma_ss(tbase, aD + 3 * aU, bD + 3 * bU, idesc, 1u);
+            } else if (pair) {
+              // K-step 0 in units 0-1 (hi, lo) of A and B, K-step 1 in units 2-3
+              mma_ss(tbase, aD, bD, idesc, acc);
+              mma_ss(tbase, aD, bD + bU, idesc, 1u);
+              mma_ss(tbase, aD + aU, bD, idesc, 1u);
+              mma_ss(tbase + (uint32_t)kAccCols, aD + aT, bD, idesc, acc);
+              mma_ss(tbase + (uint32_t)kAccCols, aD + aT, bD + bU, idesc, 1u);
+              mma_ss(tbase + (uint32_t)kAccCols, aD + aU + aT, bD, idesc, 1u);
+              mma_ss(tbase, aD + 2 * aU, bD + 2 * bU, idesc, 1u);
+              mma_ss(tbase, aD + 2 * aU, bD + 3 * bU, idesc, 1u);
+              mma_ss(tbase, aD + 3 * aU, bD + 2 * bU, idesc, 1u);
+              mma_ss(tbase + (uint32_t)kAccCols, aD + 2 * aU + aT, bD + 3 * bU, idesc, 1u);
+              mma_ss(tbase + (uint32_t)kAccCols, aD + 3 * aU + aT, bD + 2 * bU, idesc, 1u);
             } else {
-              mma_ss(tbase, aDesc, bDesc, idesc, acc);
-              mma_ss_if(tbase, aDesc, bDesc + bStepLo, idesc, 1u, bLo0);
-              mma_ss_if(tbase, aDesc + aStepLo, bDesc, idesc, 1u, aLo0);
-              mma_ss(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc, idesc, acc);
-              mma_ss_if(tbase + (uint32_t)kAccCols, aDesc + aStepT, bDesc + bStepLo, idesc, 1u, bLo0);
-              mma_ss_if(tbase + (uint32_t)kAccCols, aDesc + aStepT + aStepLo, bDesc, idesc, 1u, aLo0);
-              mma_ss(tbase, aDesc1, bDesc1, idesc, 1u);
-              mma_ss_if(tbase, aDesc1, bDesc1 + bStepLo, idesc, 1u, bLo1);
-              mma_ss_if(tbase, aDesc1 + aStepLo, bDesc1, idesc, 1u, aLo1);
-              mma_ss_if(tbase + (uint32_t)kAccCols, aDesc1 + aStepT, bDesc1 + bStepLo, idesc, 1u, bLo1);
-              mma_ss_if(tbase + (uint32_t)kAccCols, aDesc1 + aStepT + aStepLo, bDesc1, idesc, 1u, aLo1);
+              uint64_t a = aD, b = bD;
+              for (uint32_t k = 0; k < n; ++k) {
+                const uint32_t f = (fl >> (2 * k)) & 3u, bLo = f & 1u, aLo = f & 2u;
+                const uint32_t ak = k == 0 ? acc : 1u;
+                mma_ss(tbase, a, b, idesc, ak);
+                mma_ss_if(tbase, a, b + bU, idesc, 1u, bLo);
+                mma_ss_if(tbase, a + aU, b, idesc, 1u, aLo);
+                mma_ss(tbase + (uint32_t)kAccCols, a + aT, b, idesc, ak);
+                mma_ss_if(tbase + (uint32_t)kAccCols, a + aT, b + bU, idesc, 1u, bLo);
+                mma_ss_if(tbase + (uint32_t)kAccCols, a + aU + aT, b, idesc, 1u, aLo);
+                a += aLo ? 2 * aU : aU;
+                b += bLo ? 2 * bU : bU;
+              }
             }
           }
           ready = __all_sync(0xffffffffu, more && mbar_test_wait(&bars->full[sn], phn));
           if (leader) {
-            mma_ss(tbase + (uint32_t)kAccCols, aDesc1 + aStepT, bDesc1, idesc, 1u);
+            if (quad) mma_ss(tbase + (uint32_t)kAccCols, aD + 3 * aU + aT, bD + 3 * bU, idesc, 1u);
+            else if (pair) mma_ss(tbase + (uint32_t)kAccCols, aD + 2 * aU + aT, bD + 2 * bU, idesc, 1u);
             mma_commit(&bars->empty[s]);
           }
           __syncwarp();
@@ -353,7 +377,7 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
     const int t = gi >> 7, row = gi & 127;
     const uint32_t rowOff = (uint32_t)((row >> 3) * 128 + (row & 7) * 16);
     uint32_t s = 0, ph = 0;
-    int g = 0;  // the next K-step's place in its stage
+    uint32_t ua = 0;  // A units of the current stage already written
     bool ok = true;
     for (int64_t i = 0; i < count && ok; ++i) {
       w.get(i, v);
@@ -366,58 +390,69 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
         x0 = v.x[p * 3 + 0] / P.corrL[0];
         x1 = v.x[p * 3 + 1] / P.corrL[1];
       }
-      float2 e1[kOuterMaxN1P];
-#pragma unroll
-      for (int u = 0; u < kOuterMaxN1P; ++u)
-        e1[u] = (u < n1) ? axis_phasor(P.kDelta[0], u, x0) : make_float2(0.f, 0.f);
       const float2 e2step = axis_phasor(P.kDelta[1], 1, x1);
-      for (int32_t c = 0; c < P.oNR && ok; ++c) {
-        for (int32_t s2 = 0; s2 < 2 && ok; ++s2) {
-          float2 e2 = make_float2(1.f, 0.f);  // E2(i2), walked by angle addition
-          for (int32_t i2 = 0; i2 < n2 && ok; ++i2) {
-            const float2 E = make_float2(e2.x, s2 ? -e2.y : e2.y);
-            // A stage is written once its barrier says the MMAs have
-            // released it; the proxy fence and the arrival are paid once per
-            // stage, after its last K-step (stages run across the blocks).
+      const int32_t oNR = P.oNR;
+      const double kd0 = P.kDelta[0];
+      for (int32_t c = 0; c < oNR && ok; ++c) {
+        // K-steps in order j = 0, 1, ... (i2 fastest, then s2, then jj);
+        // the A lo and stage-end flags read 32 at a time
+        int32_t j = 0;
+        uint32_t aw = 0, ew = 0;
+        for (int32_t jj = 0; jj < nJJ && ok; ++jj) {
+          // the block's 8 axis-1 phasors E1(8 jj + u), from FP64-reduced
+          // phases (8 per block and chunk against 2 n2 K-steps)
+          float2 e1[8];
 #pragma unroll
-            for (int jj = 0; jj < kOuterMaxN1P / 8; ++jj) {
-              if (jj < nJJ) {
-                const int32_t j = jj + nJJ * (i2 + n2 * s2);
-                if (g == 0 && !mbar_wait_warp(&bars->empty[s], ph ^ 1, abort_flag)) {
-                  ok = false;
-                  break;
-                }
-                float2 pv[8];
-                uint32_t hi[8];
+          for (int u = 0; u < 8; ++u)
+            e1[u] = (8 * jj + u < n1) ? axis_phasor(kd0, 8 * jj + u, x0) : make_float2(0.f, 0.f);
+          for (int32_t s2 = 0; s2 < 2 && ok; ++s2) {
+            float2 e2 = make_float2(1.f, 0.f);  // E2(i2), walked by angle addition
+            for (int32_t i2 = 0; i2 < n2; ++i2) {
+              const float2 E = make_float2(e2.x, s2 ? -e2.y : e2.y);
+              if ((j & 31) == 0) {
+                aw = P.aLoMask[j >> 5];
+                ew = P.oStageEnd[j >> 5];
+              }
+              const bool aLo = (aw >> (j & 31)) & 1u, end = (ew >> (j & 31)) & 1u;
+              // A stage is written once its barrier says the MMAs have
+              // released it; the proxy fence and the arrival are paid once
+              // per stage, after its last K-step.
+              if (ua == 0 && !mbar_wait_warp(&bars->empty[s], ph ^ 1, abort_flag)) {
+                ok = false;
+                break;
+              }
+              float2 pv[8];
+              uint32_t hi[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) {
+                const float2 q = e1[u];
+                pv[u] = make_float2(q.x * E.x - q.y * E.y, q.x * E.y + q.y * E.x);
+                hi[u] = pack16<PREC>(pv[u].x, pv[u].y);
+              }
+              unsigned char* A = slots + (size_t)s * slotBytes + ua * kAUnitBytes + t * kATileBytes + rowOff;
+              *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+              *reinterpret_cast<uint4*>(A + 2048) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+              if (aLo) {  // the residual of the 16-bit rounding, rounded again, in the next unit
+                uint32_t lo[8];
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
-                  const float2 q = e1[8 * jj + u];
-                  pv[u] = make_float2(q.x * E.x - q.y * E.y, q.x * E.y + q.y * E.x);
-                  hi[u] = pack16<PREC>(pv[u].x, pv[u].y);
+                  const float2 h = unpack16<PREC>(hi[u]);
+                  lo[u] = pack16<PREC>(pv[u].x - h.x, pv[u].y - h.y);
                 }
-                unsigned char* A = slots + (size_t)s * slotBytes + g * aBytes + t * kATileBytes + rowOff;
-                *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-                *reinterpret_cast<uint4*>(A + 2048) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
-                if (outer_a_lo(P, j)) {  // the residual of the 16-bit rounding, rounded again
-                  uint32_t lo[8];
-#pragma unroll
-                  for (int u = 0; u < 8; ++u) {
-                    const float2 h = unpack16<PREC>(hi[u]);
-                    lo[u] = pack16<PREC>(pv[u].x - h.x, pv[u].y - h.y);
-                  }
-                  *reinterpret_cast<uint4*>(A + 2 * kATileBytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-                  *reinterpret_cast<uint4*>(A + 2 * kATileBytes + 2048) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
-                }
-                if (++g == kStageK) {
-                  g = 0;
-                  fence_proxy_async_smem();
-                  __syncwarp();
-                  if (lane == 0) mbar_arrive(&bars->full[s]);
-                  if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
-                }
+                *reinterpret_cast<uint4*>(A + kAUnitBytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+                *reinterpret_cast<uint4*>(A + kAUnitBytes + 2048) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
               }
+              ua += aLo ? 2u : 1u;
+              if (end) {
+                ua = 0;
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bars->full[s]);
+                if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+              }
+              e2 = make_float2(e2.x * e2step.x - e2.y * e2step.y, e2.x * e2step.y + e2.y * e2step.x);
+              ++j;
             }
-            e2 = make_float2(e2.x * e2step.x - e2.y * e2step.y, e2.x * e2step.y + e2.y * e2step.x);
           }
         }
       }
@@ -444,10 +479,15 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
 #pragma unroll
       for (int u = 0; u < LPAD; ++u)
         e3[u] = (u < P.kNStep[2]) ? axis_phasor(P.kDelta[2], u, x2) : make_float2(0.f, 0.f);
-      for (int32_t c = 0; c < P.oNR; ++c) {
+      const int32_t oNR = P.oNR, oRc = P.oRc, nmcBlk = P.nmcBlk;
+      const int64_t rOff = P.rOff, n = P.n, nOut = P.blend ? P.gTotal : P.n;
+      [[maybe_unused]] const int64_t outLen = (int64_t)P.Nmc * nOut;  // the index checks' bound
+      const bool blend = P.blend, marg = P.applyMarginal, logn = P.lognormal;
+      const double outScale = P.outScale, margSd = P.margSd, margAvg = P.margAvg;
+      for (int32_t c = 0; c < oNR; ++c) {
         if (!mbar_wait_warp(&bars->acc_full, accPh, abort_flag)) { ok = false; break; }
         tc_fence_after();
-        const int32_t rc = min(P.oRc, P.nmcBlk - c * P.oRc);
+        const int32_t rc = min(oRc, nmcBlk - c * oRc);
         for (int32_t rl = 0; rl < rc; ++rl) {
           // the realization's 2 LPAD columns in 32-column round trips (a load
           // then a wait for it; the last piece of an odd LH is 16 columns)
@@ -468,12 +508,17 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
             }
           }
           if (valid) {
-            const int64_t r = (int64_t)P.rOff + c * P.oRc + rl;
-            if (P.blend) {
-              if (RF_IN_BOUNDS(r * P.gTotal + bg, (int64_t)P.Nmc * P.gTotal, err))
-                atomicAdd(&v.out[r * P.gTotal + bg], bw * ((double)acc * P.outScale));
-            } else if (RF_IN_BOUNDS(r * P.n + p, (int64_t)P.Nmc * P.n, err)) {
-              v.out[r * P.n + p] = outer_finish(P, acc);
+            const int64_t r = rOff + (int64_t)c * oRc + rl;
+            if (blend) {
+              if (RF_IN_BOUNDS(r * nOut + bg, outLen, err))
+                atomicAdd(&v.out[r * nOut + bg], bw * ((double)acc * outScale));
+            } else if (RF_IN_BOUNDS(r * n + p, outLen, err)) {
+              double f = (double)acc * outScale;
+              if (marg) {
+                f = f * margSd + margAvg;
+                if (logn) f = exp(f);
+              }
+              v.out[r * n + p] = f;
             }
           }
         }
@@ -505,21 +550,10 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_group_kernel(const 
   outer_body<PREC, kGroupLPad>(w, g.S, g.slotBytes, g.aBytes, g.err);
 }
 
-// Stage layout of a plan: per K-step an A area (two tiles, twice with a lo
-// term somewhere) and a B block (twice with a lo block somewhere); a stage
-// holds kStageK A areas and then kStageK B blocks.
-void outer_slot(const Plan& P, int32_t* aBytes, int32_t* bBytes) {
-  bool aLo = false, bLo = false;
-  for (int32_t j = 0; j < P.oNK; ++j) {
-    aLo = aLo || outer_a_lo(P, j);
-    bLo = bLo || outer_b_lo(P, j);
-  }
-  *aBytes = 2 * kATileBytes * (aLo ? 2 : 1);
-  *bBytes = (int32_t)(P.oKstepBytes * (bLo ? 2 : 1));
-}
-
-int32_t outer_stage_bytes(int32_t aBytes, int32_t bBytes) {
-  return (kStageK * (aBytes + bBytes) + 127) / 128 * 128;
+// Stage layout: the A area (kOuterStageUnits units of kAUnitBytes), then
+// kOuterStageUnits B units of bUnit bytes (one K-step block of B).
+int32_t outer_stage_bytes(int64_t bUnit) {
+  return (int32_t)((kStageABytes + kOuterStageUnits * bUnit + 127) / 128 * 128);
 }
 
 template <int PREC, int LPAD>
@@ -559,21 +593,14 @@ size_t outer_fit(int32_t slotBytes, int* stages, int maxStages = 0) {
 }  // namespace
 
 size_t outer_smem_bytes(const Plan& P, int* stages) {
-  int32_t aBytes = 0, bBytes = 0;
-  outer_slot(P, &aBytes, &bBytes);
-  return outer_fit(outer_stage_bytes(aBytes, bBytes), stages);
+  return outer_fit(outer_stage_bytes(P.oKstepBytes), stages);
 }
 
 size_t outer_group_layout(const Plan* const* plans, size_t count, int maxStages, OuterGroupArgs* g) {
-  int32_t aMax = 2 * kATileBytes, bMax = 0;
-  for (size_t i = 0; i < count; ++i) {
-    int32_t a = 0, b = 0;
-    outer_slot(*plans[i], &a, &b);
-    aMax = a > aMax ? a : aMax;
-    bMax = b > bMax ? b : bMax;
-  }
-  g->aBytes = aMax;
-  g->slotBytes = outer_stage_bytes(aMax, bMax);
+  int64_t bMax = 0;
+  for (size_t i = 0; i < count; ++i) bMax = plans[i]->oKstepBytes > bMax ? plans[i]->oKstepBytes : bMax;
+  g->aBytes = kStageABytes;
+  g->slotBytes = outer_stage_bytes(bMax);
   int S = 0;
   const size_t smem = outer_fit(g->slotBytes, &S, maxStages);
   g->S = S;
@@ -602,9 +629,8 @@ cudaError_t launch_outer(const Plan& P, const double* dX, const void* dB, double
   a.err = dErr;
   a.row0 = row0;
   a.rows = rows;
-  int32_t bBytes = 0;
-  outer_slot(P, &a.aBytes, &bBytes);
-  a.slotBytes = outer_stage_bytes(a.aBytes, bBytes);
+  a.aBytes = kStageABytes;
+  a.slotBytes = outer_stage_bytes(P.oKstepBytes);
   int S = 0;
   const size_t smem = outer_smem_bytes(P, &S);
   if (smem == 0) return cudaErrorInvalidValue;

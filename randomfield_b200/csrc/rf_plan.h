@@ -100,6 +100,7 @@ struct Plan {
   int64_t oKstepBytes;        // bytes of one K-step block of B: 16 x (2 lPad oRc) x 2
   int64_t oChunkBytes;        // bytes of one chunk of B, lo blocks included
   uint32_t aLoMask[8];        // K-steps whose A tile carries the lo term (up to 256)
+  uint32_t oStageEnd[8];      // K-steps that close a ring stage (outer_stage_layout)
   // GEN_TABLE, BF16 single requests: the trig tile also carries its lo term
   // (the stage's A columns twice, one more MMA per K-step)
   int32_t tableALo;
@@ -153,12 +154,34 @@ __host__ __device__ inline int64_t mask_rank(const uint32_t* m, int64_t j) {
   if (j & 31) c += popcount32(m[j >> 5] & ((1u << (j & 31)) - 1u));
   return c;
 }
+// K-step j of a GEN_OUTER chunk holds the 8 outer groups (i1 = 8 jj ..
+// 8 jj + 7, i2, s2) with j = i2 + n2 (s2 + 2 jj): the axis-1 block jj is the
+// slowest index, so that a generator needs the 8 axis-1 phasors of one block
+// at a time, and the K-steps that keep lo terms (small k1 and k2) come in
+// runs.
+__host__ __device__ inline int64_t outer_kstep(const Plan& P, int32_t jj, int32_t i2, int32_t s2) {
+  return (int64_t)i2 + (int64_t)P.kNStep[1] * (s2 + 2 * (int64_t)jj);
+}
+__host__ __device__ inline void outer_kstep_groups(const Plan& P, int64_t j, int32_t* jj, int32_t* i2, int32_t* s2) {
+  const int64_t n2 = P.kNStep[1];
+  *i2 = (int32_t)(j % n2);
+  *s2 = (int32_t)((j / n2) % 2);
+  *jj = (int32_t)(j / (2 * n2));
+}
 // GEN_OUTER: byte offset of K-step j's hi block inside a chunk of B.
 __host__ __device__ inline int64_t outer_kstep_offset(const Plan& P, int64_t j) {
   return (j + (P.loSkip ? mask_rank(P.loMask, j) : 0)) * P.oKstepBytes;
 }
 __host__ __device__ inline bool outer_b_lo(const Plan& P, int64_t j) { return P.loSkip && mask_bit(P.loMask, j); }
 __host__ __device__ inline bool outer_a_lo(const Plan& P, int64_t j) { return mask_bit(P.aLoMask, j); }
+// GEN_OUTER ring stages (rf_outer.cu): a stage holds kOuterStageUnits A
+// units (one unit: both tiles' hi K-step; a K-step with an A lo term takes
+// two) and as many B units (one K-step block of B; two with its lo block).
+// The K-steps of a chunk fill stages in order, a stage closing before the
+// K-step that would overflow either side: four K-steps without lo terms, or
+// two with both, per stage.
+constexpr int kOuterStageUnits = 4;
+__host__ __device__ inline bool outer_stage_end(const Plan& P, int64_t j) { return mask_bit(P.oStageEnd, j); }
 
 // Bytes of the contraction operand of a plan (one realization block).
 __host__ __device__ inline int64_t operand_bytes(const Plan& P) {

@@ -354,7 +354,7 @@ __device__ __forceinline__ void outer_element(const Plan& P, const JumpTable& jt
   if (SINK) return;
   // K-step j of the chunk, element k = 2 (i1 % 8) + e; column n = rl 2 lPad + 2 i3 + cs
   const int32_t c = rc / P.oRc, rl = rc % P.oRc;
-  const int64_t j = (int64_t)(i1 >> 3) + (int64_t)(P.n1p >> 3) * (i2 + (int64_t)n2 * s2);
+  const int64_t j = outer_kstep(P, i1 >> 3, i2, s2);
   unsigned char* blk = B + (int64_t)c * P.oChunkBytes + outer_kstep_offset(P, j);
   const int32_t nRows = 2 * P.lPad * P.oRc;
   const bool lo = outer_b_lo(P, j);

@@ -177,16 +177,16 @@ def test_outer_group_bf16_error_budget():
                 W[gg, 0, :, 0], W[gg, 1, :, 0] = bcP + bcM, bsP + bsM
                 W[gg, 0, :, 1], W[gg, 1, :, 1] = bsP - bsM, bcM - bcP
     W = W.reshape(2 * G, 2 * n3 * Nmc)
-    # K-step j = jj + 3 (i2 + n2 s2) holds the groups i1 = 8 jj .. 8 jj + 7
+    # K-step j = i2 + n2 (s2 + 2 jj) holds the groups i1 = 8 jj .. 8 jj + 7 (rf_plan.h outer_kstep)
     pi_ref = 3.1415926535898
-    w = np.array([np.exp(-(kd[0] * np.arange(8 * (j % 3), 8 * (j % 3) + 8)) ** 2 / (4 * pi_ref)).sum()
-                  * np.exp(-(kd[1] * ((j // 3) % n2)) ** 2 / (4 * pi_ref)) for j in range(3 * n2 * 2)])
+    w = np.array([np.exp(-(kd[0] * np.arange(8 * (j // (2 * n2)), 8 * (j // (2 * n2)) + 8)) ** 2 / (4 * pi_ref)).sum()
+                  * np.exp(-(kd[1] * (j % n2)) ** 2 / (4 * pi_ref)) for j in range(3 * n2 * 2)])
     lo = np.zeros(w.size, bool)
     cov = 0.0
     for j in sorted(range(w.size), key=lambda j: (-w[j], j)):
         lo[j] = cov < 0.7 * w.sum()
         cov += w[j]
-    g_lo = np.array([lo[i1 // 8 + 3 * (i2 + n2 * s2)] for s2 in range(2) for i2 in range(n2) for i1 in range(n1)])
+    g_lo = np.array([lo[i2 + n2 * (s2 + 2 * (i1 // 8))] for s2 in range(2) for i2 in range(n2) for i1 in range(n1)])
     k_lo = np.repeat(g_lo, 2)
     rs = np.random.RandomState(3)
     J1, J2 = rs.randint(0, N, 96), rs.randint(0, N, 96)
