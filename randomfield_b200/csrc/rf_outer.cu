@@ -392,19 +392,34 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
       }
       const float2 e2step = axis_phasor(P.kDelta[1], 1, x1);
       const int32_t oNR = P.oNR;
-      const double kd0 = P.kDelta[0];
+      // E1(u) of block 0 and the block step E1(8), from FP64-reduced phases
+      // once per work item; block jj follows from block jj-1 by one complex
+      // product per phasor (the direct FP64 reduction and sincos of 8
+      // phasors per block and chunk took 13 % of the kernel's time)
+      float2 e1base[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) e1base[u] = axis_phasor(P.kDelta[0], u, x0);
+      const float2 e1step = axis_phasor(P.kDelta[0], 8, x0);
       for (int32_t c = 0; c < oNR && ok; ++c) {
         // K-steps in order j = 0, 1, ... (i2 fastest, then s2, then jj);
         // the A lo and stage-end flags read 32 at a time
         int32_t j = 0;
         uint32_t aw = 0, ew = 0;
+        float2 e1cur[8];
         for (int32_t jj = 0; jj < nJJ && ok; ++jj) {
-          // the block's 8 axis-1 phasors E1(8 jj + u), from FP64-reduced
-          // phases (8 per block and chunk against 2 n2 K-steps)
+          // the block's 8 axis-1 phasors E1(8 jj + u), zero past n1
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            if (jj > 0) {
+              const float2 q = e1cur[u];
+              e1cur[u] = make_float2(q.x * e1step.x - q.y * e1step.y, q.x * e1step.y + q.y * e1step.x);
+            } else {
+              e1cur[u] = e1base[u];
+            }
+          }
           float2 e1[8];
 #pragma unroll
-          for (int u = 0; u < 8; ++u)
-            e1[u] = (8 * jj + u < n1) ? axis_phasor(kd0, 8 * jj + u, x0) : make_float2(0.f, 0.f);
+          for (int u = 0; u < 8; ++u) e1[u] = (8 * jj + u < n1) ? e1cur[u] : make_float2(0.f, 0.f);
           for (int32_t s2 = 0; s2 < 2 && ok; ++s2) {
             float2 e2 = make_float2(1.f, 0.f);  // E2(i2), walked by angle addition
             for (int32_t i2 = 0; i2 < n2; ++i2) {
