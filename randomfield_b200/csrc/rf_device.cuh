@@ -300,16 +300,6 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<uint32_t*>(&v);
 }
-// The same pair packed on the integer pipes: each value rounded to BF16 by
-// adding half a unit of its 16th bit to its bit pattern (round half away from
-// zero, which differs from round-to-nearest-even only at exact ties), then
-// the two high halves joined by one byte permute.  For finite inputs.  The
-// table generator's SFU-bound loop uses it: the conversion instruction of
-// pack_bf16x2 issues to the same pipe as the MUFU sin and cos.
-__device__ __forceinline__ uint32_t pack_bf16x2_int(float lo, float hi) {
-  const uint32_t a = __float_as_uint(lo) + 0x8000u, b = __float_as_uint(hi) + 0x8000u;
-  return __byte_perm(a, b, 0x7632);
-}
 // Four e4m3 values (round to nearest, saturating) in K order: byte 0 = c0,
 // byte 1 = s0, byte 2 = c1, byte 3 = s1.
 __device__ __forceinline__ uint32_t pack_e4m3x4(float c0, float s0, float c1, float s1) {

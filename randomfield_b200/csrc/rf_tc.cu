@@ -195,8 +195,13 @@ __device__ __forceinline__ bool issue_stage(bool leader, uint32_t tbase, uint32_
 
 // The pipeline of one CTA over the work items of `w`.
 // GEN: GEN_TABLE, GEN_GRID3 (axis-3 length padded to LPAD) or GEN_MIXED
-// (chosen per tile; its GEN_GRID3 tiles have lPad == LPAD).
-template <int GEN, int PREC, int LPAD, class Work>
+// (chosen per tile; its GEN_GRID3 tiles have lPad == LPAD).  TALO: a
+// GEN_TABLE BF16 kernel whose plans carry the trig tile's lo term
+// (tableALo); single-request kernels compile it apart, because the residual
+// code in the generator loop cost the other GEN_TABLE requests 2.5 % even
+// when skipped (the grouped kernel keeps it: its small table requests take
+// the lo term).
+template <int GEN, int PREC, int LPAD, bool TALO, class Work>
 __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint32_t* err) {
   constexpr bool kHasGrid = GEN != GEN_TABLE;
   constexpr bool kHasTable = GEN != GEN_GRID3;
@@ -346,7 +351,7 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
                                                phn, &bars->empty[s]);
         else
           ready = issue_stage<kTabSteps, kF8>(leader, tbase, aBase, d0, jStep, idesc, acc0, more, &bars->full[sn],
-                                              phn, &bars->empty[s], P.tableALo ? (uint32_t)P.chunkK : 0u);
+                                              phn, &bars->empty[s], (TALO && P.tableALo) ? (uint32_t)P.chunkK : 0u);
         s = sn;
         ph = phn;
       }
@@ -457,8 +462,8 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
           constexpr int T = kTableChunk / kParts;  // pairs of this thread
           constexpr int NW = kF8 ? T / 2 : T;
           uint32_t words[NW];
-          uint32_t lows[PREC == PREC_BF16 ? NW : 1];  // the BF16 residuals (tableALo)
-          const bool aLo = PREC == PREC_BF16 && P.tableALo;
+          uint32_t lows[(TALO && PREC == PREC_BF16) ? NW : 1];  // the BF16 residuals (tableALo)
+          const bool aLo = TALO && PREC == PREC_BF16 && P.tableALo;
           float pc0 = 0.f, ps0 = 0.f;
           auto emit = [&](int idx, float c, float sn) {
             if (kF8) {
@@ -469,11 +474,10 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
                 words[idx >> 1] = pack_e4m3x4(pc0, ps0, c, sn);
               }
             } else {
-              // BF16 packed on the integer pipes: the SFU pipe is this loop's bound
-              words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2_int(c, sn);
+              words[idx] = (PREC == PREC_FP16) ? pack_f16x2(c, sn) : pack_bf16x2(c, sn);
               if (PREC == PREC_BF16 && aLo) {
                 const uint32_t w = words[idx];
-                lows[idx] = pack_bf16x2_int(c - __uint_as_float(w << 16), sn - __uint_as_float(w & 0xffff0000u));
+                lows[idx] = pack_bf16x2(c - __uint_as_float(w << 16), sn - __uint_as_float(w & 0xffff0000u));
               }
             }
           };
@@ -540,21 +544,21 @@ __device__ __forceinline__ void tc_body(const Work& w, const SlotLayout& L, uint
 }
 
 // LPAD: GEN_GRID3 axis-3 length padded to 8/16/24/32 (0 for GEN_TABLE).
-template <int GEN, int PREC, int LPAD>
+template <int GEN, int PREC, int LPAD, bool TALO>
 __global__ void __launch_bounds__(Roles<GEN>::kThreads, 1) rf_tc_kernel(const __grid_constant__ TcArgs a) {
   const SingleWork w{&a, (a.rows + kTileM - 1) / kTileM};
-  tc_body<GEN, PREC, LPAD>(w, a.L, a.err);
+  tc_body<GEN, PREC, LPAD, TALO>(w, a.L, a.err);
 }
 
 template <int PREC>
 __global__ void __launch_bounds__(Roles<GEN_MIXED>::kThreads, 1) rf_group_kernel(const __grid_constant__ GroupArgs g) {
   const GroupWork w{&g, g.ctaStart[blockIdx.x], g.ctaStart[blockIdx.x + 1]};
-  tc_body<GEN_MIXED, PREC, kGroupLPad>(w, g.L, g.err);
+  tc_body<GEN_MIXED, PREC, kGroupLPad, true>(w, g.L, g.err);
 }
 
-template <int GEN, int PREC, int LPAD>
+template <int GEN, int PREC, int LPAD, bool TALO = false>
 cudaError_t launch_one(const TcArgs& args, size_t smem, int grid, cudaStream_t st) {
-  auto fn = rf_tc_kernel<GEN, PREC, LPAD>;
+  auto fn = rf_tc_kernel<GEN, PREC, LPAD, TALO>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   fn<<<grid, Roles<GEN>::kThreads, smem, st>>>(args);
@@ -563,7 +567,12 @@ cudaError_t launch_one(const TcArgs& args, size_t smem, int grid, cudaStream_t s
 
 template <int PREC>
 cudaError_t launch_prec(const Plan& P, const TcArgs& args, size_t smem, int grid, cudaStream_t st) {
-  if (P.gen != GEN_GRID3) return launch_one<GEN_TABLE, PREC, 0>(args, smem, grid, st);
+  if (P.gen != GEN_GRID3) {
+    if constexpr (PREC == PREC_BF16) {
+      if (P.tableALo) return launch_one<GEN_TABLE, PREC, 0, true>(args, smem, grid, st);
+    }
+    return launch_one<GEN_TABLE, PREC, 0>(args, smem, grid, st);
+  }
   switch (P.lPad) {
     case 8: return launch_one<GEN_GRID3, PREC, 8>(args, smem, grid, st);
     case 16: return launch_one<GEN_GRID3, PREC, 16>(args, smem, grid, st);
