@@ -554,6 +554,20 @@ void outer_layout(Plan& P) {
     ub += b;
   }
   P.oStageEnd[(nK - 1) >> 5] |= 1u << ((nK - 1) & 31);
+  // the draw of wavevector (s3 = -) lies n1 n2 n3 calls after that of (s3 = +)
+  {
+    const JumpTable& jt = jump_table();
+    const uint64_t d = (uint64_t)n1 * (uint64_t)n2 * (uint64_t)P.kNStep[2];
+    unsigned __int128 m1 = 1, m2 = 1;
+    for (int j = 0; j < 64; ++j) {
+      if ((d >> j) & 1u) {
+        m1 = (m1 * (unsigned __int128)jt.p1[j]) % (unsigned __int128)kM1;
+        m2 = (m2 * (unsigned __int128)jt.p2[j]) % (unsigned __int128)kM2;
+      }
+    }
+    P.oStepM1 = (int64_t)m1;
+    P.oStepM2 = (int64_t)m2;
+  }
   // FP16: B holds sums of two amplitudes (|W| <= 2), scaled so that the
   // largest sits near 2^15
   if (P.prec == PREC_FP16) {

@@ -11,7 +11,7 @@
 //   Y (points x (r, i3, cos|sin)) = A (points x 2G) B (2G x N),
 //
 // with A = (Re P_g, Im P_g) generated on chip and B built from the phases
-// (rf_tables.cu, outer_element).  Against the plain contraction
+// (rf_tables.cu, outer_run).  Against the plain contraction
 // [cos Kx | sin Kx] x [a cos phi; -a sin phi] this is the same number of
 // multiply-adds and the same operand bytes, but the generated operand shrinks
 // from 2K = 8 n1 n2 n3 to 2G = 4 n1 n2 values per point and chunk, the MMAs

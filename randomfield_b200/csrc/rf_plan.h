@@ -101,6 +101,7 @@ struct Plan {
   int64_t oChunkBytes;        // bytes of one chunk of B, lo blocks included
   uint32_t aLoMask[8];        // K-steps whose A tile carries the lo term (up to 256)
   uint32_t oStageEnd[8];      // K-steps that close a ring stage (outer_stage_layout)
+  int64_t oStepM1, oStepM2;   // rnglib multipliers a^(n1 n2 n3) mod m: the s3 = - draw from the s3 = + one
   // GEN_TABLE, BF16 single requests: the trig tile also carries its lo term
   // (the stage's A columns twice, one more MMA per K-step)
   int32_t tableALo;

@@ -315,86 +315,147 @@ __device__ __forceinline__ int32_t table_run_length(const Plan& P, int64_t j) {
 // plain operand's pair (a cos phi, -a sin phi) = (bc, bs):
 //   W(re, cos) = bc+ + bc-,  W(im, cos) = bs+ + bs-,
 //   W(re, sin) = bs+ - bs-,  W(im, sin) = bc- - bc+.
+// W of group (i1, i2, s2), axis-3 index i3 and realization column rc (zero
+// in the padding); with SINK the draws are recorded instead.  The amplitude
+// sqrt(S(k)) is the FP64 product of the per-axis factors exp(-k_d^2 / 8 pi)
+// (a23: axes 2 and 3, fixed per run), the draws are rnglib's to the bit (the
+// s3 = - draw from the s3 = + one by the plan's multiplier, one modular
+// product per stream), and cos, sin of the phase 2 pi U are FP32 (sincospi
+// of 2U; the operand is stored as 16-bit hi/lo pairs, about 16 bits).
 template <bool SINK>
-__device__ __forceinline__ void outer_element(const Plan& P, const JumpTable& jt, unsigned char* __restrict__ B,
-                                              int32_t i1, int32_t i2, int32_t s2, int32_t i3, int32_t rc,
-                                              RunCursors& cu, const DrawSink& sink) {
+__device__ __forceinline__ void outer_w(const Plan& P, const JumpTable& jt, int32_t i1, int32_t i2, int32_t s2,
+                                        int32_t i3, int32_t rc, double a23, RunCursors& cu, const DrawSink& sink,
+                                        float W[4]) {
   const int32_t n1 = P.kNStep[0], n2 = P.kNStep[1], n3 = P.kNStep[2];
-  double W[4] = {0.0, 0.0, 0.0, 0.0};  // (re, cos), (im, cos), (re, sin), (im, sin)
+  W[0] = W[1] = W[2] = W[3] = 0.f;  // (re, cos), (im, cos), (re, sin), (im, sin)
   if (i1 < n1 && i3 < n3 && rc < P.nmcBlk) {
     const int64_t n123 = (int64_t)n1 * n2 * n3;
     const int64_t refP = (int64_t)(2 * s2) * n123 + i1 + (int64_t)n1 * (i2 + (int64_t)n2 * i3);
     const int64_t refM = refP + n123;
     const int64_t rg = (int64_t)P.rOff + rc;
-    double k[3];
-    k[0] = 0.0 + P.kDelta[0] * (double)i1;
-    k[1] = (0.0 + P.kDelta[1] * (double)i2) * (s2 ? -1.0 : 1.0);
-    k[2] = 0.0 + P.kDelta[2] * (double)i3;
     double aP, aM;
     if (P.corrMod == 1) {
-      aP = aM = sqrt(gauss_spectrum(k, 3));  // S(k) is even in k3
+      const double k1 = 0.0 + P.kDelta[0] * (double)i1;
+      aP = aM = a23 * exp(-(k1 * k1) / (8.0 * kRefPi));  // S(k) is even in k3
     } else {
       aP = (refP == 5) ? 1.0 : 0.0;  // cm_COS, spectra_RF.f90:210-220
       aM = (refM == 5) ? 1.0 : 0.0;
     }
-    const double phP = 2.0 * kRefPi * draw_r8(P, jt, P.ig1, P.ig2, cu.rA, (uint64_t)(rg * P.K + refP + 1));
-    const double phM = 2.0 * kRefPi * draw_r8(P, jt, P.ig1, P.ig2, cu.rB, (uint64_t)(rg * P.K + refM + 1));
+    double uP, uM;
+    if (P.dDraws) {
+      uP = draw_r8(P, jt, P.ig1, P.ig2, cu.rA, (uint64_t)(rg * P.K + refP + 1));
+      uM = draw_r8(P, jt, P.ig1, P.ig2, cu.rB, (uint64_t)(rg * P.K + refM + 1));
+    } else {
+      uP = draw_r8(P, jt, P.ig1, P.ig2, cu.rA, (uint64_t)(rg * P.K + refP + 1));
+      cu.rB.c1 = mulmod(P.oStepM1, cu.rA.c1, kM1);
+      cu.rB.c2 = mulmod(P.oStepM2, cu.rA.c2, kM2);
+      cu.rB.pos = cu.rA.pos + (uint64_t)n123;
+      cu.rB.last = uni_value(cu.rB.c1, cu.rB.c2);
+      uM = (double)cu.rB.last * kR8Scale;
+    }
     if (SINK) {
       sink.rk[rg * P.K + refP] = cu.rA.last;
       sink.rk[rg * P.K + refM] = cu.rB.last;
       return;
     }
-    const double bcP = aP * cos(phP), bsP = -aP * sin(phP);
-    const double bcM = aM * cos(phM), bsM = -aM * sin(phM);
-    W[0] = bcP + bcM;
-    W[1] = bsP + bsM;
-    W[2] = bsP - bsM;
-    W[3] = bcM - bcP;
+    float sP, cP, sM, cM;
+    sincospif((float)(2.0 * uP), &sP, &cP);
+    sincospif((float)(2.0 * uM), &sM, &cM);
+    const float fP = (float)aP, fM = (float)aM;
+    // bc = a cos phi, bs = -a sin phi
+    W[0] = fP * cP + fM * cM;
+    W[1] = -(fP * sP + fM * sM);
+    W[2] = fM * sM - fP * sP;
+    W[3] = fM * cM - fP * cP;
   }
-  if (SINK) return;
-  // K-step j of the chunk, element k = 2 (i1 % 8) + e; column n = rl 2 lPad + 2 i3 + cs
+}
+
+// Two 16-bit values of the operand in one word (a: low half): BF16, or
+// FP16 scaled by 2^bScaleLog2; *res gets the BF16 rounding residuals.
+__device__ __forceinline__ uint32_t outer_pack(const Plan& P, float a, float b, uint32_t* res) {
+  if (P.prec == PREC_FP16) {
+    const float sc = ldexpf(1.f, P.bScaleLog2);
+    *res = 0u;
+    return pack_f16x2(a * sc, b * sc);
+  }
+  const uint32_t h = pack_bf16x2(a, b);
+  *res = pack_bf16x2(a - __uint_as_float(h << 16), b - __uint_as_float(h & 0xffff0000u));
+  return h;
+}
+
+// One run of the GEN_OUTER operand: group (i2, s2), axis-3 index i3 and
+// realization column rc over i1 = 0 .. n1p-1.  For the outer group g = (i1,
+// i2, s2) the two wavevectors s3 = +/- give C+- = a+- e^{i phi+-}; with P =
+// C+ + C-, Q = C+ - C- the field's term is
+//   Re[E1 E2^{s2} (P cos(k3 x3) + i Q sin(k3 x3))]
+//     = pr c3 Re P - pi c3 Im P - pr s3 Im Q - pi s3 Re Q
+// (pr, pi: the outer phasor, the A operand; c3, s3: the epilogue's factors),
+// so B row (g, re) holds (Re P, -Im Q) and row (g, im) holds (-Im P, -Re Q)
+// in the (i3, cos) and (i3, sin) columns of realization r.  In terms of the
+// plain operand's pair (a cos phi, -a sin phi) = (bc, bs):
+//   W(re, cos) = bc+ + bc-,  W(im, cos) = bs+ + bs-,
+//   W(re, sin) = bs+ - bs-,  W(im, sin) = bc- - bc+.
+// K-step j = outer_kstep(i1 / 8, i2, s2) holds element k = 2 (i1 % 8) + e
+// of rows n = rl 2 lPad + 2 i3 + cs (cs = 0 cos, 1 sin): the run owns two
+// rows of every K-step block, and each four consecutive i1 fill one 16-byte
+// core-matrix row of each, stored whole (neighbouring threads hold the
+// neighbouring rows, so a warp's stores fill whole lines).
+template <bool SINK>
+__device__ __forceinline__ void outer_run(const Plan& P, const JumpTable& jt, unsigned char* __restrict__ B,
+                                          int32_t i2, int32_t s2, int32_t i3, int32_t rc, RunCursors& cu,
+                                          const DrawSink& sink) {
   const int32_t c = rc / P.oRc, rl = rc % P.oRc;
-  const int64_t j = outer_kstep(P, i1 >> 3, i2, s2);
-  unsigned char* blk = B + (int64_t)c * P.oChunkBytes + outer_kstep_offset(P, j);
   const int32_t nRows = 2 * P.lPad * P.oRc;
-  const bool lo = outer_b_lo(P, j);
-  if (!RF_IN_BOUNDS((int64_t)c * P.oChunkBytes + outer_kstep_offset(P, j) + (lo ? 2 : 1) * P.oKstepBytes - 1,
-                    operand_bytes(P), P.dbgErr))
-    return;
+  const int32_t row0 = rl * 2 * P.lPad + 2 * i3;  // cs = 0; cs = 1 is the next row
+  const double k2 = 0.0 + P.kDelta[1] * (double)i2, k3 = 0.0 + P.kDelta[2] * (double)i3;
+  const double a23 = exp(-(k2 * k2) / (8.0 * kRefPi)) * exp(-(k3 * k3) / (8.0 * kRefPi));
+  for (int32_t i0 = 0; i0 < P.n1p; i0 += 4) {  // n1p is a multiple of 8
+    uint32_t hi[2][4], lo[2][4];
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int32_t e = q & 1, cs = q >> 1;
-    const int32_t kel = 2 * (i1 & 7) + e, row = rl * 2 * P.lPad + 2 * i3 + cs;
-    const int64_t off = tc_b_offset(nRows, row, kel);
-    if (P.prec == PREC_FP16) {
-      *reinterpret_cast<__half*>(blk + off) = __double2half(W[q] * ldexp(1.0, P.bScaleLog2));
-    } else {
-      const __nv_bfloat16 h = __double2bfloat16(W[q]);
-      *reinterpret_cast<__nv_bfloat16*>(blk + off) = h;
-      if (lo) *reinterpret_cast<__nv_bfloat16*>(blk + P.oKstepBytes + off) = __double2bfloat16(W[q] - (double)__bfloat162float(h));
+    for (int u = 0; u < 4; ++u) {
+      float W[4];
+      outer_w<SINK>(P, jt, i0 + u, i2, s2, i3, rc, a23, cu, sink, W);
+#pragma unroll
+      for (int cs = 0; cs < 2; ++cs) hi[cs][u] = outer_pack(P, W[2 * cs], W[2 * cs + 1], &lo[cs][u]);
+    }
+    if (SINK) continue;
+    const int32_t i1 = i0 + 3;
+    const int64_t j = outer_kstep(P, i1 >> 3, i2, s2);
+    const int64_t base = (int64_t)c * P.oChunkBytes + outer_kstep_offset(P, j);
+    const bool blo = outer_b_lo(P, j);
+    if (!RF_IN_BOUNDS(base + (blo ? 2 : 1) * P.oKstepBytes - 1, operand_bytes(P), P.dbgErr)) continue;
+    const int64_t half = (int64_t)((i1 >> 2) & 1) * (nRows * 16);  // K half of the block
+#pragma unroll
+    for (int cs = 0; cs < 2; ++cs) {
+      const int32_t row = row0 + cs;
+      unsigned char* dst = B + base + half + (row >> 3) * 128 + (row & 7) * 16;
+      *reinterpret_cast<uint4*>(dst) = make_uint4(hi[cs][0], hi[cs][1], hi[cs][2], hi[cs][3]);
+      if (blo) *reinterpret_cast<uint4*>(dst + P.oKstepBytes) = make_uint4(lo[cs][0], lo[cs][1], lo[cs][2], lo[cs][3]);
     }
   }
 }
 
-// Thread t = j * cols + r: run j for realization column r.
+// Thread t = j * cols + r: run j for realization column r (GEN_OUTER:
+// t = r * runs + j, so that neighbouring threads fill neighbouring rows).
 template <bool SINK = false>
 __device__ __forceinline__ void table_run(const Plan& P, const JumpTable& jt, void* __restrict__ B,
                                          double* __restrict__ ktab, int64_t literalSlab, int64_t nSlab, int64_t t,
                                          const DrawSink& sink = DrawSink{nullptr, nullptr}) {
   const int32_t cols = table_cols(P);
-  const int64_t j = t / cols;
-  const int r = (int)(t % cols);
-  if (j >= table_runs(P)) return;
+  const int64_t runs = table_runs(P);
+  const bool outer = P.gen == GEN_OUTER;
+  const int64_t j = outer ? t % runs : t / cols;
+  const int r = (int)(outer ? t / runs : t % cols);
+  if (j >= runs || r >= cols) return;
   RunCursors cu;
   cu.kA.pos = cu.kB.pos = cu.rA.pos = cu.rB.pos = 0;
   cu.kA.last = cu.kB.last = cu.rA.last = cu.rB.last = 0;
-  if (P.gen == GEN_OUTER) {
+  if (outer) {
     // run j = i3 + lPad (i2 + n2 s2): i1 = 0 .. n1p-1, consecutive draws per sign s3
     const int32_t i3 = (int32_t)(j % P.lPad);
     const int64_t t2 = j / P.lPad;
     const int32_t i2 = (int32_t)(t2 % P.kNStep[1]), s2 = (int32_t)(t2 / P.kNStep[1]);
-    for (int32_t i1 = 0; i1 < P.n1p; ++i1)
-      outer_element<SINK>(P, jt, reinterpret_cast<unsigned char*>(B), i1, i2, s2, i3, r, cu, sink);
+    outer_run<SINK>(P, jt, reinterpret_cast<unsigned char*>(B), i2, s2, i3, r, cu, sink);
     return;
   }
   const int32_t len = table_run_length(P, j);
