@@ -711,6 +711,42 @@ def run_iso_case(args):
     ctx.close()
 
 
+def run_batch_case(args):
+    """--case batch: a batch of --batch-requests requests of the batched mix
+    with point counts capped at --batch-max-points (the operand tables are as
+    large as in the full mix, the device footprint small), run through the
+    grouped launch --warmup + --steps times; one JSON line with the grouped
+    launch's phase times.  For profiler captures of the grouped kernels."""
+    import torch
+    import randomfield_b200 as rf
+
+    rs = np.random.RandomState(2024)
+    ctx = rf.Context(0)
+    keep, reqs = [], []
+    for i in range(args.batch_requests):
+        m = draw_request(rs)
+        pts = m["points"][: args.batch_max_points]
+        dx = torch.from_numpy(np.ascontiguousarray(pts)).cuda()
+        dout = torch.empty((m["Nmc"], pts.shape[0]), dtype=torch.float64, device="cuda")
+        keep.append((dx, dout))
+        reqs.append(rf.make_request(dx, "gaussian", m["marg"], m["corrL"], m["avg"], m["var"], m["Nmc"], m["method"],
+                                    dout, precision=args.precision, seed_start=i, nDim=3, n=pts.shape[0],
+                                    **m["opts"]))
+    tab, con = [], []
+    for it in range(args.warmup + args.steps):
+        ctx.generate_batch_device(reqs)
+        torch.cuda.synchronize()
+        st = ctx.batch_stats()
+        if it >= args.warmup:
+            tab.append(st["tables_ms"])
+            con.append(st["contract_ms"])
+    print(json.dumps({"case": "batch", "workload": f"{args.batch_requests} requests of the batched mix, points capped "
+                      f"at {args.batch_max_points}", "precision": args.precision, "units": st["units"],
+                      "tables_ms": float(np.mean(tab)), "contract_ms": float(np.mean(con)), "steps": args.steps,
+                      "warmup": args.warmup}))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -730,10 +766,13 @@ def main():
                     help="duration of the Poisson arrival stream (the serving config: 60 s)")
     ap.add_argument("--serve-sat-rate", type=float, default=600.0,
                     help="arrival rate (requests/s) of the saturated serving run")
-    ap.add_argument("--case", default="headline", choices=["headline", "iso", "grid"],
+    ap.add_argument("--case", default="headline", choices=["headline", "iso", "grid", "batch"],
                     help="iso: only the isotropic request of config 2 (GEN_TABLE), on --points points; grid: only "
-                         "the structured-grid path (rf_generate_grid) on --grid; both for profiler captures of "
-                         "those kernels, each printing one JSON line of its own")
+                         "the structured-grid path (rf_generate_grid) on --grid; batch: a small batch of the "
+                         "batched mix (--batch-requests, --batch-max-points); all for profiler captures of those "
+                         "kernels, each printing one JSON line of its own")
+    ap.add_argument("--batch-requests", type=int, default=24, help="requests of the --case batch batch")
+    ap.add_argument("--batch-max-points", type=int, default=5000, help="point cap of the --case batch requests")
     ap.add_argument("--points", type=int, default=200000, help="points of the --case iso request")
     ap.add_argument("--grid", default="128,128,128",
                     help="grid points per axis; a smaller grid (e.g. 32,32,18 = one wave of 144 tiles) "
@@ -753,6 +792,9 @@ def main():
         return
     if args.case == "grid":
         run_grid_case(args)
+        return
+    if args.case == "batch":
+        run_batch_case(args)
         return
 
     import torch
