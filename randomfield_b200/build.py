@@ -32,7 +32,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "--expt-relaxed-constexpr", "-I", os.path.join(HERE, "..", "include")]
-SOURCES = ["rf_tables.cu", "rf_tc.cu", "rf_outer.cu", "rf_fp32.cu", "rf_post.cu", "rf_host.cu", "rf_noalloc.cu", "rf_batch.cu", "rf_serve.cu", "rf_selftest.cu", "rf_stats.cu", "rf_fft.cu", "rf_grid.cu", "rf_writer.cu"]
+SOURCES = ["rf_tables.cu", "rf_tc.cu", "rf_outer.cu", "rf_outer_pair.cu", "rf_fp32.cu", "rf_post.cu", "rf_host.cu", "rf_noalloc.cu", "rf_batch.cu", "rf_serve.cu", "rf_selftest.cu", "rf_stats.cu", "rf_fft.cu", "rf_grid.cu", "rf_writer.cu"]
 
 
 def _deps(src: str) -> list[str]:

@@ -505,6 +505,7 @@ void outer_layout(Plan& P) {
   P.gen = GEN_OUTER;
   P.n1p = n1p;
   P.oNK = nK;
+  P.oPair = 0;
   P.oRc = std::min<int32_t>(P.nmcBlk, 256 / (2 * P.lPad));
   P.oNR = (P.nmcBlk + P.oRc - 1) / P.oRc;
   P.oKstepBytes = (int64_t)16 * (2 * P.lPad * P.oRc) * 2;
@@ -576,6 +577,23 @@ void outer_layout(Plan& P) {
   }
 }
 
+// The CTA-pair form of a GEN_OUTER plan (rf_outer_pair.cu) for single
+// requests of at least two 256-point items and two realizations: an MMA of
+// M = 256 (one 128-point tile per CTA) per N half, two halves of oRc
+// realizations per chunk, so that a chunk covers twice the realizations and
+// the generators build A for half as many chunks.  The last chunk's missing
+// realizations are zero columns of B (their MMAs run, their values are not
+// stored).
+void outer_pair_layout(Plan& P) {
+  if (P.gen != GEN_OUTER || P.nmcBlk < 2 || P.n < 2 * 2 * kTileM) return;
+  P.oPair = 1;
+  P.oRc = std::min<int32_t>((P.nmcBlk + 1) / 2, 256 / (2 * P.lPad));
+  P.oNR = (P.nmcBlk + 2 * P.oRc - 1) / (2 * P.oRc);
+  // per rank: the K-step block holds lPad oRc rows of each half
+  P.oKstepBytes = (int64_t)16 * (2 * P.lPad * P.oRc) * 2;
+  P.oChunkBytes = 2 * (int64_t)(P.oNK + mask_rank(P.loMask, P.oNK)) * P.oKstepBytes;
+}
+
 // Realizations per launch: one MMA holds at most 256 accumulator columns,
 // and the hi/lo form uses two per realization.
 int32_t realization_block(const Plan& P) {
@@ -601,6 +619,7 @@ int run_plan(rf_context* c, const Plan& P0, const double* dX, double* dOut, cuda
     if (int rc = layout(P)) return rc;
     lo_layout(P);
     outer_layout(P);
+    outer_pair_layout(P);
     table_alo_layout(P);
     P.dbgErr = c->dErr;
     if (int rc = run_block(c, P, dX, dOut, st)) return rc;
@@ -675,6 +694,7 @@ int run_plan_slabs(rf_context* c, const Plan& P0, double* dX, double* dOut, doub
   if (int rc = layout(P)) return rc;
   lo_layout(P);
   outer_layout(P);
+  outer_pair_layout(P);
   table_alo_layout(P);
   P.dbgErr = c->dErr;
   if (tc_smem_bytes(P, nullptr) == 0)
@@ -814,6 +834,7 @@ int host_block_layout(Plan* P, int32_t rOff, int32_t nmcBlk) {
   if (int rc = layout(*P)) return rc;
   lo_layout(*P);
   outer_layout(*P);
+  outer_pair_layout(*P);
   table_alo_layout(*P);
   return RF_OK;
 }

@@ -31,6 +31,11 @@ cudaError_t launch_tc(const Plan& P, const double* dX, const void* dB, const dou
 cudaError_t launch_outer(const Plan& P, const double* dX, const void* dB, double* dOut, int64_t row0, int64_t rows,
                          uint32_t* dErr, int numSMs, cudaStream_t st);
 size_t outer_smem_bytes(const Plan& P, int* stages);
+// The CTA-pair form (P.oPair, rf_outer_pair.cu): clusters of two CTAs, one
+// 256-point item per pair.
+cudaError_t launch_outer_pair(const Plan& P, const double* dX, const void* dB, double* dOut, int64_t row0,
+                              int64_t rows, uint32_t* dErr, int numSMs, cudaStream_t st);
+size_t outer_pair_smem_bytes(const Plan& P, int* stages);
 
 // Plain FP32 contraction (FFMA) + the same epilogue.
 cudaError_t launch_fp32(const Plan& P, const double* dX, const void* dB, const double* dKtab, double* dOut,

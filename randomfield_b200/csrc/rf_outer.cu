@@ -608,6 +608,7 @@ size_t outer_fit(int32_t slotBytes, int* stages, int maxStages = 0) {
 }  // namespace
 
 size_t outer_smem_bytes(const Plan& P, int* stages) {
+  if (P.oPair) return outer_pair_smem_bytes(P, stages);
   return outer_fit(outer_stage_bytes(P.oKstepBytes), stages);
 }
 
@@ -636,6 +637,7 @@ cudaError_t launch_outer_group(int prec, const OuterGroupArgs& g, size_t smem, i
 
 cudaError_t launch_outer(const Plan& P, const double* dX, const void* dB, double* dOut, int64_t row0, int64_t rows,
                          uint32_t* dErr, int numSMs, cudaStream_t st) {
+  if (P.oPair) return launch_outer_pair(P, dX, dB, dOut, row0, rows, dErr, numSMs, st);
   OuterArgs a;
   a.P = P;
   a.x = dX;

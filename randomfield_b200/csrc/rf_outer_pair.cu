@@ -1,0 +1,660 @@
+// rf_outer_pair.cu -- the outer-group contraction (rf_outer.cu) on a CTA
+// pair: one tcgen05 MMA of M = 256 covers both CTAs' 128-point tiles.
+//
+// Replaces the hot loop of gen_Std_Gauss_Shinozuka (randomFieldND.f90:276-330)
+// for single 3-D requests whose wavevectors form the set_kPoints tensor grid
+// (spectra_RF.f90:87-133), with the factorisation of rf_outer.cu: f(x, r) =
+// ampMult sum_i3 [c3 Yc + s3 Ys], Y = A (points x 2G) B (2G x N), A the outer
+// phasors E1(i1) E2(i2)^{s2} generated on chip.
+//
+// A cluster of two CTAs works on a 256-point item, one 128-point tile per CTA.
+// An N chunk is two halves of oRc realizations (N = 2 lPad oRc <= 256 each);
+// the even CTA issues, per K-step and half, one tcgen05.mma.cta_group::2 of
+// M = 256: each CTA contributes its tile's A (its own shared memory) and half
+// of the half's B rows (lPad oRc rows each, the same shared-memory offset in
+// both), and each CTA's TMEM receives its tile's 128 x N accumulator.  Against
+// the one-CTA kernel a chunk covers twice the realizations at the same MMA
+// count per K-step, so the generators build A for half as many chunks, the
+// MMAs issued per flop halve, and a CTA's ring stage (one tile's A, half of
+// B) is 46 KB instead of 62: four stages instead of three.
+//
+// Warp roles (576 threads, in each CTA):
+//   warp 0      rank 0: MMA issuer (tcgen05.mma.cta_group::2, commits
+//               multicast to both CTAs); rank 1: forwards each completed
+//               stage of its own ring to rank 0's stage barrier (one
+//               cluster-scope arrive), so that rank 0's barrier completes
+//               when both CTAs' stages are full;
+//   warp 1      producer (one thread): 1-D bulk copy (TMA, no multicast) of
+//               the CTA's part of a stage's B blocks from HBM/L2;
+//   warps 2-9   generators: two threads per point, each 4 of the K-step's
+//               8 outer phasors (one 16-byte K half), the lo residual where
+//               the plan keeps it;
+//   warps 10-17 epilogue: tcgen05.ld of one N half's accumulator (warp % 4
+//               picks the TMEM lane quarter), the i3 sum, ampMult, marginal
+//               map, FP64 stores; rank 1's release the accumulators to rank
+//               0's issuer with cluster-scope arrives.
+// Every wait is bounded (globaltimer); a final cluster barrier keeps each CTA
+// alive until its peer no longer addresses its shared memory.
+#include "rf_blend.cuh"
+#include "rf_device.cuh"
+#include "rf_gen.cuh"
+#include "rf_launch.h"
+
+namespace rfb {
+
+namespace {
+
+constexpr int kPIssuerWarp = 0, kPProducerWarp = 1, kPGenWarp0 = 2, kPGenWarps = 8;
+constexpr int kPEpiWarp0 = kPGenWarp0 + kPGenWarps, kPEpiWarps = 8;
+constexpr int kPThreads = (kPEpiWarp0 + kPEpiWarps) * 32;
+constexpr int kPMaxSlots = 8;
+constexpr int kPAUnitBytes = kTileM * 16 * 2;  // one tile's hi A of one K-step: 128 rows x 16 K x 16 bits
+constexpr int kPStageABytes = kOuterStageUnits * kPAUnitBytes;
+constexpr uint32_t kPTmemCols = 512;
+constexpr int kPAccCols = 256;  // accumulator columns per N half
+
+struct PairBars {
+  uint64_t full[kPMaxSlots];   // rank 0: 8 generators + producer + rank 1's forward; rank 1: 8 + producer
+  uint64_t empty[kPMaxSlots];  // the issuer's commit, multicast to both CTAs
+  uint64_t acc_full;           // the issuer's commit after a chunk, multicast
+  uint64_t acc_empty[2];       // rank 0: the 4 epilogue warps of a half in each CTA
+  uint64_t done;               // rank 0: the issuer's last commit
+  uint64_t dealloc_ok;         // rank 1: rank 0's MMAs have drained
+  uint32_t tmem_base;
+  int abort_flag;
+  int32_t nStages;
+  uint32_t stab[kOuterMaxKsteps];  // the issuer's stage table (rf_outer.cu's layout)
+};
+constexpr int kPHeader = 2048;
+static_assert(sizeof(PairBars) <= kPHeader, "header");
+
+struct OuterPairArgs {
+  Plan P;
+  const double* x;
+  const unsigned char* B;
+  double* out;
+  uint32_t* err;
+  int64_t row0, rows;
+  int32_t S;          // ring stages
+  int32_t slotBytes;  // one stage: A area (kPStageABytes), then kOuterStageUnits B units
+};
+
+// ------------------------------------------------------------ cluster helpers
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// The shared::cluster address of this CTA's shared-memory word `p` in CTA `rank`.
+__device__ __forceinline__ uint32_t map_to_rank(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+  return r;
+}
+// Arrive on an mbarrier of another CTA of the cluster, releasing this thread's
+// prior writes (and what it has acquired) at cluster scope.
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t clusterAddr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(clusterAddr) : "memory");
+}
+__device__ __forceinline__ bool mbar_test_wait_cluster(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity, uint32_t suspendNs) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(suspendNs)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait with cluster-scope acquire (barriers that remote arrivals
+// complete), the same limits as mbar_wait_for.
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                                  uint64_t limitNs = kWaitLimitNs) {
+  if (mbar_test_wait_cluster(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  const long long c0 = clock64();
+  const long long minCycles = (long long)(limitNs / 2);
+  while (true) {
+    if (mbar_try_wait_cluster(bar, parity, kWaitSuspendNs)) return true;
+    if (*abort) return false;
+    if (globaltimer_ns() - t0 > limitNs && clock64() - c0 > minCycles) return false;
+  }
+}
+__device__ __forceinline__ bool mbar_wait_cluster_warp(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  bool ok = true;
+  if ((threadIdx.x & 31) == 0) ok = mbar_wait_cluster(bar, parity, abort);
+  return __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t* dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish_pair() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc_pair(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// D (both CTAs' TMEM) (+)= A (256 rows: 128 from each CTA) x B (N rows: N/2
+// from each CTA), kind::f16, FP32 accumulate; issued by one thread of rank 0.
+__device__ __forceinline__ void mma_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void mma_pair_if(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            uint32_t accumulate, uint32_t issue) {
+  asm volatile(
+      "{\n\t.reg .pred p, g;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "setp.ne.b32 g, %5, 0;\n\t"
+      "@g tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(issue)
+      : "memory");
+}
+// Arrive once on `bar` in both CTAs (the same offset) when the issuing
+// thread's prior tcgen05 operations have completed.
+__device__ __forceinline__ void mma_commit_pair_both(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "h"((uint16_t)3)
+      : "memory");
+}
+// The same, on this CTA's barrier only.
+__device__ __forceinline__ void mma_commit_pair_local(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void pair_abort(PairBars* bars, uint32_t* err) {
+  *reinterpret_cast<volatile int*>(&bars->abort_flag) = 1;
+  atomicOr(err, kErrTimeout);
+}
+
+// Stages per chunk of a plan (the stage-end marks; the last K-step closes one).
+__device__ __forceinline__ int32_t pair_stage_count(const Plan& P) {
+  int32_t ns = 0;
+  for (int32_t j = 0; j < P.oNK; ++j) ns += (outer_stage_end(P, j) || j + 1 == P.oNK) ? 1 : 0;
+  return ns;
+}
+
+template <int PREC, int LPAD>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+    rf_outer_pair_kernel(const __grid_constant__ OuterPairArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  PairBars* bars = reinterpret_cast<PairBars*>(smem);
+  unsigned char* slots = smem + kPHeader;
+  volatile int* abort_flag = &bars->abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const int S = a.S;
+  const int32_t slotBytes = a.slotBytes;
+  uint32_t* err = a.err;
+  const Plan& P = a.P;
+  const int64_t items = ((a.rows + kTileM - 1) / kTileM + 1) / 2;  // 256-point items
+  const int64_t pairIdx = blockIdx.x >> 1, nPairs = gridDim.x >> 1;
+  const int64_t count = pairIdx < items ? (items - 1 - pairIdx) / nPairs + 1 : 0;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&bars->full[s], kPGenWarps + 1 + (rank == 0 ? 1 : 0));
+      mbar_init(&bars->empty[s], 1);
+    }
+    mbar_init(&bars->acc_full, 1);
+    mbar_init(&bars->acc_empty[0], 8);
+    mbar_init(&bars->acc_empty[1], 8);
+    mbar_init(&bars->done, 1);
+    mbar_init(&bars->dealloc_ok, 1);
+    bars->abort_flag = 0;
+    mbar_fence_init();
+  }
+  if (warp == kPIssuerWarp) {
+    tmem_alloc_pair(&bars->tmem_base, kPTmemCols);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  cluster_sync_all();  // both CTAs' barriers and TMEM allocation before any remote arrive or MMA
+  tc_fence_after();
+  const uint32_t tbase = bars->tmem_base;
+  const int32_t oNK = P.oNK, oNR = P.oNR, oRc = P.oRc, nmcBlk = P.nmcBlk, lPad = P.lPad;
+  const int32_t halfRows = lPad * oRc;                 // B rows of a half in one CTA
+  const int64_t kstepBytes = P.oKstepBytes;            // one K-step block of this CTA's B part
+
+  if (warp == kPProducerWarp) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      uint32_t s = 0, ph = 0;
+      bool ok = true;
+      const int64_t chunkBytes = P.oChunkBytes, opBytes = operand_bytes(P);
+      for (int64_t i = 0; i < count && ok; ++i) {
+        for (int32_t c = 0; c < oNR && ok; ++c) {
+          int64_t off = (int64_t)c * chunkBytes + (int64_t)rank * (chunkBytes / 2);
+          for (int32_t j = 0; j < oNK;) {
+            if (!mbar_wait(&bars->empty[s], ph ^ 1, abort_flag)) {
+              ok = false;
+              break;
+            }
+            uint32_t bytes = 0;
+            bool end = false;
+            for (; j < oNK && !end; ++j) {
+              bytes += (uint32_t)(outer_b_lo(P, j) ? 2 * kstepBytes : kstepBytes);
+              end = outer_stage_end(P, j);
+            }
+            if (!RF_IN_BOUNDS(off + bytes - 1, opBytes, err)) {
+              ok = false;  // no copy: the stage stays empty, and the waits on it end the kernel
+              break;
+            }
+            mbar_arrive_expect_tx(&bars->full[s], bytes);
+            bulk_g2s(slots + (size_t)s * slotBytes + kPStageABytes, a.B + off, bytes, &bars->full[s]);
+            off += bytes;
+            if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+          }
+        }
+      }
+      if (!ok) pair_abort(bars, err);
+      if (*abort_flag) {
+        // copies still in flight complete_tx on full barriers whose other
+        // arrivals may never come: wait for them by time before going on
+        const uint64_t t0 = globaltimer_ns();
+        while (globaltimer_ns() - t0 < 1000000ull) {
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == kPIssuerWarp && rank == 1) {
+    // ----------------------------------------------- rank 1: stage forwarder
+    // Each stage of this CTA's ring, once full (its generators' and its bulk
+    // copy's arrivals, acquired here), completes rank 0's barrier of the same
+    // stage through one cluster-scope release.
+    uint32_t s = 0, ph = 0;
+    bool ok = true;
+    const int32_t nSt = pair_stage_count(P);
+    for (int64_t i = 0; i < count && ok; ++i) {
+      for (int32_t c = 0; c < oNR && ok; ++c) {
+        for (int32_t st = 0; st < nSt; ++st) {
+          if (!mbar_wait_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
+          if (lane == 0) mbar_arrive_remote(map_to_rank(&bars->full[s], 0));
+          __syncwarp();
+          if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+        }
+      }
+    }
+    if (!ok && lane == 0) pair_abort(bars, err);
+    // rank 0's MMAs write this CTA's TMEM: free it only after they drained
+    // (rank 0 arrives after its last commit completed, on every path)
+    volatile int never = 0;
+    mbar_wait_cluster_warp(&bars->dealloc_ok, 0, &never);
+  } else if (warp == kPIssuerWarp) {
+    // ------------------------------------------------ rank 0: MMA issuer
+    // As rf_outer.cu's issuer, the two tiles' MMAs replaced by the two N
+    // halves' MMAs of M = 256 (both tiles at once).  The stage barriers
+    // complete only with rank 1's forwarded arrival, so their waits acquire
+    // at cluster scope.
+    const bool leader = elect_one();
+    uint32_t s = 0, ph = 0, accPh = 0;
+    bool ok = true, ready = false;
+    const uint32_t ab = PREC == PREC_FP16 ? 0u : 1u;
+    const uint64_t aU = (uint64_t)(kPAUnitBytes >> 4);          // descriptor step of one A unit
+    const uint64_t bU = (uint64_t)((uint32_t)kstepBytes >> 4);  // descriptor step of one B unit
+    const uint64_t bH = (uint64_t)((uint32_t)(halfRows * 32) >> 4);  // to the second half's rows
+    const uint32_t idesc = make_idesc(ab, 256u, (uint32_t)(2 * lPad * oRc));
+    if (lane == 0) {
+      int32_t ns = 0, j0 = 0, n = 0;
+      uint32_t fl = 0;
+      for (int32_t j = 0; j < oNK; ++j) {
+        fl |= ((outer_b_lo(P, j) ? 1u : 0u) | (outer_a_lo(P, j) ? 2u : 0u)) << (2 * n);
+        ++n;
+        if (outer_stage_end(P, j) || j + 1 == oNK) {
+          bars->stab[ns++] = (uint32_t)j0 | ((uint32_t)n << 9) | (fl << 12);
+          j0 = j + 1;
+          n = 0;
+          fl = 0;
+        }
+      }
+      bars->nStages = ns;
+    }
+    __syncwarp();
+    const int32_t nSt = *reinterpret_cast<volatile int32_t*>(&bars->nStages);
+    const uint32_t t0 = tbase, t1 = tbase + (uint32_t)kPAccCols;
+    for (int64_t i = 0; i < count && ok; ++i) {
+      for (int32_t c = 0; c < oNR && ok; ++c) {
+        // both halves' accumulators are free once both CTAs' epilogues read the last chunk
+        if (!mbar_wait_cluster_warp(&bars->acc_empty[0], accPh ^ 1, abort_flag) ||
+            !mbar_wait_cluster_warp(&bars->acc_empty[1], accPh ^ 1, abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        uint32_t eNext = bars->stab[0];
+        for (int32_t st = 0; st < nSt; ++st) {
+          if (!ready && !mbar_wait_cluster_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t e = eNext;
+          if (st + 1 < nSt) eNext = bars->stab[st + 1];
+          const uint32_t n = (e >> 9) & 7u, fl = e >> 12;
+          const uint32_t acc = (e & 0x1ffu) ? 1u : 0u;
+          const uint32_t base = smem_u32(slots + (size_t)s * slotBytes);
+          const uint64_t aD = make_sdesc(base, 2048u, 128u);
+          const uint64_t bD = make_sdesc(base + (uint32_t)kPStageABytes, (uint32_t)halfRows * 16u, 128u);
+          const uint32_t sn = (s + 1 == (uint32_t)S) ? 0u : s + 1;
+          const uint32_t phn = (s + 1 == (uint32_t)S) ? ph ^ 1 : ph;
+          const bool more = (st + 1 < nSt) || (c + 1 < oNR) || (i + 1 < count);
+          const bool quad = fl == 0u && n == 4u, pair = fl == 0xFu && n == 2u;
+          if (leader) {
+            if (quad) {
+              mma_pair(t0, aD, bD, idesc, acc);
+              mma_pair(t1, aD, bD + bH, idesc, acc);
+              mma_pair(t0, aD + aU, bD + bU, idesc, 1u);
+              mma_pair(t1, aD + aU, bD + bU + bH, idesc, 1u);
+              mma_pair(t0, aD + 2 * aU, bD + 2 * bU, idesc, 1u);
+              mma_pair(t1, aD + 2 * aU, bD + 2 * bU + bH, idesc, 1u);
+              mma_pair(t0, aD + 3 * aU, bD + 3 * bU, idesc, 1u);
+            } else if (pair) {
+              // K-step 0 in units 0-1 (hi, lo) of A and B, K-step 1 in units 2-3
+              mma_pair(t0, aD, bD, idesc, acc);
+              mma_pair(t0, aD, bD + bU, idesc, 1u);
+              mma_pair(t0, aD + aU, bD, idesc, 1u);
+              mma_pair(t1, aD, bD + bH, idesc, acc);
+              mma_pair(t1, aD, bD + bU + bH, idesc, 1u);
+              mma_pair(t1, aD + aU, bD + bH, idesc, 1u);
+              mma_pair(t0, aD + 2 * aU, bD + 2 * bU, idesc, 1u);
+              mma_pair(t0, aD + 2 * aU, bD + 3 * bU, idesc, 1u);
+              mma_pair(t0, aD + 3 * aU, bD + 2 * bU, idesc, 1u);
+              mma_pair(t1, aD + 2 * aU, bD + 3 * bU + bH, idesc, 1u);
+              mma_pair(t1, aD + 3 * aU, bD + 2 * bU + bH, idesc, 1u);
+            } else {
+              uint64_t ad = aD, bd = bD;
+              for (uint32_t k = 0; k < n; ++k) {
+                const uint32_t f = (fl >> (2 * k)) & 3u, bLo = f & 1u, aLo = f & 2u;
+                const uint32_t ak = k == 0 ? acc : 1u;
+                mma_pair(t0, ad, bd, idesc, ak);
+                mma_pair_if(t0, ad, bd + bU, idesc, 1u, bLo);
+                mma_pair_if(t0, ad + aU, bd, idesc, 1u, aLo);
+                mma_pair(t1, ad, bd + bH, idesc, ak);
+                mma_pair_if(t1, ad, bd + bU + bH, idesc, 1u, bLo);
+                mma_pair_if(t1, ad + aU, bd + bH, idesc, 1u, aLo);
+                ad += aLo ? 2 * aU : aU;
+                bd += bLo ? 2 * bU : bU;
+              }
+            }
+          }
+          ready = __all_sync(0xffffffffu, more && mbar_test_wait_cluster(&bars->full[sn], phn));
+          if (leader) {
+            if (quad) mma_pair(t1, aD + 3 * aU, bD + 3 * bU + bH, idesc, 1u);
+            else if (pair) mma_pair(t1, aD + 2 * aU, bD + 2 * bU + bH, idesc, 1u);
+            mma_commit_pair_both(&bars->empty[s]);
+          }
+          __syncwarp();
+          s = sn;
+          ph = phn;
+        }
+        if (!ok) break;
+        if (leader) mma_commit_pair_both(&bars->acc_full);
+        __syncwarp();
+        accPh ^= 1;
+      }
+    }
+    if (!ok && lane == 0) pair_abort(bars, err);
+    if (leader) mma_commit_pair_local(&bars->done);
+    __syncwarp();
+    volatile int never = 0;
+    mbar_wait(&bars->done, 0, &never);  // every MMA issued, drained
+    if (lane == 0) mbar_arrive_remote(map_to_rank(&bars->dealloc_ok, 1));
+    __syncwarp();
+  } else if (warp < kPEpiWarp0) {
+    // ---------------------------------------------------------- generators
+    const int gi = threadIdx.x - kPGenWarp0 * 32;  // 0 .. 255
+    const int row = gi & 127, hk = gi >> 7;        // point of the tile; K half (phasors 4 hk .. 4 hk + 3)
+    const uint32_t rowOff = (uint32_t)((row >> 3) * 128 + (row & 7) * 16 + hk * 2048);
+    uint32_t s = 0, ph = 0;
+    uint32_t ua = 0;  // A units of the current stage already written
+    bool ok = true;
+    const int32_t n1 = P.kNStep[0], n2 = P.kNStep[1], nJJ = P.n1p >> 3;
+    for (int64_t i = 0; i < count && ok; ++i) {
+      const int64_t item = pairIdx + i * nPairs;
+      const int64_t p = a.row0 + item * 2 * kTileM + (int64_t)rank * kTileM + row;
+      const bool valid = p < a.row0 + a.rows;
+      double x0 = 0.0, x1 = 0.0;
+      if (valid && RF_IN_BOUNDS(p * 3 + 2, P.n * 3, err)) {
+        x0 = a.x[p * 3 + 0] / P.corrL[0];
+        x1 = a.x[p * 3 + 1] / P.corrL[1];
+      }
+      const float2 e2step = axis_phasor(P.kDelta[1], 1, x1);
+      // E1(4 hk + u) of block 0 and the block step E1(8), from FP64-reduced
+      // phases once per item; later blocks by angle addition
+      float2 e1base[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) e1base[u] = axis_phasor(P.kDelta[0], 4 * hk + u, x0);
+      const float2 e1step = axis_phasor(P.kDelta[0], 8, x0);
+      for (int32_t c = 0; c < oNR && ok; ++c) {
+        int32_t j = 0;
+        uint32_t aw = 0, ew = 0;
+        float2 e1cur[4];
+        for (int32_t jj = 0; jj < nJJ && ok; ++jj) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (jj > 0) {
+              const float2 q = e1cur[u];
+              e1cur[u] = make_float2(q.x * e1step.x - q.y * e1step.y, q.x * e1step.y + q.y * e1step.x);
+            } else {
+              e1cur[u] = e1base[u];
+            }
+          }
+          float2 e1[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) e1[u] = (8 * jj + 4 * hk + u < n1) ? e1cur[u] : make_float2(0.f, 0.f);
+          for (int32_t s2 = 0; s2 < 2 && ok; ++s2) {
+            float2 e2 = make_float2(1.f, 0.f);
+            for (int32_t i2 = 0; i2 < n2; ++i2) {
+              const float2 E = make_float2(e2.x, s2 ? -e2.y : e2.y);
+              if ((j & 31) == 0) {
+                aw = P.aLoMask[j >> 5];
+                ew = P.oStageEnd[j >> 5];
+              }
+              const bool aLo = (aw >> (j & 31)) & 1u, end = (ew >> (j & 31)) & 1u;
+              if (ua == 0 && !mbar_wait_warp(&bars->empty[s], ph ^ 1, abort_flag)) {
+                ok = false;
+                break;
+              }
+              float2 pv[4];
+              uint32_t hi[4];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const float2 q = e1[u];
+                pv[u] = make_float2(q.x * E.x - q.y * E.y, q.x * E.y + q.y * E.x);
+                hi[u] = PREC == PREC_FP16 ? pack_f16x2(pv[u].x, pv[u].y) : pack_bf16x2(pv[u].x, pv[u].y);
+              }
+              unsigned char* A = slots + (size_t)s * slotBytes + ua * kPAUnitBytes + rowOff;
+              *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+              if (aLo) {  // the residual of the 16-bit rounding, rounded again, in the next unit
+                uint32_t lo[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                  float hx, hy;
+                  if (PREC == PREC_FP16) {
+                    const __half2 h = *reinterpret_cast<const __half2*>(&hi[u]);
+                    const float2 f = __half22float2(h);
+                    hx = f.x;
+                    hy = f.y;
+                  } else {
+                    hx = __uint_as_float(hi[u] << 16);
+                    hy = __uint_as_float(hi[u] & 0xffff0000u);
+                  }
+                  lo[u] = PREC == PREC_FP16 ? pack_f16x2(pv[u].x - hx, pv[u].y - hy)
+                                            : pack_bf16x2(pv[u].x - hx, pv[u].y - hy);
+                }
+                *reinterpret_cast<uint4*>(A + kPAUnitBytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+              }
+              ua += aLo ? 2u : 1u;
+              if (end) {
+                ua = 0;
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bars->full[s]);
+                if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+              }
+              e2 = make_float2(e2.x * e2step.x - e2.y * e2step.y, e2.x * e2step.y + e2.y * e2step.x);
+              ++j;
+            }
+          }
+        }
+      }
+    }
+    if (!ok) pair_abort(bars, err);
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3, h = (warp - kPEpiWarp0) >> 2;  // lane quarter, N half
+    const int row = q * 32 + lane;
+    const uint32_t taddr0 = tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * kPAccCols);
+    constexpr int LH = LPAD / 8;
+    uint32_t accPh = 0;
+    bool ok = true;
+    const uint32_t releaseAddr = map_to_rank(&bars->acc_empty[h], 0);
+    const int64_t rOff = P.rOff, n = P.n, nOut = P.blend ? P.gTotal : P.n;
+    [[maybe_unused]] const int64_t outLen = (int64_t)P.Nmc * nOut;  // the index checks' bound
+    const bool blend = P.blend, marg = P.applyMarginal, logn = P.lognormal;
+    const double outScale = P.outScale, margSd = P.margSd, margAvg = P.margAvg;
+    for (int64_t i = 0; i < count && ok; ++i) {
+      const int64_t item = pairIdx + i * nPairs;
+      const int64_t p = a.row0 + item * 2 * kTileM + (int64_t)rank * kTileM + row;
+      const bool valid = p < a.row0 + a.rows;
+      const double x2 = valid ? a.x[p * 3 + 2] / P.corrL[2] : 0.0;
+      double bw = 0.0;
+      int64_t bg = 0;
+      if (blend && valid) bw = blend_weight(P, p, &bg);
+      float2 e3[LPAD];
+#pragma unroll
+      for (int u = 0; u < LPAD; ++u)
+        e3[u] = (u < P.kNStep[2]) ? axis_phasor(P.kDelta[2], u, x2) : make_float2(0.f, 0.f);
+      for (int32_t c = 0; c < oNR; ++c) {
+        if (!mbar_wait_warp(&bars->acc_full, accPh, abort_flag)) { ok = false; break; }
+        tc_fence_after();
+        const int32_t r0 = c * 2 * oRc + h * oRc;  // the half's first realization of the block
+        const int32_t rc = min(oRc, nmcBlk - r0);
+        for (int32_t rl = 0; rl < rc; ++rl) {
+          float acc = 0.f;
+#pragma unroll
+          for (int hh = 0; hh < LH; hh += 2) {
+            uint32_t y[32];
+            const uint32_t col = taddr0 + (uint32_t)(rl * 2 * LPAD + 16 * hh);
+            if (hh + 1 < LH) tmem_ld32(col, y);
+            else tmem_ld16(col, y);
+            tmem_ld_wait();
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+              if (hh + (u >> 3) < LH) {
+                acc = fmaf(e3[8 * hh + u].x, __uint_as_float(y[2 * u]), acc);
+                acc = fmaf(e3[8 * hh + u].y, __uint_as_float(y[2 * u + 1]), acc);
+              }
+            }
+          }
+          if (valid) {
+            const int64_t r = rOff + r0 + rl;
+            if (blend) {
+              if (RF_IN_BOUNDS(r * nOut + bg, outLen, err)) atomicAdd(&a.out[r * nOut + bg], bw * ((double)acc * outScale));
+            } else if (RF_IN_BOUNDS(r * n + p, outLen, err)) {
+              double f = (double)acc * outScale;
+              if (marg) {
+                f = f * margSd + margAvg;
+                if (logn) f = exp(f);
+              }
+              a.out[r * n + p] = f;
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_remote(releaseAddr);  // rank 0's barrier (its own CTA's too)
+        accPh ^= 1;
+      }
+    }
+    if (!ok) pair_abort(bars, err);
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == kPIssuerWarp) tmem_dealloc_pair(tbase, kPTmemCols);
+  cluster_sync_all();  // neither CTA leaves while its peer may still address its shared memory
+}
+
+template <int PREC, int LPAD>
+cudaError_t launch_pair_t(const OuterPairArgs& a, size_t smem, int grid, cudaStream_t st) {
+  auto fn = rf_outer_pair_kernel<PREC, LPAD>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fn<<<grid, kPThreads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int PREC>
+cudaError_t launch_pair_p(const OuterPairArgs& a, size_t smem, int grid, cudaStream_t st) {
+  switch (a.P.lPad) {
+    case 8: return launch_pair_t<PREC, 8>(a, smem, grid, st);
+    case 16: return launch_pair_t<PREC, 16>(a, smem, grid, st);
+    case 24: return launch_pair_t<PREC, 24>(a, smem, grid, st);
+    case 32: return launch_pair_t<PREC, 32>(a, smem, grid, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace
+
+// Stage bytes of a CTA-pair plan: one tile's A units, then this CTA's part of
+// kOuterStageUnits B units.
+size_t outer_pair_smem_bytes(const Plan& P, int* stages) {
+  const int64_t slot = (kPStageABytes + kOuterStageUnits * P.oKstepBytes + 127) / 128 * 128;
+  const size_t limit = 227 * 1024, floor = 120 * 1024;
+  int S = (int)((limit - kPHeader) / (size_t)slot);
+  if (S > kPMaxSlots) S = kPMaxSlots;
+  if (stages) *stages = S;
+  if (S < 2) return 0;
+  const size_t total = (size_t)kPHeader + (size_t)S * (size_t)slot;
+  return total < floor ? floor : total;
+}
+
+cudaError_t launch_outer_pair(const Plan& P, const double* dX, const void* dB, double* dOut, int64_t row0,
+                              int64_t rows, uint32_t* dErr, int numSMs, cudaStream_t st) {
+  OuterPairArgs a;
+  a.P = P;
+  a.x = dX;
+  a.B = reinterpret_cast<const unsigned char*>(dB);
+  a.out = dOut;
+  a.err = dErr;
+  a.row0 = row0;
+  a.rows = rows;
+  a.slotBytes = (int32_t)((kPStageABytes + kOuterStageUnits * P.oKstepBytes + 127) / 128 * 128);
+  int S = 0;
+  const size_t smem = outer_pair_smem_bytes(P, &S);
+  if (smem == 0) return cudaErrorInvalidValue;
+  a.S = S;
+  const int64_t items = ((rows + kTileM - 1) / kTileM + 1) / 2;
+  int64_t pairs = items < numSMs / 2 ? items : numSMs / 2;
+  if (pairs < 1) pairs = 1;
+  const int grid = (int)(2 * pairs);
+  if (P.prec == PREC_FP16) return launch_pair_p<PREC_FP16>(a, smem, grid, st);
+  return launch_pair_p<PREC_BF16>(a, smem, grid, st);
+}
+
+}  // namespace rfb

@@ -101,6 +101,13 @@ struct Plan {
   int64_t oChunkBytes;        // bytes of one chunk of B, lo blocks included
   uint32_t aLoMask[8];        // K-steps whose A tile carries the lo term (up to 256)
   uint32_t oStageEnd[8];      // K-steps that close a ring stage (outer_stage_layout)
+  // CTA-pair form (rf_outer_pair.cu, single requests): N chunk c is two
+  // halves of oRc realizations each, [c 2 oRc + h oRc, + oRc); a CTA pair
+  // computes a 256-point item (one tile per CTA), each CTA holding its half
+  // (lPad oRc rows) of both halves' B rows.  B of chunk c is rank 0's part
+  // then rank 1's, each its oNK K-step blocks of oKstepBytes (half 0's rows,
+  // then half 1's), each followed by its lo block where loMask says.
+  int32_t oPair;
   int64_t oStepM1, oStepM2;   // rnglib multipliers a^(n1 n2 n3) mod m: the s3 = - draw from the s3 = + one
   // GEN_TABLE, BF16 single requests: the trig tile also carries its lo term
   // (the stage's A columns twice, one more MMA per K-step)
@@ -201,7 +208,7 @@ __host__ __device__ inline int64_t table_runs(const Plan& P) {
 }
 // Realization columns of the builder: GEN_OUTER lays out whole N chunks.
 __host__ __device__ inline int32_t table_cols(const Plan& P) {
-  return P.gen == GEN_OUTER ? P.oNR * P.oRc : P.nmcPad;
+  return P.gen == GEN_OUTER ? P.oNR * P.oRc * (P.oPair ? 2 : 1) : P.nmcPad;
 }
 __host__ __device__ inline int64_t table_threads(const Plan& P) { return table_runs(P) * table_cols(P); }
 

@@ -404,9 +404,27 @@ template <bool SINK>
 __device__ __forceinline__ void outer_run(const Plan& P, const JumpTable& jt, unsigned char* __restrict__ B,
                                           int32_t i2, int32_t s2, int32_t i3, int32_t rc, RunCursors& cu,
                                           const DrawSink& sink) {
-  const int32_t c = rc / P.oRc, rl = rc % P.oRc;
-  const int32_t nRows = 2 * P.lPad * P.oRc;
-  const int32_t row0 = rl * 2 * P.lPad + 2 * i3;  // cs = 0; cs = 1 is the next row
+  // realization column rc -> chunk c, block rows nRows, row0 of (cs = 0)
+  // (cs = 1 is the next row) and the byte offset of that block in the chunk
+  int32_t c, nRows, row0;
+  int64_t part = 0, inblk = 0;  // CTA-pair form: the rank's part of the chunk; the half inside a K-step block
+  if (P.oPair) {
+    const int32_t per = 2 * P.oRc;  // realizations per chunk
+    c = rc / per;
+    const int32_t hh = (rc % per) / P.oRc, rl = rc % P.oRc;
+    const int32_t half = P.lPad * P.oRc;  // rows of a half per rank
+    const int32_t nh = rl * 2 * P.lPad + 2 * i3;  // column of the half
+    const int32_t rank = nh / half;
+    nRows = half;
+    row0 = nh % half;
+    part = (int64_t)rank * (P.oChunkBytes / 2);
+    inblk = (int64_t)hh * (half * 32);
+  } else {
+    c = rc / P.oRc;
+    const int32_t rl = rc % P.oRc;
+    nRows = 2 * P.lPad * P.oRc;
+    row0 = rl * 2 * P.lPad + 2 * i3;
+  }
   const double k2 = 0.0 + P.kDelta[1] * (double)i2, k3 = 0.0 + P.kDelta[2] * (double)i3;
   const double a23 = exp(-(k2 * k2) / (8.0 * kRefPi)) * exp(-(k3 * k3) / (8.0 * kRefPi));
   for (int32_t i0 = 0; i0 < P.n1p; i0 += 4) {  // n1p is a multiple of 8
@@ -421,14 +439,14 @@ __device__ __forceinline__ void outer_run(const Plan& P, const JumpTable& jt, un
     if (SINK) continue;
     const int32_t i1 = i0 + 3;
     const int64_t j = outer_kstep(P, i1 >> 3, i2, s2);
-    const int64_t base = (int64_t)c * P.oChunkBytes + outer_kstep_offset(P, j);
+    const int64_t base = (int64_t)c * P.oChunkBytes + part + outer_kstep_offset(P, j);
     const bool blo = outer_b_lo(P, j);
     if (!RF_IN_BOUNDS(base + (blo ? 2 : 1) * P.oKstepBytes - 1, operand_bytes(P), P.dbgErr)) continue;
     const int64_t half = (int64_t)((i1 >> 2) & 1) * (nRows * 16);  // K half of the block
 #pragma unroll
     for (int cs = 0; cs < 2; ++cs) {
       const int32_t row = row0 + cs;
-      unsigned char* dst = B + base + half + (row >> 3) * 128 + (row & 7) * 16;
+      unsigned char* dst = B + base + inblk + half + (row >> 3) * 128 + (row & 7) * 16;
       *reinterpret_cast<uint4*>(dst) = make_uint4(hi[cs][0], hi[cs][1], hi[cs][2], hi[cs][3]);
       if (blo) *reinterpret_cast<uint4*>(dst + P.oKstepBytes) = make_uint4(lo[cs][0], lo[cs][1], lo[cs][2], lo[cs][3]);
     }
