@@ -18,7 +18,8 @@
 // MMAs issued per flop halve, and a CTA's ring stage (one tile's A, half of
 // B) is 46 KB instead of 62: four stages instead of three.
 //
-// Warp roles (576 threads, in each CTA):
+// Warp roles (448 threads, in each CTA: 14 warps leave a thread 128
+// registers):
 //   warp 0      rank 0: MMA issuer (tcgen05.mma.cta_group::2, commits
 //               multicast to both CTAs); rank 1: forwards each completed
 //               stage of its own ring to rank 0's stage barrier (one
@@ -26,10 +27,13 @@
 //               when both CTAs' stages are full;
 //   warp 1      producer (one thread): 1-D bulk copy (TMA, no multicast) of
 //               the CTA's part of a stage's B blocks from HBM/L2;
-//   warps 2-9   generators: two threads per point, each 4 of the K-step's
-//               8 outer phasors (one 16-byte K half), the lo residual where
-//               the plan keeps it;
-//   warps 10-17 epilogue: tcgen05.ld of one N half's accumulator (warp % 4
+//   warps 2-5   generators: one thread per point of the CTA's tile, the
+//               K-step's 8 outer phasors (E1 of block 0 and the block step
+//               from FP64-reduced phases once per item, later blocks and E2
+//               by angle addition), the lo residual where the plan keeps it
+//               (8 generator warps with half the phasors each measured 3 %
+//               slower);
+//   warps 6-13  epilogue: tcgen05.ld of one N half's accumulator (warp % 4
 //               picks the TMEM lane quarter), the i3 sum, ampMult, marginal
 //               map, FP64 stores; rank 1's release the accumulators to rank
 //               0's issuer with cluster-scope arrives.
@@ -44,7 +48,7 @@ namespace rfb {
 
 namespace {
 
-constexpr int kPIssuerWarp = 0, kPProducerWarp = 1, kPGenWarp0 = 2, kPGenWarps = 8;
+constexpr int kPIssuerWarp = 0, kPProducerWarp = 1, kPGenWarp0 = 2, kPGenWarps = 4;
 constexpr int kPEpiWarp0 = kPGenWarp0 + kPGenWarps, kPEpiWarps = 8;
 constexpr int kPThreads = (kPEpiWarp0 + kPEpiWarps) * 32;
 constexpr int kPMaxSlots = 8;
@@ -424,9 +428,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     __syncwarp();
   } else if (warp < kPEpiWarp0) {
     // ---------------------------------------------------------- generators
-    const int gi = threadIdx.x - kPGenWarp0 * 32;  // 0 .. 255
-    const int row = gi & 127, hk = gi >> 7;        // point of the tile; K half (phasors 4 hk .. 4 hk + 3)
-    const uint32_t rowOff = (uint32_t)((row >> 3) * 128 + (row & 7) * 16 + hk * 2048);
+    const int gi = threadIdx.x - kPGenWarp0 * 32;  // 0 .. 127
+    const int row = gi;
+    const uint32_t rowOff = (uint32_t)((row >> 3) * 128 + (row & 7) * 16);
     uint32_t s = 0, ph = 0;
     uint32_t ua = 0;  // A units of the current stage already written
     bool ok = true;
@@ -441,19 +445,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
         x1 = a.x[p * 3 + 1] / P.corrL[1];
       }
       const float2 e2step = axis_phasor(P.kDelta[1], 1, x1);
-      // E1(4 hk + u) of block 0 and the block step E1(8), from FP64-reduced
-      // phases once per item; later blocks by angle addition
-      float2 e1base[4];
+      // E1(u) of block 0 and the block step E1(8), from FP64-reduced phases
+      // once per item; later blocks by angle addition
+      float2 e1base[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) e1base[u] = axis_phasor(P.kDelta[0], 4 * hk + u, x0);
+      for (int u = 0; u < 8; ++u) e1base[u] = axis_phasor(P.kDelta[0], u, x0);
       const float2 e1step = axis_phasor(P.kDelta[0], 8, x0);
       for (int32_t c = 0; c < oNR && ok; ++c) {
         int32_t j = 0;
         uint32_t aw = 0, ew = 0;
-        float2 e1cur[4];
+        float2 e1cur[8];
         for (int32_t jj = 0; jj < nJJ && ok; ++jj) {
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
+          for (int u = 0; u < 8; ++u) {
             if (jj > 0) {
               const float2 q = e1cur[u];
               e1cur[u] = make_float2(q.x * e1step.x - q.y * e1step.y, q.x * e1step.y + q.y * e1step.x);
@@ -461,9 +465,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
               e1cur[u] = e1base[u];
             }
           }
-          float2 e1[4];
+          float2 e1[8];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) e1[u] = (8 * jj + 4 * hk + u < n1) ? e1cur[u] : make_float2(0.f, 0.f);
+          for (int u = 0; u < 8; ++u) e1[u] = (8 * jj + u < n1) ? e1cur[u] : make_float2(0.f, 0.f);
           for (int32_t s2 = 0; s2 < 2 && ok; ++s2) {
             float2 e2 = make_float2(1.f, 0.f);
             for (int32_t i2 = 0; i2 < n2; ++i2) {
@@ -477,20 +481,21 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
                 ok = false;
                 break;
               }
-              float2 pv[4];
-              uint32_t hi[4];
+              float2 pv[8];
+              uint32_t hi[8];
 #pragma unroll
-              for (int u = 0; u < 4; ++u) {
+              for (int u = 0; u < 8; ++u) {
                 const float2 q = e1[u];
                 pv[u] = make_float2(q.x * E.x - q.y * E.y, q.x * E.y + q.y * E.x);
                 hi[u] = PREC == PREC_FP16 ? pack_f16x2(pv[u].x, pv[u].y) : pack_bf16x2(pv[u].x, pv[u].y);
               }
               unsigned char* A = slots + (size_t)s * slotBytes + ua * kPAUnitBytes + rowOff;
               *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+              *reinterpret_cast<uint4*>(A + 2048) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
               if (aLo) {  // the residual of the 16-bit rounding, rounded again, in the next unit
-                uint32_t lo[4];
+                uint32_t lo[8];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
+                for (int u = 0; u < 8; ++u) {
                   float hx, hy;
                   if (PREC == PREC_FP16) {
                     const __half2 h = *reinterpret_cast<const __half2*>(&hi[u]);
@@ -505,6 +510,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
                                             : pack_bf16x2(pv[u].x - hx, pv[u].y - hy);
                 }
                 *reinterpret_cast<uint4*>(A + kPAUnitBytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+                *reinterpret_cast<uint4*>(A + kPAUnitBytes + 2048) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
               }
               ua += aLo ? 2u : 1u;
               if (end) {
