@@ -907,8 +907,9 @@ def main():
     hbm_bytes = 8.0 * n * NMC + 24.0 * n + 2.0 * (2 * K) * (2 * NMC)
     bounds = {"tensor_ms": flops / (peak * 1e12) * 1e3, "sfu_ms": pairs / sfu * 1e3,
               "hbm_ms": hbm_bytes / (pk.get("hbm_gbs", 6650.0) * 1e9) * 1e3}
-    # the 16-bit forms of this 3-D grid workload run the outer-group contraction, FP8 the trig-tile one
-    kname = ("rf_outer_kernel (outer-group tcgen05 contraction + fused i3 epilogue)"
+    # the 16-bit forms of this 3-D grid workload run the outer-group contraction on CTA pairs, FP8 the
+    # trig-tile one
+    kname = ("rf_outer_pair_kernel (outer-group tcgen05.mma.cta_group::2 contraction + fused i3 epilogue)"
              if args.precision in ("bf16", "fp16", "bf16_fast") else
              "rf_tc_kernel (tcgen05 contraction + fused epilogue)")
     roof = {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s", "frac": tflops / peak,
