@@ -312,6 +312,10 @@ __device__ __forceinline__ uint32_t pack_f16x2(float lo, float hi) {
   __half2 v = __floats2half2_rn(lo, hi);
   return *reinterpret_cast<uint32_t*>(&v);
 }
+// x rounded to TF32 (10 mantissa bits; nearest, ties away from zero) in its
+// 32-bit container: half a TF32 unit added to the magnitude bits, the low
+// 13 bits cleared.  Finite |x| below the largest float only.
+__device__ __forceinline__ uint32_t tf32_bits(float x) { return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u; }
 
 // --------------------------------------------------------------- rnglib
 // a^(2^j) mod m for j = 0..63, filled by the host (64-bit arithmetic).

@@ -493,6 +493,70 @@ void table_alo_layout(Plan& P) {
 // terms alone; (0.1, 0.2) 8.5e-4 at 1.71x; (0, 0) 3e-6 at 3x.
 constexpr double kOuterALoLeft = 0.30;
 constexpr double kOuterBLoLeft = 0.30;
+// The CTA-pair form's TF32 K-steps (A and B rounded to TF32, two MMAs of
+// K = 8 per K-step instead of three BF16 ones): on the same sample, leaving
+// 0.3 of the variance to the BF16 K-steps gives relative L2 1.19e-3 (worst
+// realization 1.31e-3) at 1.23x the MMA cycles of the hi terms alone; 0.25
+// gives 1.08e-3 (1.17e-3) at 1.26x; 0.2 9.8e-4 at 1.30x.
+constexpr double kOuterTf32Left = 0.25;
+
+// The K-steps that keep their lo terms: ranked by the field variance they
+// carry (the Gaussian spectrum's axis-1 and axis-2 factors summed over the
+// K-step's 8 groups), A keeps its lo term on the K-steps above the share
+// leftA of the total, B on those above leftB (cm_COS: every K-step keeps
+// both).
+void outer_rank_masks(Plan& P, double leftA, double leftB) {
+  const int32_t n1 = P.kNStep[0], nK = P.oNK;
+  memset(P.loMask, 0, sizeof(P.loMask));
+  memset(P.aLoMask, 0, sizeof(P.aLoMask));
+  std::vector<std::pair<double, int32_t>> E((size_t)nK);
+  double total = 0.0;
+  for (int32_t j = 0; j < nK; ++j) {
+    int32_t jj = 0, i2 = 0, s2 = 0;
+    outer_kstep_groups(P, j, &jj, &i2, &s2);
+    double w = 0.0;
+    for (int32_t i1 = 8 * jj; i1 < std::min(n1, 8 * jj + 8); ++i1) {
+      if (P.corrMod != RF_CM_GAUSSIAN) {
+        w += 1.0;  // cm_COS: no ranking, every K-step keeps both lo terms
+        continue;
+      }
+      const double k1 = P.kDelta[0] * i1, k2 = P.kDelta[1] * i2;
+      w += std::exp(-(k1 * k1) / (4.0 * kRefPi)) * std::exp(-(k2 * k2) / (4.0 * kRefPi));
+    }
+    E[(size_t)j] = {w, j};
+    total += w;
+  }
+  std::sort(E.begin(), E.end(), [](const std::pair<double, int32_t>& a, const std::pair<double, int32_t>& b) {
+    return a.first > b.first || (a.first == b.first && a.second < b.second);
+  });
+  const bool all = P.corrMod != RF_CM_GAUSSIAN;
+  double covered = 0.0;
+  for (const auto& e : E) {
+    const int32_t j = e.second;
+    if (all || covered < (1.0 - leftA) * total) P.aLoMask[j >> 5] |= 1u << (j & 31);
+    if (all || covered < (1.0 - leftB) * total) P.loMask[j >> 5] |= 1u << (j & 31);
+    covered += e.first;
+  }
+}
+
+// Ring stages of a GEN_OUTER chunk (kOuterStageUnits A and B units per
+// stage, K-steps in order) and the chunk's B bytes.
+void outer_stage_layout(Plan& P) {
+  const int32_t nK = P.oNK;
+  P.oChunkBytes = (int64_t)(nK + mask_rank(P.loMask, nK)) * P.oKstepBytes * (P.oPair ? 2 : 1);
+  memset(P.oStageEnd, 0, sizeof(P.oStageEnd));
+  int32_t ua = 0, ub = 0;
+  for (int32_t j = 0; j < nK; ++j) {
+    const int32_t a = outer_a_lo(P, j) ? 2 : 1, b = outer_b_lo(P, j) ? 2 : 1;
+    if (ua + a > kOuterStageUnits || ub + b > kOuterStageUnits) {
+      P.oStageEnd[(j - 1) >> 5] |= 1u << ((j - 1) & 31);
+      ua = ub = 0;
+    }
+    ua += a;
+    ub += b;
+  }
+  P.oStageEnd[(nK - 1) >> 5] |= 1u << ((nK - 1) & 31);
+}
 
 void outer_layout(Plan& P) {
   if (P.gen != GEN_GRID3 || P.literal) return;
@@ -506,55 +570,15 @@ void outer_layout(Plan& P) {
   P.n1p = n1p;
   P.oNK = nK;
   P.oPair = 0;
+  P.oTf32 = 0;
   P.oRc = std::min<int32_t>(P.nmcBlk, 256 / (2 * P.lPad));
   P.oNR = (P.nmcBlk + P.oRc - 1) / P.oRc;
   P.oKstepBytes = (int64_t)16 * (2 * P.lPad * P.oRc) * 2;
   memset(P.loMask, 0, sizeof(P.loMask));
   memset(P.aLoMask, 0, sizeof(P.aLoMask));
   P.loSkip = 1;  // B lo blocks only where loMask says
-  if (P.prec == PREC_BF16) {
-    std::vector<std::pair<double, int32_t>> E((size_t)nK);
-    double total = 0.0;
-    for (int32_t j = 0; j < nK; ++j) {
-      int32_t jj = 0, i2 = 0, s2 = 0;
-      outer_kstep_groups(P, j, &jj, &i2, &s2);
-      double w = 0.0;
-      for (int32_t i1 = 8 * jj; i1 < std::min(n1, 8 * jj + 8); ++i1) {
-        if (P.corrMod != RF_CM_GAUSSIAN) {
-          w += 1.0;  // cm_COS: no ranking, every K-step keeps both lo terms
-          continue;
-        }
-        const double k1 = P.kDelta[0] * i1, k2 = P.kDelta[1] * i2;
-        w += std::exp(-(k1 * k1) / (4.0 * kRefPi)) * std::exp(-(k2 * k2) / (4.0 * kRefPi));
-      }
-      E[(size_t)j] = {w, j};
-      total += w;
-    }
-    std::sort(E.begin(), E.end(), [](const std::pair<double, int32_t>& a, const std::pair<double, int32_t>& b) {
-      return a.first > b.first || (a.first == b.first && a.second < b.second);
-    });
-    const bool all = P.corrMod != RF_CM_GAUSSIAN;
-    double covered = 0.0;
-    for (const auto& e : E) {
-      const int32_t j = e.second;
-      if (all || covered < (1.0 - kOuterALoLeft) * total) P.aLoMask[j >> 5] |= 1u << (j & 31);
-      if (all || covered < (1.0 - kOuterBLoLeft) * total) P.loMask[j >> 5] |= 1u << (j & 31);
-      covered += e.first;
-    }
-  }
-  P.oChunkBytes = (int64_t)(nK + mask_rank(P.loMask, nK)) * P.oKstepBytes;
-  memset(P.oStageEnd, 0, sizeof(P.oStageEnd));
-  int32_t ua = 0, ub = 0;
-  for (int32_t j = 0; j < nK; ++j) {
-    const int32_t a = outer_a_lo(P, j) ? 2 : 1, b = outer_b_lo(P, j) ? 2 : 1;
-    if (ua + a > kOuterStageUnits || ub + b > kOuterStageUnits) {
-      P.oStageEnd[(j - 1) >> 5] |= 1u << ((j - 1) & 31);
-      ua = ub = 0;
-    }
-    ua += a;
-    ub += b;
-  }
-  P.oStageEnd[(nK - 1) >> 5] |= 1u << ((nK - 1) & 31);
+  if (P.prec == PREC_BF16) outer_rank_masks(P, kOuterALoLeft, kOuterBLoLeft);
+  outer_stage_layout(P);
   // the draw of wavevector (s3 = -) lies n1 n2 n3 calls after that of (s3 = +)
   {
     const JumpTable& jt = jump_table();
@@ -583,7 +607,9 @@ void outer_layout(Plan& P) {
 // realizations per chunk, so that a chunk covers twice the realizations and
 // the generators build A for half as many chunks.  The last chunk's missing
 // realizations are zero columns of B (their MMAs run, their values are not
-// stored).
+// stored).  BF16: the K-steps that carry all but kOuterTf32Left of the
+// variance take both operands as TF32 (oTf32) instead of hi/lo pairs: the
+// same A and B units, two MMAs instead of three, a smaller error.
 void outer_pair_layout(Plan& P) {
   if (P.gen != GEN_OUTER || P.nmcBlk < 2 || P.n < 2 * 2 * kTileM) return;
   P.oPair = 1;
@@ -591,7 +617,11 @@ void outer_pair_layout(Plan& P) {
   P.oNR = (P.nmcBlk + 2 * P.oRc - 1) / (2 * P.oRc);
   // per rank: the K-step block holds lPad oRc rows of each half
   P.oKstepBytes = (int64_t)16 * (2 * P.lPad * P.oRc) * 2;
-  P.oChunkBytes = 2 * (int64_t)(P.oNK + mask_rank(P.loMask, P.oNK)) * P.oKstepBytes;
+  if (P.prec == PREC_BF16) {
+    P.oTf32 = 1;
+    outer_rank_masks(P, kOuterTf32Left, kOuterTf32Left);
+  }
+  outer_stage_layout(P);
 }
 
 // Realizations per launch: one MMA holds at most 256 accumulator columns,

@@ -18,6 +18,13 @@
 // MMAs issued per flop halve, and a CTA's ring stage (one tile's A, half of
 // B) is 46 KB instead of 62: four stages instead of three.
 //
+// BF16 plans (oTf32) carry the K-steps of the largest variance share as
+// TF32: both A units of such a K-step hold its 16 K values in FP32
+// containers (groups 0-3, then 4-7), both B blocks likewise, and the issuer
+// runs two kind::tf32 MMAs (K = 8) per half where a hi/lo K-step takes three
+// BF16 ones; the TF32 rounding (10 bits) of both operands costs the field
+// less than the BF16 hi/lo split's residual on the other K-steps.
+//
 // Warp roles (448 threads, in each CTA: 14 warps leave a thread 128
 // registers):
 //   warp 0      rank 0: MMA issuer (tcgen05.mma.cta_group::2, commits
@@ -30,9 +37,9 @@
 //   warps 2-5   generators: one thread per point of the CTA's tile, the
 //               K-step's 8 outer phasors (E1 of block 0 and the block step
 //               from FP64-reduced phases once per item, later blocks and E2
-//               by angle addition), the lo residual where the plan keeps it
-//               (8 generator warps with half the phasors each measured 3 %
-//               slower);
+//               by angle addition), the lo residual where the plan keeps it,
+//               or the TF32 values of a TF32 K-step (8 generator warps with
+//               half the phasors each measured 3 % slower);
 //   warps 6-13  epilogue: tcgen05.ld of one N half's accumulator (warp % 4
 //               picks the TMEM lane quarter), the i3 sum, ampMult, marginal
 //               map, FP64 stores; rank 1's release the accumulators to rank
@@ -176,6 +183,17 @@ __device__ __forceinline__ void mma_pair_if(uint32_t d_tmem, uint64_t a_desc, ui
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(issue)
       : "memory");
 }
+// The same MMA of kind::tf32 (K = 8: A and B rows of 32 bytes, two TF32
+// core-matrix columns, as one K = 16 step of the 16-bit kinds).
+__device__ __forceinline__ void mma_pair_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                              uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
 // Arrive once on `bar` in both CTAs (the same offset) when the issuing
 // thread's prior tcgen05 operations have completed.
 __device__ __forceinline__ void mma_commit_pair_both(uint64_t* bar) {
@@ -203,7 +221,7 @@ __device__ __forceinline__ int32_t pair_stage_count(const Plan& P) {
   return ns;
 }
 
-template <int PREC, int LPAD>
+template <int PREC, int LPAD, bool TF32>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     rf_outer_pair_kernel(const __grid_constant__ OuterPairArgs a) {
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -323,6 +341,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     const uint64_t bU = (uint64_t)((uint32_t)kstepBytes >> 4);  // descriptor step of one B unit
     const uint64_t bH = (uint64_t)((uint32_t)(halfRows * 32) >> 4);  // to the second half's rows
     const uint32_t idesc = make_idesc(ab, 256u, (uint32_t)(2 * lPad * oRc));
+    const uint32_t idescT = make_idesc(2u, 256u, (uint32_t)(2 * lPad * oRc));  // A, B TF32
     if (lane == 0) {
       int32_t ns = 0, j0 = 0, n = 0;
       uint32_t fl = 0;
@@ -374,6 +393,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
               mma_pair(t0, aD + 2 * aU, bD + 2 * bU, idesc, 1u);
               mma_pair(t1, aD + 2 * aU, bD + 2 * bU + bH, idesc, 1u);
               mma_pair(t0, aD + 3 * aU, bD + 3 * bU, idesc, 1u);
+            } else if (pair && TF32) {
+              // K-step 0 in units 0-1 (K 0-7, 8-15 as TF32) of A and B, K-step 1 in units 2-3
+              mma_pair_tf32(t0, aD, bD, idescT, acc);
+              mma_pair_tf32(t0, aD + aU, bD + bU, idescT, 1u);
+              mma_pair_tf32(t1, aD, bD + bH, idescT, acc);
+              mma_pair_tf32(t1, aD + aU, bD + bU + bH, idescT, 1u);
+              mma_pair_tf32(t0, aD + 2 * aU, bD + 2 * bU, idescT, 1u);
+              mma_pair_tf32(t0, aD + 3 * aU, bD + 3 * bU, idescT, 1u);
+              mma_pair_tf32(t1, aD + 2 * aU, bD + 2 * bU + bH, idescT, 1u);
             } else if (pair) {
               // K-step 0 in units 0-1 (hi, lo) of A and B, K-step 1 in units 2-3
               mma_pair(t0, aD, bD, idesc, acc);
@@ -392,6 +420,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
               for (uint32_t k = 0; k < n; ++k) {
                 const uint32_t f = (fl >> (2 * k)) & 3u, bLo = f & 1u, aLo = f & 2u;
                 const uint32_t ak = k == 0 ? acc : 1u;
+                if (TF32 && f) {  // the plan marks TF32 K-steps in both masks
+                  mma_pair_tf32(t0, ad, bd, idescT, ak);
+                  mma_pair_tf32(t0, ad + aU, bd + bU, idescT, 1u);
+                  mma_pair_tf32(t1, ad, bd + bH, idescT, ak);
+                  mma_pair_tf32(t1, ad + aU, bd + bU + bH, idescT, 1u);
+                  ad += 2 * aU;
+                  bd += 2 * bU;
+                  continue;
+                }
                 mma_pair(t0, ad, bd, idesc, ak);
                 mma_pair_if(t0, ad, bd + bU, idesc, 1u, bLo);
                 mma_pair_if(t0, ad + aU, bd, idesc, 1u, aLo);
@@ -406,6 +443,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
           ready = __all_sync(0xffffffffu, more && mbar_test_wait_cluster(&bars->full[sn], phn));
           if (leader) {
             if (quad) mma_pair(t1, aD + 3 * aU, bD + 3 * bU + bH, idesc, 1u);
+            else if (pair && TF32) mma_pair_tf32(t1, aD + 3 * aU, bD + 3 * bU + bH, idescT, 1u);
             else if (pair) mma_pair(t1, aD + 2 * aU, bD + 2 * bU + bH, idesc, 1u);
             mma_commit_pair_both(&bars->empty[s]);
           }
@@ -482,14 +520,37 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
                 break;
               }
               float2 pv[8];
-              uint32_t hi[8];
 #pragma unroll
               for (int u = 0; u < 8; ++u) {
                 const float2 q = e1[u];
                 pv[u] = make_float2(q.x * E.x - q.y * E.y, q.x * E.y + q.y * E.x);
-                hi[u] = PREC == PREC_FP16 ? pack_f16x2(pv[u].x, pv[u].y) : pack_bf16x2(pv[u].x, pv[u].y);
               }
               unsigned char* A = slots + (size_t)s * slotBytes + ua * kPAUnitBytes + rowOff;
+              if (TF32 && aLo) {
+                // TF32 K-step: unit 0 holds groups 0-3 (K 0-7), unit 1 groups
+                // 4-7, each unit's core-matrix columns two groups (re, im)
+#pragma unroll
+                for (int h2 = 0; h2 < 4; ++h2) {
+                  const float2 p0 = pv[2 * h2], p1 = pv[2 * h2 + 1];
+                  *reinterpret_cast<uint4*>(A + (h2 >> 1) * kPAUnitBytes + (h2 & 1) * 2048) =
+                      make_uint4(tf32_bits(p0.x), tf32_bits(p0.y), tf32_bits(p1.x), tf32_bits(p1.y));
+                }
+                ua += 2u;
+                if (end) {
+                  ua = 0;
+                  fence_proxy_async_smem();
+                  __syncwarp();
+                  if (lane == 0) mbar_arrive(&bars->full[s]);
+                  if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
+                }
+                e2 = make_float2(e2.x * e2step.x - e2.y * e2step.y, e2.x * e2step.y + e2.y * e2step.x);
+                ++j;
+                continue;
+              }
+              uint32_t hi[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u)
+                hi[u] = PREC == PREC_FP16 ? pack_f16x2(pv[u].x, pv[u].y) : pack_bf16x2(pv[u].x, pv[u].y);
               *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
               *reinterpret_cast<uint4*>(A + 2048) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
               if (aLo) {  // the residual of the 16-bit rounding, rounded again, in the next unit
@@ -607,7 +668,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
 
 template <int PREC, int LPAD>
 cudaError_t launch_pair_t(const OuterPairArgs& a, size_t smem, int grid, cudaStream_t st) {
-  auto fn = rf_outer_pair_kernel<PREC, LPAD>;
+  auto fn = a.P.oTf32 ? rf_outer_pair_kernel<PREC, LPAD, PREC == PREC_BF16> : rf_outer_pair_kernel<PREC, LPAD, false>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   fn<<<grid, kPThreads, smem, st>>>(a);

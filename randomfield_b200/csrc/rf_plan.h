@@ -108,6 +108,10 @@ struct Plan {
   // then rank 1's, each its oNK K-step blocks of oKstepBytes (half 0's rows,
   // then half 1's), each followed by its lo block where loMask says.
   int32_t oPair;
+  // CTA-pair form, BF16: the K-steps of aLoMask (= loMask) carry A and B as
+  // TF32 (kind::tf32, two MMAs of K = 8 in the two units of a hi/lo K-step)
+  // instead of BF16 hi/lo pairs (three MMAs of K = 16)
+  int32_t oTf32;
   int64_t oStepM1, oStepM2;   // rnglib multipliers a^(n1 n2 n3) mod m: the s3 = - draw from the s3 = + one
   // GEN_TABLE, BF16 single requests: the trig tile also carries its lo term
   // (the stage's A columns twice, one more MMA per K-step)

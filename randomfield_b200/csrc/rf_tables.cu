@@ -428,21 +428,38 @@ __device__ __forceinline__ void outer_run(const Plan& P, const JumpTable& jt, un
   const double k2 = 0.0 + P.kDelta[1] * (double)i2, k3 = 0.0 + P.kDelta[2] * (double)i3;
   const double a23 = exp(-(k2 * k2) / (8.0 * kRefPi)) * exp(-(k3 * k3) / (8.0 * kRefPi));
   for (int32_t i0 = 0; i0 < P.n1p; i0 += 4) {  // n1p is a multiple of 8
-    uint32_t hi[2][4], lo[2][4];
+    float W[4][4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      float W[4];
-      outer_w<SINK>(P, jt, i0 + u, i2, s2, i3, rc, a23, cu, sink, W);
-#pragma unroll
-      for (int cs = 0; cs < 2; ++cs) hi[cs][u] = outer_pack(P, W[2 * cs], W[2 * cs + 1], &lo[cs][u]);
-    }
+    for (int u = 0; u < 4; ++u) outer_w<SINK>(P, jt, i0 + u, i2, s2, i3, rc, a23, cu, sink, W[u]);
     if (SINK) continue;
     const int32_t i1 = i0 + 3;
     const int64_t j = outer_kstep(P, i1 >> 3, i2, s2);
     const int64_t base = (int64_t)c * P.oChunkBytes + part + outer_kstep_offset(P, j);
     const bool blo = outer_b_lo(P, j);
     if (!RF_IN_BOUNDS(base + (blo ? 2 : 1) * P.oKstepBytes - 1, operand_bytes(P), P.dbgErr)) continue;
-    const int64_t half = (int64_t)((i1 >> 2) & 1) * (nRows * 16);  // K half of the block
+    const int64_t kh = (i1 >> 2) & 1;  // which K half of the K-step these four groups fill
+    if (blo && P.oTf32) {
+      // TF32 K-step: the block of MMA kh (K = 8: groups 4 kh .. 4 kh + 3),
+      // its first core-matrix column groups 4 kh, 4 kh + 1 and its second
+      // 4 kh + 2, 4 kh + 3, each group (re, im)
+#pragma unroll
+      for (int cs = 0; cs < 2; ++cs) {
+        const int32_t row = row0 + cs;
+        unsigned char* dst = B + base + kh * P.oKstepBytes + inblk + (row >> 3) * 128 + (row & 7) * 16;
+        *reinterpret_cast<uint4*>(dst) = make_uint4(tf32_bits(W[0][2 * cs]), tf32_bits(W[0][2 * cs + 1]),
+                                                    tf32_bits(W[1][2 * cs]), tf32_bits(W[1][2 * cs + 1]));
+        *reinterpret_cast<uint4*>(dst + nRows * 16) = make_uint4(tf32_bits(W[2][2 * cs]), tf32_bits(W[2][2 * cs + 1]),
+                                                                 tf32_bits(W[3][2 * cs]), tf32_bits(W[3][2 * cs + 1]));
+      }
+      continue;
+    }
+    uint32_t hi[2][4], lo[2][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+#pragma unroll
+      for (int cs = 0; cs < 2; ++cs) hi[cs][u] = outer_pack(P, W[u][2 * cs], W[u][2 * cs + 1], &lo[cs][u]);
+    }
+    const int64_t half = kh * (nRows * 16);  // K half of the block
 #pragma unroll
     for (int cs = 0; cs < 2; ++cs) {
       const int32_t row = row0 + cs;

@@ -150,15 +150,18 @@ def _bf16(a):
     return r.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-def test_outer_group_bf16_error_budget():
-    """The BF16 form of the outer-group contraction (rf_outer.cu) emulated on
-    the 128^3 workload (24^3 x 4 wavevectors, corrL (2, 1, 0.5), Nmc 64) on a
-    sample of 96 point columns x 128 points: A = the outer phasors and W = the
-    coefficients rounded to BF16, each with its lo term (the rounding residual,
-    rounded again) on the K-steps that carry all but 30 % of the field variance,
-    ranked as rf_host.cu outer_layout ranks them; the epilogue's i3 sum exact.
-    Without lo terms the relative L2 error is about 2.1e-3 (above the 2e-3
-    bound); with them it is about 1.2e-3, the worst realization under 1.5e-3."""
+def _tf32(a):
+    """Round to TF32 (10 mantissa bits, nearest, ties away from zero: half a
+    unit added to the magnitude bits, the low 13 bits cleared), as float64."""
+    u = np.asarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = (u + 0x1000) & 0xFFFFE000
+    return r.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def _outer_sample():
+    """The 128^3 workload's outer-group operands on a sample of 96 point
+    columns x 128 points: (A, W, the K-step variance weights, field(a, b),
+    the exact field, K-step mask -> K-element mask)."""
     n1 = n2 = n3 = 24
     Nmc, corrL, h, N = 64, (2.0, 1.0, 0.5), 0.05, 128
     req = O.OracleRequest(np.zeros((1, 3)), Nmc=Nmc, kNStep=(24, 24, 24), corrL=corrL, xRange=((N - 1) * h,) * 3)
@@ -181,13 +184,12 @@ def test_outer_group_bf16_error_budget():
     pi_ref = 3.1415926535898
     w = np.array([np.exp(-(kd[0] * np.arange(8 * (j // (2 * n2)), 8 * (j // (2 * n2)) + 8)) ** 2 / (4 * pi_ref)).sum()
                   * np.exp(-(kd[1] * (j % n2)) ** 2 / (4 * pi_ref)) for j in range(3 * n2 * 2)])
-    lo = np.zeros(w.size, bool)
-    cov = 0.0
-    for j in sorted(range(w.size), key=lambda j: (-w[j], j)):
-        lo[j] = cov < 0.7 * w.sum()
-        cov += w[j]
-    g_lo = np.array([lo[i2 + n2 * (s2 + 2 * (i1 // 8))] for s2 in range(2) for i2 in range(n2) for i1 in range(n1)])
-    k_lo = np.repeat(g_lo, 2)
+
+    def kmask(lo):
+        g_lo = np.array([lo[i2 + n2 * (s2 + 2 * (i1 // 8))] for s2 in range(2) for i2 in range(n2)
+                         for i1 in range(n1)])
+        return np.repeat(g_lo, 2)
+
     rs = np.random.RandomState(3)
     J1, J2 = rs.randint(0, N, 96), rs.randint(0, N, 96)
     x = np.arange(N) * h
@@ -201,14 +203,64 @@ def test_outer_group_bf16_error_budget():
 
     def field(a, b):
         Y = (a @ b).reshape(96, n3, 2, Nmc)
-        return np.einsum('ji,pir->pjr', E3.real, Y[:, :, 0]) + np.einsum('ji,pir->pjr', E3.imag, Y[:, :, 1])
+        return (np.einsum('ji,pir->pjr', E3.real, Y[:, :, 0])
+                + np.einsum('ji,pir->pjr', E3.imag, Y[:, :, 1])).reshape(-1, Nmc)
 
-    exact = field(A, W).reshape(-1, Nmc)
+    return A, W, w, field, field(A, W), kmask
+
+
+def _variance_mask(w, left):
+    """The K-steps carrying all but `left` of the variance, ranked as
+    rf_host.cu outer_rank_masks ranks them."""
+    lo = np.zeros(w.size, bool)
+    cov = 0.0
+    for j in sorted(range(w.size), key=lambda j: (-w[j], j)):
+        lo[j] = cov < (1.0 - left) * w.sum()
+        cov += w[j]
+    return lo
+
+
+def _errors(f, exact):
+    rel = np.sqrt(((f - exact) ** 2).sum() / (exact ** 2).sum())
+    per = np.sqrt(((f - exact) ** 2).sum(0) / (exact ** 2).sum(0))
+    return rel, per.max()
+
+
+def test_outer_group_bf16_error_budget():
+    """The BF16 form of the outer-group contraction (rf_outer.cu) emulated on
+    the 128^3 workload (24^3 x 4 wavevectors, corrL (2, 1, 0.5), Nmc 64) on a
+    sample of 96 point columns x 128 points: A = the outer phasors and W = the
+    coefficients rounded to BF16, each with its lo term (the rounding residual,
+    rounded again) on the K-steps that carry all but 30 % of the field variance,
+    ranked as rf_host.cu outer_layout ranks them; the epilogue's i3 sum exact.
+    Without lo terms the relative L2 error is about 2.1e-3 (above the 2e-3
+    bound); with them it is about 1.2e-3, the worst realization under 1.5e-3."""
+    A, W, w, field, exact, kmask = _outer_sample()
+    k_lo = kmask(_variance_mask(w, 0.3))
     Ah, Wh = _bf16(A), _bf16(W)
-    none = field(Ah, Wh).reshape(-1, Nmc)
-    split = field(Ah + np.where(k_lo[None, :], _bf16(A - Ah), 0.0),
-                  Wh + np.where(k_lo[:, None], _bf16(W - Wh), 0.0)).reshape(-1, Nmc)
-    rel = lambda d: np.sqrt((d ** 2).sum() / (exact ** 2).sum())
-    per = np.sqrt(((split - exact) ** 2).sum(0) / (exact ** 2).sum(0))
-    assert rel(none - exact) > 2e-3
-    assert rel(split - exact) < 1.3e-3 and per.max() < 1.5e-3, (rel(split - exact), per.max())
+    none = field(Ah, Wh)
+    split = field(Ah + np.where(k_lo[None, :], _bf16(A - Ah), 0.0), Wh + np.where(k_lo[:, None], _bf16(W - Wh), 0.0))
+    assert _errors(none, exact)[0] > 2e-3
+    rel, worst = _errors(split, exact)
+    assert rel < 1.3e-3 and worst < 1.5e-3, (rel, worst)
+
+
+def test_outer_group_tf32_error_budget():
+    """The CTA-pair form's BF16 plans (rf_outer_pair.cu, oTf32): the K-steps
+    carrying all but 25 % of the variance take A and W rounded to TF32 (two
+    kind::tf32 MMAs of K = 8, the values rounded by tf32_bits as the generators
+    and rf_tables.cu outer_run round them), the others A and W rounded to BF16
+    alone.  Relative L2 about 1.08e-3, worst realization about 1.17e-3: below
+    the BF16 hi/lo form at 0.3 (1.16e-3, 1.30e-3), at 1.26x the MMA cycles of
+    the BF16 hi terms alone against 1.46x."""
+    A, W, w, field, exact, kmask = _outer_sample()
+    lo = _variance_mask(w, 0.25)
+    k_tf = kmask(lo)
+    mixed = field(np.where(k_tf[None, :], _tf32(A), _bf16(A)), np.where(k_tf[:, None], _tf32(W), _bf16(W)))
+    rel, worst = _errors(mixed, exact)
+    assert rel < 1.12e-3 and worst < 1.22e-3, (rel, worst)
+    cycles = (lo.size - lo.sum()) + 2 * lo.sum()  # BF16 K-step: one MMA per half; TF32: two of the same length
+    assert cycles / lo.size < 1.3
+    # the rounding is the nearest TF32 value, ties away from zero
+    v = np.array([1.0 + 2.0 ** -11, 1.0 + 3 * 2.0 ** -11, -(1.0 + 2.0 ** -11), 1.0 + 2.0 ** -12], np.float32)
+    assert list(_tf32(v)) == [1.0 + 2.0 ** -10, 1.0 + 2 * 2.0 ** -10, -(1.0 + 2.0 ** -10), 1.0]
