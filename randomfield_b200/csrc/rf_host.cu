@@ -540,15 +540,19 @@ void outer_rank_masks(Plan& P, double leftA, double leftB) {
 }
 
 // Ring stages of a GEN_OUTER chunk (kOuterStageUnits A and B units per
-// stage, K-steps in order) and the chunk's B bytes.
+// stage, K-steps in order) and the chunk's B bytes.  CTA-pair plans also
+// close a stage before every K-step that starts an i2 run (i2 = 0), so that
+// a stage's K-steps share s2 and the axis-1 block (rf_outer_pair.cu's
+// generators rely on it).
 void outer_stage_layout(Plan& P) {
-  const int32_t nK = P.oNK;
+  const int32_t nK = P.oNK, n2 = P.kNStep[1];
   P.oChunkBytes = (int64_t)(nK + mask_rank(P.loMask, nK)) * P.oKstepBytes * (P.oPair ? 2 : 1);
   memset(P.oStageEnd, 0, sizeof(P.oStageEnd));
   int32_t ua = 0, ub = 0;
   for (int32_t j = 0; j < nK; ++j) {
     const int32_t a = outer_a_lo(P, j) ? 2 : 1, b = outer_b_lo(P, j) ? 2 : 1;
-    if (ua + a > kOuterStageUnits || ub + b > kOuterStageUnits) {
+    const bool runStart = P.oPair && j > 0 && j % n2 == 0;
+    if (runStart || ua + a > kOuterStageUnits || ub + b > kOuterStageUnits) {
       P.oStageEnd[(j - 1) >> 5] |= 1u << ((j - 1) & 31);
       ua = ub = 0;
     }

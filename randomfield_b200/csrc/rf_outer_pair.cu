@@ -38,8 +38,10 @@
 //               K-step's 8 outer phasors (E1 of block 0 and the block step
 //               from FP64-reduced phases once per item, later blocks and E2
 //               by angle addition), the lo residual where the plan keeps it,
-//               or the TF32 values of a TF32 K-step (8 generator warps with
-//               half the phasors each measured 3 % slower);
+//               or the TF32 values of a TF32 K-step; driven by the stage
+//               table, four hi-only K-steps (or two TF32 ones) straight-line
+//               (8 generator warps with half the phasors each measured 3 %
+//               slower);
 //   warps 6-13  epilogue: tcgen05.ld of one N half's accumulator (warp % 4
 //               picks the TMEM lane quarter), the i3 sum, ampMult, marginal
 //               map, FP64 stores; rank 1's release the accumulators to rank
@@ -214,6 +216,57 @@ __device__ __forceinline__ void pair_abort(PairBars* bars, uint32_t* err) {
   atomicOr(err, kErrTimeout);
 }
 
+__device__ __forceinline__ float2 cmulf(float2 p, float2 q) {
+  return make_float2(p.x * q.x - p.y * q.y, p.x * q.y + p.y * q.x);
+}
+// One tile row's hi A unit of a K-step: the 8 groups E1(u) E, (re, im) as
+// 16-bit pairs, groups 0-3 in the first core-matrix column, 4-7 in the
+// second (2048 bytes on).
+template <int PREC>
+__device__ __forceinline__ void gen_hi(unsigned char* A, const float2* e1, float2 E) {
+  uint32_t h[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const float2 v = cmulf(e1[u], E);
+    h[u] = PREC == PREC_FP16 ? pack_f16x2(v.x, v.y) : pack_bf16x2(v.x, v.y);
+  }
+  *reinterpret_cast<uint4*>(A) = make_uint4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<uint4*>(A + 2048) = make_uint4(h[4], h[5], h[6], h[7]);
+}
+// The lo unit: the residual of the 16-bit rounding, rounded again.
+template <int PREC>
+__device__ __forceinline__ void gen_lo(unsigned char* A, const float2* e1, float2 E) {
+  uint32_t l[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const float2 v = cmulf(e1[u], E);
+    float hx, hy;
+    if (PREC == PREC_FP16) {
+      const __half2 hv = __floats2half2_rn(v.x, v.y);
+      const float2 f = __half22float2(hv);
+      hx = f.x;
+      hy = f.y;
+    } else {
+      const uint32_t hb = pack_bf16x2(v.x, v.y);
+      hx = __uint_as_float(hb << 16);
+      hy = __uint_as_float(hb & 0xffff0000u);
+    }
+    l[u] = PREC == PREC_FP16 ? pack_f16x2(v.x - hx, v.y - hy) : pack_bf16x2(v.x - hx, v.y - hy);
+  }
+  *reinterpret_cast<uint4*>(A) = make_uint4(l[0], l[1], l[2], l[3]);
+  *reinterpret_cast<uint4*>(A + 2048) = make_uint4(l[4], l[5], l[6], l[7]);
+}
+// A TF32 K-step's two units: unit 0 groups 0-3 (K 0-7), unit 1 groups 4-7,
+// each unit's core-matrix columns two groups (re, im) in FP32 containers.
+__device__ __forceinline__ void gen_tf32(unsigned char* A, const float2* e1, float2 E) {
+#pragma unroll
+  for (int h2 = 0; h2 < 4; ++h2) {
+    const float2 p0 = cmulf(e1[2 * h2], E), p1 = cmulf(e1[2 * h2 + 1], E);
+    *reinterpret_cast<uint4*>(A + (h2 >> 1) * kPAUnitBytes + (h2 & 1) * 2048) =
+        make_uint4(tf32_bits(p0.x), tf32_bits(p0.y), tf32_bits(p1.x), tf32_bits(p1.y));
+  }
+}
+
 // Stages per chunk of a plan (the stage-end marks; the last K-step closes one).
 __device__ __forceinline__ int32_t pair_stage_count(const Plan& P) {
   int32_t ns = 0;
@@ -249,6 +302,28 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     mbar_init(&bars->done, 1);
     mbar_init(&bars->dealloc_ok, 1);
     bars->abort_flag = 0;
+    // the stage table (issuer and generators): first K-step (9 bits), K-steps
+    // (3 bits), per K-step the B and A lo (TF32) flags; a stage must not span
+    // the end of an i2 run (outer_stage_layout closes one there)
+    int32_t ns = 0, j0 = 0, n = 0;
+    uint32_t fl = 0;
+    bool bad = false;
+    for (int32_t j = 0; j < P.oNK; ++j) {
+      fl |= ((outer_b_lo(P, j) ? 1u : 0u) | (outer_a_lo(P, j) ? 2u : 0u)) << (2 * n);
+      ++n;
+      if (outer_stage_end(P, j) || j + 1 == P.oNK) {
+        bad |= (j0 % P.kNStep[1]) + n > P.kNStep[1] || n > 4;
+        bars->stab[ns++] = (uint32_t)j0 | ((uint32_t)n << 9) | (fl << 12);
+        j0 = j + 1;
+        n = 0;
+        fl = 0;
+      }
+    }
+    bars->nStages = ns;
+    if (bad) {  // not a layout of outer_stage_layout: no stage runs
+      bars->abort_flag = 1;
+      atomicOr(err, kErrBounds);
+    }
     mbar_fence_init();
   }
   if (warp == kPIssuerWarp) {
@@ -342,23 +417,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     const uint64_t bH = (uint64_t)((uint32_t)(halfRows * 32) >> 4);  // to the second half's rows
     const uint32_t idesc = make_idesc(ab, 256u, (uint32_t)(2 * lPad * oRc));
     const uint32_t idescT = make_idesc(2u, 256u, (uint32_t)(2 * lPad * oRc));  // A, B TF32
-    if (lane == 0) {
-      int32_t ns = 0, j0 = 0, n = 0;
-      uint32_t fl = 0;
-      for (int32_t j = 0; j < oNK; ++j) {
-        fl |= ((outer_b_lo(P, j) ? 1u : 0u) | (outer_a_lo(P, j) ? 2u : 0u)) << (2 * n);
-        ++n;
-        if (outer_stage_end(P, j) || j + 1 == oNK) {
-          bars->stab[ns++] = (uint32_t)j0 | ((uint32_t)n << 9) | (fl << 12);
-          j0 = j + 1;
-          n = 0;
-          fl = 0;
-        }
-      }
-      bars->nStages = ns;
-    }
-    __syncwarp();
-    const int32_t nSt = *reinterpret_cast<volatile int32_t*>(&bars->nStages);
+    const int32_t nSt = bars->nStages;
     const uint32_t t0 = tbase, t1 = tbase + (uint32_t)kPAccCols;
     for (int64_t i = 0; i < count && ok; ++i) {
       for (int32_t c = 0; c < oNR && ok; ++c) {
@@ -466,13 +525,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     __syncwarp();
   } else if (warp < kPEpiWarp0) {
     // ---------------------------------------------------------- generators
+    // Stage by stage from the stage table.  A stage lies inside one i2 run
+    // (fixed s2 and axis-1 block), so its K-steps' E2 powers follow by angle
+    // addition from the run's walk; four hi-only K-steps (and two TF32 ones)
+    // run straight-line.  The padded axis-1 groups (i1 >= n1) keep their
+    // phasors: their B rows are zero.
     const int gi = threadIdx.x - kPGenWarp0 * 32;  // 0 .. 127
     const int row = gi;
     const uint32_t rowOff = (uint32_t)((row >> 3) * 128 + (row & 7) * 16);
     uint32_t s = 0, ph = 0;
-    uint32_t ua = 0;  // A units of the current stage already written
-    bool ok = true;
-    const int32_t n1 = P.kNStep[0], n2 = P.kNStep[1], nJJ = P.n1p >> 3;
+    bool ok = !*abort_flag;
+    const int32_t n2 = P.kNStep[1];
+    const int32_t nSt = bars->nStages;
     for (int64_t i = 0; i < count && ok; ++i) {
       const int64_t item = pairIdx + i * nPairs;
       const int64_t p = a.row0 + item * 2 * kTileM + (int64_t)rank * kTileM + row;
@@ -490,101 +554,59 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
       for (int u = 0; u < 8; ++u) e1base[u] = axis_phasor(P.kDelta[0], u, x0);
       const float2 e1step = axis_phasor(P.kDelta[0], 8, x0);
       for (int32_t c = 0; c < oNR && ok; ++c) {
-        int32_t j = 0;
-        uint32_t aw = 0, ew = 0;
-        float2 e1cur[8];
-        for (int32_t jj = 0; jj < nJJ && ok; ++jj) {
+        float2 e1[8];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            if (jj > 0) {
-              const float2 q = e1cur[u];
-              e1cur[u] = make_float2(q.x * e1step.x - q.y * e1step.y, q.x * e1step.y + q.y * e1step.x);
-            } else {
-              e1cur[u] = e1base[u];
-            }
+        for (int u = 0; u < 8; ++u) e1[u] = e1base[u];
+        float2 e2 = make_float2(1.f, 0.f);
+        int32_t jjCur = 0;
+        for (int32_t st = 0; st < nSt; ++st) {
+          const uint32_t e = bars->stab[st];
+          const int32_t j0 = (int32_t)(e & 0x1ffu), n = (int32_t)((e >> 9) & 7u);
+          const uint32_t fl = e >> 12;
+          const int32_t run = j0 / n2, jj = run >> 1;
+          if (j0 - run * n2 == 0) e2 = make_float2(1.f, 0.f);  // a new i2 run
+          if (jj != jjCur) {  // the next axis-1 block (blocks come in order)
+            jjCur = jj;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) e1[u] = cmulf(e1[u], e1step);
           }
-          float2 e1[8];
+          const float sg = (run & 1) ? -1.f : 1.f;  // s2 = 1: the conjugate of E2
+          if (!mbar_wait_warp(&bars->empty[s], ph ^ 1, abort_flag)) {
+            ok = false;
+            break;
+          }
+          unsigned char* A = slots + (size_t)s * slotBytes + rowOff;
+          if (fl == 0u && n == 4) {
 #pragma unroll
-          for (int u = 0; u < 8; ++u) e1[u] = (8 * jj + u < n1) ? e1cur[u] : make_float2(0.f, 0.f);
-          for (int32_t s2 = 0; s2 < 2 && ok; ++s2) {
-            float2 e2 = make_float2(1.f, 0.f);
-            for (int32_t i2 = 0; i2 < n2; ++i2) {
-              const float2 E = make_float2(e2.x, s2 ? -e2.y : e2.y);
-              if ((j & 31) == 0) {
-                aw = P.aLoMask[j >> 5];
-                ew = P.oStageEnd[j >> 5];
-              }
-              const bool aLo = (aw >> (j & 31)) & 1u, end = (ew >> (j & 31)) & 1u;
-              if (ua == 0 && !mbar_wait_warp(&bars->empty[s], ph ^ 1, abort_flag)) {
-                ok = false;
-                break;
-              }
-              float2 pv[8];
+            for (int k = 0; k < 4; ++k) {
+              gen_hi<PREC>(A + k * kPAUnitBytes, e1, make_float2(e2.x, sg * e2.y));
+              e2 = cmulf(e2, e2step);
+            }
+          } else if (TF32 && fl == 0xFu && n == 2) {
 #pragma unroll
-              for (int u = 0; u < 8; ++u) {
-                const float2 q = e1[u];
-                pv[u] = make_float2(q.x * E.x - q.y * E.y, q.x * E.y + q.y * E.x);
-              }
-              unsigned char* A = slots + (size_t)s * slotBytes + ua * kPAUnitBytes + rowOff;
+            for (int k = 0; k < 2; ++k) {
+              gen_tf32(A + 2 * k * kPAUnitBytes, e1, make_float2(e2.x, sg * e2.y));
+              e2 = cmulf(e2, e2step);
+            }
+          } else {
+            uint32_t ua = 0;  // A units of the stage already written
+            for (int32_t k = 0; k < n; ++k) {
+              const bool aLo = (fl >> (2 * k + 1)) & 1u;
+              const float2 E = make_float2(e2.x, sg * e2.y);
               if (TF32 && aLo) {
-                // TF32 K-step: unit 0 holds groups 0-3 (K 0-7), unit 1 groups
-                // 4-7, each unit's core-matrix columns two groups (re, im)
-#pragma unroll
-                for (int h2 = 0; h2 < 4; ++h2) {
-                  const float2 p0 = pv[2 * h2], p1 = pv[2 * h2 + 1];
-                  *reinterpret_cast<uint4*>(A + (h2 >> 1) * kPAUnitBytes + (h2 & 1) * 2048) =
-                      make_uint4(tf32_bits(p0.x), tf32_bits(p0.y), tf32_bits(p1.x), tf32_bits(p1.y));
-                }
-                ua += 2u;
-                if (end) {
-                  ua = 0;
-                  fence_proxy_async_smem();
-                  __syncwarp();
-                  if (lane == 0) mbar_arrive(&bars->full[s]);
-                  if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
-                }
-                e2 = make_float2(e2.x * e2step.x - e2.y * e2step.y, e2.x * e2step.y + e2.y * e2step.x);
-                ++j;
-                continue;
-              }
-              uint32_t hi[8];
-#pragma unroll
-              for (int u = 0; u < 8; ++u)
-                hi[u] = PREC == PREC_FP16 ? pack_f16x2(pv[u].x, pv[u].y) : pack_bf16x2(pv[u].x, pv[u].y);
-              *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-              *reinterpret_cast<uint4*>(A + 2048) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
-              if (aLo) {  // the residual of the 16-bit rounding, rounded again, in the next unit
-                uint32_t lo[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                  float hx, hy;
-                  if (PREC == PREC_FP16) {
-                    const __half2 h = *reinterpret_cast<const __half2*>(&hi[u]);
-                    const float2 f = __half22float2(h);
-                    hx = f.x;
-                    hy = f.y;
-                  } else {
-                    hx = __uint_as_float(hi[u] << 16);
-                    hy = __uint_as_float(hi[u] & 0xffff0000u);
-                  }
-                  lo[u] = PREC == PREC_FP16 ? pack_f16x2(pv[u].x - hx, pv[u].y - hy)
-                                            : pack_bf16x2(pv[u].x - hx, pv[u].y - hy);
-                }
-                *reinterpret_cast<uint4*>(A + kPAUnitBytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-                *reinterpret_cast<uint4*>(A + kPAUnitBytes + 2048) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+                gen_tf32(A + ua * kPAUnitBytes, e1, E);
+              } else {
+                gen_hi<PREC>(A + ua * kPAUnitBytes, e1, E);
+                if (aLo) gen_lo<PREC>(A + (ua + 1) * kPAUnitBytes, e1, E);
               }
               ua += aLo ? 2u : 1u;
-              if (end) {
-                ua = 0;
-                fence_proxy_async_smem();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&bars->full[s]);
-                if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
-              }
-              e2 = make_float2(e2.x * e2step.x - e2.y * e2step.y, e2.x * e2step.y + e2.y * e2step.x);
-              ++j;
+              e2 = cmulf(e2, e2step);
             }
           }
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&bars->full[s]);
+          if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
         }
       }
     }
