@@ -5,8 +5,9 @@
 Workload (one "step" = one full generation request):
   Shinozuka-Deodatis method 2 on a 128^3 structured grid, spacing 0.05,
   corrL = (2, 1, 0.5), gaussian marginal, Nmc = 64, 24^3 wavenumbers x 4 sign
-  quadrants (K = 55,296), seed_start = rank; BF16 trig tiles with hi/lo BF16
-  amplitude side on tcgen05, FP32 accumulation, FP64 phase reduction.
+  quadrants (K = 55,296), seed_start = rank; the outer-group contraction on
+  CTA pairs: BF16 operands, TF32 on the K-steps that carry 75 % of the field
+  variance, tcgen05 with FP32 accumulation, FP64 phase reduction.
   n * Nmc = 134,217,728 field values per step.  Synthetic inputs (the
   reference publishes no dataset).
 
@@ -892,7 +893,7 @@ def main():
 
     pk, src = peaks()
     K = 4 * KN ** 3
-    flops = 2.0 * n * (2 * K) * NMC  # algorithmic: the hi/lo split's second MMA is not credited
+    flops = 2.0 * n * (2 * K) * NMC  # algorithmic: the TF32 K-steps' second MMA is not credited
     tflops = flops / (kern_ms / 1e3) / 1e12
     peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
     traffic = None
@@ -917,9 +918,10 @@ def main():
             "kernel_ms": kern_ms, "peak_source": f"bf16_tflops_sustained, {src}",
             "algorithmic_flops_per_launch": flops, "bounds": bounds,
             "sfu_pairs_per_s": sfu, "sfu_pairs_per_launch": pairs,
-            "note": "the slowest of the three bounds is the tensor MMA (algorithmic FLOPs 2 n 2K Nmc; the hi/lo "
-                    "terms' extra MMAs are not credited); the tensor-grid generators need sincos only for the "
-                    "per-axis phasors (n1 + n2 + n3 per point), GEN_TABLE one pair per (point, wavevector)"}
+            "note": "the slowest of the three bounds is the tensor MMA (algorithmic FLOPs 2 n 2K Nmc; the extra "
+                    "MMA cycles of the TF32 K-steps and of zero realization columns are not credited); the "
+                    "outer-group generators need sincos only for the per-axis phasors (n1 + n2 + n3 per point), "
+                    "GEN_TABLE one pair per (point, wavevector)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -964,6 +966,9 @@ def main():
             "dtype": {"bf16": "bf16", "fp16": "f16", "bf16_fast": "bf16", "fp8": "e4m3", "fp32": "f32"}[args.precision],
             "data": "synthetic",
             "config": {"workload": WORKLOAD if GRID == (128, 128, 128) else f"{WORKLOAD} on a {GRID} grid", "n_points": n, "Nmc": NMC, "K": K, "precision": args.precision,
+                       "operands": {"bf16": "bf16; tf32 on the K-steps carrying 75 % of the variance",
+                                    "fp16": "f16", "bf16_fast": "bf16", "fp8": "e4m3 hi/lo",
+                                    "fp32": "f32"}[args.precision],
                        "l2": "flushed between timed steps (256 MiB write); output 1 GiB per step",
                        "parallelism": f"replicas x{world}"},
             "gpu_launches": launches,
