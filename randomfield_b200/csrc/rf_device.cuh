@@ -177,6 +177,17 @@ __device__ __forceinline__ void mma_ss(uint32_t d_tmem, uint64_t a_desc, uint64_
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
+// The same MMA of kind::tf32 (K = 8: rows of 32 bytes, two TF32 core-matrix
+// columns, as one K = 16 step of the 16-bit kinds).
+__device__ __forceinline__ void mma_ss_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
 // The same MMA issued only when `issue` is nonzero, through a guard predicate
 // (no branch between the MMAs of a K-step).
 __device__ __forceinline__ void mma_ss_if(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,

@@ -477,27 +477,20 @@ void table_alo_layout(Plan& P) {
 
 // GEN_OUTER (rf_outer.cu) for single 3-D Shinozuka requests on the 16-bit
 // tensor-core forms: the same sum as GEN_GRID3 with the outer phasors as the
-// generated operand.  Its BF16 form splits both operands into hi and lo
-// terms where they matter: a 16-bit rounding of either operand leaves a
-// relative error of about 1.3e-3 in the field, in proportion to the share of
+// generated operand.  A 16-bit rounding of both operands leaves a relative
+// error of about 2.1e-3 in the field (BF16), in proportion to the share of
 // the field's variance the rounded terms carry.  The K-steps (8 outer groups
 // each) are ranked by that share (sum of S1(k1) S2(k2) over the K-step's
-// groups; the axis-3 factor is common), and the top ones keep a lo term:
-// A's on those carrying all but kOuterALoLeft of the variance, B's on those
-// carrying all but kOuterBLoLeft.  An A lo term costs one more MMA per tile
-// and K-step and no operand bytes; a B lo term one more MMA per tile and a
-// second B block.  A numpy emulation of this rounding on the 128^3 workload
-// (24^3 x 4 wavevectors, Nmc 64, 24,576 points) gives, per (A, B) share
-// left without a lo term: (1, 1) relative L2 2.1e-3 (no lo term at all);
-// (0.3, 0.3) 1.16e-3, worst realization 1.27e-3, 1.46x the MMAs of the hi
-// terms alone; (0.1, 0.2) 8.5e-4 at 1.71x; (0, 0) 3e-6 at 3x.
-constexpr double kOuterALoLeft = 0.30;
-constexpr double kOuterBLoLeft = 0.30;
-// The CTA-pair form's TF32 K-steps (A and B rounded to TF32, two MMAs of
-// K = 8 per K-step instead of three BF16 ones): on the same sample, leaving
-// 0.3 of the variance to the BF16 K-steps gives relative L2 1.19e-3 (worst
-// realization 1.31e-3) at 1.23x the MMA cycles of the hi terms alone; 0.25
-// gives 1.08e-3 (1.17e-3) at 1.26x; 0.2 9.8e-4 at 1.30x.
+// groups; the axis-3 factor is common), and in the BF16 form those carrying
+// all but kOuterTf32Left of the variance take both operands as TF32 (oTf32):
+// the two units of a K-step hold its 16 K values in 32-bit containers, and
+// two kind::tf32 MMAs of K = 8 replace the one BF16 MMA.  A numpy emulation
+// on the 128^3 workload (24^3 x 4 wavevectors, Nmc 64, 12,288 points) gives
+// relative L2 1.08e-3, worst realization 1.17e-3, at 1.26x the MMA cycles of
+// BF16 alone; 0.3 left: 1.19e-3 at 1.23x; 0.2: 9.8e-4 at 1.30x.  The BF16
+// hi/lo split it replaced (the rounding residual of both operands as a
+// second BF16 term, three MMAs per K-step) gave 1.16e-3 and 1.27e-3 at 1.46x
+// with 0.3 of the variance left.
 constexpr double kOuterTf32Left = 0.25;
 
 // The K-steps that keep their lo terms: ranked by the field variance they
@@ -581,7 +574,10 @@ void outer_layout(Plan& P) {
   memset(P.loMask, 0, sizeof(P.loMask));
   memset(P.aLoMask, 0, sizeof(P.aLoMask));
   P.loSkip = 1;  // B lo blocks only where loMask says
-  if (P.prec == PREC_BF16) outer_rank_masks(P, kOuterALoLeft, kOuterBLoLeft);
+  if (P.prec == PREC_BF16) {  // TF32 K-steps (both masks) where the variance needs them
+    P.oTf32 = 1;
+    outer_rank_masks(P, kOuterTf32Left, kOuterTf32Left);
+  }
   outer_stage_layout(P);
   // the draw of wavevector (s3 = -) lies n1 n2 n3 calls after that of (s3 = +)
   {
@@ -611,9 +607,7 @@ void outer_layout(Plan& P) {
 // realizations per chunk, so that a chunk covers twice the realizations and
 // the generators build A for half as many chunks.  The last chunk's missing
 // realizations are zero columns of B (their MMAs run, their values are not
-// stored).  BF16: the K-steps that carry all but kOuterTf32Left of the
-// variance take both operands as TF32 (oTf32) instead of hi/lo pairs: the
-// same A and B units, two MMAs instead of three, a smaller error.
+// stored).  The TF32 K-steps (BF16) are outer_layout's.
 void outer_pair_layout(Plan& P) {
   if (P.gen != GEN_OUTER || P.nmcBlk < 2 || P.n < 2 * 2 * kTileM) return;
   P.oPair = 1;
@@ -621,10 +615,6 @@ void outer_pair_layout(Plan& P) {
   P.oNR = (P.nmcBlk + 2 * P.oRc - 1) / (2 * P.oRc);
   // per rank: the K-step block holds lPad oRc rows of each half
   P.oKstepBytes = (int64_t)16 * (2 * P.lPad * P.oRc) * 2;
-  if (P.prec == PREC_BF16) {
-    P.oTf32 = 1;
-    outer_rank_masks(P, kOuterTf32Left, kOuterTf32Left);
-  }
   outer_stage_layout(P);
 }
 

@@ -175,6 +175,8 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
   volatile int* abort_flag = &bars->abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t count = w.count();
+  // BF16 plans carry their high-variance K-steps as TF32 (Plan::oTf32)
+  constexpr bool TF32 = PREC == PREC_BF16;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -289,6 +291,7 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
       for (int32_t c = 0; c < oNR && ok; ++c) {
         const int32_t rc = min(oRc, nmcBlk - c * oRc);
         const uint32_t idesc = make_idesc(ab, 128u, (uint32_t)(2 * lPad * rc));
+        const uint32_t idescT = make_idesc(2u, 128u, (uint32_t)(2 * lPad * rc));  // A, B TF32
         // both accumulators are free once the epilogue has read the last chunk
         if (!mbar_wait_warp(&bars->acc_empty[0], accPh ^ 1, abort_flag) ||
             !mbar_wait_warp(&bars->acc_empty[1], accPh ^ 1, abort_flag)) {
@@ -320,6 +323,15 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
               mma_ss(tbase, aD + 2 * aU, bD + 2 * bU, idesc, 1u);
               mma_ss(tbase + (uint32_t)kAccCols, aD + 2 * aU + aT, bD + 2 * bU, idesc, 1u);
               mma_ss(tbase, aD + 3 * aU, bD + 3 * bU, idesc, 1u);
+            } else if (pair && TF32) {
+              // K-step 0 in units 0-1 (K 0-7, 8-15 as TF32) of A and B, K-step 1 in units 2-3
+              mma_ss_tf32(tbase, aD, bD, idescT, acc);
+              mma_ss_tf32(tbase, aD + aU, bD + bU, idescT, 1u);
+              mma_ss_tf32(tbase + (uint32_t)kAccCols, aD + aT, bD, idescT, acc);
+              mma_ss_tf32(tbase + (uint32_t)kAccCols, aD + aU + aT, bD + bU, idescT, 1u);
+              mma_ss_tf32(tbase, aD + 2 * aU, bD + 2 * bU, idescT, 1u);
+              mma_ss_tf32(tbase, aD + 3 * aU, bD + 3 * bU, idescT, 1u);
+              mma_ss_tf32(tbase + (uint32_t)kAccCols, aD + 2 * aU + aT, bD + 2 * bU, idescT, 1u);
             } else if (pair) {
               // K-step 0 in units 0-1 (hi, lo) of A and B, K-step 1 in units 2-3
               mma_ss(tbase, aD, bD, idesc, acc);
@@ -338,6 +350,15 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
               for (uint32_t k = 0; k < n; ++k) {
                 const uint32_t f = (fl >> (2 * k)) & 3u, bLo = f & 1u, aLo = f & 2u;
                 const uint32_t ak = k == 0 ? acc : 1u;
+                if (TF32 && f) {  // the plan marks TF32 K-steps in both masks
+                  mma_ss_tf32(tbase, a, b, idescT, ak);
+                  mma_ss_tf32(tbase, a + aU, b + bU, idescT, 1u);
+                  mma_ss_tf32(tbase + (uint32_t)kAccCols, a + aT, b, idescT, ak);
+                  mma_ss_tf32(tbase + (uint32_t)kAccCols, a + aU + aT, b + bU, idescT, 1u);
+                  a += 2 * aU;
+                  b += 2 * bU;
+                  continue;
+                }
                 mma_ss(tbase, a, b, idesc, ak);
                 mma_ss_if(tbase, a, b + bU, idesc, 1u, bLo);
                 mma_ss_if(tbase, a + aU, b, idesc, 1u, aLo);
@@ -352,6 +373,7 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
           ready = __all_sync(0xffffffffu, more && mbar_test_wait(&bars->full[sn], phn));
           if (leader) {
             if (quad) mma_ss(tbase + (uint32_t)kAccCols, aD + 3 * aU + aT, bD + 3 * bU, idesc, 1u);
+            else if (pair && TF32) mma_ss_tf32(tbase + (uint32_t)kAccCols, aD + 3 * aU + aT, bD + 3 * bU, idescT, 1u);
             else if (pair) mma_ss(tbase + (uint32_t)kAccCols, aD + 2 * aU + aT, bD + 2 * bU, idesc, 1u);
             mma_commit(&bars->empty[s]);
           }
@@ -437,17 +459,29 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
                 break;
               }
               float2 pv[8];
-              uint32_t hi[8];
 #pragma unroll
               for (int u = 0; u < 8; ++u) {
                 const float2 q = e1[u];
                 pv[u] = make_float2(q.x * E.x - q.y * E.y, q.x * E.y + q.y * E.x);
-                hi[u] = pack16<PREC>(pv[u].x, pv[u].y);
               }
               unsigned char* A = slots + (size_t)s * slotBytes + ua * kAUnitBytes + t * kATileBytes + rowOff;
-              *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-              *reinterpret_cast<uint4*>(A + 2048) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
-              if (aLo) {  // the residual of the 16-bit rounding, rounded again, in the next unit
+              uint32_t hi[8];
+              if (TF32 && aLo) {
+                // TF32 K-step: unit 0 holds groups 0-3 (K 0-7), unit 1 groups
+                // 4-7, each unit's core-matrix columns two groups (re, im)
+#pragma unroll
+                for (int h2 = 0; h2 < 4; ++h2) {
+                  const float2 p0 = pv[2 * h2], p1 = pv[2 * h2 + 1];
+                  *reinterpret_cast<uint4*>(A + (h2 >> 1) * kAUnitBytes + (h2 & 1) * 2048) =
+                      make_uint4(tf32_bits(p0.x), tf32_bits(p0.y), tf32_bits(p1.x), tf32_bits(p1.y));
+                }
+              } else {
+#pragma unroll
+                for (int u = 0; u < 8; ++u) hi[u] = pack16<PREC>(pv[u].x, pv[u].y);
+                *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+                *reinterpret_cast<uint4*>(A + 2048) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+              }
+              if (!TF32 && aLo) {  // the residual of the 16-bit rounding, rounded again, in the next unit
                 uint32_t lo[8];
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
