@@ -24,8 +24,11 @@
 // realization block is cut into N chunks of oRc realizations (TMEM: one
 // 256-column accumulator per tile); for each chunk the K-steps (16 K = 8
 // outer groups of consecutive i1) stream through a ring of shared-memory
-// stages, each holding two to four consecutive K-steps: both tiles' A (hi,
-// and lo where the plan keeps it) and B's K-step blocks (hi, and lo).
+// stages, each holding two to four consecutive K-steps: both tiles' A and
+// B's K-step blocks.  BF16 plans carry the K-steps of the largest variance
+// share as TF32 (Plan::oTf32): two A units and two B blocks hold the K-step's
+// 16 K values in 32-bit containers, and two kind::tf32 MMAs (K = 8) per tile
+// replace the one BF16 MMA.
 //
 // Warp roles (576 threads):
 //   warp 0      MMA issuer: the warp runs the stage loop, one elected lane
@@ -35,7 +38,7 @@
 //               a stage's B blocks from HBM/L2 into the ring;
 //   warps 2-9   generators: one point each (256 = two tiles); per K-step the
 //               8 outer phasors E1(i1) E2(i2)^{s2} of the point, rounded to
-//               16 bits (and the lo residual), stored in the K-major core-
+//               16 bits (or to TF32), stored in the K-major core-
 //               matrix layout; the K-steps run axis-1 block by block (E1 of
 //               the block's 8 i1 from FP64-reduced phases), E2 walked by
 //               angle addition over i2;
@@ -67,7 +70,8 @@ constexpr int kAccCols = 256;  // accumulator columns per tile
 // when it issues about eight or more MMAs per loop pass (measured on this
 // kernel's MMA shape: 4 MMAs per pass ran at 1.4x the pipe's time per MMA,
 // 8 at 1.03x, 12 at 1.0x, whatever the pass did besides), and a stage of
-// four K-steps without lo terms carries 8, one of two K-steps with both 12.
+// four 16-bit K-steps carries 8, one of two TF32 K-steps 8 of twice the
+// length.
 constexpr int kAUnitBytes = 2 * kATileBytes;                    // both tiles' hi A of one K-step
 constexpr int kStageABytes = kOuterStageUnits * kAUnitBytes;    // A area of a stage
 
@@ -155,15 +159,6 @@ template <int PREC>
 __device__ __forceinline__ uint32_t pack16(float lo, float hi) {
   return PREC == PREC_FP16 ? pack_f16x2(lo, hi) : pack_bf16x2(lo, hi);
 }
-// The 16-bit values of a packed pair back in FP32.
-template <int PREC>
-__device__ __forceinline__ float2 unpack16(uint32_t w) {
-  if (PREC == PREC_FP16) {
-    const __half2 h = *reinterpret_cast<const __half2*>(&w);
-    return __half22float2(h);
-  }
-  return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
-}
 
 // The pipeline of one CTA over the work items of `w`.  LPAD: axis-3 length
 // padded to 8, 16, 24 or 32 (every item of a launch has this lPad).
@@ -250,12 +245,11 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
     // The whole warp runs the loop (warp-uniform state); one elected lane
     // issues.  A stage's MMAs go out back to back, and the next stage's
     // barrier is probed before the last MMA so that the wait proper runs only
-    // when the probe failed.  Stages of four K-steps without lo terms and of
-    // two K-steps with both (nearly all of them: the lo K-steps are the top
-    // of a variance ranking and come in runs) take straight paths, whose last
-    // MMA is a tile-1 hi MMA that may accumulate in any order (acc = 1) and
-    // so goes after the probe; other stages loop over their K-steps with the
-    // lo terms under a guard predicate.
+    // when the probe failed.  Stages of four 16-bit K-steps and of two TF32
+    // ones (nearly all of them: the TF32 K-steps are the top of a variance
+    // ranking and come in runs) take straight paths, whose last MMA is a
+    // tile-1 MMA that may accumulate in any order (acc = 1) and so goes after
+    // the probe; other stages loop over their K-steps.
     const bool leader = elect_one();
     uint32_t s = 0, ph = 0, accPh = 0;
     bool ok = true, ready = false;  // ready: full[s] of the next stage already observed
@@ -323,7 +317,7 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
               mma_ss(tbase, aD + 2 * aU, bD + 2 * bU, idesc, 1u);
               mma_ss(tbase + (uint32_t)kAccCols, aD + 2 * aU + aT, bD + 2 * bU, idesc, 1u);
               mma_ss(tbase, aD + 3 * aU, bD + 3 * bU, idesc, 1u);
-            } else if (pair && TF32) {
+            } else if (TF32 && pair) {
               // K-step 0 in units 0-1 (K 0-7, 8-15 as TF32) of A and B, K-step 1 in units 2-3
               mma_ss_tf32(tbase, aD, bD, idescT, acc);
               mma_ss_tf32(tbase, aD + aU, bD + bU, idescT, 1u);
@@ -332,49 +326,31 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
               mma_ss_tf32(tbase, aD + 2 * aU, bD + 2 * bU, idescT, 1u);
               mma_ss_tf32(tbase, aD + 3 * aU, bD + 3 * bU, idescT, 1u);
               mma_ss_tf32(tbase + (uint32_t)kAccCols, aD + 2 * aU + aT, bD + 2 * bU, idescT, 1u);
-            } else if (pair) {
-              // K-step 0 in units 0-1 (hi, lo) of A and B, K-step 1 in units 2-3
-              mma_ss(tbase, aD, bD, idesc, acc);
-              mma_ss(tbase, aD, bD + bU, idesc, 1u);
-              mma_ss(tbase, aD + aU, bD, idesc, 1u);
-              mma_ss(tbase + (uint32_t)kAccCols, aD + aT, bD, idesc, acc);
-              mma_ss(tbase + (uint32_t)kAccCols, aD + aT, bD + bU, idesc, 1u);
-              mma_ss(tbase + (uint32_t)kAccCols, aD + aU + aT, bD, idesc, 1u);
-              mma_ss(tbase, aD + 2 * aU, bD + 2 * bU, idesc, 1u);
-              mma_ss(tbase, aD + 2 * aU, bD + 3 * bU, idesc, 1u);
-              mma_ss(tbase, aD + 3 * aU, bD + 2 * bU, idesc, 1u);
-              mma_ss(tbase + (uint32_t)kAccCols, aD + 2 * aU + aT, bD + 3 * bU, idesc, 1u);
-              mma_ss(tbase + (uint32_t)kAccCols, aD + 3 * aU + aT, bD + 2 * bU, idesc, 1u);
             } else {
               uint64_t a = aD, b = bD;
               for (uint32_t k = 0; k < n; ++k) {
-                const uint32_t f = (fl >> (2 * k)) & 3u, bLo = f & 1u, aLo = f & 2u;
+                const uint32_t f = (fl >> (2 * k)) & 3u;  // both set on a TF32 K-step
                 const uint32_t ak = k == 0 ? acc : 1u;
-                if (TF32 && f) {  // the plan marks TF32 K-steps in both masks
+                if (TF32 && f) {
                   mma_ss_tf32(tbase, a, b, idescT, ak);
                   mma_ss_tf32(tbase, a + aU, b + bU, idescT, 1u);
                   mma_ss_tf32(tbase + (uint32_t)kAccCols, a + aT, b, idescT, ak);
                   mma_ss_tf32(tbase + (uint32_t)kAccCols, a + aU + aT, b + bU, idescT, 1u);
                   a += 2 * aU;
                   b += 2 * bU;
-                  continue;
+                } else {
+                  mma_ss(tbase, a, b, idesc, ak);
+                  mma_ss(tbase + (uint32_t)kAccCols, a + aT, b, idesc, ak);
+                  a += aU;
+                  b += bU;
                 }
-                mma_ss(tbase, a, b, idesc, ak);
-                mma_ss_if(tbase, a, b + bU, idesc, 1u, bLo);
-                mma_ss_if(tbase, a + aU, b, idesc, 1u, aLo);
-                mma_ss(tbase + (uint32_t)kAccCols, a + aT, b, idesc, ak);
-                mma_ss_if(tbase + (uint32_t)kAccCols, a + aT, b + bU, idesc, 1u, bLo);
-                mma_ss_if(tbase + (uint32_t)kAccCols, a + aU + aT, b, idesc, 1u, aLo);
-                a += aLo ? 2 * aU : aU;
-                b += bLo ? 2 * bU : bU;
               }
             }
           }
           ready = __all_sync(0xffffffffu, more && mbar_test_wait(&bars->full[sn], phn));
           if (leader) {
             if (quad) mma_ss(tbase + (uint32_t)kAccCols, aD + 3 * aU + aT, bD + 3 * bU, idesc, 1u);
-            else if (pair && TF32) mma_ss_tf32(tbase + (uint32_t)kAccCols, aD + 3 * aU + aT, bD + 3 * bU, idescT, 1u);
-            else if (pair) mma_ss(tbase + (uint32_t)kAccCols, aD + 2 * aU + aT, bD + 2 * bU, idesc, 1u);
+            else if (TF32 && pair) mma_ss_tf32(tbase + (uint32_t)kAccCols, aD + 3 * aU + aT, bD + 3 * bU, idescT, 1u);
             mma_commit(&bars->empty[s]);
           }
           __syncwarp();
@@ -424,7 +400,7 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
       const float2 e1step = axis_phasor(P.kDelta[0], 8, x0);
       for (int32_t c = 0; c < oNR && ok; ++c) {
         // K-steps in order j = 0, 1, ... (i2 fastest, then s2, then jj);
-        // the A lo and stage-end flags read 32 at a time
+        // the TF32 and stage-end flags read 32 at a time
         int32_t j = 0;
         uint32_t aw = 0, ew = 0;
         float2 e1cur[8];
@@ -450,7 +426,7 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
                 aw = P.aLoMask[j >> 5];
                 ew = P.oStageEnd[j >> 5];
               }
-              const bool aLo = (aw >> (j & 31)) & 1u, end = (ew >> (j & 31)) & 1u;
+              const bool tf = (aw >> (j & 31)) & 1u, end = (ew >> (j & 31)) & 1u;  // a TF32 K-step
               // A stage is written once its barrier says the MMAs have
               // released it; the proxy fence and the arrival are paid once
               // per stage, after its last K-step.
@@ -465,8 +441,7 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
                 pv[u] = make_float2(q.x * E.x - q.y * E.y, q.x * E.y + q.y * E.x);
               }
               unsigned char* A = slots + (size_t)s * slotBytes + ua * kAUnitBytes + t * kATileBytes + rowOff;
-              uint32_t hi[8];
-              if (TF32 && aLo) {
+              if (TF32 && tf) {
                 // TF32 K-step: unit 0 holds groups 0-3 (K 0-7), unit 1 groups
                 // 4-7, each unit's core-matrix columns two groups (re, im)
 #pragma unroll
@@ -476,22 +451,13 @@ __device__ __forceinline__ void outer_body(const Work& w, int S, int32_t slotByt
                       make_uint4(tf32_bits(p0.x), tf32_bits(p0.y), tf32_bits(p1.x), tf32_bits(p1.y));
                 }
               } else {
+                uint32_t hi[8];
 #pragma unroll
                 for (int u = 0; u < 8; ++u) hi[u] = pack16<PREC>(pv[u].x, pv[u].y);
                 *reinterpret_cast<uint4*>(A) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
                 *reinterpret_cast<uint4*>(A + 2048) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
               }
-              if (!TF32 && aLo) {  // the residual of the 16-bit rounding, rounded again, in the next unit
-                uint32_t lo[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                  const float2 h = unpack16<PREC>(hi[u]);
-                  lo[u] = pack16<PREC>(pv[u].x - h.x, pv[u].y - h.y);
-                }
-                *reinterpret_cast<uint4*>(A + kAUnitBytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-                *reinterpret_cast<uint4*>(A + kAUnitBytes + 2048) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
-              }
-              ua += aLo ? 2u : 1u;
+              ua += tf ? 2u : 1u;
               if (end) {
                 ua = 0;
                 fence_proxy_async_smem();

@@ -21,9 +21,7 @@
 // BF16 plans (oTf32) carry the K-steps of the largest variance share as
 // TF32: both A units of such a K-step hold its 16 K values in FP32
 // containers (groups 0-3, then 4-7), both B blocks likewise, and the issuer
-// runs two kind::tf32 MMAs (K = 8) per half where a hi/lo K-step takes three
-// BF16 ones; the TF32 rounding (10 bits) of both operands costs the field
-// less than the BF16 hi/lo split's residual on the other K-steps.
+// runs two kind::tf32 MMAs (K = 8) per half where a BF16 K-step takes one.
 //
 // Warp roles (448 threads, in each CTA: 14 warps leave a thread 128
 // registers):
@@ -37,9 +35,9 @@
 //   warps 2-5   generators: one thread per point of the CTA's tile, the
 //               K-step's 8 outer phasors (E1 of block 0 and the block step
 //               from FP64-reduced phases once per item, later blocks and E2
-//               by angle addition), the lo residual where the plan keeps it,
-//               or the TF32 values of a TF32 K-step; driven by the stage
-//               table, four hi-only K-steps (or two TF32 ones) straight-line
+//               by angle addition), rounded to 16 bits or, on a TF32
+//               K-step, to TF32; driven by the stage table, four 16-bit
+//               K-steps (or two TF32 ones) straight-line
 //               (8 generator warps with half the phasors each measured 3 %
 //               slower);
 //   warps 6-13  epilogue: tcgen05.ld of one N half's accumulator (warp % 4
@@ -175,16 +173,6 @@ __device__ __forceinline__ void mma_pair(uint32_t d_tmem, uint64_t a_desc, uint6
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
-__device__ __forceinline__ void mma_pair_if(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
-                                            uint32_t accumulate, uint32_t issue) {
-  asm volatile(
-      "{\n\t.reg .pred p, g;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "setp.ne.b32 g, %5, 0;\n\t"
-      "@g tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(issue)
-      : "memory");
-}
 // The same MMA of kind::tf32 (K = 8: A and B rows of 32 bytes, two TF32
 // core-matrix columns, as one K = 16 step of the 16-bit kinds).
 __device__ __forceinline__ void mma_pair_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
@@ -233,29 +221,6 @@ __device__ __forceinline__ void gen_hi(unsigned char* A, const float2* e1, float
   *reinterpret_cast<uint4*>(A) = make_uint4(h[0], h[1], h[2], h[3]);
   *reinterpret_cast<uint4*>(A + 2048) = make_uint4(h[4], h[5], h[6], h[7]);
 }
-// The lo unit: the residual of the 16-bit rounding, rounded again.
-template <int PREC>
-__device__ __forceinline__ void gen_lo(unsigned char* A, const float2* e1, float2 E) {
-  uint32_t l[8];
-#pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    const float2 v = cmulf(e1[u], E);
-    float hx, hy;
-    if (PREC == PREC_FP16) {
-      const __half2 hv = __floats2half2_rn(v.x, v.y);
-      const float2 f = __half22float2(hv);
-      hx = f.x;
-      hy = f.y;
-    } else {
-      const uint32_t hb = pack_bf16x2(v.x, v.y);
-      hx = __uint_as_float(hb << 16);
-      hy = __uint_as_float(hb & 0xffff0000u);
-    }
-    l[u] = PREC == PREC_FP16 ? pack_f16x2(v.x - hx, v.y - hy) : pack_bf16x2(v.x - hx, v.y - hy);
-  }
-  *reinterpret_cast<uint4*>(A) = make_uint4(l[0], l[1], l[2], l[3]);
-  *reinterpret_cast<uint4*>(A + 2048) = make_uint4(l[4], l[5], l[6], l[7]);
-}
 // A TF32 K-step's two units: unit 0 groups 0-3 (K 0-7), unit 1 groups 4-7,
 // each unit's core-matrix columns two groups (re, im) in FP32 containers.
 __device__ __forceinline__ void gen_tf32(unsigned char* A, const float2* e1, float2 E) {
@@ -303,7 +268,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     mbar_init(&bars->dealloc_ok, 1);
     bars->abort_flag = 0;
     // the stage table (issuer and generators): first K-step (9 bits), K-steps
-    // (3 bits), per K-step the B and A lo (TF32) flags; a stage must not span
+    // (3 bits), per K-step two TF32 flags (B, A); a stage must not span
     // the end of an i2 run (outer_stage_layout closes one there)
     int32_t ns = 0, j0 = 0, n = 0;
     uint32_t fl = 0;
@@ -452,7 +417,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
               mma_pair(t0, aD + 2 * aU, bD + 2 * bU, idesc, 1u);
               mma_pair(t1, aD + 2 * aU, bD + 2 * bU + bH, idesc, 1u);
               mma_pair(t0, aD + 3 * aU, bD + 3 * bU, idesc, 1u);
-            } else if (pair && TF32) {
+            } else if (TF32 && pair) {
               // K-step 0 in units 0-1 (K 0-7, 8-15 as TF32) of A and B, K-step 1 in units 2-3
               mma_pair_tf32(t0, aD, bD, idescT, acc);
               mma_pair_tf32(t0, aD + aU, bD + bU, idescT, 1u);
@@ -461,49 +426,31 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
               mma_pair_tf32(t0, aD + 2 * aU, bD + 2 * bU, idescT, 1u);
               mma_pair_tf32(t0, aD + 3 * aU, bD + 3 * bU, idescT, 1u);
               mma_pair_tf32(t1, aD + 2 * aU, bD + 2 * bU + bH, idescT, 1u);
-            } else if (pair) {
-              // K-step 0 in units 0-1 (hi, lo) of A and B, K-step 1 in units 2-3
-              mma_pair(t0, aD, bD, idesc, acc);
-              mma_pair(t0, aD, bD + bU, idesc, 1u);
-              mma_pair(t0, aD + aU, bD, idesc, 1u);
-              mma_pair(t1, aD, bD + bH, idesc, acc);
-              mma_pair(t1, aD, bD + bU + bH, idesc, 1u);
-              mma_pair(t1, aD + aU, bD + bH, idesc, 1u);
-              mma_pair(t0, aD + 2 * aU, bD + 2 * bU, idesc, 1u);
-              mma_pair(t0, aD + 2 * aU, bD + 3 * bU, idesc, 1u);
-              mma_pair(t0, aD + 3 * aU, bD + 2 * bU, idesc, 1u);
-              mma_pair(t1, aD + 2 * aU, bD + 3 * bU + bH, idesc, 1u);
-              mma_pair(t1, aD + 3 * aU, bD + 2 * bU + bH, idesc, 1u);
             } else {
               uint64_t ad = aD, bd = bD;
               for (uint32_t k = 0; k < n; ++k) {
-                const uint32_t f = (fl >> (2 * k)) & 3u, bLo = f & 1u, aLo = f & 2u;
+                const uint32_t f = (fl >> (2 * k)) & 3u;  // both set on a TF32 K-step
                 const uint32_t ak = k == 0 ? acc : 1u;
-                if (TF32 && f) {  // the plan marks TF32 K-steps in both masks
+                if (TF32 && f) {
                   mma_pair_tf32(t0, ad, bd, idescT, ak);
                   mma_pair_tf32(t0, ad + aU, bd + bU, idescT, 1u);
                   mma_pair_tf32(t1, ad, bd + bH, idescT, ak);
                   mma_pair_tf32(t1, ad + aU, bd + bU + bH, idescT, 1u);
                   ad += 2 * aU;
                   bd += 2 * bU;
-                  continue;
+                } else {
+                  mma_pair(t0, ad, bd, idesc, ak);
+                  mma_pair(t1, ad, bd + bH, idesc, ak);
+                  ad += aU;
+                  bd += bU;
                 }
-                mma_pair(t0, ad, bd, idesc, ak);
-                mma_pair_if(t0, ad, bd + bU, idesc, 1u, bLo);
-                mma_pair_if(t0, ad + aU, bd, idesc, 1u, aLo);
-                mma_pair(t1, ad, bd + bH, idesc, ak);
-                mma_pair_if(t1, ad, bd + bU + bH, idesc, 1u, bLo);
-                mma_pair_if(t1, ad + aU, bd + bH, idesc, 1u, aLo);
-                ad += aLo ? 2 * aU : aU;
-                bd += bLo ? 2 * bU : bU;
               }
             }
           }
           ready = __all_sync(0xffffffffu, more && mbar_test_wait_cluster(&bars->full[sn], phn));
           if (leader) {
             if (quad) mma_pair(t1, aD + 3 * aU, bD + 3 * bU + bH, idesc, 1u);
-            else if (pair && TF32) mma_pair_tf32(t1, aD + 3 * aU, bD + 3 * bU + bH, idescT, 1u);
-            else if (pair) mma_pair(t1, aD + 2 * aU, bD + 2 * bU + bH, idesc, 1u);
+            else if (TF32 && pair) mma_pair_tf32(t1, aD + 3 * aU, bD + 3 * bU + bH, idescT, 1u);
             mma_commit_pair_both(&bars->empty[s]);
           }
           __syncwarp();
@@ -591,15 +538,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
           } else {
             uint32_t ua = 0;  // A units of the stage already written
             for (int32_t k = 0; k < n; ++k) {
-              const bool aLo = (fl >> (2 * k + 1)) & 1u;
+              const bool tf = (fl >> (2 * k + 1)) & 1u;  // a TF32 K-step
               const float2 E = make_float2(e2.x, sg * e2.y);
-              if (TF32 && aLo) {
-                gen_tf32(A + ua * kPAUnitBytes, e1, E);
-              } else {
-                gen_hi<PREC>(A + ua * kPAUnitBytes, e1, E);
-                if (aLo) gen_lo<PREC>(A + (ua + 1) * kPAUnitBytes, e1, E);
-              }
-              ua += aLo ? 2u : 1u;
+              if (TF32 && tf) gen_tf32(A + ua * kPAUnitBytes, e1, E);
+              else gen_hi<PREC>(A + ua * kPAUnitBytes, e1, E);
+              ua += tf ? 2u : 1u;
               e2 = cmulf(e2, e2step);
             }
           }

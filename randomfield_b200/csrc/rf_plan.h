@@ -90,9 +90,11 @@ struct Plan {
   // tensor-core forms).  K = 2 x outer groups g = (i1, i2, s2) (re, im of
   // E1 E2^{s2}), in K-steps of 16 = 8 groups of consecutive i1; N chunk c
   // = realizations [c oRc, (c+1) oRc) of the block, each 2 lPad columns
-  // (i3, cos|sin).  B of chunk c is oNK K-step blocks of oKstepBytes (hi),
-  // each followed by its lo block where bit j of loMask is set; A carries its
-  // lo term on the K-steps of aLoMask.
+  // (i3, cos|sin).  B of chunk c is oNK K-step blocks of oKstepBytes, each
+  // followed by a second block where bit j of loMask is set; A takes two
+  // units on the K-steps of aLoMask.  The BF16 form sets both masks on its
+  // TF32 K-steps (oTf32): the two blocks and units hold K 0-7 and K 8-15 in
+  // 32-bit containers.
   int32_t n1p;                // axis-1 wavenumbers padded to a multiple of 8 (8, 16, 24)
   int32_t oRc;                // realizations per N chunk
   int32_t oNR;                // N chunks of the realization block
@@ -108,9 +110,8 @@ struct Plan {
   // then rank 1's, each its oNK K-step blocks of oKstepBytes (half 0's rows,
   // then half 1's), each followed by its lo block where loMask says.
   int32_t oPair;
-  // CTA-pair form, BF16: the K-steps of aLoMask (= loMask) carry A and B as
-  // TF32 (kind::tf32, two MMAs of K = 8 in the two units of a hi/lo K-step)
-  // instead of BF16 hi/lo pairs (three MMAs of K = 16)
+  // BF16: the K-steps of aLoMask (= loMask) carry A and B as TF32
+  // (kind::tf32, two MMAs of K = 8 over the K-step's two units and blocks)
   int32_t oTf32;
   int64_t oStepM1, oStepM2;   // rnglib multipliers a^(n1 n2 n3) mod m: the s3 = - draw from the s3 = + one
   // GEN_TABLE, BF16 single requests: the trig tile also carries its lo term

@@ -9,7 +9,7 @@ into seconds of BLAS.  It is pinned here on the CPU against the oracle's
 point-by-point sum (rfo_generate) on rows of the same 128^3 workload and on
 small grids in 1-D to 3-D; the GPU tests then compare all 134 M values of the
 BF16 and FP16 forms (relative-L2 <= 2e-3 overall and for every
-realization; the BF16 form, the outer-group contraction with its hi/lo terms,
+realization; the BF16 form, the outer-group contraction with its TF32 K-steps,
 also within 1.5e-3 for every realization, its margin under the bound) and of
 the structured-grid path (<= 1e-11).
 """

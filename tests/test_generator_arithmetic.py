@@ -227,12 +227,14 @@ def _errors(f, exact):
 
 
 def test_outer_group_bf16_error_budget():
-    """The BF16 form of the outer-group contraction (rf_outer.cu) emulated on
-    the 128^3 workload (24^3 x 4 wavevectors, corrL (2, 1, 0.5), Nmc 64) on a
+    """A BF16 hi/lo split of the outer-group operands (the alternative the
+    TF32 K-steps of rf_outer.cu are measured against) emulated on the 128^3
+    workload (24^3 x 4 wavevectors, corrL (2, 1, 0.5), Nmc 64) on a
     sample of 96 point columns x 128 points: A = the outer phasors and W = the
     coefficients rounded to BF16, each with its lo term (the rounding residual,
     rounded again) on the K-steps that carry all but 30 % of the field variance,
-    ranked as rf_host.cu outer_layout ranks them; the epilogue's i3 sum exact.
+    ranked as rf_host.cu outer_rank_masks ranks them; the epilogue's i3 sum
+    exact.
     Without lo terms the relative L2 error is about 2.1e-3 (above the 2e-3
     bound); with them it is about 1.2e-3, the worst realization under 1.5e-3."""
     A, W, w, field, exact, kmask = _outer_sample()
@@ -246,8 +248,8 @@ def test_outer_group_bf16_error_budget():
 
 
 def test_outer_group_tf32_error_budget():
-    """The CTA-pair form's BF16 plans (rf_outer_pair.cu, oTf32): the K-steps
-    carrying all but 25 % of the variance take A and W rounded to TF32 (two
+    """The BF16 outer-group plans (rf_outer.cu, rf_outer_pair.cu, oTf32):
+    the K-steps carrying all but 25 % of the variance take A and W rounded to TF32 (two
     kind::tf32 MMAs of K = 8, the values rounded by tf32_bits as the generators
     and rf_tables.cu outer_run round them), the others A and W rounded to BF16
     alone.  Relative L2 about 1.08e-3, worst realization about 1.17e-3: below

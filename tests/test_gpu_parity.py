@@ -3,7 +3,7 @@ oracle on the same seeded inputs.
 
 Tolerances (stated here and in the bench):
   plain FP32 form      max-abs <= 1e-5 * field std
-  BF16 form (hi/lo B)  relative-L2 <= 2e-3 per realization
+  BF16 form           relative-L2 <= 2e-3 per realization (TF32 K-steps, or hi/lo B rows)
   FP16 form            relative-L2 <= 2e-3 per realization
   BF16 fast form       relative-L2 <= 3e-3 (single BF16 amplitude side)
   FP8 e4m3 form        relative-L2 <= 5e-2 (stated option: 3 significand bits in the trig tile)
