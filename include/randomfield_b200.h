@@ -34,7 +34,8 @@ extern "C" {
 #define RF_FOM_LOGNORMAL 2
 
 /* Precision forms of the contraction. */
-#define RF_PREC_BF16 0      /* BF16 trig tiles, hi/lo BF16 amplitude side, tcgen05 (default) */
+#define RF_PREC_BF16 0      /* BF16 operands on tcgen05 (default): hi/lo BF16 amplitude rows where a trig tile is
+                               generated, TF32 on the high-variance K-steps of the outer-group contraction */
 #define RF_PREC_FP16 1      /* FP16 trig tiles and scaled FP16 amplitude side, tcgen05     */
 #define RF_PREC_FP32 2      /* plain FP32 operands on the FFMA pipes                       */
 #define RF_PREC_BF16_FAST 3 /* BF16 trig tiles, single BF16 amplitude side, tcgen05        */
