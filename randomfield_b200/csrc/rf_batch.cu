@@ -51,7 +51,7 @@ double outer_pair_cost(const Plan& P) {
 // two grouped kernels (tcgen05 contraction; outer-group contraction) its CTA
 // slices and work items.
 struct DescLayout {
-  size_t subs, prefix, cta, items, octa, oitems, total;
+  size_t subs, prefix, stab, nst, cta, items, octa, oitems, total;
   size_t capUnits, capItems;
 };
 
@@ -61,7 +61,9 @@ DescLayout desc_layout(size_t capUnits, size_t capItems, int numSMs) {
   d.capItems = capItems;
   d.subs = kAlign;  // header: the unit count
   d.prefix = d.subs + align_up(capUnits * sizeof(GroupSub));
-  d.cta = d.prefix + align_up((capUnits + 1) * sizeof(int64_t));
+  d.stab = d.prefix + align_up((capUnits + 1) * sizeof(int64_t));  // outer-group units' stage tables
+  d.nst = d.stab + align_up(capUnits * kOuterMaxKsteps * sizeof(uint32_t));
+  d.cta = d.nst + align_up(capUnits * sizeof(int32_t));
   d.items = d.cta + align_up((size_t)(numSMs + 1) * sizeof(int32_t));
   d.octa = d.items + align_up(capItems * sizeof(GroupItem));
   d.oitems = d.octa + align_up((size_t)(numSMs + 1) * sizeof(int32_t));
@@ -128,7 +130,7 @@ struct GroupRun {
   int rblk = 0;
   SlotLayout L{};
   size_t smem = 0;
-  OuterGroupArgs og{};  // slot layout of the outer-group kernel
+  OuterPairGroupArgs og{};  // slot layout of the outer-group kernel (CTA pairs)
   size_t osmem = 0;
   int64_t units = 0, items = 0;
   bool replayed = false;
@@ -173,7 +175,10 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, int sTc, i
       if (int rc = layout(P)) return rc;
       if (!B.blend.empty() && B.blend[i].gTotal > 0) apply_blend(P, B.blend[i]);
       lo_layout(P);
-      if (P.gen == GEN_GRID3 && P.lPad == kGroupLPad) outer_layout(P);  // the outer-group kernel
+      if (P.gen == GEN_GRID3 && P.lPad == kGroupLPad) {  // the outer-group kernel, on CTA pairs
+        outer_layout(P);
+        outer_pair_layout(P, true);
+      }
       GroupSub g;
       memset(&g, 0, sizeof(g));
       P.dbgErr = c->dErr;
@@ -213,7 +218,7 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, int sTc, i
     if (run.smem == 0) return fail(RF_ENOTSUP, "grouped launch: stages of %lld bytes do not fit", (long long)maxStage);
   }
   if (!outerUnits.empty()) {
-    run.osmem = outer_group_layout(outerPlans.data(), outerPlans.size(), sOuter, &run.og);
+    run.osmem = outer_pair_group_layout(outerPlans.data(), outerPlans.size(), sOuter, &run.og);
     if (run.osmem == 0) return fail(RF_ENOTSUP, "grouped launch: outer-group slots do not fit");
   }
 
@@ -231,9 +236,9 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, int sTc, i
 
   // ---- schedules: LPT over each kernel's items (tiles; pairs of tiles for
   // the outer-group kernel), longest units first
-  const int nCta = c->numSMs;
+  const int nCta = c->numSMs, nPairs = c->numSMs / 2;
   const auto perCta = lpt_schedule(tcUnits, tiles, tileCost, nCta);
-  const auto perCtaO = lpt_schedule(outerUnits, tiles, tileCost, nCta);
+  const auto perCtaO = lpt_schedule(outerUnits, tiles, tileCost, nPairs);
   int64_t nItems = 0, nItemsO = 0;
   for (size_t u : tcUnits) nItems += tiles[u];
   for (size_t u : outerUnits) nItemsO += tiles[u];
@@ -263,6 +268,11 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, int sTc, i
   int64_t* pre = reinterpret_cast<int64_t*>(h + D.prefix);
   pre[0] = 0;
   for (size_t u = 0; u < nU; ++u) pre[u + 1] = pre[u] + elems[u];
+  uint32_t* stabs = reinterpret_cast<uint32_t*>(h + D.stab);
+  int32_t* nst = reinterpret_cast<int32_t*>(h + D.nst);
+  for (size_t u : outerUnits)
+    if (!pair_group_stage_table(subs[u].P, stabs + u * kOuterMaxKsteps, nst + u))
+      return fail(RF_ENOTSUP, "grouped launch: unit %d has no CTA-pair stage table", (int)u);
   put_schedule(perCta, reinterpret_cast<int32_t*>(h + D.cta), reinterpret_cast<GroupItem*>(h + D.items));
   put_schedule(perCtaO, reinterpret_cast<int32_t*>(h + D.octa), reinterpret_cast<GroupItem*>(h + D.oitems));
   RF_CUDA(cudaMemcpyAsync(c->dDesc, h, D.oitems + (size_t)nItemsO * sizeof(GroupItem), cudaMemcpyHostToDevice, st),
@@ -275,10 +285,12 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, int sTc, i
   g.ctaStart = reinterpret_cast<const int32_t*>(c->dDesc + D.cta);
   g.err = c->dErr;
   g.L = run.L;
-  OuterGroupArgs og = run.og;
+  OuterPairGroupArgs og = run.og;
   og.subs = g.subs;
   og.items = reinterpret_cast<const GroupItem*>(c->dDesc + D.oitems);
   og.ctaStart = reinterpret_cast<const int32_t*>(c->dDesc + D.octa);
+  og.stabs = reinterpret_cast<const uint32_t*>(c->dDesc + D.stab);
+  og.nStages = reinterpret_cast<const int32_t*>(c->dDesc + D.nst);
   og.err = c->dErr;
   const bool hasTc = !tcUnits.empty(), hasOuter = !outerUnits.empty();
   const GroupSub* dSubs = g.subs;
@@ -287,9 +299,9 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, int sTc, i
   for (auto& e : c->bev)
     if (!e) RF_CUDA(cudaEventCreate(&e), "cudaEventCreate");
   if (hasTc) RF_CUDA(group_set_smem(prec, run.smem), "grouped kernel attributes");
-  if (hasOuter) RF_CUDA(outer_group_set_smem(prec, run.osmem), "outer-group kernel attributes");
+  if (hasOuter) RF_CUDA(outer_pair_group_set_smem(prec, run.osmem), "outer-group kernel attributes");
   rf_context::GraphKey key{prec,          hasTc ? run.L.S : 0, hasTc ? run.L.aCol0 : 0, hasTc ? run.L.slotBytes : 0,
-                           hasOuter ? og.S : 0, hasOuter ? og.slotBytes : 0, hasOuter ? og.aBytes : 0,
+                           hasOuter ? og.S : 0, hasOuter ? og.slotBytes : 0, 0,
                            hasTc ? 1 : 0, c->dDesc};
   auto found = c->graphs.find(key);
   cudaGraphExec_t exec = nullptr;
@@ -303,7 +315,7 @@ int group_run(rf_context* c, const BatchState& B, int prec, int rblk, int sTc, i
     cudaError_t e2 = launch_group_tables(dSubs, dPrefix, dCount, jump_table(), nCta * 8, st);
     cudaError_t e3 = cudaEventRecordWithFlags(c->bev[1], st, cudaEventRecordExternal);
     cudaError_t e4 = hasTc ? launch_group(prec, g, run.smem, nCta, st) : cudaSuccess;
-    cudaError_t e4o = hasOuter ? launch_outer_group(prec, og, run.osmem, nCta, st) : cudaSuccess;
+    cudaError_t e4o = hasOuter ? launch_outer_pair_group(prec, og, run.osmem, 2 * nPairs, st) : cudaSuccess;
     cudaError_t e5 = cudaEventRecordWithFlags(c->bev[2], st, cudaEventRecordExternal);
     cudaError_t ee = cudaStreamEndCapture(st, &graph);
     for (cudaError_t e : {e1, e2, e3, e4, e4o, e5, ee})
@@ -478,7 +490,10 @@ int request_footprint(const Request& rq, const double* ext, int rblk, size_t* by
     P.nmcBlk = std::min(rblk, P0.Nmc - r0);
     if (int rc = layout(P)) return rc;
     lo_layout(P);
-    if (P.gen == GEN_GRID3 && P.lPad == kGroupLPad) outer_layout(P);  // as group_run plans it
+    if (P.gen == GEN_GRID3 && P.lPad == kGroupLPad) {  // as group_run plans it
+      outer_layout(P);
+      outer_pair_layout(P, true);
+    }
     b += align_up((size_t)operand_bytes(P));
     if (P.gen == GEN_TABLE) b += align_up((size_t)P.nChunks * kKtabStageBytes);
   }

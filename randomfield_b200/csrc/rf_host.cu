@@ -607,9 +607,13 @@ void outer_layout(Plan& P) {
 // realizations per chunk, so that a chunk covers twice the realizations and
 // the generators build A for half as many chunks.  The last chunk's missing
 // realizations are zero columns of B (their MMAs run, their values are not
-// stored).  The TF32 K-steps (BF16) are outer_layout's.
-void outer_pair_layout(Plan& P) {
-  if (P.gen != GEN_OUTER || P.nmcBlk < 2 || P.n < 2 * 2 * kTileM) return;
+// stored).  The TF32 K-steps (BF16) are outer_layout's.  `always`: every
+// GEN_OUTER plan, whatever its size (the grouped kernel of a batch runs all
+// its outer-group units on CTA pairs; a unit of one realization leaves a half
+// of zero columns, one of fewer than 256 points the rows past its end).
+void outer_pair_layout(Plan& P, bool always) {
+  if (P.gen != GEN_OUTER) return;
+  if (!always && (P.nmcBlk < 2 || P.n < 2 * 2 * kTileM)) return;
   P.oPair = 1;
   P.oRc = std::min<int32_t>((P.nmcBlk + 1) / 2, 256 / (2 * P.lPad));
   P.oNR = (P.nmcBlk + 2 * P.oRc - 1) / (2 * P.oRc);

@@ -143,6 +143,9 @@ void lo_layout(rfb::Plan& P);
 // Single-request 3-D Shinozuka plans on the 16-bit tensor-core forms: the
 // outer-group contraction (rf_outer.cu) and its lo masks (rf_host.cu)
 void outer_layout(rfb::Plan& P);
+// Its CTA-pair form (rf_outer_pair.cu): single requests of at least two
+// items and two realizations, or every GEN_OUTER plan when `always`
+void outer_pair_layout(rfb::Plan& P, bool always = false);
 // Small single BF16 table-generator requests: the trig tile's lo term (rf_host.cu)
 void table_alo_layout(rfb::Plan& P);
 int32_t realization_block(const rfb::Plan& P);

@@ -84,24 +84,32 @@ size_t group_layout(int32_t maxBRows, int64_t maxStageBytes, int32_t maxStages, 
 cudaError_t group_set_smem(int prec, size_t smem);
 cudaError_t launch_group(int prec, const GroupArgs& g, size_t smem, int grid, cudaStream_t st);
 
-// Grouped outer-group contraction (rf_outer.cu): every CTA b runs the items
-// items[ctaStart[b] .. ctaStart[b+1]) of the GEN_OUTER units `subs` (an
-// item's `tile` is a pair of 128-point tiles; lPad == kGroupLPad), with one
-// slot layout for all: S slots of slotBytes, the A area aBytes.
-struct OuterGroupArgs {
+// Grouped outer-group contraction on CTA pairs (rf_outer_pair.cu): every
+// pair b (CTAs 2b, 2b + 1) runs the items items[ctaStart[b] ..
+// ctaStart[b+1]) of the GEN_OUTER units `subs` in the CTA-pair layout
+// (outer_pair_layout; an item's `tile` is its 256-point item; lPad ==
+// kGroupLPad); unit u's stage table is stabs[u * kOuterMaxKsteps ..], its
+// length nStages[u] (pair_group_stage_table).  One slot layout for all: S
+// slots of slotBytes.
+struct OuterPairGroupArgs {
   const GroupSub* subs;
   const GroupItem* items;
   const int32_t* ctaStart;
+  const uint32_t* stabs;
+  const int32_t* nStages;
   uint32_t* err;
-  int32_t S, slotBytes, aBytes;
+  int32_t S, slotBytes;
 };
-// Slot layout covering every plan (its largest A and B areas), at most
-// maxStages slots (0: as many as fit); returns the shared-memory bytes (0:
-// none fits) and fills S, slotBytes, aBytes.
-size_t outer_group_layout(const Plan* const* plans, size_t count, int maxStages, OuterGroupArgs* g);
-// Sets the kernel's shared-memory size (outside any stream capture).
-cudaError_t outer_group_set_smem(int prec, size_t smem);
-cudaError_t launch_outer_group(int prec, const OuterGroupArgs& g, size_t smem, int grid, cudaStream_t st);
+// The stage table of a CTA-pair plan as the grouped kernel reads it (false
+// when the plan's stage marks break the kernel's rule).
+bool pair_group_stage_table(const Plan& P, uint32_t* stab, int32_t* nStages);
+// Slot layout covering every plan, at most maxStages slots (0: as many as
+// fit); returns the shared-memory bytes (0: none fits) and fills S and
+// slotBytes.
+size_t outer_pair_group_layout(const Plan* const* plans, size_t count, int maxStages, OuterPairGroupArgs* g);
+cudaError_t outer_pair_group_set_smem(int prec, size_t smem);
+// grid: two CTAs per pair of the schedule
+cudaError_t launch_outer_pair_group(int prec, const OuterPairGroupArgs& g, size_t smem, int grid, cudaStream_t st);
 
 // Grouped table builder: B (and the wavevector chunks) of every unit; the
 // element range of unit u is [prefix[u], prefix[u+1]) of prefix[*nsubs]

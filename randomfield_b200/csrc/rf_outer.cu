@@ -19,7 +19,9 @@
 // contraction over i3 (2 lPad multiply-adds per output) runs in the epilogue
 // in FP32 with FP64-reduced per-point phasors.
 //
-// One persistent CTA per SM; a work item is a pair of 128-point tiles that
+// This one-CTA form serves the single requests that the CTA-pair form
+// (rf_outer_pair.cu) does not take: fewer than 512 points, or one
+// realization.  One persistent CTA per SM; a work item is a pair of 128-point tiles that
 // share every B stage (M = 256 per operand byte streamed from L2).  The
 // realization block is cut into N chunks of oRc realizations (TMEM: one
 // 256-column accumulator per tile); for each chunk the K-steps (16 K = 8
@@ -131,24 +133,6 @@ struct SingleOuterWork {
   }
 };
 
-// This CTA's slice [ctaStart[b], ctaStart[b+1]) of a grouped work list; an
-// item's `tile` field holds its pair index.
-struct GroupOuterWork {
-  const OuterGroupArgs* g;
-  int64_t begin, end;
-  __device__ __forceinline__ int64_t count() const { return end - begin; }
-  __device__ __forceinline__ void get(int64_t i, OuterView& v) const {
-    const GroupItem it = g->items[begin + i];
-    const GroupSub& s = g->subs[it.sub];
-    v.P = &s.P;
-    v.x = s.x;
-    v.out = s.out;
-    v.B = s.B;
-    v.row0 = 0;
-    v.rows = s.P.n;
-    v.pair = it.tile;
-  }
-};
 
 __device__ __forceinline__ void outer_abort(OuterBars* bars, uint32_t* err) {
   *reinterpret_cast<volatile int*>(&bars->abort_flag) = 1;
@@ -559,11 +543,6 @@ __global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_kernel(const __grid
   outer_body<PREC, LPAD>(w, a.S, a.slotBytes, a.aBytes, a.err);
 }
 
-template <int PREC>
-__global__ void __launch_bounds__(kOuterThreads, 1) rf_outer_group_kernel(const __grid_constant__ OuterGroupArgs g) {
-  const GroupOuterWork w{&g, g.ctaStart[blockIdx.x], g.ctaStart[blockIdx.x + 1]};
-  outer_body<PREC, kGroupLPad>(w, g.S, g.slotBytes, g.aBytes, g.err);
-}
 
 // Stage layout: the A area (kOuterStageUnits units of kAUnitBytes), then
 // kOuterStageUnits B units of bUnit bytes (one K-step block of B).
@@ -610,29 +589,6 @@ size_t outer_fit(int32_t slotBytes, int* stages, int maxStages = 0) {
 size_t outer_smem_bytes(const Plan& P, int* stages) {
   if (P.oPair) return outer_pair_smem_bytes(P, stages);
   return outer_fit(outer_stage_bytes(P.oKstepBytes), stages);
-}
-
-size_t outer_group_layout(const Plan* const* plans, size_t count, int maxStages, OuterGroupArgs* g) {
-  int64_t bMax = 0;
-  for (size_t i = 0; i < count; ++i) bMax = plans[i]->oKstepBytes > bMax ? plans[i]->oKstepBytes : bMax;
-  g->aBytes = kStageABytes;
-  g->slotBytes = outer_stage_bytes(bMax);
-  int S = 0;
-  const size_t smem = outer_fit(g->slotBytes, &S, maxStages);
-  g->S = S;
-  return smem;
-}
-
-cudaError_t outer_group_set_smem(int prec, size_t smem) {
-  const int b = (int)smem;
-  if (prec == PREC_FP16) return cudaFuncSetAttribute(rf_outer_group_kernel<PREC_FP16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-  return cudaFuncSetAttribute(rf_outer_group_kernel<PREC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-}
-
-cudaError_t launch_outer_group(int prec, const OuterGroupArgs& g, size_t smem, int grid, cudaStream_t st) {
-  if (prec == PREC_FP16) rf_outer_group_kernel<PREC_FP16><<<grid, kOuterThreads, smem, st>>>(g);
-  else rf_outer_group_kernel<PREC_BF16><<<grid, kOuterThreads, smem, st>>>(g);
-  return cudaGetLastError();
 }
 
 cudaError_t launch_outer(const Plan& P, const double* dX, const void* dB, double* dOut, int64_t row0, int64_t rows,

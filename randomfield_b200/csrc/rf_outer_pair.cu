@@ -2,10 +2,15 @@
 // pair: one tcgen05 MMA of M = 256 covers both CTAs' 128-point tiles.
 //
 // Replaces the hot loop of gen_Std_Gauss_Shinozuka (randomFieldND.f90:276-330)
-// for single 3-D requests whose wavevectors form the set_kPoints tensor grid
+// for 3-D requests whose wavevectors form the set_kPoints tensor grid
 // (spectra_RF.f90:87-133), with the factorisation of rf_outer.cu: f(x, r) =
 // ampMult sum_i3 [c3 Yc + s3 Ys], Y = A (points x 2G) B (2G x N), A the outer
 // phasors E1(i1) E2(i2)^{s2} generated on chip.
+//
+// Two kernels share one body: rf_outer_pair_kernel for a single request (of
+// at least two items and two realizations) and rf_outer_pair_group_kernel
+// for the outer-group units of a batch (each pair its own slice of the
+// batch's items, each unit its own plan and stage table).
 //
 // A cluster of two CTAs works on a 256-point item, one 128-point tile per CTA.
 // An N chunk is two halves of oRc realizations (N = 2 lPad oRc <= 256 each);
@@ -232,29 +237,103 @@ __device__ __forceinline__ void gen_tf32(unsigned char* A, const float2* e1, flo
   }
 }
 
-// Stages per chunk of a plan (the stage-end marks; the last K-step closes one).
-__device__ __forceinline__ int32_t pair_stage_count(const Plan& P) {
-  int32_t ns = 0;
-  for (int32_t j = 0; j < P.oNK; ++j) ns += (outer_stage_end(P, j) || j + 1 == P.oNK) ? 1 : 0;
-  return ns;
+
+// The stage table of a plan (issuer and generators): per stage its first
+// K-step (9 bits), K-steps (3 bits) and per K-step two TF32 flags (B, A).  A
+// stage must not span the end of an i2 run (outer_stage_layout closes one
+// there); false when the plan's marks break that.
+__host__ __device__ inline bool pair_stage_table(const Plan& P, uint32_t* stab, int32_t* nStages) {
+  int32_t ns = 0, j0 = 0, n = 0;
+  uint32_t fl = 0;
+  bool bad = false;
+  for (int32_t j = 0; j < P.oNK; ++j) {
+    fl |= ((outer_b_lo(P, j) ? 1u : 0u) | (outer_a_lo(P, j) ? 2u : 0u)) << (2 * n);
+    ++n;
+    if (outer_stage_end(P, j) || j + 1 == P.oNK) {
+      bad |= (j0 % P.kNStep[1]) + n > P.kNStep[1] || n > 4;
+      stab[ns++] = (uint32_t)j0 | ((uint32_t)n << 9) | (fl << 12);
+      j0 = j + 1;
+      n = 0;
+      fl = 0;
+    }
+  }
+  *nStages = ns;
+  return !bad;
 }
 
-template <int PREC, int LPAD, bool TF32>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
-    rf_outer_pair_kernel(const __grid_constant__ OuterPairArgs a) {
+// One 256-point item (one 128-point tile per CTA) as every role sees it.
+struct PairView {
+  const Plan* P;
+  const double* x;
+  double* out;
+  const unsigned char* B;
+  int64_t row0, rows;     // point range of the request covered by the launch
+  int64_t item;           // 256-point item inside that range
+  const uint32_t* stab;   // the plan's stage table
+  int32_t nSt;
+};
+
+// The items pairIdx, pairIdx + nPairs, ... of one request; its stage table
+// is built into shared memory at kernel start.
+struct SinglePairWork {
+  const OuterPairArgs* a;
+  const uint32_t* stab;
+  int64_t items;
+  __device__ __forceinline__ int64_t count() const {
+    const int64_t pairIdx = blockIdx.x >> 1, nPairs = gridDim.x >> 1;
+    return pairIdx < items ? (items - 1 - pairIdx) / nPairs + 1 : 0;
+  }
+  __device__ __forceinline__ bool prepare(PairBars* bars) const {
+    return pair_stage_table(a->P, bars->stab, &bars->nStages);
+  }
+  __device__ __forceinline__ void get(int64_t i, const PairBars* bars, PairView& v) const {
+    v.P = &a->P;
+    v.x = a->x;
+    v.out = a->out;
+    v.B = a->B;
+    v.row0 = a->row0;
+    v.rows = a->rows;
+    v.item = (int64_t)(blockIdx.x >> 1) + i * (int64_t)(gridDim.x >> 1);
+    v.stab = stab;
+    v.nSt = bars->nStages;
+  }
+};
+
+// This pair's slice [ctaStart[b], ctaStart[b+1]) of a grouped work list (b
+// the pair's index); an item's `tile` field holds its 256-point item, and
+// each unit's stage table comes with the launch's descriptors.
+struct GroupPairWork {
+  const OuterPairGroupArgs* g;
+  int64_t begin, end;
+  __device__ __forceinline__ int64_t count() const { return end - begin; }
+  __device__ __forceinline__ bool prepare(PairBars*) const { return true; }
+  __device__ __forceinline__ void get(int64_t i, const PairBars*, PairView& v) const {
+    const GroupItem it = g->items[begin + i];
+    const GroupSub& s = g->subs[it.sub];
+    v.P = &s.P;
+    v.x = s.x;
+    v.out = s.out;
+    v.B = s.B;
+    v.row0 = 0;
+    v.rows = s.P.n;
+    v.item = it.tile;
+    v.stab = g->stabs + (size_t)it.sub * kOuterMaxKsteps;
+    v.nSt = g->nStages[it.sub];
+  }
+};
+
+// The pipeline of one CTA pair over the items of `w`.  LPAD: axis-3 length
+// padded to 8, 16, 24 or 32 (every item of a launch has this lPad).
+template <int PREC, int LPAD, bool TF32, class Work>
+__device__ __forceinline__ void pair_body(const Work& w, int S, int32_t slotBytes, uint32_t* err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   PairBars* bars = reinterpret_cast<PairBars*>(smem);
   unsigned char* slots = smem + kPHeader;
   volatile int* abort_flag = &bars->abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = cluster_rank();
-  const int S = a.S;
-  const int32_t slotBytes = a.slotBytes;
-  uint32_t* err = a.err;
-  const Plan& P = a.P;
-  const int64_t items = ((a.rows + kTileM - 1) / kTileM + 1) / 2;  // 256-point items
-  const int64_t pairIdx = blockIdx.x >> 1, nPairs = gridDim.x >> 1;
-  const int64_t count = pairIdx < items ? (items - 1 - pairIdx) / nPairs + 1 : 0;
+  const int64_t count = w.count();
+  PairView v;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < S; ++s) {
@@ -267,25 +346,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     mbar_init(&bars->done, 1);
     mbar_init(&bars->dealloc_ok, 1);
     bars->abort_flag = 0;
-    // the stage table (issuer and generators): first K-step (9 bits), K-steps
-    // (3 bits), per K-step two TF32 flags (B, A); a stage must not span
-    // the end of an i2 run (outer_stage_layout closes one there)
-    int32_t ns = 0, j0 = 0, n = 0;
-    uint32_t fl = 0;
-    bool bad = false;
-    for (int32_t j = 0; j < P.oNK; ++j) {
-      fl |= ((outer_b_lo(P, j) ? 1u : 0u) | (outer_a_lo(P, j) ? 2u : 0u)) << (2 * n);
-      ++n;
-      if (outer_stage_end(P, j) || j + 1 == P.oNK) {
-        bad |= (j0 % P.kNStep[1]) + n > P.kNStep[1] || n > 4;
-        bars->stab[ns++] = (uint32_t)j0 | ((uint32_t)n << 9) | (fl << 12);
-        j0 = j + 1;
-        n = 0;
-        fl = 0;
-      }
-    }
-    bars->nStages = ns;
-    if (bad) {  // not a layout of outer_stage_layout: no stage runs
+    if (!w.prepare(bars)) {  // not a layout of outer_stage_layout: no stage runs
       bars->abort_flag = 1;
       atomicOr(err, kErrBounds);
     }
@@ -299,17 +360,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
   cluster_sync_all();  // both CTAs' barriers and TMEM allocation before any remote arrive or MMA
   tc_fence_after();
   const uint32_t tbase = bars->tmem_base;
-  const int32_t oNK = P.oNK, oNR = P.oNR, oRc = P.oRc, nmcBlk = P.nmcBlk, lPad = P.lPad;
-  const int32_t halfRows = lPad * oRc;                 // B rows of a half in one CTA
-  const int64_t kstepBytes = P.oKstepBytes;            // one K-step block of this CTA's B part
 
   if (warp == kPProducerWarp) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
       uint32_t s = 0, ph = 0;
       bool ok = true;
-      const int64_t chunkBytes = P.oChunkBytes, opBytes = operand_bytes(P);
       for (int64_t i = 0; i < count && ok; ++i) {
+        w.get(i, bars, v);
+        const Plan& P = *v.P;
+        const int32_t oNK = P.oNK, oNR = P.oNR;
+        const int64_t kstepBytes = P.oKstepBytes, chunkBytes = P.oChunkBytes, opBytes = operand_bytes(P);
         for (int32_t c = 0; c < oNR && ok; ++c) {
           int64_t off = (int64_t)c * chunkBytes + (int64_t)rank * (chunkBytes / 2);
           for (int32_t j = 0; j < oNK;) {
@@ -328,7 +389,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
               break;
             }
             mbar_arrive_expect_tx(&bars->full[s], bytes);
-            bulk_g2s(slots + (size_t)s * slotBytes + kPStageABytes, a.B + off, bytes, &bars->full[s]);
+            bulk_g2s(slots + (size_t)s * slotBytes + kPStageABytes, v.B + off, bytes, &bars->full[s]);
             off += bytes;
             if (++s == (uint32_t)S) { s = 0; ph ^= 1; }
           }
@@ -351,8 +412,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     // stage through one cluster-scope release.
     uint32_t s = 0, ph = 0;
     bool ok = true;
-    const int32_t nSt = pair_stage_count(P);
     for (int64_t i = 0; i < count && ok; ++i) {
+      w.get(i, bars, v);
+      const int32_t oNR = v.P->oNR, nSt = v.nSt;
       for (int32_t c = 0; c < oNR && ok; ++c) {
         for (int32_t st = 0; st < nSt; ++st) {
           if (!mbar_wait_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
@@ -377,14 +439,21 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     uint32_t s = 0, ph = 0, accPh = 0;
     bool ok = true, ready = false;
     const uint32_t ab = PREC == PREC_FP16 ? 0u : 1u;
-    const uint64_t aU = (uint64_t)(kPAUnitBytes >> 4);          // descriptor step of one A unit
-    const uint64_t bU = (uint64_t)((uint32_t)kstepBytes >> 4);  // descriptor step of one B unit
-    const uint64_t bH = (uint64_t)((uint32_t)(halfRows * 32) >> 4);  // to the second half's rows
-    const uint32_t idesc = make_idesc(ab, 256u, (uint32_t)(2 * lPad * oRc));
-    const uint32_t idescT = make_idesc(2u, 256u, (uint32_t)(2 * lPad * oRc));  // A, B TF32
-    const int32_t nSt = bars->nStages;
+    const uint64_t aU = (uint64_t)(kPAUnitBytes >> 4);  // descriptor step of one A unit
     const uint32_t t0 = tbase, t1 = tbase + (uint32_t)kPAccCols;
     for (int64_t i = 0; i < count && ok; ++i) {
+      w.get(i, bars, v);
+      // the item's loop bounds in registers: every tcgen05 and mbarrier
+      // statement clobbers memory, and a plan field read inside the loop
+      // would be loaded again after each of them
+      const Plan& P = *v.P;
+      const int32_t oNR = P.oNR, oRc = P.oRc, lPad = P.lPad, nSt = v.nSt;
+      const int32_t halfRows = lPad * oRc;  // B rows of a half in one CTA
+      const uint64_t bU = (uint64_t)((uint32_t)P.oKstepBytes >> 4);    // descriptor step of one B unit
+      const uint64_t bH = (uint64_t)((uint32_t)(halfRows * 32) >> 4);  // to the second half's rows
+      const uint32_t idesc = make_idesc(ab, 256u, (uint32_t)(2 * lPad * oRc));
+      const uint32_t idescT = make_idesc(2u, 256u, (uint32_t)(2 * lPad * oRc));  // A, B TF32
+      const uint32_t* stab = v.stab;
       for (int32_t c = 0; c < oNR && ok; ++c) {
         // both halves' accumulators are free once both CTAs' epilogues read the last chunk
         if (!mbar_wait_cluster_warp(&bars->acc_empty[0], accPh ^ 1, abort_flag) ||
@@ -393,12 +462,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
           break;
         }
         tc_fence_after();
-        uint32_t eNext = bars->stab[0];
+        uint32_t eNext = stab[0];
         for (int32_t st = 0; st < nSt; ++st) {
           if (!ready && !mbar_wait_cluster_warp(&bars->full[s], ph, abort_flag)) { ok = false; break; }
           tc_fence_after();
           const uint32_t e = eNext;
-          if (st + 1 < nSt) eNext = bars->stab[st + 1];
+          if (st + 1 < nSt) eNext = stab[st + 1];
           const uint32_t n = (e >> 9) & 7u, fl = e >> 12;
           const uint32_t acc = (e & 0x1ffu) ? 1u : 0u;
           const uint32_t base = smem_u32(slots + (size_t)s * slotBytes);
@@ -482,16 +551,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     const uint32_t rowOff = (uint32_t)((row >> 3) * 128 + (row & 7) * 16);
     uint32_t s = 0, ph = 0;
     bool ok = !*abort_flag;
-    const int32_t n2 = P.kNStep[1];
-    const int32_t nSt = bars->nStages;
     for (int64_t i = 0; i < count && ok; ++i) {
-      const int64_t item = pairIdx + i * nPairs;
-      const int64_t p = a.row0 + item * 2 * kTileM + (int64_t)rank * kTileM + row;
-      const bool valid = p < a.row0 + a.rows;
+      w.get(i, bars, v);
+      const Plan& P = *v.P;
+      const int32_t n2 = P.kNStep[1], oNR = P.oNR, nSt = v.nSt;
+      const uint32_t* stab = v.stab;
+      const int64_t p = v.row0 + v.item * 2 * kTileM + (int64_t)rank * kTileM + row;
+      const bool valid = p < v.row0 + v.rows;
       double x0 = 0.0, x1 = 0.0;
       if (valid && RF_IN_BOUNDS(p * 3 + 2, P.n * 3, err)) {
-        x0 = a.x[p * 3 + 0] / P.corrL[0];
-        x1 = a.x[p * 3 + 1] / P.corrL[1];
+        x0 = v.x[p * 3 + 0] / P.corrL[0];
+        x1 = v.x[p * 3 + 1] / P.corrL[1];
       }
       const float2 e2step = axis_phasor(P.kDelta[1], 1, x1);
       // E1(u) of block 0 and the block step E1(8), from FP64-reduced phases
@@ -507,7 +577,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
         float2 e2 = make_float2(1.f, 0.f);
         int32_t jjCur = 0;
         for (int32_t st = 0; st < nSt; ++st) {
-          const uint32_t e = bars->stab[st];
+          const uint32_t e = stab[st];
           const int32_t j0 = (int32_t)(e & 0x1ffu), n = (int32_t)((e >> 9) & 7u);
           const uint32_t fl = e >> 12;
           const int32_t run = j0 / n2, jj = run >> 1;
@@ -563,15 +633,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     uint32_t accPh = 0;
     bool ok = true;
     const uint32_t releaseAddr = map_to_rank(&bars->acc_empty[h], 0);
-    const int64_t rOff = P.rOff, n = P.n, nOut = P.blend ? P.gTotal : P.n;
-    [[maybe_unused]] const int64_t outLen = (int64_t)P.Nmc * nOut;  // the index checks' bound
-    const bool blend = P.blend, marg = P.applyMarginal, logn = P.lognormal;
-    const double outScale = P.outScale, margSd = P.margSd, margAvg = P.margAvg;
     for (int64_t i = 0; i < count && ok; ++i) {
-      const int64_t item = pairIdx + i * nPairs;
-      const int64_t p = a.row0 + item * 2 * kTileM + (int64_t)rank * kTileM + row;
-      const bool valid = p < a.row0 + a.rows;
-      const double x2 = valid ? a.x[p * 3 + 2] / P.corrL[2] : 0.0;
+      w.get(i, bars, v);
+      const Plan& P = *v.P;
+      const int32_t oNR = P.oNR, oRc = P.oRc, nmcBlk = P.nmcBlk;
+      const int64_t rOff = P.rOff, n = P.n, nOut = P.blend ? P.gTotal : P.n;
+      [[maybe_unused]] const int64_t outLen = (int64_t)P.Nmc * nOut;  // the index checks' bound
+      const bool blend = P.blend, marg = P.applyMarginal, logn = P.lognormal;
+      const double outScale = P.outScale, margSd = P.margSd, margAvg = P.margAvg;
+      double* out = v.out;
+      const int64_t p = v.row0 + v.item * 2 * kTileM + (int64_t)rank * kTileM + row;
+      const bool valid = p < v.row0 + v.rows;
+      const double x2 = valid ? v.x[p * 3 + 2] / P.corrL[2] : 0.0;
       double bw = 0.0;
       int64_t bg = 0;
       if (blend && valid) bw = blend_weight(P, p, &bg);
@@ -604,14 +677,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
           if (valid) {
             const int64_t r = rOff + r0 + rl;
             if (blend) {
-              if (RF_IN_BOUNDS(r * nOut + bg, outLen, err)) atomicAdd(&a.out[r * nOut + bg], bw * ((double)acc * outScale));
+              if (RF_IN_BOUNDS(r * nOut + bg, outLen, err)) atomicAdd(&out[r * nOut + bg], bw * ((double)acc * outScale));
             } else if (RF_IN_BOUNDS(r * n + p, outLen, err)) {
               double f = (double)acc * outScale;
               if (marg) {
                 f = f * margSd + margAvg;
                 if (logn) f = exp(f);
               }
-              a.out[r * n + p] = f;
+              out[r * n + p] = f;
             }
           }
         }
@@ -629,6 +702,22 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
   tc_fence_after();
   if (warp == kPIssuerWarp) tmem_dealloc_pair(tbase, kPTmemCols);
   cluster_sync_all();  // neither CTA leaves while its peer may still address its shared memory
+}
+
+template <int PREC, int LPAD, bool TF32>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+    rf_outer_pair_kernel(const __grid_constant__ OuterPairArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const SinglePairWork w{&a, reinterpret_cast<const PairBars*>(smem)->stab, ((a.rows + kTileM - 1) / kTileM + 1) / 2};
+  pair_body<PREC, LPAD, TF32>(w, a.S, a.slotBytes, a.err);
+}
+
+template <int PREC>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+    rf_outer_pair_group_kernel(const __grid_constant__ OuterPairGroupArgs g) {
+  const int64_t b = blockIdx.x >> 1;
+  const GroupPairWork w{&g, g.ctaStart[b], g.ctaStart[b + 1]};
+  pair_body<PREC, kGroupLPad, PREC == PREC_BF16>(w, g.S, g.slotBytes, g.err);
 }
 
 template <int PREC, int LPAD>
@@ -664,6 +753,38 @@ size_t outer_pair_smem_bytes(const Plan& P, int* stages) {
   if (S < 2) return 0;
   const size_t total = (size_t)kPHeader + (size_t)S * (size_t)slot;
   return total < floor ? floor : total;
+}
+
+bool pair_group_stage_table(const Plan& P, uint32_t* stab, int32_t* nStages) {
+  return pair_stage_table(P, stab, nStages);
+}
+
+size_t outer_pair_group_layout(const Plan* const* plans, size_t count, int maxStages, OuterPairGroupArgs* g) {
+  int64_t bMax = 0;
+  for (size_t i = 0; i < count; ++i) bMax = plans[i]->oKstepBytes > bMax ? plans[i]->oKstepBytes : bMax;
+  const int64_t slot = (kPStageABytes + kOuterStageUnits * bMax + 127) / 128 * 128;
+  const size_t limit = 227 * 1024, floor = 120 * 1024;
+  int S = (int)((limit - kPHeader) / (size_t)slot);
+  if (S > kPMaxSlots) S = kPMaxSlots;
+  if (maxStages > 0 && S > maxStages) S = maxStages;
+  g->S = S;
+  g->slotBytes = (int32_t)slot;
+  if (S < 2) return 0;
+  const size_t total = (size_t)kPHeader + (size_t)S * (size_t)slot;
+  return total < floor ? floor : total;
+}
+
+cudaError_t outer_pair_group_set_smem(int prec, size_t smem) {
+  const int b = (int)smem;
+  if (prec == PREC_FP16)
+    return cudaFuncSetAttribute(rf_outer_pair_group_kernel<PREC_FP16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  return cudaFuncSetAttribute(rf_outer_pair_group_kernel<PREC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+}
+
+cudaError_t launch_outer_pair_group(int prec, const OuterPairGroupArgs& g, size_t smem, int grid, cudaStream_t st) {
+  if (prec == PREC_FP16) rf_outer_pair_group_kernel<PREC_FP16><<<grid, kPThreads, smem, st>>>(g);
+  else rf_outer_pair_group_kernel<PREC_BF16><<<grid, kPThreads, smem, st>>>(g);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_outer_pair(const Plan& P, const double* dX, const void* dB, double* dOut, int64_t row0,

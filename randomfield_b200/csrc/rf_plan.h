@@ -103,7 +103,8 @@ struct Plan {
   int64_t oChunkBytes;        // bytes of one chunk of B, lo blocks included
   uint32_t aLoMask[8];        // K-steps whose A tile carries the lo term (up to 256)
   uint32_t oStageEnd[8];      // K-steps that close a ring stage (outer_stage_layout)
-  // CTA-pair form (rf_outer_pair.cu, single requests): N chunk c is two
+  // CTA-pair form (rf_outer_pair.cu; single requests, and every
+  // outer-group unit of a batch): N chunk c is two
   // halves of oRc realizations each, [c 2 oRc + h oRc, + oRc); a CTA pair
   // computes a 256-point item (one tile per CTA), each CTA holding its half
   // (lPad oRc rows) of both halves' B rows.  B of chunk c is rank 0's part
