@@ -40,11 +40,15 @@ double stage_cost(const Plan& P) {
   return P.gen == GEN_GRID3 ? 1130.0 * std::max(0.6, n) : 600.0 * std::max(0.6, n);
 }
 
-// Relative device cost of one pair of tiles of a GEN_OUTER unit: MMAs of
-// N columns per K-step and tile, lo terms included.
+// Relative device cost of one 256-point item of a GEN_OUTER unit on a CTA
+// pair: its ring stages, one chunk after another.  The pair kernel's stage
+// loop costs about the same per stage whatever the stage holds and however
+// many realization columns a chunk carries (the generators write the same A
+// and the bulk copy lands at the same pace), so a unit's width does not enter;
+// one stage more per chunk stands for the epilogue between chunks.
 double outer_pair_cost(const Plan& P) {
-  const double mmas = (double)P.oNK + (double)mask_rank(P.loMask, P.oNK) + (double)mask_rank(P.aLoMask, P.oNK);
-  return (double)P.oNR * mmas * (double)(2 * P.lPad * P.oRc);
+  const double stages = (double)mask_rank(P.oStageEnd, P.oNK) + (outer_stage_end(P, P.oNK - 1) ? 0.0 : 1.0);
+  return (double)P.oNR * (stages + 1.0);
 }
 
 // Descriptor buffer: unit count, units, table prefix, then for each of the
